@@ -1,0 +1,354 @@
+"""Benchmark: spin*sample*coil/s of the BlochHighOrder path on one B200 per rank.
+
+Workload: the 3D 32-coil configuration (100x100x35 grid at 2 mm, 350,000
+spins, 4 stack-of-spiral interleaves x 9,500 ADC samples at 1 us, full
+third-order field waveforms, mask 1111), synthetic and seed-generated.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--mode split|plain]
+    python bench.py --impl reference ...   # CPU oracle on the host cores
+
+`value` is whole-job throughput with inputs resident on the device (a
+prepared plan, signal written to device memory); `e2e` is the same metric
+through the C ABI (homs_simulate) from pinned host buffers, with all
+host<->device copies inside the timed region.  With N > 1 every rank runs an
+independent replica (the engine does not shard spins across GPUs).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "highordermrisim.jl_b200"), ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "spin*sample*coil/s"
+UNIT = "spin*sample*coil/s"
+CONFIG_INDEX = 2
+FLOPS_PER_UNIT = 8.0  # one complex multiply-accumulate per spin*sample*coil
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            p = json.load(fh)
+        return float(p["bf16_tflops"]), float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 1590.0, 6650.0, "fallback"
+
+
+def _traffic_per_launch():
+    """DRAM bytes per launch of the split kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "split_precession_kernel_cfg2.md")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch_full:"):
+                return float(line.split(":", 1)[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _workload(stride=1):
+    from homs import workloads as W
+    return W.config(CONFIG_INDEX, spins_stride=stride)
+
+
+def _units(w):
+    from homs.model import count_block_adc
+    return len(w.obj) * sum(count_block_adc(w.seq.adc, w.parts)) * w.obj.ncoils
+
+
+def cpu_baseline(seconds_target=15.0, threads=None):
+    """Time the CPU oracle (a port of the reference's CPU Float64 path) on a
+    deterministic spin subsample of the workload, on all host threads."""
+    from homs.model import BlochHighOrder
+    from oracle import oracle as orc
+    orc.build()
+    if threads is None:
+        threads = max(1, len(os.sched_getaffinity(0)))
+    probe = _workload(stride=4000)
+    flags = BlochHighOrder(probe.mask).flags
+    t0 = time.perf_counter()
+    orc.simulate_c(probe.obj, probe.seq, probe.parts, probe.excitation, flags, nthreads=threads)
+    rate = _units(probe) / max(time.perf_counter() - t0, 1e-3)
+    full = 350000 * 38000 * 32
+    stride = int(max(1, min(4000, full / max(rate * seconds_target, 1.0))))
+    w = _workload(stride=stride)
+    t0 = time.perf_counter()
+    orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": _units(w) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"every {stride}th spin ({len(w.obj)} spins) x 38000 samples x 32 coils, full sequence, "
+                      f"{dt:.1f} s"}, dt
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    base, _ = cpu_baseline(seconds_target=max(5.0, 20.0 / max(args.steps, 1)))
+    vals = []
+    for _ in range(args.warmup):
+        cpu_baseline(seconds_target=2.0)
+    for _ in range(args.steps):
+        b, _ = cpu_baseline(seconds_target=max(5.0, 20.0 / max(args.steps, 1)))
+        vals.append(b["value"])
+    v = statistics.median(vals)
+    base["value"] = v
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": _units(_workload(1)) / v * 1e3 if v else None, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "3d_stack_of_spirals_100x100x35_350000spins_32coils_4x9500adc",
+                      "spins": 350000, "samples": 38000, "coils": 32, "mask": "1111"},
+           "impl": "reference", "cpu_baseline": base,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def run_homs(args):
+    import torch
+    import torch.distributed as dist
+
+    import homs
+    from homs import _lib
+    from homs.model import BlochHighOrder
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    stream = torch.cuda.current_stream()
+    ctx = _lib.Context(local, stream.cuda_stream)
+    lib = _lib.load()
+    w = _workload()
+    units = _units(w)
+    method = BlochHighOrder(w.mask)
+    params = {"sim_method": method, "precision": "f64", "homs_precision": args.mode}
+    plan = homs.prepare_simulation(w.obj, w.seq, sim_params=params, parts=w.parts, excitation=w.excitation,
+                                   context=ctx)
+    nadc, nc = plan.nadc, plan.nc
+    sig_dev = torch.empty((nc, nadc), dtype=torch.complex128, device="cuda")
+
+    def device_step():
+        _lib.check(lib.homs_plan_run(plan.handle, ctypes.c_void_p(sig_dev.data_ptr()), _lib.HOMS_DEVICE, None),
+                   ctx.handle)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        device_step()
+    barrier()
+    fused_ms, fused_n, launches = 0.0, 0, 0
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            device_step()
+            t = _lib.Timing()
+            _lib.check(lib.homs_plan_timing(plan.handle, ctypes.byref(t)))
+            fused_ms += t.fused_kernel_ms
+            fused_n += t.fused_launches
+            launches += t.kernel_launches
+        stop.record(stream)
+        barrier()
+    ms = start.elapsed_time(stop) / args.steps
+    ms_t = torch.tensor([ms], device="cuda")
+    if ws > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = ws * units / (ms_max / 1e3)
+    plan.close()
+
+    # End to end through the C ABI from pinned host memory.
+    e2e = None
+    if not args.no_e2e:
+        keep = _lib._Keep()
+        pin = lambda a: _pinned(torch, a)  # noqa: E731
+        obj, seq = w.obj, w.seq
+        ph = _lib.Phantom(len(obj), nc, _lib.HOMS_F64, _lib.HOMS_HOST,
+                          *[keep.ptr(pin(np.asarray(v, np.float64))) for v in
+                            (obj.x, obj.y, obj.z, obj.rho, obj.T1, obj.T2, obj.dw)],
+                          keep.ptr(pin(np.asfortranarray(obj.csm.astype(np.complex128)))))
+        hp = [pin(np.ascontiguousarray(seq.h[k], np.float64)) for k in range(16)]
+        keep.items.extend(hp)
+        first = np.array([p[0] for p in w.parts], np.int64)
+        last = np.array([p[1] for p in w.parts], np.int64)
+        exc = np.array(w.excitation, np.uint8)
+        sq = _lib.Sequence(len(seq.t), _lib.HOMS_F64, _lib.HOMS_HOST,
+                           *[keep.ptr(pin(np.asarray(v, np.float64))) for v in (seq.t, seq.dt, seq.gx, seq.gy, seq.gz)],
+                           keep.ptr(pin(np.asarray(seq.b1, np.complex128))), keep.ptr(pin(np.asarray(seq.df, np.float64))),
+                           keep.ptr(pin(np.asarray(seq.psi, np.float64))),
+                           keep.ptr(pin(np.asarray(seq.adc, np.uint8))),
+                           (ctypes.c_void_p * 16)(*[a.ctypes.data for a in hp]), len(w.parts), keep.ptr(first),
+                           keep.ptr(last), keep.ptr(exc), homs.GAMMA)
+        sig_h = pin(np.zeros((nc, nadc), np.complex128))
+        xy_h = pin(np.zeros(len(obj), np.complex128))
+        z_h = pin(np.asarray(obj.rho, np.float64).copy())
+        st = _lib.State(xy_h.ctypes.data, z_h.ctypes.data, _lib.HOMS_HOST)
+        opts = _lib.RunOptions()
+        opts.method = method.flags
+        opts.mode = _lib.HOMS_SPLIT if args.mode == "split" else _lib.HOMS_PLAIN
+        h2d = sum(a.nbytes for a in keep.items if isinstance(a, np.ndarray)) + xy_h.nbytes + z_h.nbytes
+        d2h = sig_h.nbytes + xy_h.nbytes + z_h.nbytes
+
+        def e2e_step():
+            xy_h[:] = 0
+            z_h[:] = obj.rho
+            _lib.check(lib.homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
+                                         ctypes.byref(st), sig_h.ctypes.data, _lib.HOMS_HOST), ctx.handle)
+
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        n_e2e = max(1, min(args.steps, 3))
+        for _ in range(n_e2e):
+            e2e_step()
+        barrier()
+        e_ms = (time.perf_counter() - t0) * 1e3 / n_e2e
+        e_t = torch.tensor([e_ms], device="cuda")
+        if ws > 1:
+            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
+        e2e = {"value": ws * units / (float(e_t.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e_t.item())}
+
+    if rank != 0:
+        if ws > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    bf16_peak, hbm_peak, peak_kind = _peaks()
+    seg_units = len(w.obj) * 9500 * nc
+    avg_launch_ms = fused_ms / max(fused_n, 1)
+    achieved_tflops = FLOPS_PER_UNIT * seg_units / (avg_launch_ms / 1e3) / 1e12 if avg_launch_ms > 0 else None
+    traffic = _traffic_per_launch()
+    roof = {"bound": "tensor", "achieved": achieved_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+            "frac": (achieved_tflops / bf16_peak) if achieved_tflops else None, "traffic": traffic,
+            "peak_source": f"{peak_kind} dense bf16 (MEASURED_PEAKS.json)" if peak_kind == "measured" else
+            "fallback 1.59 PFLOP/s", "kernel": "split_precession_kernel" if args.mode == "split" else
+            "segment_kernel", "kernel_ms_per_launch": avg_launch_ms,
+            "units_per_launch": seg_units, "flops_per_unit": FLOPS_PER_UNIT}
+    base = None
+    if ws == 1 and not args.no_cpu_baseline:
+        base, _ = cpu_baseline()
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64 phase / f32 trig / tf32x3 tensor" if args.mode == "split" else "f64",
+           "data": "synthetic",
+           "config": {"workload": "3d_stack_of_spirals_100x100x35_350000spins_32coils_4x9500adc", "spins": len(w.obj),
+                      "samples": nadc, "coils": nc, "mask": w.mask, "mode": args.mode,
+                      "l2": "inputs larger than L2 (split operand 358 MB, csm 179 MB)", "parallelism": f"replicas{ws}"},
+           "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
+           "clocks": clocks.summary()}
+    print(json.dumps(out))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _pinned(torch, a: np.ndarray) -> np.ndarray:
+    t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    out = t.numpy().view(a.dtype).reshape(a.shape, order="F" if a.flags.f_contiguous and not a.flags.c_contiguous
+                                          else "C")
+    out[...] = a  # the view's .base chain keeps the pinned tensor alive
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="homs", choices=["homs", "reference"])
+    ap.add_argument("--mode", default="split", choices=["split", "plain"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_homs(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1000 @@
+// libhoms host runtime and C ABI (include/homs.h).
+//
+// A context owns one device and one stream; calls on a context are serialised
+// by a mutex (the reference serialises runs of a prepared plan with plan.lock,
+// src/simulation/PreparedSimulation.jl:224).  Inputs are copied into resident
+// device buffers in the phantom's precision; the block loop of
+// src/simulation/SimulatorCore.jl:96-152 is planned on the host into launches
+// of the fused segment kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "homs_common.cuh"
+#include "homs_split.cuh"
+
+using namespace homs;
+
+// ---------------------------------------------------------------------------
+// Small utilities
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        else p = nullptr;
+        return e;
+    }
+    template <typename U>
+    U *as() const { return reinterpret_cast<U *>(p); }
+};
+
+struct Failure {
+    homs_status status;
+    std::string msg;
+};
+
+#define HOMS_CUDA(expr)                                                                                   \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess) {                                                                          \
+            throw Failure{e_ == cudaErrorMemoryAllocation ? HOMS_ENOMEM : HOMS_ECUDA,                     \
+                          std::string(#expr) + ": " + cudaGetErrorString(e_)};                            \
+        }                                                                                                 \
+    } while (0)
+
+#define HOMS_REQUIRE(cond, msg)                         \
+    do {                                                \
+        if (!(cond)) throw Failure{HOMS_EINVAL, (msg)}; \
+    } while (0)
+
+size_t dsize(homs_dtype d) { return d == HOMS_F64 ? 8 : 4; }
+
+// Element conversion kernel (device arrays of a different dtype).
+template <typename D, typename S>
+__global__ void convert_kernel(D *dst, const S *src, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = D(src[i]);
+}
+
+// csm column-major (s + c*ld) -> rows (s*nc + c), with type conversion.
+template <typename D, typename S>
+__global__ void transpose_csm_kernel(cplx<D> *dst, const S *src, int64_t ns, int32_t nc, int64_t ld) {
+    const int64_t total = ns * nc;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t s = i / nc;
+        const int32_t c = (int32_t)(i % nc);
+        const S *v = src + 2 * (s + (int64_t)c * ld);
+        dst[i] = cplx<D>{D(v[0]), D(v[1])};
+    }
+}
+
+inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+
+struct homs_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    std::mutex mu;
+    // reusable scratch
+    DevBuf scratch_csm, scratch_partial, scratch_acc, scratch_bnd, scratch_sig, scratch_conv;
+};
+
+namespace {
+
+homs_status fail(homs_context *ctx, const Failure &f) {
+    if (ctx) ctx->last_error = f.msg;
+    return f.status;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+// Copy `n` elements of dtype `src_dt` at `src` (host or device) into a device
+// buffer of type T.
+template <typename T>
+void upload(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype src_dt, homs_memory mem, int64_t n) {
+    HOMS_CUDA(dst.ensure(sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    if (n == 0) return;
+    HOMS_REQUIRE(src != nullptr, "a required input array is NULL");
+    const bool same = (src_dt == HOMS_F64) == (sizeof(T) == 8);
+    if (same) {
+        HOMS_CUDA(cudaMemcpyAsync(dst.p, src, sizeof(T) * (size_t)n,
+                                  mem == HOMS_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+        return;
+    }
+    if (mem == HOMS_HOST) {
+        std::vector<T> tmp((size_t)n);
+        if (src_dt == HOMS_F64) {
+            const double *s = static_cast<const double *>(src);
+            for (int64_t i = 0; i < n; ++i) tmp[i] = T(s[i]);
+        } else {
+            const float *s = static_cast<const float *>(src);
+            for (int64_t i = 0; i < n; ++i) tmp[i] = T(s[i]);
+        }
+        HOMS_CUDA(cudaMemcpyAsync(dst.p, tmp.data(), sizeof(T) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+        return;
+    }
+    if (src_dt == HOMS_F64)
+        convert_kernel<T, double><<<grid_for(n), 256, 0, ctx->stream>>>(reinterpret_cast<T *>(dst.p), static_cast<const double *>(src), n);
+    else
+        convert_kernel<T, float><<<grid_for(n), 256, 0, ctx->stream>>>(reinterpret_cast<T *>(dst.p), static_cast<const float *>(src), n);
+    HOMS_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void upload_csm_rows(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype src_dt, homs_memory mem, int64_t ns,
+                     int32_t nc, int64_t ld) {
+    const int64_t total = ns * nc;
+    HOMS_CUDA(dst.ensure(sizeof(cplx<T>) * (size_t)std::max<int64_t>(total, 1)));
+    if (total == 0) return;
+    HOMS_REQUIRE(src != nullptr, "csm is NULL");
+    const void *dsrc = src;
+    DevBuf staging;
+    if (mem == HOMS_HOST) {
+        const size_t bytes = 2 * dsize(src_dt) * (size_t)(ld * (nc - 1) + ns);
+        HOMS_CUDA(staging.ensure(bytes));
+        HOMS_CUDA(cudaMemcpyAsync(staging.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        dsrc = staging.p;
+    }
+    if (src_dt == HOMS_F64)
+        transpose_csm_kernel<T, double><<<grid_for(total), 256, 0, ctx->stream>>>(
+            reinterpret_cast<cplx<T> *>(dst.p), static_cast<const double *>(dsrc), ns, nc, ld);
+    else
+        transpose_csm_kernel<T, float><<<grid_for(total), 256, 0, ctx->stream>>>(
+            reinterpret_cast<cplx<T> *>(dst.p), static_cast<const float *>(dsrc), ns, nc, ld);
+    HOMS_CUDA(cudaGetLastError());
+    if (mem == HOMS_HOST) HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+void validate_phantom(const homs_phantom *p) {
+    HOMS_REQUIRE(p != nullptr, "phantom is NULL");
+    HOMS_REQUIRE(p->nspins >= 1, "The phantom must contain at least one spin.");
+    HOMS_REQUIRE(p->ncoils >= 1, "The CSM must contain at least one coil.");
+    HOMS_REQUIRE(p->dtype == HOMS_F32 || p->dtype == HOMS_F64, "phantom dtype must be f32 or f64");
+    HOMS_REQUIRE(p->memory == HOMS_HOST || p->memory == HOMS_DEVICE, "invalid phantom memory kind");
+    HOMS_REQUIRE(p->x && p->y && p->z && p->rho && p->T1 && p->T2 && p->dw && p->csm,
+                 "every phantom array must be provided");
+}
+
+void validate_sequence(const homs_sequence *q) {
+    HOMS_REQUIRE(q != nullptr, "sequence is NULL");
+    HOMS_REQUIRE(q->nnodes >= 2, "The sequence must contain a simulation interval.");
+    HOMS_REQUIRE(q->dtype == HOMS_F32 || q->dtype == HOMS_F64, "sequence dtype must be f32 or f64");
+    HOMS_REQUIRE(q->t && q->dt && q->gx && q->gy && q->gz && q->b1 && q->df && q->psi && q->adc,
+                 "every sequence array must be provided");
+    for (int k = 0; k < 16; ++k) HOMS_REQUIRE(q->h[k] != nullptr, "every field coefficient array must be provided");
+    HOMS_REQUIRE(q->nblocks >= 1 && q->block_first && q->block_last && q->block_excitation,
+                 "The sequence must contain a simulation interval.");
+    HOMS_REQUIRE(std::isfinite(q->gamma) && q->gamma > 0, "gamma must be finite and positive");
+    int64_t expect = q->block_first[0];
+    HOMS_REQUIRE(expect >= 0, "block ranges must be nonnegative");
+    for (int32_t k = 0; k < q->nblocks; ++k) {
+        HOMS_REQUIRE(q->block_first[k] == expect, "blocks must be contiguous and share boundary nodes");
+        HOMS_REQUIRE(q->block_last[k] > q->block_first[k], "every block must contain at least one interval");
+        HOMS_REQUIRE(q->block_last[k] < q->nnodes, "block range exceeds the sequence");
+        expect = q->block_last[k];
+    }
+}
+
+// Host copy of the ADC flags (the sequence may live on the device).
+std::vector<uint8_t> host_adc(homs_context *ctx, const homs_sequence *q) {
+    std::vector<uint8_t> adc((size_t)q->nnodes);
+    if (q->memory == HOMS_HOST) {
+        std::memcpy(adc.data(), q->adc, adc.size());
+    } else {
+        HOMS_CUDA(cudaMemcpyAsync(adc.data(), q->adc, adc.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return adc;
+}
+
+template <typename T>
+std::vector<T> host_array(homs_context *ctx, const void *src, homs_dtype dt, homs_memory mem, int64_t n) {
+    std::vector<T> out((size_t)n);
+    if (n == 0) return out;
+    std::vector<unsigned char> raw((size_t)n * dsize(dt));
+    if (mem == HOMS_HOST) {
+        std::memcpy(raw.data(), src, raw.size());
+    } else {
+        HOMS_CUDA(cudaMemcpyAsync(raw.data(), src, raw.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    for (int64_t i = 0; i < n; ++i)
+        out[i] = dt == HOMS_F64 ? T(reinterpret_cast<double *>(raw.data())[i]) : T(reinterpret_cast<float *>(raw.data())[i]);
+    return out;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Resident simulation data (used by homs_simulate and prepared plans)
+// ---------------------------------------------------------------------------
+
+struct ResidentBase {
+    virtual ~ResidentBase() = default;
+    homs_dtype dtype = HOMS_F64;
+    int64_t ns = 0, nt = 0, nadc = 0;
+    int32_t nc = 0;
+    virtual size_t device_bytes() const = 0;
+    virtual void timing(homs_timing *out) const = 0;
+};
+
+template <typename T>
+struct Resident : ResidentBase {
+    DevBuf x, y, z, rho, T1, T2, dw, csm_rows;
+    DevBuf t, dt, gx, gy, gz, b1, df, psi, adc, bnd, h[16];
+    DevBuf xy, mz, acc, rho_init;
+    DevBuf partial, sig;
+    std::vector<int64_t> first, last;
+    std::vector<uint8_t> exc, adc_host;
+    std::vector<T> dt_host;
+    double gamma = 0;
+    SplitResident split;  // split-precision operands (built on demand)
+    bool split_ready = false;
+    // Instrumentation of the last run: events around every launch of the
+    // dominant fused kernel, and a count of all kernels launched.
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+    size_t events_used = 0;
+    int64_t launches = 0;
+
+    std::pair<cudaEvent_t, cudaEvent_t> next_events() {
+        if (events_used == events.size()) {
+            cudaEvent_t a = nullptr, b = nullptr;
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            events.emplace_back(a, b);
+        }
+        return events[events_used++];
+    }
+    ~Resident() override {
+        for (auto &e : events) {
+            if (e.first) cudaEventDestroy(e.first);
+            if (e.second) cudaEventDestroy(e.second);
+        }
+    }
+
+    size_t device_bytes() const override {
+        size_t b = x.bytes + y.bytes + z.bytes + rho.bytes + T1.bytes + T2.bytes + dw.bytes + csm_rows.bytes + t.bytes +
+                   dt.bytes + gx.bytes + gy.bytes + gz.bytes + b1.bytes + df.bytes + psi.bytes + adc.bytes + bnd.bytes +
+                   xy.bytes + mz.bytes + acc.bytes + rho_init.bytes + partial.bytes + sig.bytes + split.device_bytes();
+        for (int k = 0; k < 16; ++k) b += h[k].bytes;
+        return b;
+    }
+
+    void timing(homs_timing *out) const override {
+        double ms = 0.0;
+        for (size_t i = 0; i < events_used; ++i) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, events[i].first, events[i].second) == cudaSuccess) ms += t;
+        }
+        out->fused_kernel_ms = ms;
+        out->fused_launches = (int64_t)events_used;
+        out->kernel_launches = launches;
+    }
+
+    PhantomDev<T> phantom() const {
+        return PhantomDev<T>{ns, nc, reinterpret_cast<T *>(x.p), reinterpret_cast<T *>(y.p), reinterpret_cast<T *>(z.p), reinterpret_cast<T *>(rho.p), reinterpret_cast<T *>(T1.p), reinterpret_cast<T *>(T2.p),
+                             reinterpret_cast<T *>(dw.p), reinterpret_cast<cplx<T> *>(csm_rows.p), (int64_t)nc};
+    }
+    SeqDev<T> seq() const {
+        SeqDev<T> q;
+        q.nnodes = nt;
+        q.t = reinterpret_cast<T *>(t.p);
+        q.dt = reinterpret_cast<T *>(dt.p);
+        q.gx = reinterpret_cast<T *>(gx.p);
+        q.gy = reinterpret_cast<T *>(gy.p);
+        q.gz = reinterpret_cast<T *>(gz.p);
+        q.df = reinterpret_cast<T *>(df.p);
+        q.psi = reinterpret_cast<T *>(psi.p);
+        q.b1 = reinterpret_cast<cplx<T> *>(b1.p);
+        q.adc = reinterpret_cast<uint8_t *>(adc.p);
+        q.boundary = reinterpret_cast<uint8_t *>(bnd.p);
+        for (int k = 0; k < 16; ++k) q.h[k] = reinterpret_cast<T *>(h[k].p);
+        return q;
+    }
+};
+
+namespace {
+
+template <typename T>
+std::unique_ptr<Resident<T>> make_resident(homs_context *ctx, const homs_phantom *p, const homs_sequence *q) {
+    auto r = std::make_unique<Resident<T>>();
+    r->dtype = sizeof(T) == 8 ? HOMS_F64 : HOMS_F32;
+    r->ns = p->nspins;
+    r->nc = p->ncoils;
+    r->nt = q->nnodes;
+    r->gamma = q->gamma;
+    const int64_t ns = p->nspins, nt = q->nnodes;
+    upload<T>(ctx, r->x, p->x, p->dtype, p->memory, ns);
+    upload<T>(ctx, r->y, p->y, p->dtype, p->memory, ns);
+    upload<T>(ctx, r->z, p->z, p->dtype, p->memory, ns);
+    upload<T>(ctx, r->rho, p->rho, p->dtype, p->memory, ns);
+    upload<T>(ctx, r->T1, p->T1, p->dtype, p->memory, ns);
+    upload<T>(ctx, r->T2, p->T2, p->dtype, p->memory, ns);
+    upload<T>(ctx, r->dw, p->dw, p->dtype, p->memory, ns);
+    upload_csm_rows<T>(ctx, r->csm_rows, p->csm, p->dtype, p->memory, ns, p->ncoils, ns);
+    upload<T>(ctx, r->t, q->t, q->dtype, q->memory, nt);
+    upload<T>(ctx, r->dt, q->dt, q->dtype, q->memory, nt - 1);
+    upload<T>(ctx, r->gx, q->gx, q->dtype, q->memory, nt);
+    upload<T>(ctx, r->gy, q->gy, q->dtype, q->memory, nt);
+    upload<T>(ctx, r->gz, q->gz, q->dtype, q->memory, nt);
+    upload<T>(ctx, r->b1, q->b1, q->dtype, q->memory, 2 * nt);
+    upload<T>(ctx, r->df, q->df, q->dtype, q->memory, nt);
+    upload<T>(ctx, r->psi, q->psi, q->dtype, q->memory, nt);
+    for (int k = 0; k < 16; ++k) upload<T>(ctx, r->h[k], q->h[k], q->dtype, q->memory, nt);
+    r->adc_host = host_adc(ctx, q);
+    HOMS_CUDA(r->adc.ensure((size_t)nt));
+    HOMS_CUDA(cudaMemcpyAsync(r->adc.p, r->adc_host.data(), (size_t)nt, cudaMemcpyHostToDevice, ctx->stream));
+    r->first.assign(q->block_first, q->block_first + q->nblocks);
+    r->last.assign(q->block_last, q->block_last + q->nblocks);
+    r->exc.assign(q->block_excitation, q->block_excitation + q->nblocks);
+    std::vector<uint8_t> bnd((size_t)nt, 0);
+    for (int64_t l : r->last) bnd[(size_t)l] = 1;
+    HOMS_CUDA(r->bnd.ensure((size_t)nt));
+    HOMS_CUDA(cudaMemcpyAsync(r->bnd.p, bnd.data(), (size_t)nt, cudaMemcpyHostToDevice, ctx->stream));
+    r->dt_host = host_array<T>(ctx, q->dt, q->dtype, q->memory, nt - 1);
+    int64_t nadc = 0;
+    for (size_t k = 0; k < r->first.size(); ++k)
+        for (int64_t n = r->first[k] + 1; n <= r->last[k]; ++n) nadc += r->adc_host[(size_t)n] ? 1 : 0;
+    r->nadc = nadc;
+    HOMS_CUDA(r->xy.ensure(sizeof(cplx<T>) * (size_t)ns));
+    HOMS_CUDA(r->mz.ensure(sizeof(T) * (size_t)ns));
+    HOMS_CUDA(r->acc.ensure(sizeof(T) * (size_t)ns));
+    HOMS_CUDA(r->sig.ensure(sizeof(cplx<T>) * (size_t)std::max<int64_t>(nadc * p->ncoils, 1)));
+    HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return r;
+}
+
+// Launch plan of the plain path: runs of same-kind blocks cut into launches
+// of at most `max_samples` ADC samples.
+struct Launch {
+    int64_t run;
+    bool rf;
+    int64_t n_lo, n_hi;
+    int block_start;
+    double tp0;  // informational; the typed value is recomputed below
+    int64_t sample0, nsamples;
+};
+
+template <typename T>
+std::vector<std::pair<Launch, T>> plan_plain(const Resident<T> &r, int64_t max_samples) {
+    std::vector<std::pair<Launch, T>> out;
+    const auto &adc = r.adc_host;
+    int64_t sample = 0;
+    size_t k = 0;
+    const size_t nb = r.first.size();
+    while (k < nb) {
+        const bool rf = r.exc[k] != 0;
+        size_t k2 = k;
+        while (k2 < nb && (r.exc[k2] != 0) == rf) ++k2;
+        // run: blocks k .. k2-1, nodes first[k] .. last[k2-1]
+        size_t blk = k;
+        T tp = T(0);
+        int64_t n = r.first[k];
+        const int64_t n_end = r.last[k2 - 1];
+        while (n < n_end) {
+            Launch L{(int64_t)k, rf, n, n, n == r.first[blk] ? 1 : 0, 0.0, sample, 0};
+            const T tp0 = tp;
+            int64_t cnt = 0;
+            int64_t m = n;
+            while (m < n_end) {
+                // interval m -> node m+1
+                tp = tp + r.dt_host[(size_t)m];
+                const bool a = adc[(size_t)(m + 1)] != 0;
+                if (a) ++cnt;
+                ++m;
+                if (m == r.last[blk]) {
+                    tp = T(0);
+                    if (blk + 1 < k2) ++blk;
+                }
+                if (cnt >= max_samples) break;
+            }
+            L.n_hi = m;
+            L.nsamples = cnt;
+            sample += cnt;
+            out.emplace_back(L, tp0);
+            n = m;
+        }
+        k = k2;
+    }
+    return out;
+}
+
+template <typename T>
+void run_plain(homs_context *ctx, Resident<T> &r, uint32_t method) {
+    const int grid = (int)((r.ns + PLAIN_THREADS - 1) / PLAIN_THREADS);
+    const size_t row_bytes = sizeof(cplx<T>) * (size_t)r.nc * (size_t)grid;
+    const size_t budget = size_t(768) << 20;
+    int64_t max_samples = std::max<int64_t>(PLAIN_STAGE, (int64_t)(budget / row_bytes));
+    max_samples = std::min<int64_t>(max_samples, std::max<int64_t>(r.nadc, 1));
+    auto plan = plan_plain<T>(r, max_samples);
+    int64_t need = 0;
+    for (auto &pl : plan) need = std::max(need, pl.first.nsamples);
+    HOMS_CUDA(r.partial.ensure(row_bytes * (size_t)std::max<int64_t>(need, 1)));
+    PhantomDev<T> p = r.phantom();
+    SeqDev<T> q = r.seq();
+    StateDev<T> st{reinterpret_cast<cplx<T> *>(r.xy.p), reinterpret_cast<T *>(r.mz.p), reinterpret_cast<T *>(r.acc.p)};
+    for (auto &pl : plan) {
+        const Launch &L = pl.first;
+        SegmentArgs<T> a;
+        a.n_lo = L.n_lo;
+        a.n_hi = L.n_hi;
+        a.block_start = L.block_start;
+        a.tp0 = pl.second;
+        a.nsamples = L.nsamples;
+        a.method = method;
+        a.gamma = T(r.gamma);
+        a.gamma_d = r.gamma;
+        a.partial = reinterpret_cast<cplx<T> *>(r.partial.p);
+        auto ev = r.next_events();
+        HOMS_CUDA(cudaEventRecord(ev.first, ctx->stream));
+        HOMS_CUDA(launch_segment<T>(L.rf, p, q, st, a, grid, ctx->stream));
+        HOMS_CUDA(cudaEventRecord(ev.second, ctx->stream));
+        r.launches += 1;
+        if (L.nsamples > 0) {
+            HOMS_CUDA(launch_partial_finalize<T>(a.partial, grid, L.nsamples, r.nc,
+                                                 reinterpret_cast<cplx<T> *>(r.sig.p) + L.sample0, r.nadc, ctx->stream));
+            r.launches += 1;
+        }
+    }
+}
+
+template <typename T>
+void init_state(homs_context *ctx, Resident<T> &r, const homs_state *state, homs_dtype pdt) {
+    if (state && state->xy && state->z) {
+        HOMS_REQUIRE(state->memory == HOMS_HOST || state->memory == HOMS_DEVICE, "invalid state memory kind");
+        upload<T>(ctx, r.xy, state->xy, pdt, state->memory, 2 * r.ns);
+        upload<T>(ctx, r.mz, state->z, pdt, state->memory, r.ns);
+    } else {
+        HOMS_CUDA(cudaMemsetAsync(r.xy.p, 0, sizeof(cplx<T>) * (size_t)r.ns, ctx->stream));
+        HOMS_CUDA(cudaMemcpyAsync(r.mz.p, r.rho.p, sizeof(T) * (size_t)r.ns, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    HOMS_CUDA(cudaMemsetAsync(r.acc.p, 0, sizeof(T) * (size_t)r.ns, ctx->stream));
+}
+
+template <typename T>
+void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opts) {
+    r.events_used = 0;
+    r.launches = 0;
+    const uint32_t method = opts ? opts->method : 0x3Fu;
+    const homs_mode mode = opts ? opts->mode : HOMS_PLAIN;
+    HOMS_REQUIRE((method & ~0x3Fu) == 0, "unknown method flag bits");
+    if (mode == HOMS_PLAIN) {
+        run_plain<T>(ctx, r, method);
+    } else if (mode == HOMS_SPLIT) {
+        if (sizeof(T) != 8)
+            throw Failure{HOMS_EUNSUPPORTED,
+                          "split mode takes FP64 phantom and sequence arrays: FP32 positions alone carry phase "
+                          "errors above the split path's error budget"};
+        if (!r.split_ready) {
+            std::string err;
+            cudaError_t e = split_prepare(r.split, r.ns, r.nc, r.x.p, r.y.p, r.z.p, r.dw.p, r.csm_rows.p, true,
+                                          ctx->stream, &err);
+            if (e != cudaSuccess) throw Failure{e == cudaErrorMemoryAllocation ? HOMS_ENOMEM : HOMS_ECUDA,
+                                                std::string("split_prepare: ") + cudaGetErrorString(e)};
+            if (!err.empty()) throw Failure{HOMS_EUNSUPPORTED, err};
+            r.split_ready = true;
+        }
+        HOMS_CUDA(split_reset_error(r.split, ctx->stream));
+        SplitRunArgs sa;
+        sa.sizeof_T = sizeof(T);
+        sa.ns = r.ns;
+        sa.nc = r.nc;
+        sa.nt = r.nt;
+        sa.nadc = r.nadc;
+        sa.method = method;
+        sa.gamma = r.gamma;
+        sa.first = r.first.data();
+        sa.last = r.last.data();
+        sa.exc = r.exc.data();
+        sa.nblocks = (int32_t)r.first.size();
+        sa.adc_host = r.adc_host.data();
+        sa.t = r.t.p;
+        sa.dt = r.dt.p;
+        sa.gx = r.gx.p;
+        sa.gy = r.gy.p;
+        sa.gz = r.gz.p;
+        sa.b1 = r.b1.p;
+        sa.df = r.df.p;
+        sa.psi = r.psi.p;
+        sa.adc = r.adc.p;
+        sa.bnd = r.bnd.p;
+        for (int k = 0; k < 16; ++k) sa.h[k] = r.h[k].p;
+        sa.x = r.x.p;
+        sa.y = r.y.p;
+        sa.z = r.z.p;
+        sa.rho = r.rho.p;
+        sa.T1 = r.T1.p;
+        sa.T2 = r.T2.p;
+        sa.dw = r.dw.p;
+        sa.csm_rows = r.csm_rows.p;
+        sa.xy = r.xy.p;
+        sa.mz = r.mz.p;
+        sa.acc = r.acc.p;
+        sa.sig = r.sig.p;
+        // RF runs use the plain FP64 excitation kernel; precession runs are
+        // whole segments on the split kernel.
+        const int grid = (int)((r.ns + PLAIN_THREADS - 1) / PLAIN_THREADS);
+        const size_t row_bytes = sizeof(cplx<T>) * (size_t)r.nc * (size_t)grid;
+        const int64_t max_samples =
+            std::max<int64_t>(PLAIN_STAGE, (int64_t)((size_t(512) << 20) / row_bytes));
+        auto plan = plan_plain<T>(r, max_samples);
+        size_t i = 0;
+        PhantomDev<T> p = r.phantom();
+        SeqDev<T> q = r.seq();
+        StateDev<T> st{reinterpret_cast<cplx<T> *>(r.xy.p), reinterpret_cast<T *>(r.mz.p), reinterpret_cast<T *>(r.acc.p)};
+        while (i < plan.size()) {
+            const Launch &L = plan[i].first;
+            if (L.rf) {
+                HOMS_CUDA(r.partial.ensure(row_bytes * (size_t)std::max<int64_t>(L.nsamples, 1)));
+                SegmentArgs<T> a;
+                a.n_lo = L.n_lo;
+                a.n_hi = L.n_hi;
+                a.block_start = L.block_start;
+                a.tp0 = plan[i].second;
+                a.nsamples = L.nsamples;
+                a.method = method;
+                a.gamma = T(r.gamma);
+                a.gamma_d = r.gamma;
+                a.partial = reinterpret_cast<cplx<T> *>(r.partial.p);
+                HOMS_CUDA(launch_segment<T>(true, p, q, st, a, grid, ctx->stream));
+                r.launches += 1;
+                if (L.nsamples > 0) {
+                    HOMS_CUDA(launch_partial_finalize<T>(a.partial, grid, L.nsamples, r.nc,
+                                                         reinterpret_cast<cplx<T> *>(r.sig.p) + L.sample0, r.nadc, ctx->stream));
+                    r.launches += 1;
+                }
+                ++i;
+                continue;
+            }
+            // merge consecutive precession launches of one run
+            size_t j = i;
+            int64_t ns_total = 0;
+            while (j < plan.size() && !plan[j].first.rf && plan[j].first.run == L.run) {
+                ns_total += plan[j].first.nsamples;
+                ++j;
+            }
+            std::string err;
+            auto ev = r.next_events();
+            sa.ev_start = ev.first;
+            sa.ev_stop = ev.second;
+            sa.launches = &r.launches;
+            cudaError_t e = split_run_segment(r.split, sa, L.n_lo, plan[j - 1].first.n_hi, L.sample0, ns_total,
+                                              ctx->stream, &err);
+            if (ns_total == 0) {
+                // no fused launch happened: keep the pair unused
+                --r.events_used;
+            }
+            if (e != cudaSuccess) throw Failure{e == cudaErrorMemoryAllocation ? HOMS_ENOMEM : HOMS_ECUDA,
+                                                std::string("split segment: ") + cudaGetErrorString(e)};
+            if (!err.empty()) throw Failure{HOMS_EUNSUPPORTED, err};
+            i = j;
+        }
+        std::string err;
+        HOMS_CUDA(split_check(r.split, ctx->stream, &err));
+        if (!err.empty())
+            throw Failure{err.find("timed out") != std::string::npos ? HOMS_ETIMEDOUT : HOMS_EUNSUPPORTED, err};
+    } else {
+        throw Failure{HOMS_EINVAL, "unknown run mode"};
+    }
+}
+
+template <typename T>
+void copy_out(homs_context *ctx, Resident<T> &r, void *sig, homs_memory sig_memory, homs_state *state) {
+    const size_t sig_bytes = sizeof(cplx<T>) * (size_t)(r.nadc * r.nc);
+    if (sig_bytes > 0) {
+        HOMS_REQUIRE(sig != nullptr, "sig is NULL");
+        HOMS_CUDA(cudaMemcpyAsync(sig, r.sig.p, sig_bytes,
+                                  sig_memory == HOMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+    }
+    if (state && state->xy && state->z) {
+        const cudaMemcpyKind kind = state->memory == HOMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+        HOMS_CUDA(cudaMemcpyAsync(state->xy, r.xy.p, sizeof(cplx<T>) * (size_t)r.ns, kind, ctx->stream));
+        HOMS_CUDA(cudaMemcpyAsync(state->z, r.mz.p, sizeof(T) * (size_t)r.ns, kind, ctx->stream));
+    }
+    HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Plans
+// ---------------------------------------------------------------------------
+
+struct homs_plan {
+    homs_context *ctx = nullptr;
+    homs_run_options opts{};
+    std::unique_ptr<ResidentBase> res;
+    std::vector<unsigned char> state_snapshot;  // unused: runs restart from Mxy=0, Mz=rho
+};
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int homs_abi_version(void) { return HOMS_ABI_VERSION; }
+
+const char *homs_status_string(homs_status s) {
+    switch (s) {
+        case HOMS_OK: return "ok";
+        case HOMS_EINVAL: return "invalid argument";
+        case HOMS_ENOMEM: return "out of memory";
+        case HOMS_EUNSUPPORTED: return "unsupported";
+        case HOMS_ETIMEDOUT: return "timed out";
+        case HOMS_ECUDA: return "CUDA error";
+        case HOMS_ECLOSED: return "closed";
+        case HOMS_EBUSY: return "busy";
+    }
+    return "unknown status";
+}
+
+homs_status homs_context_create(int device, void *stream, homs_context **out) {
+    if (!out) return HOMS_EINVAL;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return HOMS_EUNSUPPORTED;
+    }
+    if (device < 0 || device >= count) return HOMS_EINVAL;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return HOMS_ECUDA;
+    if (prop.major != 10) return HOMS_EUNSUPPORTED;  // sm_100a code only
+    auto *ctx = new (std::nothrow) homs_context();
+    if (!ctx) return HOMS_ENOMEM;
+    ctx->device = device;
+    DeviceGuard g(device);
+    if (stream) {
+        ctx->stream = static_cast<cudaStream_t>(stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete ctx;
+            return HOMS_ECUDA;
+        }
+        ctx->own_stream = true;
+    }
+    *out = ctx;
+    return HOMS_OK;
+}
+
+homs_status homs_context_destroy(homs_context *ctx) {
+    if (!ctx) return HOMS_EINVAL;
+    {
+        DeviceGuard g(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->scratch_csm.release();
+        ctx->scratch_partial.release();
+        ctx->scratch_acc.release();
+        ctx->scratch_bnd.release();
+        ctx->scratch_sig.release();
+        ctx->scratch_conv.release();
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return HOMS_OK;
+}
+
+const char *homs_last_error(const homs_context *ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+homs_status homs_synchronize(homs_context *ctx) {
+    if (!ctx) return HOMS_EINVAL;
+    DeviceGuard g(ctx->device);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, Failure{HOMS_ECUDA, cudaGetErrorString(e)});
+    return HOMS_OK;
+}
+
+homs_status homs_count_adc(const homs_sequence *seq, int64_t *nadc) {
+    if (!seq || !nadc || !seq->adc || !seq->block_first || !seq->block_last) return HOMS_EINVAL;
+    if (seq->memory != HOMS_HOST) return HOMS_EINVAL;
+    int64_t c = 0;
+    for (int32_t k = 0; k < seq->nblocks; ++k)
+        for (int64_t n = seq->block_first[k] + 1; n <= seq->block_last[k] && n < seq->nnodes; ++n) c += seq->adc[n] ? 1 : 0;
+    *nadc = c;
+    return HOMS_OK;
+}
+
+homs_status homs_simulate(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                          const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory) {
+    if (!ctx) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        validate_phantom(phantom);
+        validate_sequence(seq);
+        HOMS_REQUIRE(sig_memory == HOMS_HOST || sig_memory == HOMS_DEVICE, "invalid signal memory kind");
+        if (phantom->dtype == HOMS_F64) {
+            auto r = make_resident<double>(ctx, phantom, seq);
+            init_state<double>(ctx, *r, state, phantom->dtype);
+            run_resident<double>(ctx, *r, opts);
+            copy_out<double>(ctx, *r, sig, sig_memory, state);
+        } else {
+            auto r = make_resident<float>(ctx, phantom, seq);
+            init_state<float>(ctx, *r, state, phantom->dtype);
+            run_resident<float>(ctx, *r, opts);
+            copy_out<float>(ctx, *r, sig, sig_memory, state);
+        }
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, Failure{HOMS_ENOMEM, "host allocation failed"});
+    }
+}
+
+homs_status homs_plan_create(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                             const homs_run_options *opts, homs_plan **out) {
+    if (!ctx || !out) return HOMS_EINVAL;
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        validate_phantom(phantom);
+        validate_sequence(seq);
+        auto plan = std::make_unique<homs_plan>();
+        plan->ctx = ctx;
+        if (opts) plan->opts = *opts;
+        else plan->opts.method = 0x3Fu;
+        if (phantom->dtype == HOMS_F64) plan->res = make_resident<double>(ctx, phantom, seq);
+        else plan->res = make_resident<float>(ctx, phantom, seq);
+        *out = plan.release();
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, Failure{HOMS_ENOMEM, "host allocation failed"});
+    }
+}
+
+homs_status homs_plan_run(homs_plan *plan, void *sig, homs_memory sig_memory, homs_state *state_out) {
+    if (!plan || !plan->res) return plan ? HOMS_ECLOSED : HOMS_EINVAL;
+    homs_context *ctx = plan->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        HOMS_REQUIRE(sig_memory == HOMS_HOST || sig_memory == HOMS_DEVICE, "invalid signal memory kind");
+        if (plan->res->dtype == HOMS_F64) {
+            auto &r = static_cast<Resident<double> &>(*plan->res);
+            init_state<double>(ctx, r, nullptr, HOMS_F64);
+            run_resident<double>(ctx, r, &plan->opts);
+            copy_out<double>(ctx, r, sig, sig_memory, state_out);
+        } else {
+            auto &r = static_cast<Resident<float> &>(*plan->res);
+            init_state<float>(ctx, r, nullptr, HOMS_F32);
+            run_resident<float>(ctx, r, &plan->opts);
+            copy_out<float>(ctx, r, sig, sig_memory, state_out);
+        }
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    }
+}
+
+homs_status homs_plan_device_bytes(const homs_plan *plan, size_t *bytes) {
+    if (!plan || !bytes) return HOMS_EINVAL;
+    if (!plan->res) return HOMS_ECLOSED;
+    *bytes = plan->res->device_bytes();
+    return HOMS_OK;
+}
+
+homs_status homs_plan_timing(const homs_plan *plan, homs_timing *out) {
+    if (!plan || !out) return HOMS_EINVAL;
+    if (!plan->res) return HOMS_ECLOSED;
+    plan->res->timing(out);
+    return HOMS_OK;
+}
+
+homs_status homs_plan_destroy(homs_plan *plan) {
+    if (!plan) return HOMS_EINVAL;
+    if (plan->ctx) {
+        std::lock_guard<std::mutex> lock(plan->ctx->mu);
+        DeviceGuard g(plan->ctx->device);
+        cudaStreamSynchronize(plan->ctx->stream);
+        plan->res.reset();
+    }
+    delete plan;
+    return HOMS_OK;
+}
+
+}  // extern "C"
+
+// ---- block kernels on caller device arrays -----------------------------------
+
+namespace {
+
+template <typename T>
+homs_status block_impl(homs_context *ctx, bool rf, const homs_phantom *p, const homs_sequence *q, int64_t first,
+                       int64_t last, uint32_t method, homs_state *state, void *sig, int64_t ldsig) {
+    validate_phantom(p);
+    HOMS_REQUIRE(p->memory == HOMS_DEVICE, "block kernels take device arrays");
+    HOMS_REQUIRE(q && q->memory == HOMS_DEVICE && q->dtype == p->dtype, "sequence must be device arrays of the phantom dtype");
+    HOMS_REQUIRE(q->nnodes >= 2, "The sequence must contain a simulation interval.");
+    HOMS_REQUIRE(first >= 0 && last > first && last < q->nnodes, "invalid block node range");
+    HOMS_REQUIRE(state && state->xy && state->z && state->memory == HOMS_DEVICE, "state must be device arrays");
+    HOMS_REQUIRE((method & ~0x3Fu) == 0, "unknown method flag bits");
+    const int64_t ns = p->nspins, nt = q->nnodes;
+    const int32_t nc = p->ncoils;
+    // ADC count of the block.
+    std::vector<uint8_t> adc((size_t)(last - first));
+    HOMS_CUDA(cudaMemcpyAsync(adc.data(), q->adc + first + 1, adc.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+    int64_t nadc = 0;
+    for (auto v : adc) nadc += v ? 1 : 0;
+    HOMS_REQUIRE(nadc == 0 || (sig != nullptr && ldsig >= nadc), "sig is NULL or its leading dimension is too small");
+    // Boundary flags: only `last` ends a block.
+    HOMS_CUDA(ctx->scratch_bnd.ensure((size_t)nt));
+    HOMS_CUDA(cudaMemsetAsync(ctx->scratch_bnd.p, 0, (size_t)nt, ctx->stream));
+    const uint8_t one = 1;
+    HOMS_CUDA(cudaMemcpyAsync(reinterpret_cast<uint8_t *>(ctx->scratch_bnd.p) + last, &one, 1, cudaMemcpyHostToDevice, ctx->stream));
+    upload_csm_rows<T>(ctx, ctx->scratch_csm, p->csm, p->dtype, HOMS_DEVICE, ns, nc, ns);
+    HOMS_CUDA(ctx->scratch_acc.ensure(sizeof(T) * (size_t)ns));
+    const int grid = (int)((ns + PLAIN_THREADS - 1) / PLAIN_THREADS);
+    HOMS_CUDA(ctx->scratch_partial.ensure(sizeof(cplx<T>) * (size_t)grid * (size_t)std::max<int64_t>(nadc, 1) * nc));
+    HOMS_CUDA(ctx->scratch_sig.ensure(sizeof(cplx<T>) * (size_t)std::max<int64_t>(nadc, 1) * nc));
+    PhantomDev<T> pd{ns, nc, (const T *)p->x, (const T *)p->y, (const T *)p->z, (const T *)p->rho, (const T *)p->T1,
+                     (const T *)p->T2, (const T *)p->dw, reinterpret_cast<cplx<T> *>(ctx->scratch_csm.p), nc};
+    SeqDev<T> qd;
+    qd.nnodes = nt;
+    qd.t = (const T *)q->t;
+    qd.dt = (const T *)q->dt;
+    qd.gx = (const T *)q->gx;
+    qd.gy = (const T *)q->gy;
+    qd.gz = (const T *)q->gz;
+    qd.df = (const T *)q->df;
+    qd.psi = (const T *)q->psi;
+    qd.b1 = (const cplx<T> *)q->b1;
+    qd.adc = q->adc;
+    qd.boundary = reinterpret_cast<uint8_t *>(ctx->scratch_bnd.p);
+    for (int k = 0; k < 16; ++k) qd.h[k] = (const T *)q->h[k];
+    StateDev<T> st{(cplx<T> *)state->xy, (T *)state->z, reinterpret_cast<T *>(ctx->scratch_acc.p)};
+    SegmentArgs<T> a;
+    a.n_lo = first;
+    a.n_hi = last;
+    a.block_start = 1;
+    a.tp0 = T(0);
+    a.nsamples = nadc;
+    a.method = method;
+    a.gamma = T(q->gamma);
+    a.gamma_d = q->gamma;
+    a.partial = reinterpret_cast<cplx<T> *>(ctx->scratch_partial.p);
+    HOMS_CUDA(launch_segment<T>(rf, pd, qd, st, a, grid, ctx->stream));
+    if (nadc > 0) {
+        HOMS_CUDA(launch_partial_finalize<T>(a.partial, grid, nadc, nc, reinterpret_cast<cplx<T> *>(ctx->scratch_sig.p), nadc, ctx->stream));
+        HOMS_CUDA(cudaMemcpy2DAsync(sig, sizeof(cplx<T>) * (size_t)ldsig, ctx->scratch_sig.p, sizeof(cplx<T>) * (size_t)nadc,
+                                    sizeof(cplx<T>) * (size_t)nadc, (size_t)nc, cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return HOMS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+homs_status homs_precession_block(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                                  int64_t first, int64_t last, uint32_t method, homs_state *state, void *sig,
+                                  int64_t ldsig) {
+    if (!ctx) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        if (!phantom) throw Failure{HOMS_EINVAL, "phantom is NULL"};
+        return phantom->dtype == HOMS_F64
+                   ? block_impl<double>(ctx, false, phantom, seq, first, last, method, state, sig, ldsig)
+                   : block_impl<float>(ctx, false, phantom, seq, first, last, method, state, sig, ldsig);
+    } catch (const Failure &f) {
+        return fail(ctx, f);
+    }
+}
+
+homs_status homs_excitation_block(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                                  int64_t first, int64_t last, uint32_t method, homs_state *state, void *sig,
+                                  int64_t ldsig) {
+    if (!ctx) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        if (!phantom) throw Failure{HOMS_EINVAL, "phantom is NULL"};
+        return phantom->dtype == HOMS_F64
+                   ? block_impl<double>(ctx, true, phantom, seq, first, last, method, state, sig, ldsig)
+                   : block_impl<float>(ctx, true, phantom, seq, first, last, method, state, sig, ldsig);
+    } catch (const Failure &f) {
+        return fail(ctx, f);
+    }
+}
+
+homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins, int64_t nadc, int32_t ncoils,
+                             const void *states, int64_t ldstates, const void *csm, int64_t ldcsm, void *sig,
+                             int64_t ldsig) {
+    if (!ctx) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        HOMS_REQUIRE(dtype == HOMS_F32 || dtype == HOMS_F64, "dtype must be f32 or f64");
+        HOMS_REQUIRE(nspins >= 0 && nadc >= 0 && ncoils >= 1, "States, CSM, and signal dimensions do not match.");
+        HOMS_REQUIRE(nadc == 0 || (sig && ldsig >= nadc), "sig is NULL or its leading dimension is too small");
+        HOMS_REQUIRE(nspins == 0 || nadc == 0 || (states && ldstates >= nspins), "states is NULL or ldstates < nspins");
+        HOMS_REQUIRE(nspins == 0 || (csm && ldcsm >= nspins), "csm is NULL or ldcsm < nspins");
+        if (nadc == 0) return HOMS_OK;
+        const size_t es = dtype == HOMS_F64 ? 16 : 8;
+        if (nspins == 0) {
+            HOMS_CUDA(cudaMemset2DAsync(sig, es * (size_t)ldsig, 0, es * (size_t)nadc, (size_t)ncoils, ctx->stream));
+            return HOMS_OK;
+        }
+        const int64_t tiles = (nspins + PLAIN_THREADS - 1) / PLAIN_THREADS;
+        HOMS_CUDA(ctx->scratch_partial.ensure(es * (size_t)tiles * (size_t)nadc * (size_t)ncoils));
+        if (dtype == HOMS_F64) {
+            HOMS_CUDA(launch_coil_reduce<double>(nspins, nadc, ncoils, (const cplx<double> *)states, ldstates,
+                                                 (const cplx<double> *)csm, ldcsm, reinterpret_cast<cplx<double> *>(ctx->scratch_partial.p),
+                                                 ctx->stream));
+            HOMS_CUDA(launch_partial_finalize<double>(reinterpret_cast<cplx<double> *>(ctx->scratch_partial.p), tiles, nadc, ncoils,
+                                                      (cplx<double> *)sig, ldsig, ctx->stream));
+        } else {
+            HOMS_CUDA(launch_coil_reduce<float>(nspins, nadc, ncoils, (const cplx<float> *)states, ldstates,
+                                                (const cplx<float> *)csm, ldcsm, reinterpret_cast<cplx<float> *>(ctx->scratch_partial.p),
+                                                ctx->stream));
+            HOMS_CUDA(launch_partial_finalize<float>(reinterpret_cast<cplx<float> *>(ctx->scratch_partial.p), tiles, nadc, ncoils,
+                                                     (cplx<float> *)sig, ldsig, ctx->stream));
+        }
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        return fail(ctx, f);
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,496 @@
+// Plain fused kernels of libhoms: free precession and RF excitation in the
+// phantom's own precision (FP64 or FP32) on CUDA cores, fused with a
+// deterministic multi-coil reduction.  No per-spin ADC history is written to
+// HBM: ADC states are staged in shared memory and contracted with the
+// receive sensitivities on chip, one CTA partial per (CTA, sample, coil),
+// then summed over CTAs in a fixed order.
+//
+// This translation unit is compiled with -fmad=false so that every product
+// and sum rounds exactly as in HighOrderMRISim.jl's CPU path
+// (src/simulation/Bloch/BlochHighOrderSimulatitonMethod.jl:43-134), which does
+// not contract multiply-adds; the FP64 kernel therefore agrees with the FP64
+// CPU restatement to ~1e-15.
+#include <cfloat>
+
+#include "homs_common.cuh"
+
+namespace homs {
+
+template <typename T>
+struct Math;
+
+template <>
+struct Math<double> {
+    static __device__ __forceinline__ double ex(double x) { return exp(x); }
+    static __device__ __forceinline__ void sc(double x, double *s, double *c) { sincos(x, s, c); }
+    static __device__ __forceinline__ double hyp(double a, double b) { return hypot(a, b); }
+    static __device__ __forceinline__ double sq(double a) { return sqrt(a); }
+    static __device__ __forceinline__ double eps() { return DBL_EPSILON; }
+};
+
+template <>
+struct Math<float> {
+    static __device__ __forceinline__ float ex(float x) { return expf(x); }
+    static __device__ __forceinline__ void sc(float x, float *s, float *c) { sincosf(x, s, c); }
+    static __device__ __forceinline__ float hyp(float a, float b) { return hypotf(a, b); }
+    static __device__ __forceinline__ float sq(float a) { return sqrtf(a); }
+    static __device__ __forceinline__ float eps() { return FLT_EPSILON; }
+};
+
+// Julia's complex product: (ar*br - ai*bi, ar*bi + ai*br).
+template <typename T>
+__device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    return cplx<T>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+
+// Sixteen unnormalised solid harmonics in the CPU expression order
+// (BlochHighOrderSimulatitonMethod.jl:54-68).
+template <typename T>
+__device__ __forceinline__ void basis16(T x, T y, T z, T *b) {
+    T x2 = x * x, y2 = y * y, z2 = z * z;
+    T r2 = (x2 + y2) + z2;
+    b[0] = T(1);
+    b[1] = x;
+    b[2] = y;
+    b[3] = z;
+    b[4] = x * y;
+    b[5] = z * y;
+    b[6] = T(3) * z2 - r2;
+    b[7] = x * z;
+    b[8] = x2 - y2;
+    b[9] = (T(3) * y) * x2 - (y2 * y);
+    b[10] = (x * z) * y;
+    b[11] = (T(5) * z2 - r2) * y;
+    b[12] = T(5) * (z2 * z) - (T(3) * z) * r2;
+    b[13] = (T(5) * z2 - r2) * x;
+    b[14] = x2 * z - y2 * z;
+    b[15] = (x2 * x) - (T(3) * x) * y2;
+}
+
+constexpr int NODE_CHUNK = 32;
+
+// Shared-memory node cache for one chunk of nodes [c0, c0 + NODE_CHUNK].
+template <typename T>
+struct NodeCache {
+    T dt[NODE_CHUNK + 1];
+    T g[3][NODE_CHUNK + 1];
+    T h[16][NODE_CHUNK + 1];
+    T df[NODE_CHUNK + 1];
+    T psi[NODE_CHUNK + 1];
+    cplx<T> b1[NODE_CHUNK + 1];
+    uint8_t adc[NODE_CHUNK + 1];
+    uint8_t bnd[NODE_CHUNK + 1];
+};
+
+// Bz at a cached node (BlochHighOrderSimulatitonMethod.jl:70-75).
+template <typename T>
+__device__ __forceinline__ T field_cached(const NodeCache<T> &nc, int i, const T *b, T dwterm, uint32_t m) {
+    T bz0 = (m & HOMS_HO0) ? nc.h[0][i] : T(0);
+    T bz1;
+    if (m & HOMS_HO1)
+        bz1 = (b[1] * nc.h[1][i] + b[2] * nc.h[2][i]) + b[3] * nc.h[3][i];
+    else
+        bz1 = (b[1] * nc.g[0][i] + b[2] * nc.g[1][i]) + b[3] * nc.g[2][i];
+    T bz2 = T(0), bz3 = T(0);
+    if (m & HOMS_HO2)
+        bz2 = (((b[4] * nc.h[4][i] + b[5] * nc.h[5][i]) + b[6] * nc.h[6][i]) + b[7] * nc.h[7][i]) +
+              b[8] * nc.h[8][i];
+    if (m & HOMS_HO3)
+        bz3 = (((((b[9] * nc.h[9][i] + b[10] * nc.h[10][i]) + b[11] * nc.h[11][i]) + b[12] * nc.h[12][i]) +
+                b[13] * nc.h[13][i]) +
+               b[14] * nc.h[14][i]) +
+              b[15] * nc.h[15][i];
+    T bz = ((bz0 + bz1) + bz2) + bz3;
+    if (m & HOMS_DW_PRECESSION) bz = bz + dwterm;
+    return bz;
+}
+
+template <typename T, bool RF>
+__device__ void load_nodes(NodeCache<T> &nc, const SeqDev<T> &q, int64_t c0, int64_t c_end, uint32_t m) {
+    // nodes c0 .. min(c0 + NODE_CHUNK, c_end) inclusive
+    const int n = (int)imin64(NODE_CHUNK, c_end - c0) + 1;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int64_t g = c0 + i;
+        nc.dt[i] = (g < q.nnodes - 1) ? q.dt[g] : T(0);
+        nc.adc[i] = q.adc[g];
+        nc.bnd[i] = q.boundary[g];
+        if (RF) {
+            nc.g[0][i] = q.gx[g];
+            nc.g[1][i] = q.gy[g];
+            nc.g[2][i] = q.gz[g];
+            nc.b1[i] = q.b1[g];
+            nc.df[i] = q.df[g];
+            nc.psi[i] = q.psi[g];
+        } else {
+            if (!(m & HOMS_HO1)) {
+                nc.g[0][i] = q.gx[g];
+                nc.g[1][i] = q.gy[g];
+                nc.g[2][i] = q.gz[g];
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) nc.h[k][i] = q.h[k][g];
+        }
+    }
+}
+
+// Contract `na` staged ADC states X[a][s] (s < PLAIN_THREADS) with the
+// sensitivities of this CTA's spins and write one partial row per sample:
+// out[a * nc + c] = sum_s X[a][s] * csm[s][c], summed over spins in a fixed
+// order (a per-lane sweep, then splits in index order).
+template <typename T>
+__device__ void reduce_stage(const cplx<T> *X, cplx<T> *P, int na, const cplx<T> *csm_rows, int csm_ld,
+                             int nvalid, int32_t nc, cplx<T> *out) {
+    const int t = threadIdx.x;
+    for (int cg = 0; cg < nc; cg += 32) {
+        const int left = min(32, nc - cg);
+        int cw = 1;
+        while (cw < left) cw <<= 1;
+        const int cl = t % cw, split = t / cw;
+        const int c = cg + cl;
+        cplx<T> acc[PLAIN_STAGE];
+#pragma unroll
+        for (int a = 0; a < PLAIN_STAGE; ++a) acc[a] = cplx<T>{T(0), T(0)};
+        if (cl < left) {
+            for (int i = 0; i < cw; ++i) {
+                const int s = split * cw + i;
+                if (s >= nvalid) break;
+                const cplx<T> w = csm_rows[(int64_t)s * csm_ld + c];
+#pragma unroll
+                for (int a = 0; a < PLAIN_STAGE; ++a) {
+                    if (a < na) {
+                        cplx<T> v = cmul(X[a * PLAIN_THREADS + s], w);
+                        acc[a].re = acc[a].re + v.re;
+                        acc[a].im = acc[a].im + v.im;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < PLAIN_STAGE; ++a)
+            if (a < na) P[(split * PLAIN_STAGE + a) * cw + cl] = acc[a];
+        __syncthreads();
+        const int nsplit = PLAIN_THREADS / cw;
+        if (t < na * cw) {
+            const int a = t / cw, c2 = t % cw;
+            cplx<T> s{T(0), T(0)};
+            for (int j = 0; j < nsplit; ++j) {
+                cplx<T> v = P[(j * PLAIN_STAGE + a) * cw + c2];
+                s.re = s.re + v.re;
+                s.im = s.im + v.im;
+            }
+            if (c2 < left) out[(int64_t)a * nc + cg + c2] = s;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+size_t segment_smem_bytes(int32_t nc) {
+    size_t bytes = sizeof(NodeCache<T>) + 2 * sizeof(cplx<T>) * PLAIN_STAGE * PLAIN_THREADS;
+    size_t csm_bytes = sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS;
+    if (csm_bytes <= 128 * 1024) bytes += csm_bytes;
+    return (bytes + 127) & ~size_t(127);
+}
+
+// Plain segment kernel.  One thread per spin; all threads of a CTA walk the
+// same node range in lockstep, so ADC staging and the coil reduction are
+// CTA-uniform.  RF=false: free precession (per-spin sequential trapezoid in
+// the CPU order, BlochHighOrderSimulatitonMethod.jl:76-92).  RF=true:
+// excitation (per-node hard-pulse spinor, :100-134; spinor of
+// kernels/HighOrderGPU.jl:181-192).
+template <typename T, bool RF>
+__global__ void __launch_bounds__(PLAIN_THREADS)
+    segment_kernel(PhantomDev<T> p, SeqDev<T> q, StateDev<T> st, SegmentArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    NodeCache<T> &nc = *reinterpret_cast<NodeCache<T> *>(smem_raw);
+    cplx<T> *X = reinterpret_cast<cplx<T> *>(smem_raw + ((sizeof(NodeCache<T>) + 15) & ~size_t(15)));
+    cplx<T> *P = X + PLAIN_STAGE * PLAIN_THREADS;
+    cplx<T> *csm_s = P + PLAIN_STAGE * PLAIN_THREADS;
+
+    const int64_t spin0 = (int64_t)blockIdx.x * PLAIN_THREADS;
+    const int64_t s = spin0 + threadIdx.x;
+    const bool active = s < p.ns;
+    const int nvalid = (int)imin64(PLAIN_THREADS, p.ns - spin0);
+    const int32_t ncoil = p.nc;
+    const bool csm_in_smem = sizeof(cplx<T>) * (size_t)ncoil * PLAIN_THREADS <= 128 * 1024;
+
+    // Stage this CTA's sensitivities (rows s, coil-fastest).
+    const cplx<T> *csm_rows;
+    int csm_ld = ncoil;
+    if (csm_in_smem) {
+        const int64_t total = (int64_t)nvalid * ncoil;
+        for (int64_t i = threadIdx.x; i < total; i += PLAIN_THREADS) csm_s[i] = p.csm[spin0 * ncoil + i];
+        csm_rows = csm_s;
+    } else {
+        csm_rows = p.csm + spin0 * ncoil;
+    }
+
+    const uint32_t m = a.method;
+    const T gamma = a.gamma;
+    // Constants converted from FP64 exactly as the reference's T(2π*γ).
+    const double twopig_d = 2.0 * 3.141592653589793 * a.gamma_d;
+    const T c_twopig = T(twopig_d);
+    const T c_neg = T(-twopig_d);
+
+    const int64_t si = active ? s : 0;
+    const T px = p.x[si], py = p.y[si], pz = p.z[si];
+    const T T1 = p.T1[si], T2 = p.T2[si], rho = p.rho[si];
+    cplx<T> xy = active ? st.xy[si] : cplx<T>{T(0), T(0)};
+    T mz = active ? st.z[si] : T(0);
+
+    T b[16];
+    T dwterm = T(0);
+    T off = T(0);
+    T acc = T(0);
+    T tp = a.tp0;
+    T prev = T(0);
+    if (!RF) {
+        basis16(px, py, pz, b);
+        dwterm = p.dw[si] / c_twopig;
+        acc = a.block_start ? T(0) : (active ? st.acc[si] : T(0));
+    } else {
+        off = (m & HOMS_DW_EXCITATION) ? p.dw[si] / c_twopig : T(0);
+    }
+
+    int staged = 0;
+    int64_t sample = 0;
+    cplx<T> *out_base = a.partial + (int64_t)blockIdx.x * a.nsamples * ncoil;
+
+    for (int64_t c0 = a.n_lo; c0 < a.n_hi; c0 += NODE_CHUNK) {
+        __syncthreads();
+        load_nodes<T, RF>(nc, q, c0, a.n_hi, m);
+        __syncthreads();
+        const int nint = (int)imin64(NODE_CHUNK, a.n_hi - c0);
+        if (c0 == a.n_lo) {
+            if (!RF) {
+                prev = field_cached(nc, 0, b, dwterm, m);
+            } else if (a.block_start) {
+                T sn, cs;
+                Math<T>::sc(-nc.psi[0], &sn, &cs);
+                xy = cmul(xy, cplx<T>{cs, sn});
+            }
+        }
+        for (int i = 0; i < nint; ++i) {
+            const T dt = nc.dt[i];
+            cplx<T> xs;
+            bool have = false;
+            if (!RF) {
+                const T next = field_cached(nc, i + 1, b, dwterm, m);
+                const T y = (next + prev) * dt;
+                acc = acc + y;
+                tp = tp + dt;
+                prev = next;
+                if (nc.adc[i + 1] || nc.bnd[i + 1]) {
+                    const T phi = c_neg * (T(0.5) * acc);
+                    const T e = Math<T>::ex(T(0) - tp / T2);
+                    T sn, cs;
+                    Math<T>::sc(phi, &sn, &cs);
+                    xs = cmul(xy, cplx<T>{e * cs, e * sn});
+                    have = true;
+                }
+            } else {
+                const T dbz = off - nc.df[i] / gamma;
+                const T bz = ((nc.g[0][i] * px + nc.g[1][i] * py) + nc.g[2][i] * pz) + dbz;
+                const cplx<T> b1 = nc.b1[i];
+                const T ab1 = Math<T>::hyp(b1.re, b1.im);
+                T B = Math<T>::sq(ab1 * ab1 + bz * bz);
+                if (B == T(0)) B = Math<T>::eps();
+                const T phi = c_neg * (B * dt);
+                T sh, ch;
+                Math<T>::sc(phi / T(2), &sh, &ch);
+                const T nz = bz / B, nxr = b1.re / B, nxi = b1.im / B;
+                const cplx<T> al{ch, -(nz * sh)};
+                const cplx<T> be{nxi * sh, -(nxr * sh)};
+                cplx<T> t1 = cmul(cplx<T>{T(2) * al.re, -(T(2) * al.im)}, be);
+                t1.re = t1.re * mz;
+                t1.im = t1.im * mz;
+                const cplx<T> ca{al.re, -al.im};
+                const cplx<T> t2 = cmul(cmul(ca, ca), xy);
+                const cplx<T> t3 = cmul(cmul(be, be), cplx<T>{xy.re, -xy.im});
+                const cplx<T> nxy{(t1.re + t2.re) - t3.re, (t1.im + t2.im) - t3.im};
+                const T aa = Math<T>::hyp(al.re, al.im), bb = Math<T>::hyp(be.re, be.im);
+                const cplx<T> pr = cmul(cmul(al, be), cplx<T>{xy.re, -xy.im});
+                const T nz2 = (aa * aa - bb * bb) * mz - T(2) * pr.re;
+                const T e2 = Math<T>::ex(-dt / T2);
+                xy = cplx<T>{nxy.re * e2, nxy.im * e2};
+                const T e1 = Math<T>::ex(-dt / T1);
+                mz = nz2 * e1 + rho * (T(1) - e1);
+                if (nc.adc[i + 1]) {
+                    T sn, cs;
+                    Math<T>::sc(nc.psi[i + 1], &sn, &cs);
+                    xs = cmul(xy, cplx<T>{cs, sn});
+                    have = true;
+                }
+            }
+            if (nc.adc[i + 1]) {
+                X[staged * PLAIN_THREADS + threadIdx.x] = active ? xs : cplx<T>{T(0), T(0)};
+                staged++;
+                if (staged == PLAIN_STAGE) {
+                    __syncthreads();
+                    reduce_stage(X, P, staged, csm_rows, csm_ld, nvalid, ncoil, out_base + sample * ncoil);
+                    sample += staged;
+                    staged = 0;
+                }
+            }
+            if (nc.bnd[i + 1]) {
+                if (!RF) {
+                    // Block end: Mxy = last column, Mz relaxes over the block, phase restarts.
+                    (void)have;
+                    xy = xs;
+                    const T e1 = Math<T>::ex(-tp / T1);
+                    mz = mz * e1 + rho * (T(1) - e1);
+                    acc = T(0);
+                    tp = T(0);
+                } else {
+                    T sn, cs;
+                    Math<T>::sc(nc.psi[i + 1], &sn, &cs);
+                    xy = cmul(xy, cplx<T>{cs, sn});
+                    if (c0 + i + 1 < a.n_hi) {
+                        Math<T>::sc(-nc.psi[i + 1], &sn, &cs);
+                        xy = cmul(xy, cplx<T>{cs, sn});
+                    }
+                }
+            }
+        }
+    }
+    if (staged > 0) {
+        __syncthreads();
+        reduce_stage(X, P, staged, csm_rows, csm_ld, nvalid, ncoil, out_base + sample * ncoil);
+    }
+    if (active) {
+        st.xy[s] = xy;
+        st.z[s] = mz;
+        if (!RF) st.acc[s] = acc;
+    }
+}
+
+// sig[(j) + c*ldsig] = sum over parts of partial[(part*nsamples + j)*nc + c], in part order.
+template <typename T>
+__global__ void partial_finalize_kernel(const cplx<T> *partial, int64_t nparts, int64_t nsamples, int32_t nc,
+                                        cplx<T> *sig, int64_t ldsig) {
+    const int64_t total = nsamples * nc;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = i / nc;
+        const int32_t c = (int32_t)(i % nc);
+        cplx<T> acc{T(0), T(0)};
+        for (int64_t k = 0; k < nparts; ++k) {
+            cplx<T> v = partial[(k * nsamples + j) * nc + c];
+            acc.re = acc.re + v.re;
+            acc.im = acc.im + v.im;
+        }
+        sig[j + (int64_t)c * ldsig] = acc;
+    }
+}
+
+// Standalone reduction: one CTA per (spin tile, sample chunk); partial rows
+// per spin tile, summed afterwards by partial_finalize_kernel.
+template <typename T>
+__global__ void __launch_bounds__(PLAIN_THREADS)
+    coil_reduce_kernel(int64_t ns, int64_t nadc, int32_t nc, const cplx<T> *states, int64_t ldstates,
+                       const cplx<T> *csm, int64_t ldcsm, cplx<T> *partial) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<T> *X = reinterpret_cast<cplx<T> *>(smem_raw);
+    cplx<T> *P = X + PLAIN_STAGE * PLAIN_THREADS;
+    cplx<T> *csm_s = P + PLAIN_STAGE * PLAIN_THREADS;
+    const int64_t spin0 = (int64_t)blockIdx.x * PLAIN_THREADS;
+    const int nvalid = (int)imin64(PLAIN_THREADS, ns - spin0);
+    const int64_t j0 = (int64_t)blockIdx.y * PLAIN_STAGE;
+    const int na = (int)imin64(PLAIN_STAGE, nadc - j0);
+    const bool csm_in_smem = sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS <= 96 * 1024;
+    // Transposed sensitivities (rows s, coil-fastest) in shared memory, or a
+    // column-major global fallback via a row pointer with stride ldcsm.
+    const int s_local = threadIdx.x;
+    for (int a = 0; a < na; ++a) {
+        cplx<T> v{T(0), T(0)};
+        if (s_local < nvalid) v = states[(spin0 + s_local) + (j0 + a) * ldstates];
+        X[a * PLAIN_THREADS + s_local] = v;
+    }
+    if (csm_in_smem) {
+        for (int64_t i = threadIdx.x; i < (int64_t)nvalid * nc; i += PLAIN_THREADS) {
+            const int64_t sl = i / nc;
+            const int32_t c = (int32_t)(i % nc);
+            csm_s[i] = csm[(spin0 + sl) + c * ldcsm];
+        }
+    }
+    __syncthreads();
+    cplx<T> *out = partial + ((int64_t)blockIdx.x * nadc + j0) * nc;
+    if (csm_in_smem) {
+        reduce_stage(X, P, na, csm_s, nc, nvalid, nc, out);
+    } else {
+        // Large coil counts: contract straight from the column-major array.
+        const int t = threadIdx.x;
+        for (int64_t o = t; o < (int64_t)na * nc; o += PLAIN_THREADS) {
+            const int a = (int)(o / nc);
+            const int32_t c = (int32_t)(o % nc);
+            cplx<T> acc{T(0), T(0)};
+            for (int sl = 0; sl < nvalid; ++sl) {
+                cplx<T> v = cmul(X[a * PLAIN_THREADS + sl], csm[(spin0 + sl) + c * ldcsm]);
+                acc.re = acc.re + v.re;
+                acc.im = acc.im + v.im;
+            }
+            out[(int64_t)a * nc + c] = acc;
+        }
+    }
+}
+
+template <typename T>
+cudaError_t launch_segment(bool rf, const PhantomDev<T> &p, const SeqDev<T> &q, StateDev<T> &st,
+                           const SegmentArgs<T> &a, int grid, cudaStream_t stream) {
+    const size_t smem = segment_smem_bytes<T>(p.nc);
+    cudaError_t e;
+    if (rf) {
+        e = cudaFuncSetAttribute(segment_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        segment_kernel<T, true><<<grid, PLAIN_THREADS, smem, stream>>>(p, q, st, a);
+    } else {
+        e = cudaFuncSetAttribute(segment_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess) return e;
+        segment_kernel<T, false><<<grid, PLAIN_THREADS, smem, stream>>>(p, q, st, a);
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_partial_finalize(const cplx<T> *partial, int64_t nparts, int64_t nsamples, int32_t nc,
+                                    cplx<T> *sig, int64_t ldsig, cudaStream_t stream) {
+    const int64_t total = nsamples * nc;
+    if (total == 0) return cudaSuccess;
+    const int threads = 256;
+    const int64_t blocks = std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
+    partial_finalize_kernel<T><<<(int)blocks, threads, 0, stream>>>(partial, nparts, nsamples, nc, sig, ldsig);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_coil_reduce(int64_t ns, int64_t nadc, int32_t nc, const cplx<T> *states, int64_t ldstates,
+                               const cplx<T> *csm, int64_t ldcsm, cplx<T> *partial, cudaStream_t stream) {
+    const int64_t tiles = (ns + PLAIN_THREADS - 1) / PLAIN_THREADS;
+    const int64_t chunks = (nadc + PLAIN_STAGE - 1) / PLAIN_STAGE;
+    if (tiles == 0 || chunks == 0) return cudaSuccess;
+    size_t smem = 2 * sizeof(cplx<T>) * PLAIN_STAGE * PLAIN_THREADS;
+    if (sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS <= 96 * 1024) smem += sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS;
+    cudaError_t e = cudaFuncSetAttribute(coil_reduce_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((unsigned)tiles, (unsigned)chunks);
+    coil_reduce_kernel<T><<<grid, PLAIN_THREADS, smem, stream>>>(ns, nadc, nc, states, ldstates, csm, ldcsm, partial);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_segment<double>(bool, const PhantomDev<double> &, const SeqDev<double> &,
+                                            StateDev<double> &, const SegmentArgs<double> &, int, cudaStream_t);
+template cudaError_t launch_segment<float>(bool, const PhantomDev<float> &, const SeqDev<float> &,
+                                           StateDev<float> &, const SegmentArgs<float> &, int, cudaStream_t);
+template cudaError_t launch_partial_finalize<double>(const cplx<double> *, int64_t, int64_t, int32_t,
+                                                     cplx<double> *, int64_t, cudaStream_t);
+template cudaError_t launch_partial_finalize<float>(const cplx<float> *, int64_t, int64_t, int32_t, cplx<float> *,
+                                                    int64_t, cudaStream_t);
+template cudaError_t launch_coil_reduce<double>(int64_t, int64_t, int32_t, const cplx<double> *, int64_t,
+                                                const cplx<double> *, int64_t, cplx<double> *, cudaStream_t);
+template cudaError_t launch_coil_reduce<float>(int64_t, int64_t, int32_t, const cplx<float> *, int64_t,
+                                               const cplx<float> *, int64_t, cplx<float> *, cudaStream_t);
+template size_t segment_smem_bytes<double>(int32_t);
+template size_t segment_smem_bytes<float>(int32_t);
+
+}  // namespace homs

@@ -1,0 +1,809 @@
+// Split-precision fused precession + coil contraction on tcgen05 (sm_100a).
+//
+// Math (one precession segment = a run of consecutive precession blocks):
+//   phase in turns   theta(s,j) = theta0(s) + sum_k b_k(s) * kappa_k(j)
+//     b_k      : the 16 solid-harmonic basis values of spin s (FP64, resident),
+//                plus b_16 = dw/(2 pi)
+//     kappa_k  : -gamma * trapezoid integral of field column k from the segment
+//                start to ADC sample j (FP64 prefix table), kappa_16 = -t
+//   M(s,j)   = |m0| 2^(t_j * r2(s)) * cis(2 pi theta)   (r2 = -log2(e)/T2)
+//   S(j,c)   = sum_s M(s,j) csm(s,c)                      (no conjugation)
+// This is the reference's phi = -2 pi gamma cumtrapz(dt, Bz) and
+// Mxy = M0 exp(i phi - t/T2) (src/simulation/Bloch/BlochHighOrderSimulatitonMethod.jl:76-92)
+// with the cumulative integral factored into per-spin x per-sample terms.
+//
+// Precision: theta is accumulated in FP64 (17 DFMA); one FP64 add of 1.5*2^20
+// leaves frac(theta) as a 32-bit fixed-point turn count in the low mantissa
+// word (the mod-2pi range reduction, exact to 2^-32 turn).  Quadrant select
+// plus a float32 polynomial (coefficients fitted by fit_sincos.py) give
+// cos/sin; the decay is one ex2.approx.  M is split into TF32 hi + lo and the
+// contraction runs as three TF32 MMAs (hi*hi + hi*lo + lo*hi) with FP32
+// accumulation in TMEM; split-K partials are summed in FP64.
+//
+// Kernel organisation (one CTA per SM, persistent, stream-K over
+// (time tile of 128 samples) x (chunk of 32 spins) units):
+//   warps 0-7  producers: thread <-> sample row of the 128-row tile; compute
+//              M for 16 spins per chunk, write TF32 hi/lo to TMEM (A operand)
+//              with tcgen05.st; epilogue reads the accumulator with tcgen05.ld.
+//   warp 8     MMA issuer: tcgen05.mma.kind::tf32 with A in TMEM, B (the
+//              sensitivities, pre-split) in shared memory; tcgen05.commit
+//              releases shared-memory stages, A stages and accumulators.
+//   warp 9     loader: cp.async.bulk of each chunk's B operand and spin table.
+// Every wait is bounded: on time-out the kernel records the place in a device
+// error word and returns without hanging the GPU.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "homs_common.cuh"
+#include "homs_split.cuh"
+
+namespace homs {
+
+namespace split {
+
+constexpr int TM = 128;          // samples per tile (UMMA M)
+constexpr int KC = 32;           // spins per chunk
+constexpr int KSTEPS = 8;        // (2*KC real K values) / 8 per tf32 MMA
+constexpr int MAX_STAGE = 4;     // shared-memory stages (fewer for wide N)
+constexpr int SPIN_ROWS = 20;    // k-major spin table rows per chunk
+constexpr int SPIN_BYTES = SPIN_ROWS * KC * 8;
+constexpr int PREFIX_STRIDE = 20;  // doubles per prefix row: kappa[0..16], t, pad
+constexpr int NPROD_WARPS = 8;
+constexpr int MMA_WARP = 8;
+constexpr int LOAD_WARP = 9;
+constexpr int THREADS = 320;
+constexpr uint32_t TMEM_COLS = 512;
+constexpr uint32_t A_COL0 = 256;
+constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
+
+// Sine/cosine coefficients on [-pi/4, pi/4] (see fit_sincos.py).
+constexpr float S1 = -0.16666650772094727f, S2 = 0.00833197869360447f, S3 = -0.00019495606829877943f;
+constexpr float C1 = -0.5f, C2 = 0.04166662320494652f, C3 = -0.0013886763481423259f, C4 = 2.439039235468954e-05f;
+
+__host__ __device__ inline int b_bytes(int n_mma) { return 2 * KSTEPS * n_mma * 32; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (clock64() - t0 > WAIT_BUDGET) return false;
+    }
+    return true;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+        "r"(a), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
+}
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+#define HOMS_ST_X32(taddr, v)                                                                                     \
+    asm volatile(                                                                                                 \
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, " \
+        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(  \
+            taddr),                                                                                               \
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),        \
+        "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]),           \
+        "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),          \
+        "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])                       \
+        : "memory")
+
+__device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, float *v) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr)
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// No-swizzle K-major shared-memory matrix descriptor: core matrices of
+// 8 rows x 16 bytes, K-direction core stride (LBO) 128 B, row-group stride
+// (SBO) 256 B, descriptor version 1.
+__device__ __forceinline__ uint64_t bdesc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) |
+           (1ull << 46);
+}
+
+struct KernelArgs {
+    const double *prefix;      // [rows][PREFIX_STRIDE]
+    const uint8_t *b_operand;  // [nchunks][b_bytes]
+    const double *spin_table;  // [nchunks][SPIN_ROWS][KC]
+    float *partial;            // [tiles][maxp][TM][n_mma]
+    unsigned int *err;
+    int64_t nsamples;
+    int64_t n_chunks;
+    int64_t tiles;
+    int maxp;
+    int n_mma;
+    int nstage;
+};
+
+__device__ __forceinline__ int64_t cta_of(int64_t L, int64_t G, int64_t W) { return ((L + 1) * G - 1) / W; }
+
+// M(s,j) for one spin given the FP64 turn count; returns (re, im).
+__device__ __forceinline__ void magnetisation(double th, float tj, float r2, float l2m0, float &mre, float &mim) {
+    const double g = th + 1572864.0;  // 1.5 * 2^20: frac(th) * 2^32 lands in the low word
+    const uint32_t u = (uint32_t)__double2loint(g);
+    const uint32_t v = u + 0x20000000u;
+    const uint32_t q = v >> 30;
+    const int32_t rr = (int32_t)(v & 0x3FFFFFFFu) - 0x20000000;
+    const float x = (float)rr * 1.4629180792671596e-09f;  // 2 pi / 2^32
+    const float x2 = x * x;
+    const float sp = fmaf(x * x2, fmaf(x2, fmaf(x2, S3, S2), S1), x);
+    const float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, C4, C3), C2), C1), 1.0f);
+    float c, s;
+    if (q == 0) {
+        c = cp;
+        s = sp;
+    } else if (q == 1) {
+        c = -sp;
+        s = cp;
+    } else if (q == 2) {
+        c = -cp;
+        s = -sp;
+    } else {
+        c = sp;
+        s = -cp;
+    }
+    const float a = ex2_approx(fmaf(tj, r2, l2m0));
+    mre = a * c;
+    mim = a * s;
+}
+
+__global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int n_mma = args.n_mma;
+    const int NSTAGE = args.nstage;
+    const int BB = b_bytes(n_mma);
+    uint8_t *sB = smem;                                   // NSTAGE * BB
+    double *sSpin = reinterpret_cast<double *>(sB + NSTAGE * BB);  // NSTAGE * SPIN_BYTES
+    uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);
+    uint64_t *full = bars;                    // [NSTAGE] loader -> consumers (tx)
+    uint64_t *empty = bars + MAX_STAGE;       // [NSTAGE] MMA commit -> loader
+    uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] producers -> MMA
+    uint64_t *a_empty = a_full + 2;        // [2] MMA commit -> producers
+    uint64_t *d_full = a_empty + 2;        // [2] MMA commit -> epilogue
+    uint64_t *d_empty = d_full + 2;        // [2] epilogue -> MMA
+    uint64_t *done = d_empty + 2;          // [1] final MMA commit
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NSTAGE; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&a_full[i], NPROD_WARPS * 32);
+            mbar_init(&a_empty[i], 1);
+            mbar_init(&d_full[i], 1);
+            mbar_init(&d_empty[i], NPROD_WARPS * 32);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == MMA_WARP) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int64_t G = gridDim.x;
+    const int64_t W = args.tiles * args.n_chunks;
+    const int64_t u0 = W * (int64_t)blockIdx.x / G, u1 = W * ((int64_t)blockIdx.x + 1) / G;
+    bool dead = false;
+
+    if (warp == LOAD_WARP) {
+        if (lane == 0) {
+            int64_t g = 0;
+            for (int64_t u = u0; u < u1 && !dead; ++u, ++g) {
+                const int64_t chunk = u % args.n_chunks;
+                const int stage = (int)(g % NSTAGE);
+                if (!mbar_wait(&empty[stage], (uint32_t)(((g / NSTAGE) + 1) & 1))) {
+                    atomicOr(args.err, 1u);
+                    dead = true;
+                    break;
+                }
+                mbar_expect_tx(&full[stage], (uint32_t)(BB + SPIN_BYTES));
+                bulk_g2s(sB + (size_t)stage * BB, args.b_operand + (size_t)chunk * BB, (uint32_t)BB, &full[stage]);
+                bulk_g2s(reinterpret_cast<uint8_t *>(sSpin) + (size_t)stage * SPIN_BYTES,
+                         reinterpret_cast<const uint8_t *>(args.spin_table) + (size_t)chunk * SPIN_BYTES,
+                         (uint32_t)SPIN_BYTES, &full[stage]);
+            }
+        }
+        __syncwarp();
+    } else if (warp == MMA_WARP) {
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n_mma >> 3) << 17) |
+                                   ((uint32_t)(TM >> 4) << 24);
+            int64_t g = 0, piece = 0;
+            int64_t u = u0;
+            while (u < u1 && !dead) {
+                const int64_t k0 = u % args.n_chunks;
+                const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
+                const int dbuf = (int)(piece & 1);
+                if (!mbar_wait(&d_empty[dbuf], (uint32_t)(((piece >> 1) + 1) & 1))) {
+                    atomicOr(args.err, 2u);
+                    dead = true;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t dcol = tmem + (uint32_t)(dbuf * n_mma);
+                for (int64_t k = k0; k < k1; ++k, ++g) {
+                    const int stage = (int)(g % NSTAGE);
+                    const int as = (int)(g & 1);
+                    if (!mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1)) ||
+                        !mbar_wait(&a_full[as], (uint32_t)((g >> 1) & 1))) {
+                        atomicOr(args.err, 4u);
+                        dead = true;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sbase = smem_u32(sB + (size_t)stage * BB);
+                    const uint32_t a_hi = tmem + A_COL0 + (uint32_t)as * 128u;
+                    const uint32_t a_lo = a_hi + 64u;
+#pragma unroll
+                    for (int ks = 0; ks < KSTEPS; ++ks) {
+                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * n_mma * 32));
+                        const uint64_t blo = bdesc(sbase + (uint32_t)((KSTEPS + ks) * n_mma * 32));
+                        const uint32_t first = (k == k0 && ks == 0) ? 0u : 1u;
+                        tc_mma_tf32(dcol, a_hi + ks * 8, bhi, idesc, first);
+                        tc_mma_tf32(dcol, a_hi + ks * 8, blo, idesc, 1u);
+                        tc_mma_tf32(dcol, a_lo + ks * 8, bhi, idesc, 1u);
+                    }
+                    tc_commit(&empty[stage]);
+                    tc_commit(&a_empty[as]);
+                }
+                if (dead) break;
+                tc_commit(&d_full[dbuf]);
+                u += k1 - k0;
+                ++piece;
+            }
+            // Drain: wait for every issued MMA before TMEM is released.
+            tc_commit(done);
+            if (!mbar_wait(done, 0)) atomicOr(args.err, 8u);
+        }
+        __syncwarp();
+    } else {
+        // Producers / epilogue: thread <-> tile row.
+        const int quarter = warp & 3, half = warp >> 2;
+        const int row = quarter * 32 + lane;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        int64_t g = 0, piece = 0;
+        int64_t u = u0;
+        while (u < u1 && !dead) {
+            const int64_t tile = u / args.n_chunks;
+            const int64_t k0 = u % args.n_chunks;
+            const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
+            const int slot = (int)(blockIdx.x - cta_of(tile * args.n_chunks, G, W));
+            int64_t j = tile * TM + row;
+            if (j >= args.nsamples) j = args.nsamples - 1;
+            double kap[17];
+            const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
+#pragma unroll
+            for (int k = 0; k < 17; ++k) kap[k] = pr[k];
+            const float tj = (float)pr[17];
+            for (int64_t k = k0; k < k1; ++k, ++g) {
+                const int stage = (int)(g % NSTAGE);
+                const int as = (int)(g & 1);
+                bool ok = mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1));
+                ok = ok && mbar_wait(&a_empty[as], (uint32_t)(((g >> 1) + 1) & 1));
+                __syncwarp();
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(args.err, 16u);
+                    dead = true;
+                    break;
+                }
+                tc_fence_after();
+                const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
+                uint32_t hi[32], lo[32];
+#pragma unroll
+                for (int g4 = 0; g4 < 4; ++g4) {
+                    const int s0 = half * 16 + g4 * 4;
+                    double th[4];
+                    {
+                        const double2 t01 = *reinterpret_cast<const double2 *>(tab + 17 * KC + s0);
+                        const double2 t23 = *reinterpret_cast<const double2 *>(tab + 17 * KC + s0 + 2);
+                        th[0] = t01.x;
+                        th[1] = t01.y;
+                        th[2] = t23.x;
+                        th[3] = t23.y;
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < 17; ++kk) {
+                        const double2 b01 = *reinterpret_cast<const double2 *>(tab + kk * KC + s0);
+                        const double2 b23 = *reinterpret_cast<const double2 *>(tab + kk * KC + s0 + 2);
+                        th[0] = fma(b01.x, kap[kk], th[0]);
+                        th[1] = fma(b01.y, kap[kk], th[1]);
+                        th[2] = fma(b23.x, kap[kk], th[2]);
+                        th[3] = fma(b23.y, kap[kk], th[3]);
+                    }
+                    const float4 rl01 = *reinterpret_cast<const float4 *>(tab + 18 * KC + s0);
+                    const float4 rl23 = *reinterpret_cast<const float4 *>(tab + 18 * KC + s0 + 2);
+                    const float r2v[4] = {rl01.x, rl01.z, rl23.x, rl23.z};
+                    const float l2v[4] = {rl01.y, rl01.w, rl23.y, rl23.w};
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        float mre, mim;
+                        magnetisation(th[i], tj, r2v[i], l2v[i], mre, mim);
+                        const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
+                        const int e = 2 * (g4 * 4 + i);
+                        hi[e] = hr;
+                        hi[e + 1] = hm;
+                        lo[e] = tf32_rna(mre - __uint_as_float(hr));
+                        lo[e + 1] = tf32_rna(mim - __uint_as_float(hm));
+                    }
+                }
+                const uint32_t a_hi = tmem + lane_base + A_COL0 + (uint32_t)as * 128u + (uint32_t)half * 32u;
+                HOMS_ST_X32(a_hi, hi);
+                HOMS_ST_X32(a_hi + 64u, lo);
+                tmem_wait_st();
+                tc_fence_before();
+                mbar_arrive(&a_full[as]);
+            }
+            if (dead) break;
+            // Epilogue for this piece.
+            const int dbuf = (int)(piece & 1);
+            const bool ok = mbar_wait(&d_full[dbuf], (uint32_t)((piece >> 1) & 1));
+            __syncwarp();
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) atomicOr(args.err, 32u);
+                dead = true;
+                break;
+            }
+            tc_fence_after();
+            const int ncol = n_mma / 2;
+            float *dst = args.partial + (((size_t)tile * args.maxp + slot) * TM + row) * (size_t)n_mma + half * ncol;
+            for (int cc = 0; cc < ncol; cc += 8) {
+                float v[8];
+                tmem_ld_x8(tmem + lane_base + (uint32_t)(dbuf * n_mma + half * ncol + cc), v);
+                tmem_wait_ld();
+                *reinterpret_cast<float4 *>(dst + cc) = make_float4(v[0], v[1], v[2], v[3]);
+                *reinterpret_cast<float4 *>(dst + cc + 4) = make_float4(v[4], v[5], v[6], v[7]);
+            }
+            tc_fence_before();
+            mbar_arrive(&d_empty[dbuf]);
+            u += k1 - k0;
+            ++piece;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == MMA_WARP) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// Sum split-K partials of each (sample, column) in piece order (FP64) and
+// write complex samples: column n < nc is Re S(j, n), nc <= n < 2nc is Im.
+template <typename T>
+__global__ void split_finalize_kernel(const float *partial, int64_t nsamples, int32_t nc, int n_mma, int maxp,
+                                      int64_t n_chunks, int64_t G, int64_t W, cplx<T> *sig, int64_t ldsig) {
+    const int64_t total = nsamples * nc;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = i % nsamples;
+        const int32_t c = (int32_t)(i / nsamples);
+        const int64_t tile = j / TM;
+        const int row = (int)(j % TM);
+        const int64_t first = cta_of(tile * n_chunks, G, W);
+        const int64_t last = cta_of((tile + 1) * n_chunks - 1, G, W);
+        const int np = (int)(last - first + 1);
+        double re = 0.0, im = 0.0;
+        for (int p = 0; p < np; ++p) {
+            const float *src = partial + (((size_t)tile * maxp + p) * TM + row) * (size_t)n_mma;
+            re += (double)src[c];
+            im += (double)src[nc + c];
+        }
+        sig[j + (int64_t)c * ldsig] = cplx<T>{T(re), T(im)};
+    }
+}
+
+// Per-spin 16-term basis (FP64), CPU expression order.
+__global__ void basis_kernel(const double *x, const double *y, const double *z, int64_t ns, double *basis) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns; s += (int64_t)gridDim.x * blockDim.x) {
+        const double X = x[s], Y = y[s], Z = z[s];
+        const double x2 = X * X, y2 = Y * Y, z2 = Z * Z;
+        const double r2 = (x2 + y2) + z2;
+        double *b = basis + s * 16;
+        b[0] = 1.0;
+        b[1] = X;
+        b[2] = Y;
+        b[3] = Z;
+        b[4] = X * Y;
+        b[5] = Z * Y;
+        b[6] = 3.0 * z2 - r2;
+        b[7] = X * Z;
+        b[8] = x2 - y2;
+        b[9] = (3.0 * Y) * x2 - (y2 * Y);
+        b[10] = (X * Z) * Y;
+        b[11] = (5.0 * z2 - r2) * Y;
+        b[12] = 5.0 * (z2 * Z) - (3.0 * Z) * r2;
+        b[13] = (5.0 * z2 - r2) * X;
+        b[14] = x2 * Z - y2 * Z;
+        b[15] = (x2 * X) - (3.0 * X) * y2;
+    }
+}
+
+// Sensitivities -> TF32 hi/lo B operand in the no-swizzle K-major layout.
+// B[n][2s] = (n < nc ? Re c(s,n) : Im c(s,n-nc)), B[n][2s+1] = (n < nc ? -Im : Re).
+__global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_mma, int64_t nchunks,
+                                 float *out) {
+    const int64_t per_chunk = (int64_t)KSTEPS * n_mma * 8;
+    const int64_t total = nchunks * per_chunk;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t chunk = i / per_chunk;
+        int64_t r = i % per_chunk;
+        const int ks = (int)(r / (n_mma * 8));
+        r %= (n_mma * 8);
+        const int n = (int)(r / 8), kk = (int)(r % 8);
+        const int kglob = ks * 8 + kk;
+        const int64_t s = chunk * KC + kglob / 2;
+        const bool imrow = (kglob & 1) != 0;
+        double v = 0.0;
+        if (s < ns && n < 2 * nc) {
+            const cplx<double> c = csm_rows[s * nc + (n < nc ? n : n - nc)];
+            if (n < nc) v = imrow ? -c.im : c.re;
+            else v = imrow ? c.re : c.im;
+        }
+        const float vf = (float)v;
+        uint32_t hb, lb;
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(vf));
+        // lo carries what the FP32 hi misses of the FP64 value.
+        const float lf = (float)(v - (double)__uint_as_float(hb));
+        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lb) : "f"(lf));
+        const size_t off = (size_t)(n / 8) * 256 + (size_t)(kk / 4) * 128 + (size_t)(n % 8) * 16 + (size_t)(kk % 4) * 4;
+        uint8_t *base = reinterpret_cast<uint8_t *>(out) + (size_t)chunk * b_bytes(n_mma);
+        *reinterpret_cast<uint32_t *>(base + (size_t)ks * n_mma * 32 + off) = hb;
+        *reinterpret_cast<uint32_t *>(base + (size_t)(KSTEPS + ks) * n_mma * 32 + off) = lb;
+    }
+}
+
+// Spin table of a segment, from the state at its start.
+// rows 0..15: basis, 16: dw/(2 pi) (0 if dw is off in precession),
+// 17: theta0 = arg(m0)/(2 pi), 18: packed float2 (-log2(e)/T2, log2|m0|).
+// Also checks the phase range: |theta| must stay below 2^18 turns for the
+// fixed-point reduction (error bit 64 otherwise).
+__global__ void spin_table_kernel(const double *basis, const double *dw, const double *T2, const cplx<double> *xy,
+                                  int64_t ns, int64_t nchunks, uint32_t method, const double *colmax,
+                                  unsigned int *err, double *table) {
+    const int64_t total = nchunks * KC;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        double *t = table + (s / KC) * (SPIN_ROWS * KC) + (s % KC);
+        if (s < ns) {
+            for (int k = 0; k < 16; ++k) t[k * KC] = basis[s * 16 + k];
+            t[16 * KC] = (method & HOMS_DW_PRECESSION) ? dw[s] / (2.0 * 3.141592653589793) : 0.0;
+            const cplx<double> m0 = xy[s];
+            const double mag = hypot(m0.re, m0.im);
+            t[17 * KC] = atan2(m0.im, m0.re) / (2.0 * 3.141592653589793);
+            double bound = fabs(t[17 * KC]);
+            for (int k = 0; k < 17; ++k) bound += fabs(t[k * KC]) * colmax[k];
+            if (!(bound < 262144.0)) atomicOr(err, 64u);
+            float2 rl;
+            rl.x = (float)(-1.4426950408889634 / T2[s]);
+            rl.y = mag > 0.0 ? (float)log2(mag) : -INFINITY;
+            *reinterpret_cast<float2 *>(&t[18 * KC]) = rl;
+        } else {
+            for (int k = 0; k < 18; ++k) t[k * KC] = 0.0;
+            *reinterpret_cast<float2 *>(&t[18 * KC]) = make_float2(0.0f, -INFINITY);
+        }
+        t[19 * KC] = 0.0;
+    }
+}
+
+// Prefix table of one segment: for each column k (0..15 field terms, 16 the
+// dw column, 17 time) a deterministic chunked scan of the trapezoid sums
+// (f(n)+f(n+1)) dt(n) over the segment, written at every ADC node (row =
+// sample index) and at the end node (row nsamples).
+__global__ void prefix_kernel(const double *dt, const double *const *src, const uint8_t *adc, const int32_t *rank,
+                              int64_t n_lo, int64_t n_hi, int64_t nsamples, double gamma, uint32_t method,
+                              double *prefix) {
+    __shared__ double part[256];
+    const int col = blockIdx.x;
+    const double *f = src[col];  // nullptr: zero column; (double*)1: constant one
+    const bool one = f == reinterpret_cast<const double *>(1);
+    const bool zero = f == nullptr;
+    const double scale = col < 16 ? -gamma * 0.5 : (col == 16 ? -0.5 : 0.5);
+    const int64_t nint = n_hi - n_lo;
+    const int64_t per = (nint + blockDim.x - 1) / blockDim.x;
+    const int64_t i0 = min(nint, per * threadIdx.x), i1 = min(nint, i0 + per);
+    double local = 0.0;
+    for (int64_t i = i0; i < i1; ++i) {
+        const int64_t n = n_lo + i;
+        const double term = zero ? 0.0 : (one ? 2.0 : (f[n] + f[n + 1])) * dt[n];
+        local += term;
+    }
+    part[threadIdx.x] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double run = 0.0;
+        for (int i = 0; i < (int)blockDim.x; ++i) {
+            const double v = part[i];
+            part[i] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    double cum = part[threadIdx.x];
+    double peak = 0.0;
+    for (int64_t i = i0; i < i1; ++i) {
+        const int64_t n = n_lo + i;
+        const double term = zero ? 0.0 : (one ? 2.0 : (f[n] + f[n + 1])) * dt[n];
+        cum += term;
+        peak = fmax(peak, fabs(scale * cum));
+        if (adc[n + 1]) prefix[(size_t)rank[n + 1] * PREFIX_STRIDE + col] = scale * cum;
+        if (n + 1 == n_hi) prefix[(size_t)nsamples * PREFIX_STRIDE + col] = scale * cum;
+    }
+    if (nint == 0 && threadIdx.x == 0) prefix[(size_t)nsamples * PREFIX_STRIDE + col] = 0.0;
+    // Largest |kappa| of the column (row nsamples+1) for the phase-range check.
+    __syncthreads();
+    part[threadIdx.x] = peak;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double mx = 0.0;
+        for (int i = 0; i < (int)blockDim.x; ++i) mx = fmax(mx, part[i]);
+        prefix[(size_t)(nsamples + 1) * PREFIX_STRIDE + col] = mx;
+    }
+}
+
+// Final state of a segment in FP64: Mxy = |m0| e^{-T/T2} cis(2 pi theta_end),
+// Mz = Mz e^{-T/T1} + rho (1 - e^{-T/T1}).
+__global__ void state_update_kernel(const double *table, const double *endrow, const double *T1, const double *T2,
+                                    const double *rho, int64_t ns, cplx<double> *xy, double *mz) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns; s += (int64_t)gridDim.x * blockDim.x) {
+        const double *t = table + (s / KC) * (SPIN_ROWS * KC) + (s % KC);
+        double th = t[17 * KC];
+        for (int k = 0; k < 17; ++k) th = fma(t[k * KC], endrow[k], th);
+        const double T = endrow[17];
+        const cplx<double> m0 = xy[s];
+        const double mag = hypot(m0.re, m0.im);
+        const double f = th - rint(th);
+        double sn, cs;
+        sincospi(2.0 * f, &sn, &cs);
+        const double e2 = exp(-T / T2[s]);
+        xy[s] = cplx<double>{mag * e2 * cs, mag * e2 * sn};
+        const double e1 = exp(-T / T1[s]);
+        mz[s] = mz[s] * e1 + rho[s] * (1.0 - e1);
+    }
+}
+
+inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
+
+}  // namespace split
+
+using namespace split;
+
+SplitResident::~SplitResident() {
+    for (void *p : {basis, b_operand, spin_table, prefix, tvec, partial, tile_map, err})
+        if (p) cudaFree(p);
+}
+
+static cudaError_t grow(void *&p, size_t &have, size_t need) {
+    if (need <= have && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    have = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(need, 256));
+    if (e == cudaSuccess) have = std::max<size_t>(need, 256);
+    return e;
+}
+
+cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *x, const void *y, const void *z,
+                          const void *dw, const void *csm_rows, bool is_f64, cudaStream_t stream, std::string *err) {
+    (void)dw;
+    if (!is_f64) {
+        *err =
+            "split mode takes FP64 phantom and sequence arrays: FP32 positions alone carry phase errors above the "
+            "split path's error budget";
+        return cudaSuccess;
+    }
+    const int n_mma = std::max(16, ((2 * nc + 15) / 16) * 16);
+    if (n_mma > 128) {
+        *err = "split mode supports at most 64 coils per run";
+        return cudaSuccess;
+    }
+    r.ns = ns;
+    r.nc = nc;
+    r.n_mma = n_mma;
+    const int64_t nchunks = (ns + KC - 1) / KC;
+    r.ns_pad = nchunks * KC;
+    cudaError_t e;
+    if ((e = grow(r.basis, r.basis_bytes, sizeof(double) * 16 * (size_t)ns)) != cudaSuccess) return e;
+    if ((e = grow(r.b_operand, r.b_bytes, (size_t)b_bytes(n_mma) * (size_t)nchunks)) != cudaSuccess) return e;
+    if (!r.err) {
+        if ((e = cudaMalloc(&r.err, sizeof(unsigned int))) != cudaSuccess) return e;
+    }
+    basis_kernel<<<grid_for(ns), 256, 0, stream>>>((const double *)x, (const double *)y, (const double *)z, ns,
+                                                   (double *)r.basis);
+    const int64_t total = nchunks * KSTEPS * n_mma * 8;
+    b_operand_kernel<<<grid_for(total), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_mma, nchunks,
+                                                          (float *)r.b_operand);
+    return cudaGetLastError();
+}
+
+static int kernel_stages(int n_mma) {
+    const size_t budget = 220 * 1024;
+    const size_t per = (size_t)b_bytes(n_mma) + SPIN_BYTES;
+    return (int)std::max<size_t>(2, std::min<size_t>(MAX_STAGE, (budget - 2048) / per));
+}
+
+static size_t kernel_smem(int n_mma) {
+    return 1024 + (size_t)kernel_stages(n_mma) * (b_bytes(n_mma) + SPIN_BYTES) + 32 * 8 + 64;
+}
+
+// One precession segment.
+static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi,
+                                 int64_t sample0, int64_t nsamples, cudaStream_t stream, std::string *err) {
+    cudaError_t e;
+    const int64_t nchunks = r.ns_pad / KC;
+    const int64_t tiles = (nsamples + TM - 1) / TM;
+    // ADC rank per node of the segment (host), uploaded with the column sources.
+    std::vector<int32_t> rank((size_t)a.nt, 0);
+    int64_t c = 0;
+    for (int64_t n = n_lo + 1; n <= n_hi; ++n)
+        if (a.adc_host[n]) rank[(size_t)n] = (int32_t)c++;
+    if (c != nsamples) {
+        *err = "internal: segment sample count mismatch";
+        return cudaSuccess;
+    }
+    const size_t rank_bytes = sizeof(int32_t) * (size_t)a.nt;
+    const size_t src_bytes = sizeof(void *) * 18;
+    const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2);
+    if ((e = grow(r.prefix, r.prefix_bytes, prefix_rows * PREFIX_STRIDE * sizeof(double))) != cudaSuccess) return e;
+    if ((e = grow(r.tvec, r.tvec_bytes, rank_bytes + src_bytes)) != cudaSuccess) return e;
+    if ((e = grow(r.spin_table, r.spin_bytes, (size_t)nchunks * SPIN_BYTES)) != cudaSuccess) return e;
+    const double *src[18];
+    const uint32_t m = a.method;
+    src[0] = (m & HOMS_HO0) ? (const double *)a.h[0] : nullptr;
+    for (int k = 1; k <= 3; ++k)
+        src[k] = (m & HOMS_HO1) ? (const double *)a.h[k] : (const double *)(k == 1 ? a.gx : k == 2 ? a.gy : a.gz);
+    for (int k = 4; k <= 8; ++k) src[k] = (m & HOMS_HO2) ? (const double *)a.h[k] : nullptr;
+    for (int k = 9; k <= 15; ++k) src[k] = (m & HOMS_HO3) ? (const double *)a.h[k] : nullptr;
+    src[16] = (m & HOMS_DW_PRECESSION) ? reinterpret_cast<const double *>(1) : nullptr;
+    src[17] = reinterpret_cast<const double *>(1);
+    uint8_t *tv = (uint8_t *)r.tvec;
+    if ((e = cudaMemcpyAsync(tv, rank.data(), rank_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(tv + rank_bytes, src, src_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
+    // The host arrays above are stack/vector memory: finish the copies before they go away.
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(tv + rank_bytes),
+                                          (const uint8_t *)a.adc, reinterpret_cast<const int32_t *>(tv), n_lo, n_hi,
+                                          nsamples, a.gamma, m, (double *)r.prefix);
+    spin_table_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>(
+        (const double *)r.basis, (const double *)a.dw, (const double *)a.T2, (const cplx<double> *)a.xy, r.ns, nchunks,
+        m, (const double *)r.prefix + (size_t)(nsamples + 1) * PREFIX_STRIDE, (unsigned int *)r.err,
+        (double *)r.spin_table);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (nsamples > 0) {
+        int dev = 0, nsm = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t W = tiles * nchunks;
+        const int64_t G = std::min<int64_t>(nsm, W);
+        int maxp = 1;
+        for (int64_t t = 0; t < tiles; ++t) {
+            const int64_t f = ((t * nchunks + 1) * G - 1) / W;
+            const int64_t l = (((t + 1) * nchunks) * G - 1) / W;
+            maxp = std::max<int>(maxp, (int)(l - f + 1));
+        }
+        const size_t pbytes = sizeof(float) * (size_t)tiles * maxp * TM * r.n_mma;
+        if ((e = grow(r.partial, r.partial_bytes, pbytes)) != cudaSuccess) return e;
+        const size_t smem = kernel_smem(r.n_mma);
+        if ((e = cudaFuncSetAttribute(split_precession_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+            cudaSuccess)
+            return e;
+        KernelArgs ka;
+        ka.prefix = (const double *)r.prefix;
+        ka.b_operand = (const uint8_t *)r.b_operand;
+        ka.spin_table = (const double *)r.spin_table;
+        ka.partial = (float *)r.partial;
+        ka.err = (unsigned int *)r.err;
+        ka.nsamples = nsamples;
+        ka.n_chunks = nchunks;
+        ka.tiles = tiles;
+        ka.maxp = maxp;
+        ka.n_mma = r.n_mma;
+        ka.nstage = kernel_stages(r.n_mma);
+        if (a.ev_start) cudaEventRecord(a.ev_start, stream);
+        split_precession_kernel<<<(unsigned)G, THREADS, smem, stream>>>(ka);
+        if (a.ev_stop) cudaEventRecord(a.ev_stop, stream);
+        if (a.launches) *a.launches += 2;
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        const int64_t total = nsamples * r.nc;
+        if (a.sizeof_T == 8)
+            split_finalize_kernel<double><<<grid_for(total), 256, 0, stream>>>(
+                (const float *)r.partial, nsamples, r.nc, r.n_mma, maxp, nchunks, G, W,
+                (cplx<double> *)a.sig + sample0, a.nadc);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (a.launches) *a.launches += 3;
+    state_update_kernel<<<grid_for(r.ns), 256, 0, stream>>>(
+        (const double *)r.spin_table, (const double *)r.prefix + (size_t)nsamples * PREFIX_STRIDE, (const double *)a.T1,
+        (const double *)a.T2, (const double *)a.rho, r.ns, (cplx<double> *)a.xy, (double *)a.mz);
+    return cudaGetLastError();
+}
+
+cudaError_t split_reset_error(SplitResident &r, cudaStream_t stream) {
+    return cudaMemsetAsync(r.err, 0, sizeof(unsigned int), stream);
+}
+
+cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
+                              int64_t nsamples, cudaStream_t stream, std::string *err) {
+    return split_segment(r, a, n_lo, n_hi, sample0, nsamples, stream, err);
+}
+
+cudaError_t split_check(SplitResident &r, cudaStream_t stream, std::string *err) {
+    unsigned int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, r.err, sizeof(h), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
+    if (h & 64u)
+        *err = "split mode: the accumulated phase of a precession segment exceeds 2^18 turns";
+    else if (h != 0)
+        *err = "split kernel: a bounded device wait timed out (code " + std::to_string(h) + ")";
+    return cudaSuccess;
+}
+
+}  // namespace homs

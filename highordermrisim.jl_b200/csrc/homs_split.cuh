@@ -1,0 +1,75 @@
+// Split-precision path of libhoms (HOMS_SPLIT): interface between the host
+// runtime and the tcgen05 kernels in homs_split.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace homs {
+
+// Device operands that depend only on the phantom (built once per plan):
+// per-spin FP64 basis rows and the receive sensitivities split into TF32
+// hi/lo pairs, laid out in the canonical no-swizzle K-major UMMA layout.
+struct SplitResident {
+    void *basis = nullptr;     // [ns_pad][16] double
+    void *b_operand = nullptr; // [nchunks][2 (hi,lo)][8 ksteps][N rows][8 tf32]
+    void *spin_table = nullptr;  // per-run spin parameters, [ns_pad][SPIN_STRIDE] double
+    void *prefix = nullptr;    // per-segment phase table, [nadc_seg_pad][PREFIX_STRIDE] double
+    void *tvec = nullptr;      // per-segment sample times, float
+    void *partial = nullptr;   // split-K partials, float
+    void *tile_map = nullptr;  // per time tile: (first cta, npieces)
+    void *err = nullptr;       // device error word
+    size_t basis_bytes = 0, b_bytes = 0, spin_bytes = 0, prefix_bytes = 0, tvec_bytes = 0, partial_bytes = 0,
+           tile_map_bytes = 0;
+    int64_t ns = 0, ns_pad = 0;
+    int32_t nc = 0, n_mma = 0;
+    SplitResident() = default;
+    SplitResident(const SplitResident &) = delete;
+    SplitResident &operator=(const SplitResident &) = delete;
+    ~SplitResident();
+    size_t device_bytes() const {
+        return basis_bytes + b_bytes + spin_bytes + prefix_bytes + tvec_bytes + partial_bytes + tile_map_bytes;
+    }
+};
+
+struct SplitRunArgs {
+    size_t sizeof_T;
+    int64_t ns, nt, nadc;
+    int32_t nc;
+    uint32_t method;
+    double gamma;
+    const int64_t *first, *last;
+    const uint8_t *exc;
+    int32_t nblocks;
+    const uint8_t *adc_host;
+    // resident device arrays (type T = double or float per sizeof_T)
+    const void *t, *dt, *gx, *gy, *gz, *b1, *df, *psi, *adc, *bnd, *h[16];
+    const void *x, *y, *z, *rho, *T1, *T2, *dw, *csm_rows;
+    void *xy, *mz, *acc, *sig;
+    // instrumentation (optional): events bracketing the fused kernel launch and
+    // a counter of kernels launched
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    int64_t *launches = nullptr;
+};
+
+// Build the phantom-dependent operands.  Sets *err (and returns cudaSuccess)
+// for valid requests the split path does not serve.
+cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *x, const void *y, const void *z,
+                          const void *dw, const void *csm_rows, bool is_f64, cudaStream_t stream, std::string *err);
+
+// Clear the device error word before a run.
+cudaError_t split_reset_error(SplitResident &r, cudaStream_t stream);
+
+// One precession segment (a run of consecutive precession blocks, nodes
+// [n_lo, n_hi]) on the split tcgen05 kernel; its samples go to sig rows
+// sample0 .. sample0+nsamples-1.  Updates the FP64 state.
+cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
+                              int64_t nsamples, cudaStream_t stream, std::string *err);
+
+// Read the device error word (synchronises the stream).  Sets *err if a
+// bounded wait timed out or the phase range check failed.
+cudaError_t split_check(SplitResident &r, cudaStream_t stream, std::string *err);
+
+}  // namespace homs

@@ -1,0 +1,304 @@
+"""homs -- host side of the B200 BlochHighOrder engine (libhoms).
+
+Mirrors HighOrderMRISim.jl's simulation interface for the BlochHighOrder path:
+
+* ``simulate(obj, seqd, sys=None, sim_params=...)`` -- one-shot simulation
+  (``src/simulation/Simulate.jl:52-67`` / ``:204-219``);
+* ``prepare_simulation(...)`` / ``Plan.run()`` / ``Plan.close()`` -- resident
+  inputs reused across runs (``src/simulation/PreparedSimulation.jl:144-258``);
+* the sampled-sequence and phantom containers, ``BlochHighOrder``, and
+  ``get_sim_ranges`` (see ``model``).
+
+Every run executes in libhoms.so (sm_100a CUDA kernels).  There is no CPU
+fallback: without the library or a B200 the calls raise ``HomsError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Any, Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import Context, HomsError
+from .model import (GAMMA, ArgumentError, BlochHighOrder, DimensionMismatch, HO_DiscreteSequence, HO_Phantom, Mag,
+                    count_block_adc, get_sim_ranges, initialize_spins_state)
+
+__all__ = [
+    "simulate", "prepare_simulation", "Plan", "Context", "HomsError", "ArgumentError", "DimensionMismatch",
+    "BlochHighOrder", "HO_Phantom", "HO_DiscreteSequence", "Mag", "get_sim_ranges", "count_block_adc",
+    "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks",
+]
+
+# Accepted for source compatibility; every choice runs the fused libhoms kernel
+# (src/simulation/kernels/HighOrderGPU.jl:4).
+HIGH_ORDER_COIL_COMBINATIONS = ("gemm", "reduction", "fused_warp", "fused_tiled")
+
+_DEFAULTS = {
+    "precision": "f32", "return_type": "mat", "Nthreads": 1, "implementation": "auto", "coil_combination": "gemm",
+    "synchronization": "auto", "max_block_length": math.inf, "max_rf_block_length": math.inf,
+    "homs_precision": "plain", "gamma": GAMMA, "gpu_device": 0,
+}
+
+
+@dataclass
+class RawData:
+    """Minimal raw-acquisition container: one profile (samples x coils) per
+    block that acquires, plus the run's parameters (``return_type="raw"``)."""
+    profiles: List[np.ndarray]
+    params: Dict[str, Any] = field(default_factory=dict)
+
+
+def _setup(obj: HO_Phantom, seqd: HO_DiscreteSequence, sim_params, parts=None, excitation=None):
+    """Validation and block planning of ``setup_simulation`` (Simulate.jl:222-287)."""
+    if sim_params is None:
+        sim_params = {}
+    if not isinstance(sim_params, dict) or not all(isinstance(k, str) for k in sim_params):
+        raise ArgumentError("sim_params must be a dictionary with string keys.")
+    params = dict(_DEFAULTS)
+    params.update(sim_params)
+    params.setdefault("sim_method", BlochHighOrder("1111"))
+    if params["synchronization"] not in ("auto", "block"):
+        raise ArgumentError("synchronization must be auto or block.")
+    if params["implementation"] not in ("auto", "kernel", "homs", "array"):
+        raise ArgumentError("implementation must be auto, array, or kernel.")
+    if params["implementation"] == "array":
+        raise ArgumentError("implementation=array selects the reference's CPU/array path; this engine runs only "
+                            "the libhoms CUDA kernels.")
+    if params["coil_combination"] not in HIGH_ORDER_COIL_COMBINATIONS:
+        raise ArgumentError(f"Unknown coil_combination: {params['coil_combination']}.")
+    method = params["sim_method"]
+    if not isinstance(method, BlochHighOrder):
+        raise ArgumentError("HO_Phantom currently supports BlochHighOrder() on this engine.")
+    if params["return_type"] not in ("mat", "state", "raw"):
+        raise ArgumentError("return_type must be mat, state, or raw.")
+    if params["precision"] not in ("f32", "f64"):
+        raise ArgumentError("The legacy high-order path supports f32 and f64 precision.")
+    if params["homs_precision"] not in ("plain", "split"):
+        raise ArgumentError("homs_precision must be plain or split.")
+    nth = params["Nthreads"]
+    if not (isinstance(nth, (int, np.integer)) and not isinstance(nth, bool) and nth > 0):
+        raise ArgumentError("Nthreads must be a positive integer.")
+    if not isinstance(obj, HO_Phantom):
+        raise ArgumentError("obj must be an HO_Phantom.")
+    obj.validate()
+    if len(obj) == 0:
+        raise ArgumentError("The phantom must contain at least one spin.")
+    if obj.ncoils < 1:
+        raise ArgumentError("The CSM must contain at least one coil.")
+    seqd.validate()
+    if parts is None:
+        if "Nblocks" in sim_params:
+            nb = sim_params["Nblocks"]
+            if not (isinstance(nb, (int, np.integer)) and not isinstance(nb, bool) and nb > 0):
+                raise ArgumentError("Nblocks must be a positive integer.")
+            legacy = max(1, -(-len(seqd) // nb))
+            if "max_block_length" not in sim_params:
+                params["max_block_length"] = legacy
+            if "max_rf_block_length" not in sim_params:
+                params["max_rf_block_length"] = legacy
+        parts, excitation = get_sim_ranges(seqd, params["max_block_length"], params["max_rf_block_length"])
+    else:
+        if excitation is None or len(excitation) != len(parts):
+            raise DimensionMismatch("parts and excitation must have one entry per block.")
+        parts = [(int(f), int(l)) for f, l in parts]
+        excitation = [bool(e) for e in excitation]
+    if not parts:
+        raise ArgumentError("The sequence must contain a simulation interval.")
+    return params, parts, excitation
+
+
+def _dtype(params):
+    return _lib.HOMS_F64 if params["precision"] == "f64" else _lib.HOMS_F32
+
+
+def _finalize(params, sig, state_xy, state_z, parts, excitation, seqd, seconds):
+    """finalize_simulation! (Simulate.jl:195-214); the ADC phase compensation of
+    KomaMRIBase is the identity for zero-phase ADCs and is left to the caller."""
+    rt = params["return_type"]
+    if rt == "state":
+        return Mag(state_xy, state_z)
+    if rt == "mat":
+        return sig[:, :, None]
+    counts = count_block_adc(seqd.adc, parts)
+    profiles, k = [], 0
+    for n in counts:
+        if n:
+            profiles.append(sig[k:k + n])
+        k += n
+    raw_params = {key: (str(v) if key == "sim_method" else v) for key, v in params.items()}
+    raw_params.update({"Nblocks": len(parts), "type_sim_parts": list(excitation), "sim_time_sec": seconds})
+    return RawData(profiles, raw_params)
+
+
+def _run_options(params) -> _lib.RunOptions:
+    opts = _lib.RunOptions()
+    opts.method = params["sim_method"].flags
+    opts.mode = _lib.HOMS_SPLIT if params["homs_precision"] == "split" else _lib.HOMS_PLAIN
+    return opts
+
+
+_contexts: Dict[int, Context] = {}
+
+
+def _context(device: int) -> Context:
+    ctx = _contexts.get(device)
+    if ctx is None or ctx.handle is None:
+        ctx = Context(device)
+        _contexts[device] = ctx
+    return ctx
+
+
+def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params=None, parts=None, excitation=None,
+             state: Optional[Mag] = None, context: Optional[Context] = None, gpus=None, callbacks=(), verbose=False):
+    """Simulate ``obj`` under the sampled sequence ``seqd``.
+
+    ``sim_params`` keys follow the reference: ``"sim_method"``
+    (BlochHighOrder), ``"precision"`` (f32/f64), ``"return_type"``
+    (mat/state/raw), ``"max_block_length"``, ``"max_rf_block_length"``,
+    ``"Nblocks"``, plus ``"homs_precision"`` (``"plain"`` or ``"split"``).
+    ``parts``/``excitation`` give KomaMRICore's block plan explicitly
+    (0-based inclusive node ranges); by default ``get_sim_ranges`` plans it.
+    ``sys`` (the KomaMRI Scanner) is accepted and unused, as in the reference
+    path.  Returns (Nadc, Nc, 1) complex for "mat", ``Mag`` for "state".
+    The caller's dictionary is never modified.
+    """
+    if callbacks:
+        raise ArgumentError("callbacks run between blocks on the reference's Julia side; use the block entry points "
+                            "(homs_precession_block / homs_excitation_block) for per-block access.")
+    params, parts, excitation = _setup(obj, seqd, dict(sim_params or {}), parts, excitation)
+    if gpus is not None:
+        if not isinstance(gpus, (list, tuple)) or len(gpus) != 1 or not isinstance(gpus[0], (int, np.integer)) \
+                or isinstance(gpus[0], bool) or gpus[0] < 0:
+            raise ArgumentError("gpus must name exactly one visible device on this engine.")
+        params["gpu_device"] = int(gpus[0])
+    ctx = context or _context(int(params["gpu_device"]))
+    dt = _dtype(params)
+    keep = _lib._Keep()
+    ph = _lib.host_phantom(obj, keep, dt)
+    sq = _lib.host_sequence(seqd, parts, excitation, keep, dt, params["gamma"])
+    nadc = sum(count_block_adc(seqd.adc, parts))
+    cdt = np.complex128 if dt == _lib.HOMS_F64 else np.complex64
+    fdt = np.float64 if dt == _lib.HOMS_F64 else np.float32
+    sig = np.zeros((nadc, obj.ncoils), dtype=cdt, order="F")
+    if state is None:
+        xy = np.zeros(len(obj), dtype=cdt)
+        z = np.ascontiguousarray(np.asarray(obj.rho, dtype=fdt)).copy()
+    else:
+        xy = np.ascontiguousarray(np.asarray(state.xy, dtype=cdt)).copy()
+        z = np.ascontiguousarray(np.asarray(state.z, dtype=fdt)).copy()
+    st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+    opts = _run_options(params)
+    t0 = time.perf_counter()
+    lib = _lib.load()
+    _lib.check(lib.homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
+                                 ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST), ctx.handle)
+    seconds = time.perf_counter() - t0
+    return _finalize(params, np.asarray(sig), xy, z, parts, excitation, seqd, seconds)
+
+
+def run_blocks(obj: HO_Phantom, seqd: HO_DiscreteSequence, parts, excitation, method: BlochHighOrder,
+               precision: str = "f64", mode: str = "plain", state: Optional[Mag] = None,
+               context: Optional[Context] = None, gamma: float = GAMMA):
+    """Run an explicit block plan and return ``(signal (Nadc x Nc), Mxy, Mz)``:
+    the kernel-level counterpart of ``simulate_shard`` (Simulate.jl:138-193)."""
+    if precision not in ("f32", "f64"):
+        raise ArgumentError("precision must be f32 or f64")
+    if mode not in ("plain", "split"):
+        raise ArgumentError("mode must be plain or split")
+    obj.validate()
+    seqd.validate()
+    ctx = context or _context(0)
+    dt = _lib.HOMS_F64 if precision == "f64" else _lib.HOMS_F32
+    keep = _lib._Keep()
+    ph = _lib.host_phantom(obj, keep, dt)
+    sq = _lib.host_sequence(seqd, parts, excitation, keep, dt, gamma)
+    nadc = sum(count_block_adc(seqd.adc, parts))
+    cdt = np.complex128 if dt == _lib.HOMS_F64 else np.complex64
+    fdt = np.float64 if dt == _lib.HOMS_F64 else np.float32
+    sig = np.zeros((nadc, obj.ncoils), dtype=cdt, order="F")
+    if state is None:
+        xy = np.zeros(len(obj), dtype=cdt)
+        z = np.ascontiguousarray(np.asarray(obj.rho, dtype=fdt)).copy()
+    else:
+        xy = np.ascontiguousarray(np.asarray(state.xy, dtype=cdt)).copy()
+        z = np.ascontiguousarray(np.asarray(state.z, dtype=fdt)).copy()
+    st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+    opts = _lib.RunOptions()
+    opts.method = method.flags if isinstance(method, BlochHighOrder) else int(method)
+    opts.mode = _lib.HOMS_SPLIT if mode == "split" else _lib.HOMS_PLAIN
+    _lib.check(_lib.load().homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
+                                         ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST),
+               ctx.handle)
+    return np.asarray(sig), xy, z
+
+
+class Plan:
+    """Prepared simulation: inputs resident on the device, repeated runs
+    restart from Mxy = 0, Mz = rho (PreparedSimulation.jl:144-258)."""
+
+    def __init__(self, obj, seqd, sys=None, sim_params=None, parts=None, excitation=None,
+                 context: Optional[Context] = None):
+        params, parts, excitation = _setup(obj, seqd, dict(sim_params or {}), parts, excitation)
+        self.params = params
+        self.parts, self.excitation = parts, excitation
+        self.seqd = seqd
+        self.ctx = context or _context(int(params["gpu_device"]))
+        self.dtype = _dtype(params)
+        self.ns, self.nc = len(obj), obj.ncoils
+        self.nadc = sum(count_block_adc(seqd.adc, parts))
+        keep = _lib._Keep()
+        ph = _lib.host_phantom(obj, keep, self.dtype)
+        sq = _lib.host_sequence(seqd, parts, excitation, keep, self.dtype, params["gamma"])
+        opts = _run_options(params)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().homs_plan_create(self.ctx.handle, ctypes.byref(ph), ctypes.byref(sq),
+                                                ctypes.byref(opts), ctypes.byref(h)), self.ctx.handle)
+        self.handle = h
+        self.closed = False
+
+    def run(self, return_type=None):
+        if return_type is None:
+            return_type = self.params["return_type"]
+        if return_type not in ("mat", "state", "raw"):
+            raise ArgumentError("return_type must be mat, state, or raw.")
+        if self.closed:
+            raise ArgumentError("The prepared simulation is closed.")
+        cdt = np.complex128 if self.dtype == _lib.HOMS_F64 else np.complex64
+        fdt = np.float64 if self.dtype == _lib.HOMS_F64 else np.float32
+        sig = np.zeros((self.nadc, self.nc), dtype=cdt, order="F")
+        xy = np.zeros(self.ns, dtype=cdt)
+        z = np.zeros(self.ns, dtype=fdt)
+        st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+        t0 = time.perf_counter()
+        _lib.check(_lib.load().homs_plan_run(self.handle, sig.ctypes.data if self.nadc else None, _lib.HOMS_HOST,
+                                             ctypes.byref(st)), self.ctx.handle)
+        params = dict(self.params)
+        params["return_type"] = return_type
+        return _finalize(params, np.asarray(sig), xy, z, self.parts, self.excitation, self.seqd,
+                         time.perf_counter() - t0)
+
+    def device_bytes(self) -> int:
+        n = ctypes.c_size_t()
+        _lib.check(_lib.load().homs_plan_device_bytes(self.handle, ctypes.byref(n)))
+        return int(n.value)
+
+    def close(self):
+        if not self.closed:
+            _lib.load().homs_plan_destroy(self.handle)
+            self.handle = None
+            self.closed = True
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def prepare_simulation(obj, seqd, sys=None, *, sim_params=None, parts=None, excitation=None, context=None):
+    """Create a ``Plan`` (use as a context manager or call ``close()``)."""
+    return Plan(obj, seqd, sys, sim_params, parts, excitation, context)

@@ -1,0 +1,203 @@
+/*
+ * homs.h -- C ABI of libhoms, the B200 (sm_100a) engine for HighOrderMRISim.jl's
+ * BlochHighOrder simulation path.
+ *
+ * Plain C types only: pointers, sizes, enums.  A caller (Julia `ccall`, Python
+ * `ctypes`, C/C++) passes phantom and sampled-sequence arrays that live either
+ * in host memory or in device memory of the same primary CUDA context
+ * (`homs_memory`), and receives the multi-coil signal and the final spin state.
+ * Nothing keeps a caller pointer after a call returns.
+ *
+ * Array conventions follow the reference (Julia, column-major):
+ *   - complex values are interleaved (re, im) pairs of the array's dtype;
+ *   - csm is Ns x Nc, element (s, c) at index s + c*Ns;
+ *   - the signal is Nadc x Nc, element (j, c) at index j + c*ldsig;
+ *   - block ranges are 0-based inclusive node pairs (first, last); adjacent
+ *     blocks share a node and its ADC belongs to the earlier block.
+ *
+ * Errors are returned as `homs_status`; nothing aborts, exits or traps.  The
+ * message of the last failure on a context is available from
+ * `homs_last_error`.  Explicit GPU requests never fall back to a CPU path.
+ */
+#ifndef HOMS_H
+#define HOMS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HOMS_ABI_VERSION 1
+
+typedef enum homs_status {
+    HOMS_OK = 0,
+    HOMS_EINVAL = 1,       /* invalid argument (the reference's ArgumentError/DimensionMismatch) */
+    HOMS_ENOMEM = 2,       /* device or host allocation failed, or admission refused */
+    HOMS_EUNSUPPORTED = 3, /* valid request this build cannot serve (e.g. no sm_100 device) */
+    HOMS_ETIMEDOUT = 4,    /* a bounded device-side wait gave up; the context stays usable */
+    HOMS_ECUDA = 5,        /* CUDA runtime error */
+    HOMS_ECLOSED = 6,      /* object already closed */
+    HOMS_EBUSY = 7         /* request not finished yet (polling) */
+} homs_status;
+
+typedef enum homs_dtype { HOMS_F32 = 0, HOMS_F64 = 1 } homs_dtype;
+
+typedef enum homs_memory { HOMS_HOST = 0, HOMS_DEVICE = 1 } homs_memory;
+
+/* Arithmetic of a run.
+ *   HOMS_PLAIN  -- the reference's per-spin sequential trapezoid and fused coil
+ *                  sum in the phantom's dtype (CUDA cores only);
+ *   HOMS_SPLIT  -- FP64 phase (prefix-integrated field table, FP64 mod-2pi
+ *                  reduction), FP32 trigonometry/relaxation, and the coil
+ *                  contraction on tcgen05 tensor cores with TF32 hi/lo split
+ *                  operands and FP32 accumulation; RF blocks in FP64. */
+typedef enum homs_mode { HOMS_PLAIN = 0, HOMS_SPLIT = 1 } homs_mode;
+
+/* BlochHighOrder flags (src/simulation/BlochHighOrder.jl:21-43). */
+#define HOMS_HO0 0x1u           /* zeroth order h0 */
+#define HOMS_HO1 0x2u           /* first order h1..h3 (replaces nominal gradients) */
+#define HOMS_HO2 0x4u           /* second order h4..h8 */
+#define HOMS_HO3 0x8u           /* third order h9..h15 */
+#define HOMS_DW_EXCITATION 0x10u
+#define HOMS_DW_PRECESSION 0x20u
+
+/* Phantom (src/datatypes/HO_Phantom.jl:47-71), structure of arrays. */
+typedef struct homs_phantom {
+    int64_t nspins;
+    int32_t ncoils;
+    homs_dtype dtype;
+    homs_memory memory;
+    const void *x, *y, *z;   /* m */
+    const void *rho;
+    const void *T1, *T2;     /* s */
+    const void *dw;          /* rad/s */
+    const void *csm;         /* complex, Ns x Nc column-major */
+} homs_phantom;
+
+/* Sampled sequence (src/datatypes/HO_DiscreteSequence.jl:31-80) plus the
+ * block plan of KomaMRICore.get_sim_ranges (src/simulation/Simulate.jl:116-123). */
+typedef struct homs_sequence {
+    int64_t nnodes;
+    homs_dtype dtype;
+    homs_memory memory;
+    const void *t;            /* nnodes, s */
+    const void *dt;           /* nnodes-1, s */
+    const void *gx, *gy, *gz; /* nnodes, T/m */
+    const void *b1;           /* nnodes, complex, T */
+    const void *df;           /* nnodes, Hz */
+    const void *psi;          /* nnodes, rad */
+    const uint8_t *adc;       /* nnodes, 0/1 */
+    const void *h[16];        /* nnodes each; h0 T, h1..3 T/m, h4..8 T/m^2, h9..15 T/m^3 */
+    int32_t nblocks;
+    const int64_t *block_first;      /* host memory */
+    const int64_t *block_last;       /* host memory */
+    const uint8_t *block_excitation; /* host memory */
+    double gamma;                    /* Hz/T (KomaMRIBase: 42.5774688e6) */
+} homs_sequence;
+
+typedef struct homs_run_options {
+    uint32_t method; /* HOMS_HO* | HOMS_DW_* */
+    homs_mode mode;
+    int32_t reserved[6];
+} homs_run_options;
+
+/* Spin state (KomaMRICore Mag): xy complex, z real, Ns each, phantom dtype. */
+typedef struct homs_state {
+    void *xy;
+    void *z;
+    homs_memory memory;
+} homs_state;
+
+typedef struct homs_context homs_context;
+typedef struct homs_plan homs_plan;
+typedef struct homs_server homs_server;
+
+/* ---- library --------------------------------------------------------------- */
+
+int homs_abi_version(void);
+const char *homs_status_string(homs_status status);
+
+/* ---- context: one device, one stream, serialised calls ----------------------- */
+
+/* Bind a context to `device` and the caller's CUDA stream (cudaStream_t, NULL
+ * for the per-thread default created by the library).  The reference binds work
+ * to the current CUDA.jl device and stream (src/simulation/Simulate.jl:153-157). */
+homs_status homs_context_create(int device, void *stream, homs_context **out);
+homs_status homs_context_destroy(homs_context *ctx);
+const char *homs_last_error(const homs_context *ctx);
+/* Wait for all work queued by this context. */
+homs_status homs_synchronize(homs_context *ctx);
+
+/* ---- block kernels: device pointers, caller's stream --------------------------
+ * These replace the reference's per-block CUDA kernels one for one. */
+
+/* Free precession over nodes [first,last] of a sampled sequence whose arrays are
+ * DEVICE pointers in the phantom's dtype.  Updates state (device) in place and
+ * writes the block's ADC samples to sig (device, Nadc_b x Nc, leading dimension
+ * ldsig, complex of the phantom's dtype).
+ * Replaces run_high_order_precession! (src/simulation/kernels/HighOrderGPU.jl:124-140)
+ * with the fused kernel of src/simulation/kernels/FusedCoilGPU.jl:70-133. */
+homs_status homs_precession_block(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                                  int64_t first, int64_t last, uint32_t method, homs_state *state, void *sig,
+                                  int64_t ldsig);
+
+/* RF excitation over nodes [first,last] (hard-pulse spinor per node, T2/T1 per
+ * step, ADC-during-RF samples multiplied by cis(psi), psi framing at both ends).
+ * Replaces run_high_order_excitation! (src/simulation/kernels/HighOrderGPU.jl:194-233). */
+homs_status homs_excitation_block(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                                  int64_t first, int64_t last, uint32_t method, homs_state *state, void *sig,
+                                  int64_t ldsig);
+
+/* sig(Nadc x Nc) = transpose(states(Ns x Nadc)) * csm(Ns x Nc), no conjugation,
+ * deterministic two-stage reduction; device pointers, complex of `dtype`.
+ * Replaces reduce_high_order_signal! (src/simulation/kernels/CoilReductionGPU.jl:212-233)
+ * and high_order_gemm! (src/simulation/kernels/HighOrderGPU.jl:162-178). */
+homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins, int64_t nadc, int32_t ncoils,
+                             const void *states, int64_t ldstates, const void *csm, int64_t ldcsm, void *sig,
+                             int64_t ldsig);
+
+/* ---- whole simulation ---------------------------------------------------------- */
+
+/* Run every block of `seq` on `phantom` (host or device arrays).
+ * state: initial state in / final state out (NULL: start from Mxy=0, Mz=rho and
+ * discard the final state).  sig: Nadc_total x Nc complex of the phantom's dtype
+ * in `sig_memory`, leading dimension Nadc_total.
+ * Replaces simulate_shard + run_sim_time_iter! (src/simulation/Simulate.jl:138-193,
+ * src/simulation/SimulatorCore.jl:96-152).  The caller applies KomaMRI's ADC phase
+ * compensation and builds `mat`/`state`/`raw` (src/simulation/Simulate.jl:195-214). */
+homs_status homs_simulate(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                          const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory);
+
+/* Number of ADC samples the blocks of `seq` own (sum of ADC[first+1..last]). */
+homs_status homs_count_adc(const homs_sequence *seq, int64_t *nadc);
+
+/* ---- prepared plans: resident inputs, repeated runs --------------------------
+ * prepare_simulation / simulate(plan) / close(plan)
+ * (src/simulation/PreparedSimulation.jl:144-258).  Inputs are copied into the
+ * plan's device memory at creation; each run restarts from Mxy=0, Mz=rho. */
+homs_status homs_plan_create(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
+                             const homs_run_options *opts, homs_plan **out);
+homs_status homs_plan_run(homs_plan *plan, void *sig, homs_memory sig_memory, homs_state *state_out);
+/* Device bytes held by a plan (resident phantom, basis, operands, work). */
+homs_status homs_plan_device_bytes(const homs_plan *plan, size_t *bytes);
+
+/* Device timing of the plan's last run: summed CUDA-event time of the
+ * dominant fused kernel (the split tcgen05 kernel in HOMS_SPLIT, the segment
+ * kernel in HOMS_PLAIN), its launch count, and all kernels launched.  Plays
+ * the role of the reference's per-run `sim_time_sec` (src/simulation/Simulate.jl:210)
+ * at kernel granularity. */
+typedef struct homs_timing {
+    double fused_kernel_ms;
+    int64_t fused_launches;
+    int64_t kernel_launches;
+} homs_timing;
+homs_status homs_plan_timing(const homs_plan *plan, homs_timing *out);
+homs_status homs_plan_destroy(homs_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HOMS_H */

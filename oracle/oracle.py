@@ -1,0 +1,281 @@
+"""CPU oracle for the BlochHighOrder path.  TEST INFRASTRUCTURE ONLY.
+
+Two independent restatements of HighOrderMRISim.jl's CPU Float64 path:
+
+* ``simulate_c`` -- ctypes front end of ``homs_oracle.c`` (built by
+  ``make -C oracle`` into ``oracle/_build/liboracle.so``), POSIX threads over spins.
+* ``simulate_np`` -- a NumPy transcription of the Julia array code
+  (``src/simulation/Bloch/BlochHighOrderSimulatitonMethod.jl:43-134`` and the
+  block loop ``src/simulation/SimulatorCore.jl:96-152``), materialising
+  Ns x Nt matrices exactly as the reference does.  For small cases only.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg use this module, and only as the checker.
+
+Inputs are duck-typed: a phantom with ``x, y, z, rho, T1, T2, dw`` (float64,
+length Ns) and ``csm`` (complex128, Ns x Nc); a sampled sequence with ``t, dt,
+gx, gy, gz, b1, df, psi, adc, h`` (h is 16 x Nt); block ``parts`` as
+0-based inclusive (first, last) node pairs and ``excitation`` flags per block.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+# KomaMRIBase's gyromagnetic ratio for 1H in Hz/T (the reference takes it
+# from KomaMRIBase; its value is not defined inside the reference tree).
+GAMMA = 42.5774688e6
+
+HO0, HO1, HO2, HO3, DW_EXC, DW_PREC = 1, 2, 4, 8, 16, 32
+
+
+class _Phantom(ctypes.Structure):
+    _fields_ = [
+        ("ns", ctypes.c_int64),
+        ("nc", ctypes.c_int32),
+        ("x", ctypes.c_void_p), ("y", ctypes.c_void_p), ("z", ctypes.c_void_p),
+        ("rho", ctypes.c_void_p), ("T1", ctypes.c_void_p), ("T2", ctypes.c_void_p),
+        ("dw", ctypes.c_void_p), ("csm", ctypes.c_void_p),
+    ]
+
+
+class _Sequence(ctypes.Structure):
+    _fields_ = [
+        ("nt", ctypes.c_int64),
+        ("t", ctypes.c_void_p), ("dt", ctypes.c_void_p),
+        ("gx", ctypes.c_void_p), ("gy", ctypes.c_void_p), ("gz", ctypes.c_void_p),
+        ("b1", ctypes.c_void_p), ("df", ctypes.c_void_p), ("psi", ctypes.c_void_p),
+        ("adc", ctypes.c_void_p),
+        ("h", ctypes.c_void_p * 16),
+        ("nblocks", ctypes.c_int32),
+        ("first", ctypes.c_void_p), ("last", ctypes.c_void_p), ("exc", ctypes.c_void_p),
+        ("gamma", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the C oracle (gcc, POSIX threads) into oracle/_build."""
+    if force or not os.path.exists(LIB_PATH) or (
+        os.path.getmtime(LIB_PATH) < os.path.getmtime(os.path.join(HERE, "homs_oracle.c"))
+    ):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.oracle_simulate.restype = ctypes.c_int
+        lib.oracle_simulate.argtypes = [
+            ctypes.POINTER(_Phantom), ctypes.POINTER(_Sequence), ctypes.c_uint32,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+        ]
+        lib.oracle_basis.restype = None
+        lib.oracle_basis.argtypes = [ctypes.c_double] * 3 + [ctypes.c_void_p]
+        lib.oracle_coil_combine.restype = None
+        lib.oracle_coil_combine.argtypes = [
+            ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+        ]
+        _lib = lib
+    return _lib
+
+
+def _f64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def count_adc(adc, parts):
+    """ADC samples owned by the blocks: ADC[first+1 .. last] (SimulatorCore.jl:115-116)."""
+    adc = np.asarray(adc, dtype=bool)
+    return int(sum(int(adc[f + 1:l + 1].sum()) for f, l in parts))
+
+
+def simulate_c(phantom, seq, parts, excitation, method_flags, mxy0=None, mz0=None, nthreads=None,
+               gamma=GAMMA):
+    """Whole-sequence FP64 simulation by the C oracle.
+
+    Returns (signal (Nadc x Nc complex128), mxy (Ns complex128), mz (Ns float64)).
+    Initial state defaults to Mxy = 0, Mz = rho (BlochHighOrderSimulatitonMethod.jl:9-15).
+    """
+    lib = _load()
+    keep = []
+
+    def ptr(a):
+        keep.append(a)
+        return a.ctypes.data
+
+    ns = len(phantom.x)
+    csm = np.asfortranarray(np.asarray(phantom.csm, dtype=np.complex128).reshape(ns, -1))
+    nc = csm.shape[1]
+    ph = _Phantom(ns, nc, ptr(_f64(phantom.x)), ptr(_f64(phantom.y)), ptr(_f64(phantom.z)),
+                  ptr(_f64(phantom.rho)), ptr(_f64(phantom.T1)), ptr(_f64(phantom.T2)),
+                  ptr(_f64(phantom.dw)), ptr(csm))
+    nt = len(seq.t)
+    h = np.ascontiguousarray(np.asarray(seq.h, dtype=np.float64).reshape(16, nt))
+    hptr = (ctypes.c_void_p * 16)(*[h[k].ctypes.data for k in range(16)])
+    keep.append(h)
+    first = np.ascontiguousarray([p[0] for p in parts], dtype=np.int64)
+    last = np.ascontiguousarray([p[1] for p in parts], dtype=np.int64)
+    exc = np.ascontiguousarray(np.asarray(excitation, dtype=np.uint8))
+    b1 = np.ascontiguousarray(np.asarray(seq.b1, dtype=np.complex128))
+    adc = np.ascontiguousarray(np.asarray(seq.adc, dtype=np.uint8))
+    sq = _Sequence(nt, ptr(_f64(seq.t)), ptr(_f64(seq.dt)), ptr(_f64(seq.gx)), ptr(_f64(seq.gy)),
+                   ptr(_f64(seq.gz)), ptr(b1), ptr(_f64(seq.df)), ptr(_f64(seq.psi)), ptr(adc), hptr,
+                   len(parts), ptr(first), ptr(last), ptr(exc), float(gamma))
+    nadc = count_adc(seq.adc, parts)
+    mxy = np.zeros(ns, np.complex128) if mxy0 is None else np.array(mxy0, dtype=np.complex128)
+    mz = _f64(phantom.rho).copy() if mz0 is None else np.array(mz0, dtype=np.float64)
+    sig = np.zeros((nadc, nc), dtype=np.complex128, order="F")
+    if nthreads is None:
+        nthreads = max(1, min(len(os.sched_getaffinity(0)), 64))
+    rc = lib.oracle_simulate(ctypes.byref(ph), ctypes.byref(sq), int(method_flags), mxy.ctypes.data,
+                             mz.ctypes.data, sig.ctypes.data, nadc, int(nthreads))
+    if rc != 0:
+        raise ValueError(f"oracle_simulate failed with code {rc}")
+    return np.asarray(sig), mxy, mz
+
+
+def basis_c(x, y, z):
+    out = np.zeros(16)
+    _load().oracle_basis(float(x), float(y), float(z), out.ctypes.data)
+    return out
+
+
+def coil_combine_c(states, csm):
+    """transpose(states)·csm in FP64 (states Ns x Nadc, csm Ns x Nc)."""
+    states = np.asfortranarray(np.asarray(states, dtype=np.complex128))
+    csm = np.asfortranarray(np.asarray(csm, dtype=np.complex128))
+    ns, nadc = states.shape
+    nc = csm.shape[1]
+    sig = np.zeros((nadc, nc), np.complex128, order="F")
+    _load().oracle_coil_combine(ns, nadc, nc, states.ctypes.data, csm.ctypes.data, sig.ctypes.data)
+    return sig
+
+
+# ---------------------------------------------------------------------------
+# NumPy twin: a direct transcription of the Julia array code, block by block.
+# ---------------------------------------------------------------------------
+
+def basis_np(x, y, z):
+    """Basis columns (Ns x 16), CPU expression order (BlochHighOrderSimulatitonMethod.jl:54-68)."""
+    x2, y2, z2 = x * x, y * y, z * z
+    r2 = (x2 + y2) + z2
+    one = np.ones_like(x)
+    return np.stack([
+        one, x, y, z, x * y, z * y, 3.0 * z2 - r2, x * z, x2 - y2,
+        (3.0 * y) * x2 - (y2 * y), (x * z) * y, (5.0 * z2 - r2) * y,
+        5.0 * (z2 * z) - (3.0 * z) * r2, (5.0 * z2 - r2) * x, x2 * z - y2 * z, (x2 * x) - (3.0 * x) * y2,
+    ], axis=1)
+
+
+def _cmul(a, b):
+    return (a.real * b.real - a.imag * b.imag) + 1j * (a.real * b.imag + a.imag * b.real)
+
+
+def precession_np(phantom, seq, f, l, flags, mxy, mz, gamma=GAMMA):
+    """run_spin_precession! for nodes f..l (BlochHighOrderSimulatitonMethod.jl:43-94).
+    Updates mxy/mz in place and returns the block signal (Nadc_b x Nc)."""
+    x, y, z = (np.asarray(v, np.float64)[:, None] for v in (phantom.x, phantom.y, phantom.z))
+    h = np.asarray(seq.h, np.float64)[:, f:l + 1]
+    g = [np.asarray(v, np.float64)[f:l + 1][None, :] for v in (seq.gx, seq.gy, seq.gz)]
+    hr = [h[k][None, :] for k in range(16)]
+    x2, y2, z2 = x * x, y * y, z * z
+    r2 = (x2 + y2) + z2
+    bzh = [None, x * hr[1], y * hr[2], z * hr[3], (x * y) * hr[4], (z * y) * hr[5], (3.0 * z2 - r2) * hr[6],
+           (x * z) * hr[7], (x2 - y2) * hr[8], ((3.0 * y) * x2 - (y2 * y)) * hr[9], ((x * z) * y) * hr[10],
+           ((5.0 * z2 - r2) * y) * hr[11], (5.0 * (z2 * z) - (3.0 * z) * r2) * hr[12],
+           ((5.0 * z2 - r2) * x) * hr[13], (x2 * z - y2 * z) * hr[14], ((x2 * x) - (3.0 * x) * y2) * hr[15]]
+    bz0 = hr[0] if flags & HO0 else 0.0
+    bz1 = (bzh[1] + bzh[2]) + bzh[3] if flags & HO1 else (x * g[0] + y * g[1]) + z * g[2]
+    bz2 = (((bzh[4] + bzh[5]) + bzh[6]) + bzh[7]) + bzh[8] if flags & HO2 else 0.0
+    bz3 = (((((bzh[9] + bzh[10]) + bzh[11]) + bzh[12]) + bzh[13]) + bzh[14]) + bzh[15] if flags & HO3 else 0.0
+    bz = ((bz0 + bz1) + bz2) + bz3
+    if flags & DW_PREC:
+        bz = bz + np.asarray(phantom.dw, np.float64)[:, None] / (2.0 * np.pi * gamma)
+    bz = np.broadcast_to(bz, (len(phantom.x), l - f + 1))
+    dt = np.asarray(seq.dt, np.float64)[f:l]
+    y_ = (bz[:, 1:] + bz[:, :-1]) * dt[None, :]
+    phi = (-(2.0 * np.pi * gamma)) * (0.5 * np.cumsum(y_, axis=1))
+    tp = np.cumsum(dt)
+    T2 = np.asarray(phantom.T2, np.float64)[:, None]
+    e = np.exp(0.0 - tp[None, :] / T2)
+    ez = e * np.cos(phi) + 1j * (e * np.sin(phi))
+    m0 = mxy[:, None].copy()
+    states = _cmul(np.broadcast_to(m0, ez.shape), ez)
+    if l > f:
+        mxy[:] = states[:, -1]
+    dur = tp[-1] if len(tp) else 0.0
+    e1 = np.exp(-dur / np.asarray(phantom.T1, np.float64))
+    mz[:] = mz * e1 + np.asarray(phantom.rho, np.float64) * (1.0 - e1)
+    adc = np.asarray(seq.adc, bool)[f + 1:l + 1]
+    sel = states[:, adc]
+    csm = np.asarray(phantom.csm, np.complex128).reshape(len(phantom.x), -1)
+    return sel.T @ csm
+
+
+def excitation_np(phantom, seq, f, l, flags, mxy, mz, gamma=GAMMA):
+    """run_spin_excitation! for nodes f..l (BlochHighOrderSimulatitonMethod.jl:100-134)."""
+    twopig = 2.0 * np.pi * gamma
+    x, y, z = (np.asarray(v, np.float64) for v in (phantom.x, phantom.y, phantom.z))
+    rho, T1, T2 = (np.asarray(v, np.float64) for v in (phantom.rho, phantom.T1, phantom.T2))
+    csm = np.asarray(phantom.csm, np.complex128).reshape(len(x), -1)
+    psi = np.asarray(seq.psi, np.float64)
+    mxy[:] = _cmul(mxy, np.cos(-psi[f]) + 1j * np.sin(-psi[f]))
+    off = np.asarray(phantom.dw, np.float64) / twopig if flags & DW_EXC else 0.0
+    out = []
+    for n in range(f, l):
+        dbz = off - seq.df[n] / gamma
+        bz = ((seq.gx[n] * x + seq.gy[n] * y) + seq.gz[n] * z) + dbz
+        b1 = complex(seq.b1[n])
+        B = np.sqrt(np.hypot(b1.real, b1.imag) ** 2 + bz * bz)
+        B = np.where(B == 0.0, np.finfo(np.float64).eps, B)
+        phi = -twopig * (B * seq.dt[n])
+        sh, ch = np.sin(phi / 2.0), np.cos(phi / 2.0)
+        nz = bz / B
+        nx = (b1.real / B) + 1j * (b1.imag / B)
+        alpha = ch + 1j * (-(nz * sh))
+        beta = (nx.imag * sh) + 1j * (-(nx.real * sh))
+        ca = np.conj(alpha)
+        t1 = _cmul(2.0 * ca.real + 1j * (2.0 * ca.imag), beta) * mz
+        t2 = _cmul(_cmul(ca, ca), mxy)
+        t3 = _cmul(_cmul(beta, beta), np.conj(mxy))
+        nxy = (t1 + t2) - t3
+        nzz = (np.abs(alpha) ** 2 - np.abs(beta) ** 2) * mz - 2.0 * _cmul(_cmul(alpha, beta), np.conj(mxy)).real
+        mxy[:] = nxy * np.exp(-seq.dt[n] / T2)
+        e1 = np.exp(-seq.dt[n] / T1)
+        mz[:] = nzz * e1 + rho * (1.0 - e1)
+        if seq.adc[n + 1]:
+            s = _cmul(mxy, np.cos(psi[n + 1]) + 1j * np.sin(psi[n + 1]))
+            out.append(s @ csm)
+    mxy[:] = _cmul(mxy, np.cos(psi[l]) + 1j * np.sin(psi[l]))
+    if out:
+        return np.stack(out, axis=0)
+    return np.zeros((0, csm.shape[1]), np.complex128)
+
+
+def simulate_np(phantom, seq, parts, excitation, method_flags, mxy0=None, mz0=None, gamma=GAMMA):
+    """run_sim_time_iter! over blocks with the NumPy twin (single spin part)."""
+    ns = len(phantom.x)
+    mxy = np.zeros(ns, np.complex128) if mxy0 is None else np.array(mxy0, dtype=np.complex128)
+    mz = np.array(phantom.rho, dtype=np.float64) if mz0 is None else np.array(mz0, dtype=np.float64)
+    blocks = []
+    for (f, l), ex in zip(parts, excitation):
+        if ex:
+            blocks.append(excitation_np(phantom, seq, f, l, method_flags, mxy, mz, gamma))
+        else:
+            blocks.append(precession_np(phantom, seq, f, l, method_flags, mxy, mz, gamma))
+    nc = np.asarray(phantom.csm).reshape(ns, -1).shape[1]
+    sig = np.concatenate(blocks, axis=0) if blocks else np.zeros((0, nc), np.complex128)
+    return sig, mxy, mz

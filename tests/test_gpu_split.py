@@ -1,0 +1,92 @@
+"""Split-precision tcgen05 path vs the FP64 CPU oracle (signal NRMSE <= 1e-6)."""
+import numpy as np
+import pytest
+
+import homs
+from conftest import nrmse
+from homs import workloads as W
+from homs.model import BlochHighOrder, get_sim_ranges
+
+pytestmark = pytest.mark.gpu
+
+SPLIT_NRMSE = 1e-6
+
+
+def oracle_run(o, obj, seq, parts, exc, method, state=None):
+    return o.simulate_c(obj, seq, parts, exc, method.flags, None if state is None else state.xy,
+                        None if state is None else state.z)
+
+
+def split_run(obj, seq, parts, exc, method, state=None):
+    return homs.run_blocks(obj, seq, parts, exc, method, "f64", "split", state)
+
+
+@pytest.mark.parametrize("mask", [format(m, "04b") for m in range(16)])
+@pytest.mark.parametrize("ncoils", [1, 3, 32])
+def test_split_fixture_all_masks(oracle, gpu_context, mask, ncoils):
+    obj, seq, st = W.high_order_workload(nspins=259, nsteps=32, ncoils=ncoils)
+    method = BlochHighOrder(mask)
+    ref = oracle_run(oracle, obj, seq, [(0, 32)], [False], method, st)
+    got = split_run(obj, seq, [(0, 32)], [False], method, st)
+    assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+    assert nrmse(got[1], ref[1]) <= 1e-12
+    assert nrmse(got[2], ref[2]) <= 1e-12
+
+
+@pytest.mark.parametrize("nspins", [1, 31, 32, 33, 255, 257, 4099])
+@pytest.mark.parametrize("nsteps", [1, 127, 128, 129, 300])
+def test_split_tails(oracle, gpu_context, nspins, nsteps):
+    obj, seq, st = W.high_order_workload(nspins=nspins, nsteps=nsteps, ncoils=8)
+    method = BlochHighOrder("1111")
+    ref = oracle_run(oracle, obj, seq, [(0, nsteps)], [False], method, st)
+    got = split_run(obj, seq, [(0, nsteps)], [False], method, st)
+    assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+
+
+@pytest.mark.parametrize("scenario", [(0, 0, 11, True), (3, 2, 11, True), (5, 2, 0, True)])
+def test_split_with_rf_blocks(oracle, gpu_context, scenario):
+    obj, seq, _, _ = W.rf_acquisition_workload(*scenario)
+    parts, exc = get_sim_ranges(seq, 4, 5)
+    method = BlochHighOrder("1111")
+    ref = oracle_run(oracle, obj, seq, parts, exc, method)
+    got = split_run(obj, seq, parts, exc, method)
+    assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+    assert nrmse(got[1], ref[1]) <= 1e-10
+
+
+def test_split_config0_full(oracle, gpu_context):
+    w = W.config(0)
+    method = BlochHighOrder(w.mask)
+    ref = oracle_run(oracle, w.obj, w.seq, w.parts, w.excitation, method)
+    got = split_run(w.obj, w.seq, w.parts, w.excitation, method)
+    assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+
+
+@pytest.mark.parametrize("cfg,stride", [(1, 40), (2, 400)])
+def test_split_config_subsample(oracle, gpu_context, cfg, stride):
+    w = W.config(cfg, spins_stride=stride)
+    method = BlochHighOrder(w.mask)
+    ref = oracle_run(oracle, w.obj, w.seq, w.parts, w.excitation, method)
+    got = split_run(w.obj, w.seq, w.parts, w.excitation, method)
+    assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+
+
+def test_split_deterministic_and_plan(gpu_context):
+    w = W.config(2, spins_stride=200)
+    method = BlochHighOrder(w.mask)
+    a = split_run(w.obj, w.seq, w.parts, w.excitation, method)
+    b = split_run(w.obj, w.seq, w.parts, w.excitation, method)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    params = {"sim_method": method, "precision": "f64", "homs_precision": "split"}
+    with homs.prepare_simulation(w.obj, w.seq, sim_params=params, parts=w.parts, excitation=w.excitation) as plan:
+        r1 = plan.run()
+        r2 = plan.run()
+    assert np.array_equal(r1, r2)
+    assert np.array_equal(r1[:, :, 0], a[0])
+
+
+def test_split_rejects_fp32_inputs(gpu_context):
+    obj, seq, st = W.high_order_workload(nspins=33, nsteps=8, ncoils=2)
+    with pytest.raises(homs.HomsError) as e:
+        homs.run_blocks(obj, seq, [(0, 8)], [False], BlochHighOrder("1111"), "f32", "split", st)
+    assert e.value.status == 3

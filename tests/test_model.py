@@ -1,0 +1,96 @@
+"""Host-side mirror of the reference interface: validation and block planning."""
+import math
+
+import numpy as np
+import pytest
+
+import homs
+from homs import workloads as W
+from homs.model import (ArgumentError, BlochHighOrder, DimensionMismatch, HO_DiscreteSequence, HO_Phantom,
+                        count_block_adc, get_sim_ranges)
+
+
+def test_bloch_high_order_mask_rules():
+    # src/simulation/BlochHighOrder.jl:21-43
+    m = BlochHighOrder("1010")
+    assert (m.ho0, m.ho1, m.ho2, m.ho3) == (True, False, True, False)
+    assert m.flags == 1 | 4 | 16 | 32
+    assert BlochHighOrder("0000", False, True).flags == 32
+    for bad in ("111", "11111", "1a11", 1111):
+        with pytest.raises(ArgumentError):
+            BlochHighOrder(bad)
+    with pytest.raises(ArgumentError):
+        BlochHighOrder.from_flags(True, True, True, True, name="0111")
+    assert BlochHighOrder.from_flags(False, True, True, False).name == "0110"
+
+
+def test_phantom_defaults_and_validation():
+    # src/datatypes/HO_Phantom.jl:47-71, :97-109
+    p = HO_Phantom(x=[0.0, 0.01, -0.02])
+    assert p.csm.shape == (3, 1) and np.all(p.csm == 1)
+    assert np.all(p.rho == 1) and np.all(p.T1 == 1e6)
+    p.y = np.zeros(2)
+    with pytest.raises(DimensionMismatch):
+        p.validate()
+    q = HO_Phantom(x=[0.0], csm=np.ones((2, 1)))
+    with pytest.raises(DimensionMismatch):
+        q.validate()
+
+
+def test_sim_ranges_share_boundary_nodes_and_own_adc():
+    obj, seq, parts, exc = W.rf_acquisition_workload(3, 2, 11)
+    p, e = get_sim_ranges(seq)
+    assert p == parts and e == exc
+    p2, e2 = get_sim_ranges(seq, 1, 1)
+    assert all(l - f == 1 for f, l in p2)
+    assert sum(count_block_adc(seq.adc, p2)) == sum(count_block_adc(seq.adc, parts)) == 16
+    for (f1, l1), (f2, l2) in zip(p2, p2[1:]):
+        assert l1 == f2
+    with pytest.raises(ArgumentError):
+        get_sim_ranges(seq, 0)
+    with pytest.raises(ArgumentError):
+        get_sim_ranges(seq, 2.5)
+
+
+def test_setup_validation_matches_reference_errors():
+    # src/simulation/Simulate.jl:222-287
+    obj = W.compatibility_phantom()
+    seq, parts, exc, _ = W.compatibility_sequence()
+    setup = homs._setup
+    for bad in ({"return_type": "x"}, {"precision": "f16"}, {"synchronization": "x"}, {"implementation": "x"},
+                {"coil_combination": "x"}, {"Nthreads": 0}, {"sim_method": "1111"}, {"Nblocks": 0},
+                {"max_block_length": 0}, {"implementation": "array"}, {"homs_precision": "bf16"}):
+        with pytest.raises(ArgumentError):
+            setup(obj, seq, bad)
+    with pytest.raises(ArgumentError):
+        setup(obj, seq, {1: 2})
+    with pytest.raises(ArgumentError):
+        setup(obj, seq, [("precision", "f64")])
+    params = {"precision": "f64", "Nblocks": 1000}
+    snapshot = dict(params)
+    p, parts2, exc2 = setup(obj, seq, params)
+    assert params == snapshot
+    assert all(l - f == 1 for f, l in parts2)
+    empty = HO_Phantom(x=np.zeros(0))
+    with pytest.raises(ArgumentError):
+        setup(empty, seq, {})
+
+
+def test_config_shapes_and_units():
+    w0 = W.config(0)
+    assert len(w0.obj) == 4096 and w0.obj.ncoils == 1
+    assert sum(count_block_adc(w0.seq.adc, w0.parts)) == 2048
+    w1 = W.config(1)
+    n1 = sum(count_block_adc(w1.seq.adc, w1.parts))
+    assert len(w1.obj) * n1 * w1.obj.ncoils == 40000 * 40000 * 8
+    assert w1.mask == "1110"
+    # Gradient limit of the spiral readouts.
+    g = np.hypot(w1.seq.gx, w1.seq.gy)
+    assert g.max() <= 30e-3 * (1 + 1e-9)
+
+
+def test_config2_size():
+    w2 = W.config(2, spins_stride=1000)
+    n2 = sum(count_block_adc(w2.seq.adc, w2.parts))
+    assert n2 == 4 * 9500 and w2.obj.ncoils == 32
+    assert len(W.grid(100, 100, 35, 2e-3, 2e-3, 2e-3)[0]) == 350000
