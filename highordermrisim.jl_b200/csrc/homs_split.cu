@@ -22,13 +22,13 @@
 //
 // Kernel organisation (one CTA per SM, persistent, stream-K over
 // (time tile of 128 samples) x (chunk of 32 spins) units):
-//   warps 0-7  producers: thread <-> sample row of the 128-row tile; compute
-//              M for 16 spins per chunk, write TF32 hi/lo to TMEM (A operand)
+//   warps 0-15 producers: thread <-> sample row of the 128-row tile; compute
+//              M for 8 spins per chunk, write TF32 hi/lo to TMEM (A operand)
 //              with tcgen05.st; epilogue reads the accumulator with tcgen05.ld.
-//   warp 8     MMA issuer: tcgen05.mma.kind::tf32 with A in TMEM, B (the
+//   warp 16    MMA issuer: tcgen05.mma.kind::tf32 with A in TMEM, B (the
 //              sensitivities, pre-split) in shared memory; tcgen05.commit
 //              releases shared-memory stages, A stages and accumulators.
-//   warp 9     loader: cp.async.bulk of each chunk's B operand and spin table.
+//   warp 17    loader: cp.async.bulk of each chunk's B operand and spin table.
 // Every wait is bounded: on time-out the kernel records the place in a device
 // error word and returns without hanging the GPU.
 #include <algorithm>
@@ -51,13 +51,23 @@ constexpr int MAX_STAGE = 4;     // shared-memory stages (fewer for wide N)
 constexpr int SPIN_ROWS = 20;    // k-major spin table rows per chunk
 constexpr int SPIN_BYTES = SPIN_ROWS * KC * 8;
 constexpr int PREFIX_STRIDE = 20;  // doubles per prefix row: kappa[0..16], t, pad
-constexpr int NPROD_WARPS = 8;
-constexpr int MMA_WARP = 8;
-constexpr int LOAD_WARP = 9;
-constexpr int THREADS = 320;
+constexpr int NPROD_WARPS = 16;             // 4 per TMEM lane quarter
+constexpr int MMA_WARP = 16;
+constexpr int LOAD_WARP = 17;
+constexpr int THREADS = 576;
+constexpr int SPW = KC / (NPROD_WARPS / 4);  // spins per producer warp and chunk
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t A_COL0 = 256;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
+// Chunks accumulated in one FP32 TMEM generation before it is added into the
+// FP64 partials.  The tensor core's accumulator add is not round-to-nearest:
+// its error is systematic and grows with |D| and with the number of MMAs per
+// generation, so each 32-spin chunk gets its own generation.
+constexpr int FLUSH = 1;
+// Chunks summed (round to nearest, FP32) in shared memory before promotion to
+// the FP64 partials, and the row padding of that accumulator (bank spread).
+constexpr int WINDOW = 32;
+constexpr int ACC_PAD = 4;
 
 // Sine/cosine coefficients on [-pi/4, pi/4] (see fit_sincos.py).
 constexpr float S1 = -0.16666650772094727f, S2 = 0.00833197869360447f, S3 = -0.00019495606829877943f;
@@ -115,11 +125,9 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint32_t a, uint64_t bde
         "r"(a), "l"(bdesc), "r"(idesc), "r"(accum)
         : "memory");
 }
-__device__ __forceinline__ uint32_t tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
+// Round to TF32 (10 stored mantissa bits), nearest with ties away from zero:
+// add half of the 13 dropped bits to the magnitude, then clear them.
+__device__ __forceinline__ uint32_t tf32_rna(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
 __device__ __forceinline__ float ex2_approx(float x) {
     float r;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -136,6 +144,21 @@ __device__ __forceinline__ float ex2_approx(float x) {
         "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),          \
         "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])                       \
         : "memory")
+
+#define HOMS_ST_X8(taddr, v)                                                                                 \
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),  \
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])          \
+                 : "memory")
+
+__device__ __forceinline__ void tmem_ld_x4(uint32_t taddr, float *v) {
+    uint32_t r[4];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(taddr)
+                 : "memory");
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+}
 
 __device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, float *v) {
     uint32_t r[8];
@@ -161,7 +184,7 @@ struct KernelArgs {
     const double *prefix;      // [rows][PREFIX_STRIDE]
     const uint8_t *b_operand;  // [nchunks][b_bytes]
     const double *spin_table;  // [nchunks][SPIN_ROWS][KC]
-    float *partial;            // [tiles][maxp][TM][n_mma]
+    double *partial;           // [tiles][maxp][TM][n_mma], FP64 split-K partials
     unsigned int *err;
     int64_t nsamples;
     int64_t n_chunks;
@@ -184,20 +207,11 @@ __device__ __forceinline__ void magnetisation(double th, float tj, float r2, flo
     const float x2 = x * x;
     const float sp = fmaf(x * x2, fmaf(x2, fmaf(x2, S3, S2), S1), x);
     const float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, C4, C3), C2), C1), 1.0f);
-    float c, s;
-    if (q == 0) {
-        c = cp;
-        s = sp;
-    } else if (q == 1) {
-        c = -sp;
-        s = cp;
-    } else if (q == 2) {
-        c = -cp;
-        s = -sp;
-    } else {
-        c = sp;
-        s = -cp;
-    }
+    // cis(x + q*pi/2): swap for odd q, negate cos for q in {1,2}, sin for q in {2,3}.
+    const bool swap = (q & 1u) != 0;
+    const uint32_t cbits = __float_as_uint(swap ? sp : cp) ^ ((((q + 1u) >> 1) & 1u) << 31);
+    const uint32_t sbits = __float_as_uint(swap ? cp : sp) ^ ((q >> 1) << 31);
+    const float c = __uint_as_float(cbits), s = __uint_as_float(sbits);
     const float a = ex2_approx(fmaf(tj, r2, l2m0));
     mre = a * c;
     mim = a * s;
@@ -205,13 +219,14 @@ __device__ __forceinline__ void magnetisation(double th, float tj, float r2, flo
 
 __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const int n_mma = args.n_mma;
     const int NSTAGE = args.nstage;
     const int BB = b_bytes(n_mma);
     uint8_t *sB = smem;                                   // NSTAGE * BB
     double *sSpin = reinterpret_cast<double *>(sB + NSTAGE * BB);  // NSTAGE * SPIN_BYTES
-    uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);
+    float *accf = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);  // TM x (n_mma+pad)
+    uint64_t *bars = reinterpret_cast<uint64_t *>(accf + (size_t)TM * (n_mma + ACC_PAD));
     uint64_t *full = bars;                    // [NSTAGE] loader -> consumers (tx)
     uint64_t *empty = bars + MAX_STAGE;       // [NSTAGE] MMA commit -> loader
     uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] producers -> MMA
@@ -275,20 +290,27 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         if (lane == 0) {
             const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n_mma >> 3) << 17) |
                                    ((uint32_t)(TM >> 4) << 24);
-            int64_t g = 0, piece = 0;
+            int64_t g = 0, grp = 0;
             int64_t u = u0;
             while (u < u1 && !dead) {
                 const int64_t k0 = u % args.n_chunks;
                 const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
-                const int dbuf = (int)(piece & 1);
-                if (!mbar_wait(&d_empty[dbuf], (uint32_t)(((piece >> 1) + 1) & 1))) {
-                    atomicOr(args.err, 2u);
-                    dead = true;
-                    break;
-                }
-                tc_fence_after();
-                const uint32_t dcol = tmem + (uint32_t)(dbuf * n_mma);
+                // One accumulator generation per group of FLUSH chunks; the
+                // producers add each generation into FP64 partials.
+                int dbuf = 0;
+                uint32_t dcol = 0;
                 for (int64_t k = k0; k < k1; ++k, ++g) {
+                    const bool gstart = ((k - k0) % FLUSH) == 0;
+                    if (gstart) {
+                        dbuf = (int)(grp & 1);
+                        if (!mbar_wait(&d_empty[dbuf], (uint32_t)(((grp >> 1) + 1) & 1))) {
+                            atomicOr(args.err, 2u);
+                            dead = true;
+                            break;
+                        }
+                        tc_fence_after();
+                        dcol = tmem + (uint32_t)(dbuf * n_mma);
+                    }
                     const int stage = (int)(g % NSTAGE);
                     const int as = (int)(g & 1);
                     if (!mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1)) ||
@@ -302,21 +324,30 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     const uint32_t a_hi = tmem + A_COL0 + (uint32_t)as * 128u;
                     const uint32_t a_lo = a_hi + 64u;
 #pragma unroll
+                    // The accumulator add of each MMA rounds relative to |D|,
+                    // so the two small cross-term passes (hi*lo, lo*hi) go
+                    // first, while D is small, and hi*hi last.
                     for (int ks = 0; ks < KSTEPS; ++ks) {
                         const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * n_mma * 32));
                         const uint64_t blo = bdesc(sbase + (uint32_t)((KSTEPS + ks) * n_mma * 32));
-                        const uint32_t first = (k == k0 && ks == 0) ? 0u : 1u;
-                        tc_mma_tf32(dcol, a_hi + ks * 8, bhi, idesc, first);
-                        tc_mma_tf32(dcol, a_hi + ks * 8, blo, idesc, 1u);
+                        const uint32_t first = (gstart && ks == 0) ? 0u : 1u;
+                        tc_mma_tf32(dcol, a_hi + ks * 8, blo, idesc, first);
                         tc_mma_tf32(dcol, a_lo + ks * 8, bhi, idesc, 1u);
+                    }
+#pragma unroll
+                    for (int ks = 0; ks < KSTEPS; ++ks) {
+                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * n_mma * 32));
+                        tc_mma_tf32(dcol, a_hi + ks * 8, bhi, idesc, 1u);
                     }
                     tc_commit(&empty[stage]);
                     tc_commit(&a_empty[as]);
+                    if ((k - k0) % FLUSH == FLUSH - 1 || k + 1 == k1) {
+                        tc_commit(&d_full[dbuf]);
+                        ++grp;
+                    }
                 }
                 if (dead) break;
-                tc_commit(&d_full[dbuf]);
                 u += k1 - k0;
-                ++piece;
             }
             // Drain: wait for every issued MMA before TMEM is released.
             tc_commit(done);
@@ -325,16 +356,62 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         __syncwarp();
     } else {
         // Producers / epilogue: thread <-> tile row.
-        const int quarter = warp & 3, half = warp >> 2;
+        const int quarter = warp & 3, part = warp >> 2;  // TMEM lane quarter, slice of the chunk's spins
         const int row = quarter * 32 + lane;
         const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        int64_t g = 0, piece = 0;
+        const int ncol = n_mma / 4;  // accumulator columns this warp drains
+        int64_t g = 0, grp = 0;
         int64_t u = u0;
+        // Two-level drain of each chunk's accumulator generation: the FP32
+        // TMEM result is added (round to nearest) into this thread's FP32 row
+        // accumulator in shared memory; every WINDOW chunks, and at the end of
+        // a piece, that row is promoted into the FP64 split-K partial.
+        float *arow = accf + (size_t)row * (n_mma + ACC_PAD) + part * ncol;
+        int64_t pend_grp = -1;
+        double *pend_dst = nullptr;
+        bool pend_wfirst = false, pend_promote = false, pend_pfirst = false;
+        auto drain = [&]() -> bool {
+            const int dbuf = (int)(pend_grp & 1);
+            const bool ok = mbar_wait(&d_full[dbuf], (uint32_t)((pend_grp >> 1) & 1));
+            __syncwarp();
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) atomicOr(args.err, 32u);
+                return false;
+            }
+            tc_fence_after();
+            for (int cc = 0; cc < ncol; cc += 4) {
+                float v[4];
+                tmem_ld_x4(tmem + lane_base + (uint32_t)(dbuf * n_mma + part * ncol + cc), v);
+                tmem_wait_ld();
+                float4 a = pend_wfirst ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<float4 *>(arow + cc);
+                a.x += v[0];
+                a.y += v[1];
+                a.z += v[2];
+                a.w += v[3];
+                *reinterpret_cast<float4 *>(arow + cc) = a;
+            }
+            tc_fence_before();
+            mbar_arrive(&d_empty[dbuf]);
+            if (pend_promote) {
+                for (int cc = 0; cc < ncol; cc += 2) {
+                    const float2 a = *reinterpret_cast<const float2 *>(arow + cc);
+                    double2 *d = reinterpret_cast<double2 *>(pend_dst + cc);
+                    double2 o = pend_pfirst ? make_double2(0.0, 0.0) : *d;
+                    o.x += (double)a.x;
+                    o.y += (double)a.y;
+                    *d = o;
+                }
+            }
+            pend_grp = -1;
+            return true;
+        };
         while (u < u1 && !dead) {
             const int64_t tile = u / args.n_chunks;
             const int64_t k0 = u % args.n_chunks;
             const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
             const int slot = (int)(blockIdx.x - cta_of(tile * args.n_chunks, G, W));
+            double *dst_piece =
+                args.partial + (((size_t)tile * args.maxp + slot) * TM + row) * (size_t)n_mma + part * ncol;
             int64_t j = tile * TM + row;
             if (j >= args.nsamples) j = args.nsamples - 1;
             double kap[17];
@@ -355,10 +432,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 }
                 tc_fence_after();
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                uint32_t hi[32], lo[32];
+                const uint32_t a_hi =
+                    tmem + lane_base + A_COL0 + (uint32_t)as * 128u + (uint32_t)part * (2u * SPW);
 #pragma unroll
-                for (int g4 = 0; g4 < 4; ++g4) {
-                    const int s0 = half * 16 + g4 * 4;
+                for (int g4 = 0; g4 < SPW / 4; ++g4) {
+                    const int s0 = part * SPW + g4 * 4;
                     double th[4];
                     {
                         const double2 t01 = *reinterpret_cast<const double2 *>(tab + 17 * KC + s0);
@@ -381,49 +459,44 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     const float4 rl23 = *reinterpret_cast<const float4 *>(tab + 18 * KC + s0 + 2);
                     const float r2v[4] = {rl01.x, rl01.z, rl23.x, rl23.z};
                     const float l2v[4] = {rl01.y, rl01.w, rl23.y, rl23.w};
+                    uint32_t hi[8], lo[8];
 #pragma unroll
                     for (int i = 0; i < 4; ++i) {
                         float mre, mim;
                         magnetisation(th[i], tj, r2v[i], l2v[i], mre, mim);
                         const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
-                        const int e = 2 * (g4 * 4 + i);
-                        hi[e] = hr;
-                        hi[e + 1] = hm;
-                        lo[e] = tf32_rna(mre - __uint_as_float(hr));
-                        lo[e + 1] = tf32_rna(mim - __uint_as_float(hm));
+                        hi[2 * i] = hr;
+                        hi[2 * i + 1] = hm;
+                        lo[2 * i] = tf32_rna(mre - __uint_as_float(hr));
+                        lo[2 * i + 1] = tf32_rna(mim - __uint_as_float(hm));
                     }
+                    HOMS_ST_X8(a_hi + (uint32_t)g4 * 8u, hi);
+                    HOMS_ST_X8(a_hi + 64u + (uint32_t)g4 * 8u, lo);
                 }
-                const uint32_t a_hi = tmem + lane_base + A_COL0 + (uint32_t)as * 128u + (uint32_t)half * 32u;
-                HOMS_ST_X32(a_hi, hi);
-                HOMS_ST_X32(a_hi + 64u, lo);
                 tmem_wait_st();
                 tc_fence_before();
                 mbar_arrive(&a_full[as]);
+                // The previous generation has had a whole chunk of producer
+                // time to finish: add it into the FP64 partials now.
+                if (pend_grp >= 0 && !drain()) {
+                    dead = true;
+                    break;
+                }
+                if ((k - k0) % FLUSH == FLUSH - 1 || k + 1 == k1) {
+                    const int64_t i = k - k0;
+                    pend_grp = grp++;
+                    pend_dst = dst_piece;
+                    pend_wfirst = (i % WINDOW) == 0;
+                    pend_promote = (i % WINDOW) == WINDOW - 1 || k + 1 == k1;
+                    pend_pfirst = i < WINDOW;
+                }
             }
             if (dead) break;
-            // Epilogue for this piece.
-            const int dbuf = (int)(piece & 1);
-            const bool ok = mbar_wait(&d_full[dbuf], (uint32_t)((piece >> 1) & 1));
-            __syncwarp();
-            if (!__all_sync(0xffffffffu, ok)) {
-                if (lane == 0) atomicOr(args.err, 32u);
+            if (pend_grp >= 0 && !drain()) {
                 dead = true;
                 break;
             }
-            tc_fence_after();
-            const int ncol = n_mma / 2;
-            float *dst = args.partial + (((size_t)tile * args.maxp + slot) * TM + row) * (size_t)n_mma + half * ncol;
-            for (int cc = 0; cc < ncol; cc += 8) {
-                float v[8];
-                tmem_ld_x8(tmem + lane_base + (uint32_t)(dbuf * n_mma + half * ncol + cc), v);
-                tmem_wait_ld();
-                *reinterpret_cast<float4 *>(dst + cc) = make_float4(v[0], v[1], v[2], v[3]);
-                *reinterpret_cast<float4 *>(dst + cc + 4) = make_float4(v[4], v[5], v[6], v[7]);
-            }
-            tc_fence_before();
-            mbar_arrive(&d_empty[dbuf]);
             u += k1 - k0;
-            ++piece;
         }
     }
     tc_fence_before();
@@ -437,7 +510,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 // Sum split-K partials of each (sample, column) in piece order (FP64) and
 // write complex samples: column n < nc is Re S(j, n), nc <= n < 2nc is Im.
 template <typename T>
-__global__ void split_finalize_kernel(const float *partial, int64_t nsamples, int32_t nc, int n_mma, int maxp,
+__global__ void split_finalize_kernel(const double *partial, int64_t nsamples, int32_t nc, int n_mma, int maxp,
                                       int64_t n_chunks, int64_t G, int64_t W, cplx<T> *sig, int64_t ldsig) {
     const int64_t total = nsamples * nc;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
@@ -451,9 +524,9 @@ __global__ void split_finalize_kernel(const float *partial, int64_t nsamples, in
         const int np = (int)(last - first + 1);
         double re = 0.0, im = 0.0;
         for (int p = 0; p < np; ++p) {
-            const float *src = partial + (((size_t)tile * maxp + p) * TM + row) * (size_t)n_mma;
-            re += (double)src[c];
-            im += (double)src[nc + c];
+            const double *src = partial + (((size_t)tile * maxp + p) * TM + row) * (size_t)n_mma;
+            re += src[c];
+            im += src[nc + c];
         }
         sig[j + (int64_t)c * ldsig] = cplx<T>{T(re), T(im)};
     }
@@ -683,14 +756,16 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
     return cudaGetLastError();
 }
 
+static size_t acc_bytes(int n_mma) { return sizeof(float) * (size_t)TM * (n_mma + ACC_PAD); }
+
 static int kernel_stages(int n_mma) {
     const size_t budget = 220 * 1024;
     const size_t per = (size_t)b_bytes(n_mma) + SPIN_BYTES;
-    return (int)std::max<size_t>(2, std::min<size_t>(MAX_STAGE, (budget - 2048) / per));
+    return (int)std::max<size_t>(2, std::min<size_t>(MAX_STAGE, (budget - 2048 - acc_bytes(n_mma)) / per));
 }
 
 static size_t kernel_smem(int n_mma) {
-    return 1024 + (size_t)kernel_stages(n_mma) * (b_bytes(n_mma) + SPIN_BYTES) + 32 * 8 + 64;
+    return 1024 + (size_t)kernel_stages(n_mma) * (b_bytes(n_mma) + SPIN_BYTES) + acc_bytes(n_mma) + 32 * 8 + 64;
 }
 
 // One precession segment.
@@ -708,7 +783,7 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         *err = "internal: segment sample count mismatch";
         return cudaSuccess;
     }
-    const size_t rank_bytes = sizeof(int32_t) * (size_t)a.nt;
+    const size_t rank_bytes = (sizeof(int32_t) * (size_t)a.nt + 255) & ~size_t(255);  // keeps the pointer table aligned
     const size_t src_bytes = sizeof(void *) * 18;
     const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2);
     if ((e = grow(r.prefix, r.prefix_bytes, prefix_rows * PREFIX_STRIDE * sizeof(double))) != cudaSuccess) return e;
@@ -748,7 +823,7 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
             const int64_t l = (((t + 1) * nchunks) * G - 1) / W;
             maxp = std::max<int>(maxp, (int)(l - f + 1));
         }
-        const size_t pbytes = sizeof(float) * (size_t)tiles * maxp * TM * r.n_mma;
+        const size_t pbytes = sizeof(double) * (size_t)tiles * maxp * TM * r.n_mma;
         if ((e = grow(r.partial, r.partial_bytes, pbytes)) != cudaSuccess) return e;
         const size_t smem = kernel_smem(r.n_mma);
         if ((e = cudaFuncSetAttribute(split_precession_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
@@ -758,7 +833,7 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         ka.prefix = (const double *)r.prefix;
         ka.b_operand = (const uint8_t *)r.b_operand;
         ka.spin_table = (const double *)r.spin_table;
-        ka.partial = (float *)r.partial;
+        ka.partial = (double *)r.partial;
         ka.err = (unsigned int *)r.err;
         ka.nsamples = nsamples;
         ka.n_chunks = nchunks;
@@ -774,7 +849,7 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         const int64_t total = nsamples * r.nc;
         if (a.sizeof_T == 8)
             split_finalize_kernel<double><<<grid_for(total), 256, 0, stream>>>(
-                (const float *)r.partial, nsamples, r.nc, r.n_mma, maxp, nchunks, G, W,
+                (const double *)r.partial, nsamples, r.nc, r.n_mma, maxp, nchunks, G, W,
                 (cplx<double> *)a.sig + sample0, a.nadc);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }

@@ -332,6 +332,11 @@ def config(k: int, max_block_length=math.inf, spins_stride: int = 1) -> Workload
 
     seq = b.build(h_fn)
     if spins_stride > 1:
+        # A stride sharing a factor with a grid dimension would pick the same
+        # few columns (e.g. only the masked-out edge): move to a coprime one.
+        dims = {0: (64, 64), 1: (200, 200)}.get(k, (100, 100) if k == 2 else (200, 200))
+        while any(math.gcd(spins_stride, d) != 1 for d in dims):
+            spins_stride += 1
         sel = slice(0, None, spins_stride)
         x, y, z, rho, T1, T2, dw, csm = x[sel], y[sel], z[sel], rho[sel], T1[sel], T2[sel], dw[sel], csm[sel]
     obj = HO_Phantom(x=x, y=y, z=z, rho=rho, T1=T1, T2=T2, dw=dw, csm=csm, name=CONFIG_NAMES[k])

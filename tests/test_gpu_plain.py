@@ -128,8 +128,6 @@ def test_unit_coil_magnitude(gpu_context, precision):
     # test/gpu/test_gpu_compatibility.jl:61-123 ("pure density")
     obj = HO_Phantom(x=[0.0, 0.01, -0.02], rho=[1.0, 0.7, 0.3], T1=[math.inf] * 3, T2=[math.inf] * 3)
     seq, parts, exc, _ = W.compatibility_sequence()
-    for term in range(16):
-        seq.h[term, 2:] = (term + 1) * 1e-7
     sig = homs.simulate(obj, seq, sim_params={"sim_method": BlochHighOrder("1111"), "precision": precision},
                         parts=parts, excitation=exc)
     assert sig.shape == (5, 1, 1)
