@@ -1,30 +1,36 @@
-// Split-precision fused precession + coil contraction on tcgen05 (sm_100a).
+// Split-precision fused precession + coil contraction on sm_100a tensor cores.
 //
 // Math (one precession segment = a run of consecutive precession blocks):
-//   phase in turns   theta(s,j) = theta0(s) + sum_k b_k(s) * kappa_k(j)
-//     b_k      : the 16 solid-harmonic basis values of spin s (FP64, resident),
-//                plus b_16 = dw/(2 pi)
+//   phase in turns   theta(s,j) = sum_k b_k(s) * kappa_k(j),  k = 0..19
+//     b_0..15  : the 16 solid-harmonic basis values of spin s (FP64, resident)
+//     b_16     : dw/(2 pi)               kappa_16 = -t_j
+//     b_17     : theta0 = arg(m0)/(2 pi) kappa_17 = 1
 //     kappa_k  : -gamma * trapezoid integral of field column k from the segment
-//                start to ADC sample j (FP64 prefix table), kappa_16 = -t
+//                start to ADC sample j (FP64 prefix table, k < 16)
 //   M(s,j)   = |m0| 2^(t_j * r2(s)) * cis(2 pi theta)   (r2 = -log2(e)/T2)
 //   S(j,c)   = sum_s M(s,j) csm(s,c)                      (no conjugation)
 // This is the reference's phi = -2 pi gamma cumtrapz(dt, Bz) and
 // Mxy = M0 exp(i phi - t/T2) (src/simulation/Bloch/BlochHighOrderSimulatitonMethod.jl:76-92)
 // with the cumulative integral factored into per-spin x per-sample terms.
 //
-// Precision: theta is accumulated in FP64 (17 DFMA); one FP64 add of 1.5*2^20
-// leaves frac(theta) as a 32-bit fixed-point turn count in the low mantissa
-// word (the mod-2pi range reduction, exact to 2^-32 turn).  Quadrant select
-// plus a float32 polynomial (coefficients fitted by fit_sincos.py) give
-// cos/sin; the decay is one ex2.approx.  M is split into TF32 hi + lo and the
-// contraction runs as three TF32 MMAs (hi*hi + hi*lo + lo*hi) with FP32
-// accumulation in TMEM; split-K partials are summed in FP64.
+// Precision: theta(s,j) is a small FP64 GEMM (samples x 20) * (20 x spins),
+// computed with FP64 tensor-core MMAs (mma.sync m8n8k4.f64).  One FP64 add of
+// 1.5*2^20 leaves frac(theta) as a 32-bit fixed-point turn count in the low
+// mantissa word (the mod-2pi range reduction, exact to 2^-32 turn).  A
+// quadrant select plus float32 polynomials (coefficients fitted by
+// fit_sincos.py) give cos/sin; the decay is one ex2.approx.  M is split into
+// TF32 hi + lo and the coil contraction runs as three TF32 tcgen05 MMAs per
+// K-step (hi*lo and lo*hi first, hi*hi last) with FP32 accumulation in TMEM,
+// one accumulator generation per 32-spin chunk, drained through an FP32
+// shared-memory accumulator into FP64 split-K partials.
 //
 // Kernel organisation (one CTA per SM, persistent, stream-K over
 // (time tile of 128 samples) x (chunk of 32 spins) units):
-//   warps 0-15 producers: thread <-> sample row of the 128-row tile; compute
-//              M for 8 spins per chunk, write TF32 hi/lo to TMEM (A operand)
-//              with tcgen05.st; epilogue reads the accumulator with tcgen05.ld.
+//   warps 0-15 producers: warp w owns TMEM lane quarter w%4 (32 sample rows)
+//              and 8 spins (w/4) of each chunk; DMMA gives the phases in the
+//              m8n8 accumulator layout, which tcgen05.st.16x256b writes to
+//              TMEM rows unchanged (A operand).  The same warps drain the
+//              TMEM accumulator (tcgen05.ld.32x32b, thread <-> sample row).
 //   warp 16    MMA issuer: tcgen05.mma.kind::tf32 with A in TMEM, B (the
 //              sensitivities, pre-split) in shared memory; tcgen05.commit
 //              releases shared-memory stages, A stages and accumulators.
@@ -48,21 +54,23 @@ constexpr int TM = 128;          // samples per tile (UMMA M)
 constexpr int KC = 32;           // spins per chunk
 constexpr int KSTEPS = 8;        // (2*KC real K values) / 8 per tf32 MMA
 constexpr int MAX_STAGE = 4;     // shared-memory stages (fewer for wide N)
-constexpr int SPIN_ROWS = 20;    // k-major spin table rows per chunk
+constexpr int NTERM = 20;        // phase GEMM depth: 16 basis + dw + theta0 + 2 zero
+constexpr int SPIN_ROWS = 21;    // k-major spin table rows per chunk: b_0..b_19, packed (r2, log2|m0|)
+constexpr int SPIN_PACK = 20;
 constexpr int SPIN_BYTES = SPIN_ROWS * KC * 8;
-constexpr int PREFIX_STRIDE = 20;  // doubles per prefix row: kappa[0..16], t, pad
-constexpr int NPROD_WARPS = 16;             // 4 per TMEM lane quarter
+constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_19, t, pad
+constexpr int PREFIX_T = 20;
+constexpr int NPROD_WARPS = 16;  // 4 per TMEM lane quarter
 constexpr int MMA_WARP = 16;
 constexpr int LOAD_WARP = 17;
 constexpr int THREADS = 576;
-constexpr int SPW = KC / (NPROD_WARPS / 4);  // spins per producer warp and chunk
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t A_COL0 = 256;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
-// Chunks accumulated in one FP32 TMEM generation before it is added into the
-// FP64 partials.  The tensor core's accumulator add is not round-to-nearest:
-// its error is systematic and grows with |D| and with the number of MMAs per
-// generation, so each 32-spin chunk gets its own generation.
+// Chunks accumulated in one FP32 TMEM generation before it is drained.  The
+// tensor core's accumulator add is not round-to-nearest: its error is
+// systematic and grows with |D| and with the number of MMAs per generation,
+// so each 32-spin chunk gets its own generation.
 constexpr int FLUSH = 1;
 // Chunks summed (round to nearest, FP32) in shared memory before promotion to
 // the FP64 partials, and the row padding of that accumulator (bank spread).
@@ -74,6 +82,16 @@ constexpr float S1 = -0.16666650772094727f, S2 = 0.00833197869360447f, S3 = -0.0
 constexpr float C1 = -0.5f, C2 = 0.04166662320494652f, C3 = -0.0013886763481423259f, C4 = 2.439039235468954e-05f;
 
 __host__ __device__ inline int b_bytes(int n_mma) { return 2 * KSTEPS * n_mma * 32; }
+
+// K order of a chunk's A/B operands: the producer warp for spins 8P..8P+7
+// writes 16 columns 16P + j, where column j holds spin 8P + 2*((j%8)/2) +
+// j/8 (re for even j, im for odd j) -- the column order of
+// tcgen05.st.16x256b.x2 applied to the m8n8 accumulator fragments.
+__host__ __device__ inline void k_to_spin(int k, int &s_local, int &imag) {
+    const int P = k >> 4, r = k & 15;
+    s_local = 8 * P + 2 * ((r & 7) >> 1) + (r >> 3);
+    imag = r & 1;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -125,6 +143,14 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint32_t a, uint64_t bde
         "r"(a), "l"(bdesc), "r"(idesc), "r"(accum)
         : "memory");
 }
+// FP64 tensor-core MMA, 8x8x4: c += a * b in the m8n8k4 fragment layouts
+// (a: row groupID, col threadID_in_group; b: row threadID_in_group, col
+// groupID; c: row groupID, cols 2*threadID_in_group + {0,1}).
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
 // Round to TF32 (10 stored mantissa bits), nearest with ties away from zero:
 // add half of the 13 dropped bits to the magnitude, then clear them.
 __device__ __forceinline__ uint32_t tf32_rna(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
@@ -134,22 +160,13 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return r;
 }
 
-#define HOMS_ST_X32(taddr, v)                                                                                     \
-    asm volatile(                                                                                                 \
-        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, " \
-        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(  \
-            taddr),                                                                                               \
-        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),        \
-        "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]),           \
-        "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),          \
-        "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])                       \
-        : "memory")
-
-#define HOMS_ST_X8(taddr, v)                                                                                 \
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),  \
-                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])          \
-                 : "memory")
-
+// 16 TMEM lanes x 16 columns: thread t writes lanes t/4 and t/4+8, columns
+// 2*(t%4)+{0,1} (v[0..3]) and 8+2*(t%4)+{0,1} (v[4..7]).
+__device__ __forceinline__ void tmem_st_16x256b_x2(uint32_t taddr, const uint32_t *v) {
+    asm volatile("tcgen05.st.sync.aligned.16x256b.x2.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
 __device__ __forceinline__ void tmem_ld_x4(uint32_t taddr, float *v) {
     uint32_t r[4];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
@@ -158,16 +175,6 @@ __device__ __forceinline__ void tmem_ld_x4(uint32_t taddr, float *v) {
                  : "memory");
 #pragma unroll
     for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, float *v) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-                 : "r"(taddr)
-                 : "memory");
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -223,17 +230,17 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     const int n_mma = args.n_mma;
     const int NSTAGE = args.nstage;
     const int BB = b_bytes(n_mma);
-    uint8_t *sB = smem;                                   // NSTAGE * BB
+    uint8_t *sB = smem;                                             // NSTAGE * BB
     double *sSpin = reinterpret_cast<double *>(sB + NSTAGE * BB);  // NSTAGE * SPIN_BYTES
     float *accf = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);  // TM x (n_mma+pad)
     uint64_t *bars = reinterpret_cast<uint64_t *>(accf + (size_t)TM * (n_mma + ACC_PAD));
     uint64_t *full = bars;                    // [NSTAGE] loader -> consumers (tx)
     uint64_t *empty = bars + MAX_STAGE;       // [NSTAGE] MMA commit -> loader
     uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] producers -> MMA
-    uint64_t *a_empty = a_full + 2;        // [2] MMA commit -> producers
-    uint64_t *d_full = a_empty + 2;        // [2] MMA commit -> epilogue
-    uint64_t *d_empty = d_full + 2;        // [2] epilogue -> MMA
-    uint64_t *done = d_empty + 2;          // [1] final MMA commit
+    uint64_t *a_empty = a_full + 2;           // [2] MMA commit -> producers
+    uint64_t *d_full = a_empty + 2;           // [2] MMA commit -> drain
+    uint64_t *d_empty = d_full + 2;           // [2] drain -> MMA
+    uint64_t *done = d_empty + 2;             // [1] final MMA commit
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -295,8 +302,6 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             while (u < u1 && !dead) {
                 const int64_t k0 = u % args.n_chunks;
                 const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
-                // One accumulator generation per group of FLUSH chunks; the
-                // producers add each generation into FP64 partials.
                 int dbuf = 0;
                 uint32_t dcol = 0;
                 for (int64_t k = k0; k < k1; ++k, ++g) {
@@ -323,10 +328,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     const uint32_t sbase = smem_u32(sB + (size_t)stage * BB);
                     const uint32_t a_hi = tmem + A_COL0 + (uint32_t)as * 128u;
                     const uint32_t a_lo = a_hi + 64u;
-#pragma unroll
                     // The accumulator add of each MMA rounds relative to |D|,
                     // so the two small cross-term passes (hi*lo, lo*hi) go
                     // first, while D is small, and hi*hi last.
+#pragma unroll
                     for (int ks = 0; ks < KSTEPS; ++ks) {
                         const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * n_mma * 32));
                         const uint64_t blo = bdesc(sbase + (uint32_t)((KSTEPS + ks) * n_mma * 32));
@@ -355,18 +360,22 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         }
         __syncwarp();
     } else {
-        // Producers / epilogue: thread <-> tile row.
-        const int quarter = warp & 3, part = warp >> 2;  // TMEM lane quarter, slice of the chunk's spins
-        const int row = quarter * 32 + lane;
-        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-        const int ncol = n_mma / 4;  // accumulator columns this warp drains
+        // Producers.  Warp w: lane quarter Q (tile rows 32Q..32Q+31), spin
+        // group P (8 spins of each chunk).  DMMA fragment coordinates:
+        // gq = groupID (row / spin of a fragment), tq = threadID_in_group.
+        const int Q = warp & 3, P = warp >> 2;
+        const int gq = lane >> 2, tq = lane & 3;
+        const uint32_t lane_base = (uint32_t)(Q * 32) << 16;
+        // Accumulator drain: thread <-> tile row (32x32b), columns [P*ncol, (P+1)*ncol).
+        const int row = Q * 32 + lane;
+        const int ncol = n_mma / 4;
+        float *arow = accf + (size_t)row * (n_mma + ACC_PAD) + P * ncol;
         int64_t g = 0, grp = 0;
         int64_t u = u0;
         // Two-level drain of each chunk's accumulator generation: the FP32
         // TMEM result is added (round to nearest) into this thread's FP32 row
         // accumulator in shared memory; every WINDOW chunks, and at the end of
         // a piece, that row is promoted into the FP64 split-K partial.
-        float *arow = accf + (size_t)row * (n_mma + ACC_PAD) + part * ncol;
         int64_t pend_grp = -1;
         double *pend_dst = nullptr;
         bool pend_wfirst = false, pend_promote = false, pend_pfirst = false;
@@ -381,7 +390,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             tc_fence_after();
             for (int cc = 0; cc < ncol; cc += 4) {
                 float v[4];
-                tmem_ld_x4(tmem + lane_base + (uint32_t)(dbuf * n_mma + part * ncol + cc), v);
+                tmem_ld_x4(tmem + lane_base + (uint32_t)(dbuf * n_mma + P * ncol + cc), v);
                 tmem_wait_ld();
                 float4 a = pend_wfirst ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<float4 *>(arow + cc);
                 a.x += v[0];
@@ -411,14 +420,19 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
             const int slot = (int)(blockIdx.x - cta_of(tile * args.n_chunks, G, W));
             double *dst_piece =
-                args.partial + (((size_t)tile * args.maxp + slot) * TM + row) * (size_t)n_mma + part * ncol;
-            int64_t j = tile * TM + row;
-            if (j >= args.nsamples) j = args.nsamples - 1;
-            double kap[17];
-            const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
+                args.partial + (((size_t)tile * args.maxp + slot) * TM + row) * (size_t)n_mma + P * ncol;
+            // A fragments of the phase GEMM: kappa[row 32Q + 8mt + gq][k = 4ks + tq].
+            double ka[4][5];
+            float tj[4];
 #pragma unroll
-            for (int k = 0; k < 17; ++k) kap[k] = pr[k];
-            const float tj = (float)pr[17];
+            for (int mt = 0; mt < 4; ++mt) {
+                int64_t j = tile * TM + Q * 32 + mt * 8 + gq;
+                if (j >= args.nsamples) j = args.nsamples - 1;
+                const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
+#pragma unroll
+                for (int ks = 0; ks < 5; ++ks) ka[mt][ks] = pr[4 * ks + tq];
+                tj[mt] = (float)pr[PREFIX_T];
+            }
             for (int64_t k = k0; k < k1; ++k, ++g) {
                 const int stage = (int)(g % NSTAGE);
                 const int as = (int)(g & 1);
@@ -432,52 +446,49 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 }
                 tc_fence_after();
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                const uint32_t a_hi =
-                    tmem + lane_base + A_COL0 + (uint32_t)as * 128u + (uint32_t)part * (2u * SPW);
+                // B fragments: b[k = 4ks + tq][spin 8P + gq].
+                double bf[5];
 #pragma unroll
-                for (int g4 = 0; g4 < SPW / 4; ++g4) {
-                    const int s0 = part * SPW + g4 * 4;
-                    double th[4];
-                    {
-                        const double2 t01 = *reinterpret_cast<const double2 *>(tab + 17 * KC + s0);
-                        const double2 t23 = *reinterpret_cast<const double2 *>(tab + 17 * KC + s0 + 2);
-                        th[0] = t01.x;
-                        th[1] = t01.y;
-                        th[2] = t23.x;
-                        th[3] = t23.y;
-                    }
+                for (int ks = 0; ks < 5; ++ks) bf[ks] = tab[(4 * ks + tq) * KC + 8 * P + gq];
+                double th[4][2];
 #pragma unroll
-                    for (int kk = 0; kk < 17; ++kk) {
-                        const double2 b01 = *reinterpret_cast<const double2 *>(tab + kk * KC + s0);
-                        const double2 b23 = *reinterpret_cast<const double2 *>(tab + kk * KC + s0 + 2);
-                        th[0] = fma(b01.x, kap[kk], th[0]);
-                        th[1] = fma(b01.y, kap[kk], th[1]);
-                        th[2] = fma(b23.x, kap[kk], th[2]);
-                        th[3] = fma(b23.y, kap[kk], th[3]);
-                    }
-                    const float4 rl01 = *reinterpret_cast<const float4 *>(tab + 18 * KC + s0);
-                    const float4 rl23 = *reinterpret_cast<const float4 *>(tab + 18 * KC + s0 + 2);
-                    const float r2v[4] = {rl01.x, rl01.z, rl23.x, rl23.z};
-                    const float l2v[4] = {rl01.y, rl01.w, rl23.y, rl23.w};
-                    uint32_t hi[8], lo[8];
+                for (int mt = 0; mt < 4; ++mt) {
+                    th[mt][0] = 0.0;
+                    th[mt][1] = 0.0;
 #pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        float mre, mim;
-                        magnetisation(th[i], tj, r2v[i], l2v[i], mre, mim);
-                        const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
-                        hi[2 * i] = hr;
-                        hi[2 * i + 1] = hm;
-                        lo[2 * i] = tf32_rna(mre - __uint_as_float(hr));
-                        lo[2 * i + 1] = tf32_rna(mim - __uint_as_float(hm));
-                    }
-                    HOMS_ST_X8(a_hi + (uint32_t)g4 * 8u, hi);
-                    HOMS_ST_X8(a_hi + 64u + (uint32_t)g4 * 8u, lo);
+                    for (int ks = 0; ks < 5; ++ks) dmma_8x8x4(th[mt][0], th[mt][1], ka[mt][ks], bf[ks]);
                 }
+                // This thread's spins: 8P + 2tq + i.
+                const float4 rl = *reinterpret_cast<const float4 *>(tab + SPIN_PACK * KC + 8 * P + 2 * tq);
+                const float r2v[2] = {rl.x, rl.z};
+                const float l2v[2] = {rl.y, rl.w};
+                // 16x256b.x2 register order per pair of row tiles (mt, mt+1):
+                // [i*4 + (mt&1)*2 + comp] for spin 2tq + i.
+                uint32_t hi[2][8], lo[2][8];
+#pragma unroll
+                for (int mt = 0; mt < 4; ++mt) {
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) {
+                        float mre, mim;
+                        magnetisation(th[mt][i], tj[mt], r2v[i], l2v[i], mre, mim);
+                        const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
+                        const int e = i * 4 + (mt & 1) * 2;
+                        hi[mt >> 1][e] = hr;
+                        hi[mt >> 1][e + 1] = hm;
+                        lo[mt >> 1][e] = tf32_rna(mre - __uint_as_float(hr));
+                        lo[mt >> 1][e + 1] = tf32_rna(mim - __uint_as_float(hm));
+                    }
+                }
+                const uint32_t a_col = tmem + A_COL0 + (uint32_t)as * 128u + (uint32_t)P * 16u;
+                tmem_st_16x256b_x2(a_col + lane_base, hi[0]);
+                tmem_st_16x256b_x2(a_col + lane_base + (16u << 16), hi[1]);
+                tmem_st_16x256b_x2(a_col + 64u + lane_base, lo[0]);
+                tmem_st_16x256b_x2(a_col + 64u + lane_base + (16u << 16), lo[1]);
                 tmem_wait_st();
                 tc_fence_before();
                 mbar_arrive(&a_full[as]);
                 // The previous generation has had a whole chunk of producer
-                // time to finish: add it into the FP64 partials now.
+                // time to finish: drain it now.
                 if (pend_grp >= 0 && !drain()) {
                     dead = true;
                     break;
@@ -532,7 +543,8 @@ __global__ void split_finalize_kernel(const double *partial, int64_t nsamples, i
     }
 }
 
-// Per-spin 16-term basis (FP64), CPU expression order.
+// Per-spin 16-term basis (FP64), CPU expression order
+// (src/simulation/Bloch/BlochHighOrderSimulatitonMethod.jl:54-68).
 __global__ void basis_kernel(const double *x, const double *y, const double *z, int64_t ns, double *basis) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns; s += (int64_t)gridDim.x * blockDim.x) {
         const double X = x[s], Y = y[s], Z = z[s];
@@ -558,8 +570,10 @@ __global__ void basis_kernel(const double *x, const double *y, const double *z, 
     }
 }
 
-// Sensitivities -> TF32 hi/lo B operand in the no-swizzle K-major layout.
-// B[n][2s] = (n < nc ? Re c(s,n) : Im c(s,n-nc)), B[n][2s+1] = (n < nc ? -Im : Re).
+// Sensitivities -> TF32 hi/lo B operand in the no-swizzle K-major layout, K
+// permuted as k_to_spin.  With real K index kk of spin s:
+//   B[n][kk] = (n < nc ? Re c(s,n) : Im c(s,n-nc))   for the re column,
+//   B[n][kk] = (n < nc ? -Im c(s,n) : Re c(s,n-nc))  for the im column.
 __global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_mma, int64_t nchunks,
                                  float *out) {
     const int64_t per_chunk = (int64_t)KSTEPS * n_mma * 8;
@@ -571,9 +585,9 @@ __global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32
         const int ks = (int)(r / (n_mma * 8));
         r %= (n_mma * 8);
         const int n = (int)(r / 8), kk = (int)(r % 8);
-        const int kglob = ks * 8 + kk;
-        const int64_t s = chunk * KC + kglob / 2;
-        const bool imrow = (kglob & 1) != 0;
+        int s_local, imrow;
+        k_to_spin(ks * 8 + kk, s_local, imrow);
+        const int64_t s = chunk * KC + s_local;
         double v = 0.0;
         if (s < ns && n < 2 * nc) {
             const cplx<double> c = csm_rows[s * nc + (n < nc ? n : n - nc)];
@@ -581,11 +595,9 @@ __global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32
             else v = imrow ? c.re : c.im;
         }
         const float vf = (float)v;
-        uint32_t hb, lb;
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hb) : "f"(vf));
-        // lo carries what the FP32 hi misses of the FP64 value.
-        const float lf = (float)(v - (double)__uint_as_float(hb));
-        asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lb) : "f"(lf));
+        const uint32_t hb = tf32_rna(vf);
+        // lo carries what the TF32 hi misses of the FP64 value.
+        const uint32_t lb = tf32_rna((float)(v - (double)__uint_as_float(hb)));
         const size_t off = (size_t)(n / 8) * 256 + (size_t)(kk / 4) * 128 + (size_t)(n % 8) * 16 + (size_t)(kk % 4) * 4;
         uint8_t *base = reinterpret_cast<uint8_t *>(out) + (size_t)chunk * b_bytes(n_mma);
         *reinterpret_cast<uint32_t *>(base + (size_t)ks * n_mma * 32 + off) = hb;
@@ -593,11 +605,11 @@ __global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32
     }
 }
 
-// Spin table of a segment, from the state at its start.
-// rows 0..15: basis, 16: dw/(2 pi) (0 if dw is off in precession),
-// 17: theta0 = arg(m0)/(2 pi), 18: packed float2 (-log2(e)/T2, log2|m0|).
-// Also checks the phase range: |theta| must stay below 2^18 turns for the
-// fixed-point reduction (error bit 64 otherwise).
+// Spin table of a segment, from the state at its start (k-major per chunk):
+// rows 0..15 basis, 16 dw/(2 pi) (0 if dw is off in precession),
+// 17 theta0 = arg(m0)/(2 pi), 18..19 zero, 20 packed float2
+// (-log2(e)/T2, log2|m0|).  Also checks the phase range: |theta| must stay
+// below 2^18 turns for the fixed-point reduction (error bit 64 otherwise).
 __global__ void spin_table_kernel(const double *basis, const double *dw, const double *T2, const cplx<double> *xy,
                                   int64_t ns, int64_t nchunks, uint32_t method, const double *colmax,
                                   unsigned int *err, double *table) {
@@ -617,28 +629,30 @@ __global__ void spin_table_kernel(const double *basis, const double *dw, const d
             float2 rl;
             rl.x = (float)(-1.4426950408889634 / T2[s]);
             rl.y = mag > 0.0 ? (float)log2(mag) : -INFINITY;
-            *reinterpret_cast<float2 *>(&t[18 * KC]) = rl;
+            *reinterpret_cast<float2 *>(&t[SPIN_PACK * KC]) = rl;
         } else {
             for (int k = 0; k < 18; ++k) t[k * KC] = 0.0;
-            *reinterpret_cast<float2 *>(&t[18 * KC]) = make_float2(0.0f, -INFINITY);
+            *reinterpret_cast<float2 *>(&t[SPIN_PACK * KC]) = make_float2(0.0f, -INFINITY);
         }
+        t[18 * KC] = 0.0;
         t[19 * KC] = 0.0;
     }
 }
 
-// Prefix table of one segment: for each column k (0..15 field terms, 16 the
-// dw column, 17 time) a deterministic chunked scan of the trapezoid sums
-// (f(n)+f(n+1)) dt(n) over the segment, written at every ADC node (row =
-// sample index) and at the end node (row nsamples).
+// Prefix table of one segment.  Blocks 0..16: column k, a deterministic
+// chunked scan of the trapezoid sums (f(n)+f(n+1)) dt(n), written at every
+// ADC node (row = sample index) and at the end node (row nsamples), plus the
+// column's largest |value| at row nsamples+1.  Block 17: elapsed time t
+// (entry PREFIX_T) and the constant columns 17 (= 1) and 18, 19 (= 0).
 __global__ void prefix_kernel(const double *dt, const double *const *src, const uint8_t *adc, const int32_t *rank,
-                              int64_t n_lo, int64_t n_hi, int64_t nsamples, double gamma, uint32_t method,
-                              double *prefix) {
+                              int64_t n_lo, int64_t n_hi, int64_t nsamples, double gamma, double *prefix) {
     __shared__ double part[256];
     const int col = blockIdx.x;
-    const double *f = src[col];  // nullptr: zero column; (double*)1: constant one
+    const double *f = col < 17 ? src[col] : reinterpret_cast<const double *>(1);  // nullptr: zero; 1: constant one
     const bool one = f == reinterpret_cast<const double *>(1);
     const bool zero = f == nullptr;
     const double scale = col < 16 ? -gamma * 0.5 : (col == 16 ? -0.5 : 0.5);
+    const int out_col = col < 17 ? col : PREFIX_T;
     const int64_t nint = n_hi - n_lo;
     const int64_t per = (nint + blockDim.x - 1) / blockDim.x;
     const int64_t i0 = min(nint, per * threadIdx.x), i1 = min(nint, i0 + per);
@@ -666,15 +680,39 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
         const double term = zero ? 0.0 : (one ? 2.0 : (f[n] + f[n + 1])) * dt[n];
         cum += term;
         peak = fmax(peak, fabs(scale * cum));
-        if (adc[n + 1]) prefix[(size_t)rank[n + 1] * PREFIX_STRIDE + col] = scale * cum;
-        if (n + 1 == n_hi) prefix[(size_t)nsamples * PREFIX_STRIDE + col] = scale * cum;
+        if (adc[n + 1]) {
+            double *pr = prefix + (size_t)rank[n + 1] * PREFIX_STRIDE;
+            pr[out_col] = scale * cum;
+            if (col == 17) {
+                pr[17] = 1.0;
+                pr[18] = 0.0;
+                pr[19] = 0.0;
+            }
+        }
+        if (n + 1 == n_hi) {
+            double *pr = prefix + (size_t)nsamples * PREFIX_STRIDE;
+            pr[out_col] = scale * cum;
+            if (col == 17) {
+                pr[17] = 1.0;
+                pr[18] = 0.0;
+                pr[19] = 0.0;
+            }
+        }
     }
-    if (nint == 0 && threadIdx.x == 0) prefix[(size_t)nsamples * PREFIX_STRIDE + col] = 0.0;
+    if (nint == 0 && threadIdx.x == 0) {
+        double *pr = prefix + (size_t)nsamples * PREFIX_STRIDE;
+        pr[out_col] = 0.0;
+        if (col == 17) {
+            pr[17] = 1.0;
+            pr[18] = 0.0;
+            pr[19] = 0.0;
+        }
+    }
     // Largest |kappa| of the column (row nsamples+1) for the phase-range check.
     __syncthreads();
     part[threadIdx.x] = peak;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && col < 17) {
         double mx = 0.0;
         for (int i = 0; i < (int)blockDim.x; ++i) mx = fmax(mx, part[i]);
         prefix[(size_t)(nsamples + 1) * PREFIX_STRIDE + col] = mx;
@@ -689,7 +727,7 @@ __global__ void state_update_kernel(const double *table, const double *endrow, c
         const double *t = table + (s / KC) * (SPIN_ROWS * KC) + (s % KC);
         double th = t[17 * KC];
         for (int k = 0; k < 17; ++k) th = fma(t[k * KC], endrow[k], th);
-        const double T = endrow[17];
+        const double T = endrow[PREFIX_T];
         const cplx<double> m0 = xy[s];
         const double mag = hypot(m0.re, m0.im);
         const double f = th - rint(th);
@@ -784,12 +822,12 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         return cudaSuccess;
     }
     const size_t rank_bytes = (sizeof(int32_t) * (size_t)a.nt + 255) & ~size_t(255);  // keeps the pointer table aligned
-    const size_t src_bytes = sizeof(void *) * 18;
+    const size_t src_bytes = sizeof(void *) * 17;
     const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2);
     if ((e = grow(r.prefix, r.prefix_bytes, prefix_rows * PREFIX_STRIDE * sizeof(double))) != cudaSuccess) return e;
     if ((e = grow(r.tvec, r.tvec_bytes, rank_bytes + src_bytes)) != cudaSuccess) return e;
     if ((e = grow(r.spin_table, r.spin_bytes, (size_t)nchunks * SPIN_BYTES)) != cudaSuccess) return e;
-    const double *src[18];
+    const double *src[17];
     const uint32_t m = a.method;
     src[0] = (m & HOMS_HO0) ? (const double *)a.h[0] : nullptr;
     for (int k = 1; k <= 3; ++k)
@@ -797,7 +835,6 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
     for (int k = 4; k <= 8; ++k) src[k] = (m & HOMS_HO2) ? (const double *)a.h[k] : nullptr;
     for (int k = 9; k <= 15; ++k) src[k] = (m & HOMS_HO3) ? (const double *)a.h[k] : nullptr;
     src[16] = (m & HOMS_DW_PRECESSION) ? reinterpret_cast<const double *>(1) : nullptr;
-    src[17] = reinterpret_cast<const double *>(1);
     uint8_t *tv = (uint8_t *)r.tvec;
     if ((e = cudaMemcpyAsync(tv, rank.data(), rank_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(tv + rank_bytes, src, src_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
@@ -805,7 +842,7 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(tv + rank_bytes),
                                           (const uint8_t *)a.adc, reinterpret_cast<const int32_t *>(tv), n_lo, n_hi,
-                                          nsamples, a.gamma, m, (double *)r.prefix);
+                                          nsamples, a.gamma, (double *)r.prefix);
     spin_table_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>(
         (const double *)r.basis, (const double *)a.dw, (const double *)a.T2, (const cplx<double> *)a.xy, r.ns, nchunks,
         m, (const double *)r.prefix + (size_t)(nsamples + 1) * PREFIX_STRIDE, (unsigned int *)r.err,
