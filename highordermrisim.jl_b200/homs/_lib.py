@@ -25,7 +25,7 @@ EXPORTED = [
     "homs_abi_version", "homs_status_string", "homs_context_create", "homs_context_destroy", "homs_last_error",
     "homs_synchronize", "homs_precession_block", "homs_excitation_block", "homs_coil_reduce", "homs_simulate",
     "homs_count_adc", "homs_plan_create", "homs_plan_run", "homs_plan_device_bytes", "homs_plan_timing",
-    "homs_plan_destroy",
+    "homs_plan_destroy", "homs_coil_reduce_noalloc",
 ]
 
 
@@ -103,6 +103,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_plan_device_bytes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
         "homs_plan_timing": (ctypes.c_int, [vp, ctypes.POINTER(Timing)]),
         "homs_plan_destroy": (ctypes.c_int, [vp]),
+        "homs_coil_reduce_noalloc": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i32, vp, i64, vp, i64, vp, i64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -158,6 +158,23 @@ homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins
                              const void *states, int64_t ldstates, const void *csm, int64_t ldcsm, void *sig,
                              int64_t ldsig);
 
+/* homs_coil_reduce without a context and without any device allocation; it has
+ * no counterpart in the reference.  It is for callers that may not allocate
+ * once running: a host whose own pooled allocator owns and budgets all device
+ * memory (CUDA.jl's, PyTorch's), or a service loop where a cudaMalloc would
+ * synchronise the device.  The split-K partials live in a fixed 16 MiB device
+ * array inside this library (one per GPU, kept until the process exits), so
+ * 16 * ceil(nspins/256) * nadc * ncoils bytes (8 * ... for f32) must fit in
+ * 16 MiB and nadc may be at most 524280; larger requests return HOMS_EINVAL.
+ * `stream` is a cudaStream_t on the current device (NULL = default stream);
+ * the call only enqueues work.  Calls on the same device share that array, so
+ * two calls whose work can overlap on the GPU (other streams, other host
+ * threads) race: order them on one stream.  The first call on each device
+ * resolves the array's address; make it before any stream capture. */
+homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, int64_t nspins, int64_t nadc, int32_t ncoils,
+                                     const void *states, int64_t ldstates, const void *csm, int64_t ldcsm, void *sig,
+                                     int64_t ldsig);
+
 /* ---- whole simulation ---------------------------------------------------------- */
 
 /* Run every block of `seq` on `phantom` (host or device arrays).
