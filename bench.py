@@ -139,35 +139,45 @@ def cpu_baseline(seconds_target=15.0, threads=None):
     orc.build()
     if threads is None:
         threads = max(1, len(os.sched_getaffinity(0)))
-    probe = _workload(stride=4000)
-    flags = BlochHighOrder(probe.mask).flags
-    t0 = time.perf_counter()
-    orc.simulate_c(probe.obj, probe.seq, probe.parts, probe.excitation, flags, nthreads=threads)
-    rate = _units(probe) / max(time.perf_counter() - t0, 1e-3)
-    full = 350000 * 38000 * 32
-    stride = int(max(1, min(4000, full / max(rate * seconds_target, 1.0))))
-    w = _workload(stride=stride)
-    t0 = time.perf_counter()
-    orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)
-    dt = time.perf_counter() - t0
+    # The oracle's cost is linear in the spin count; grow the subsample until
+    # one run takes at least a third of the target time.
+    stride = 400
+    while True:
+        w = _workload(stride=stride)
+        flags = BlochHighOrder(w.mask).flags
+        t0 = time.perf_counter()
+        orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)
+        dt = time.perf_counter() - t0
+        if dt >= seconds_target / 3 or stride == 1:
+            break
+        stride = max(1, int(stride * dt / seconds_target))
     return {"value": _units(w) / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"every {stride}th spin ({len(w.obj)} spins) x 38000 samples x 32 coils, full sequence, "
-                      f"{dt:.1f} s"}, dt
+                      f"{dt:.1f} s"}, stride
 
 
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return 0
-    base, _ = cpu_baseline(seconds_target=max(5.0, 20.0 / max(args.steps, 1)))
+    from homs.model import BlochHighOrder
+    from oracle import oracle as orc
+    # Calibrate a spin subsample of a few seconds per step, then time each
+    # step on that same subsample.
+    base, stride = cpu_baseline(seconds_target=max(3.0, 30.0 / max(args.steps + args.warmup, 1)))
+    w = _workload(stride=stride)
+    flags = BlochHighOrder(w.mask).flags
+    threads = base["cores"]
     vals = []
-    for _ in range(args.warmup):
-        cpu_baseline(seconds_target=2.0)
-    for _ in range(args.steps):
-        b, _ = cpu_baseline(seconds_target=max(5.0, 20.0 / max(args.steps, 1)))
-        vals.append(b["value"])
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)
+        if i >= args.warmup:
+            vals.append(_units(w) / (time.perf_counter() - t0))
     v = statistics.median(vals)
     base["value"] = v
+    base["sample"] = f"every {stride}th spin ({len(w.obj)} spins) x 38000 samples x 32 coils per step, median of " \
+                     f"{args.steps} steps"
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": _units(_workload(1)) / v * 1e3 if v else None, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -194,7 +204,7 @@ def run_homs(args):
     stream = torch.cuda.current_stream()
     ctx = _lib.Context(local, stream.cuda_stream)
     lib = _lib.load()
-    w = _workload()
+    w = _workload(args.spin_stride)
     units = _units(w)
     method = BlochHighOrder(w.mask)
     params = {"sim_method": method, "precision": "f64", "homs_precision": args.mode}
@@ -313,7 +323,8 @@ def run_homs(args):
            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64 phase / f32 trig / tf32x3 tensor" if args.mode == "split" else "f64",
            "data": "synthetic",
-           "config": {"workload": "3d_stack_of_spirals_100x100x35_350000spins_32coils_4x9500adc", "spins": len(w.obj),
+           "config": {"workload": "3d_stack_of_spirals_100x100x35_350000spins_32coils_4x9500adc" +
+                                  (f"_every{args.spin_stride}thspin" if args.spin_stride > 1 else ""), "spins": len(w.obj),
                       "samples": nadc, "coils": nc, "mask": w.mask, "mode": args.mode,
                       "l2": "inputs larger than L2 (split operand 358 MB, csm 179 MB)", "parallelism": f"replicas{ws}"},
            "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
@@ -340,6 +351,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="homs", choices=["homs", "reference"])
     ap.add_argument("--mode", default="split", choices=["split", "plain"])
+    ap.add_argument("--spin-stride", type=int, default=1,
+                    help="run every k-th spin of the workload (small cases for profiling; bench lines use 1)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -26,15 +26,17 @@
 //
 // Kernel organisation (one CTA per SM, persistent, stream-K over
 // (time tile of 128 samples) x (chunk of 32 spins) units):
-//   warps 0-15 producers: warp w owns TMEM lane quarter w%4 (32 sample rows)
-//              and 8 spins (w/4) of each chunk; DMMA gives the phases in the
-//              m8n8 accumulator layout, which tcgen05.st.16x256b writes to
-//              TMEM rows unchanged (A operand).  The same warps drain the
-//              TMEM accumulator (tcgen05.ld.32x32b, thread <-> sample row).
-//   warp 16    MMA issuer: tcgen05.mma.kind::tf32 with A in TMEM, B (the
+//   warps 0-7  producers: warp w owns 16 sample rows of TMEM lane quarter
+//              w%4 and all 32 spins of each chunk; DMMA gives the phases in
+//              the m8n8 accumulator layout, which tcgen05.st.16x256b writes
+//              to TMEM rows unchanged (A operand).  The DMMAs of chunk k+1
+//              are issued between the FP32 steps of chunk k.  The same warps
+//              drain the TMEM accumulator (tcgen05.ld.32x32b, thread <->
+//              sample row).
+//   warp 8     MMA issuer: tcgen05.mma.kind::tf32 with A in TMEM, B (the
 //              sensitivities, pre-split) in shared memory; tcgen05.commit
 //              releases shared-memory stages, A stages and accumulators.
-//   warp 17    loader: cp.async.bulk of each chunk's B operand and spin table.
+//   warp 9     loader: cp.async.bulk of each chunk's B operand and spin table.
 // Every wait is bounded: on time-out the kernel records the place in a device
 // error word and returns without hanging the GPU.
 #include <algorithm>
@@ -56,22 +58,21 @@ constexpr int KSTEPS = 8;        // (2*KC real K values) / 8 per tf32 MMA
 constexpr int MAX_STAGE = 4;     // shared-memory stages (fewer for wide N)
 constexpr int NTERM = 20;        // phase GEMM depth: 16 basis + dw + theta0 + 2 zero
 constexpr int SPIN_ROWS = 21;    // k-major spin table rows per chunk: b_0..b_19, packed (r2, log2|m0|)
-constexpr int SPIN_PACK = 20;
 constexpr int SPIN_BYTES = SPIN_ROWS * KC * 8;
 constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_19, t, pad
 constexpr int PREFIX_T = 20;
-constexpr int NPROD_WARPS = 16;  // 4 per TMEM lane quarter
-constexpr int MMA_WARP = 16;
-constexpr int LOAD_WARP = 17;
-constexpr int THREADS = 576;
+// 8 producer warps (2 per TMEM lane quarter) + MMA issuer + loader: at most 3
+// warps per SM sub-partition, which leaves 168 registers per thread.
+constexpr int NPROD_WARPS = 8;
+constexpr int MMA_WARP = 8;
+constexpr int LOAD_WARP = 9;
+constexpr int THREADS = 320;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t A_COL0 = 256;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
-// Chunks accumulated in one FP32 TMEM generation before it is drained.  The
-// tensor core's accumulator add is not round-to-nearest: its error is
-// systematic and grows with |D| and with the number of MMAs per generation,
-// so each 32-spin chunk gets its own generation.
-constexpr int FLUSH = 1;
+// Each 32-spin chunk is its own FP32 TMEM accumulator generation: the tensor
+// core's accumulator add is not round-to-nearest, and its error is systematic
+// and grows with |D| and with the number of MMAs per generation.
 // Chunks summed (round to nearest, FP32) in shared memory before promotion to
 // the FP64 partials, and the row padding of that accumulator (bank spread).
 constexpr int WINDOW = 32;
@@ -81,12 +82,19 @@ constexpr int ACC_PAD = 4;
 constexpr float S1 = -0.16666650772094727f, S2 = 0.00833197869360447f, S3 = -0.00019495606829877943f;
 constexpr float C1 = -0.5f, C2 = 0.04166662320494652f, C3 = -0.0013886763481423259f, C4 = 2.439039235468954e-05f;
 
-__host__ __device__ inline int b_bytes(int n_mma) { return 2 * KSTEPS * n_mma * 32; }
+__host__ __device__ constexpr int b_bytes(int n_mma) { return 2 * KSTEPS * n_mma * 32; }
 
-// K order of a chunk's A/B operands: the producer warp for spins 8P..8P+7
-// writes 16 columns 16P + j, where column j holds spin 8P + 2*((j%8)/2) +
-// j/8 (re for even j, im for odd j) -- the column order of
-// tcgen05.st.16x256b.x2 applied to the m8n8 accumulator fragments.
+// Spin table of a chunk, in doubles: phase row k (0..19) of local spin s at
+// ((k/4)*KC + s)*4 + k%4, so that one DMMA B fragment (k = 4ks + tq, spin
+// base + gq) is 32 consecutive doubles; then one packed float2
+// (-log2(e)/T2, log2|m0|) per spin.
+__host__ __device__ inline int tab_index(int k, int s) { return (((k >> 2) * KC + s) << 2) + (k & 3); }
+constexpr int TAB_PACK = NTERM * KC;
+
+// K order of a chunk's A/B operands: spins 8P..8P+7 (one DMMA n-tile) fill
+// the 16 columns 16P + j, where column j holds spin 8P + 2*((j%8)/2) + j/8
+// (re for even j, im for odd j) -- the column order of tcgen05.st.16x256b.x2
+// applied to the m8n8 accumulator fragments.
 __host__ __device__ inline void k_to_spin(int k, int &s_local, int &imag) {
     const int P = k >> 4, r = k & 15;
     s_local = 8 * P + 2 * ((r & 7) >> 1) + (r >> 3);
@@ -167,14 +175,27 @@ __device__ __forceinline__ void tmem_st_16x256b_x2(uint32_t taddr, const uint32_
                  "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld_x4(uint32_t taddr, float *v) {
-    uint32_t r[4];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+// 32 TMEM lanes (thread <-> lane) x 8 or 16 consecutive columns.
+__device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, float *v) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
                  : "r"(taddr)
                  : "memory");
 #pragma unroll
-    for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_ld_x16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -187,53 +208,85 @@ __device__ __forceinline__ uint64_t bdesc(uint32_t saddr) {
            (1ull << 46);
 }
 
+// Work items of one launch.  The (tile x chunk) grid is cut into `slabs`
+// ranges of chunks; item i is slab z = i / tiles of tile i % tiles, and CTA b
+// takes items b, b + G, b + 2G, ...  The CTAs running at any one time thus
+// read the chunks of two or three consecutive slabs, which stay in L2 for
+// every tile that needs them.  Item (tile, z) owns partial slot z.
 struct KernelArgs {
     const double *prefix;      // [rows][PREFIX_STRIDE]
     const uint8_t *b_operand;  // [nchunks][b_bytes]
-    const double *spin_table;  // [nchunks][SPIN_ROWS][KC]
-    double *partial;           // [tiles][maxp][TM][n_mma], FP64 split-K partials
+    const double *spin_table;  // [nchunks][SPIN_ROWS * KC]
+    double *partial;           // [tiles][slabs][TM][n_mma], FP64 split-K partials
     unsigned int *err;
     int64_t nsamples;
-    int64_t n_chunks;
-    int64_t tiles;
-    int maxp;
-    int n_mma;
+    int n_chunks;
+    int tiles;
+    int slabs;
     int nstage;
 };
 
-__device__ __forceinline__ int64_t cta_of(int64_t L, int64_t G, int64_t W) { return ((L + 1) * G - 1) / W; }
+struct Item {
+    int tile, z, c0, c1;
+};
+__device__ __forceinline__ Item item_of(const KernelArgs &a, int i) {
+    Item it;
+    it.z = i / a.tiles;
+    it.tile = i - it.z * a.tiles;
+    it.c0 = (int)((int64_t)a.n_chunks * it.z / a.slabs);
+    it.c1 = (int)((int64_t)a.n_chunks * (it.z + 1) / a.slabs);
+    return it;
+}
 
 // M(s,j) for one spin given the FP64 turn count; returns (re, im).
 __device__ __forceinline__ void magnetisation(double th, float tj, float r2, float l2m0, float &mre, float &mim) {
     const double g = th + 1572864.0;  // 1.5 * 2^20: frac(th) * 2^32 lands in the low word
     const uint32_t u = (uint32_t)__double2loint(g);
+    // u = q' 2^30 + r: quadrant q = nearest quarter turn = (u + 2^29) >> 30, and
+    // (int)(u << 2) = 4 * (r as a signed 30-bit offset from it), in [-2^31, 2^31).
     const uint32_t v = u + 0x20000000u;
-    const uint32_t q = v >> 30;
-    const int32_t rr = (int32_t)(v & 0x3FFFFFFFu) - 0x20000000;
-    const float x = (float)rr * 1.4629180792671596e-09f;  // 2 pi / 2^32
+    const float x = (float)(int32_t)(u << 2) * 3.6572951981678990e-10f;  // 2 pi / 2^34
     const float x2 = x * x;
     const float sp = fmaf(x * x2, fmaf(x2, fmaf(x2, S3, S2), S1), x);
     const float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, C4, C3), C2), C1), 1.0f);
-    // cis(x + q*pi/2): swap for odd q, negate cos for q in {1,2}, sin for q in {2,3}.
-    const bool swap = (q & 1u) != 0;
-    const uint32_t cbits = __float_as_uint(swap ? sp : cp) ^ ((((q + 1u) >> 1) & 1u) << 31);
-    const uint32_t sbits = __float_as_uint(swap ? cp : sp) ^ ((q >> 1) << 31);
+    // cis(x + q*pi/2): swap for odd q (bit 30 of v), negate cos for q in {1,2}
+    // (bit 31 of v + 2^30), negate sin for q in {2,3} (bit 31 of v).
+    const bool swap = (v & 0x40000000u) != 0;
+    const uint32_t cbits = __float_as_uint(swap ? sp : cp) ^ ((v + 0x40000000u) & 0x80000000u);
+    const uint32_t sbits = __float_as_uint(swap ? cp : sp) ^ (v & 0x80000000u);
     const float c = __uint_as_float(cbits), s = __uint_as_float(sbits);
     const float a = ex2_approx(fmaf(tj, r2, l2m0));
     mre = a * c;
     mim = a * s;
 }
 
+// Phases of one chunk for a producer thread: th[mt][nt][i] of spin
+// 8nt + 2tq + i at tile row 8mt + gq (rows relative to the warp's 16).
+__device__ __forceinline__ void chunk_phases(double (&th)[2][4][2], const double (&ka)[2][5], const double *tab,
+                                             int gq, int tq, int nt) {
+    double bf[5];
+#pragma unroll
+    for (int ks = 0; ks < 5; ++ks) bf[ks] = tab[tab_index(4 * ks + tq, 8 * nt + gq)];
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt) {
+        th[mt][nt][0] = 0.0;
+        th[mt][nt][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < 5; ++ks) dmma_8x8x4(th[mt][nt][0], th[mt][nt][1], ka[mt][ks], bf[ks]);
+    }
+}
+
+template <int N_MMA>
 __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
+    constexpr int BB = b_bytes(N_MMA);
+    constexpr int NCOL = N_MMA / 2;  // accumulator columns drained per producer thread
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-    const int n_mma = args.n_mma;
     const int NSTAGE = args.nstage;
-    const int BB = b_bytes(n_mma);
     uint8_t *sB = smem;                                             // NSTAGE * BB
     double *sSpin = reinterpret_cast<double *>(sB + NSTAGE * BB);  // NSTAGE * SPIN_BYTES
-    float *accf = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);  // TM x (n_mma+pad)
-    uint64_t *bars = reinterpret_cast<uint64_t *>(accf + (size_t)TM * (n_mma + ACC_PAD));
+    float *accf = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);  // TM x (N_MMA+pad)
+    uint64_t *bars = reinterpret_cast<uint64_t *>(accf + (size_t)TM * (N_MMA + ACC_PAD));
     uint64_t *full = bars;                    // [NSTAGE] loader -> consumers (tx)
     uint64_t *empty = bars + MAX_STAGE;       // [NSTAGE] MMA commit -> loader
     uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] producers -> MMA
@@ -250,10 +303,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             mbar_init(&empty[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
-            mbar_init(&a_full[i], NPROD_WARPS * 32);
+            mbar_init(&a_full[i], NPROD_WARPS);  // one elected arrive per producer warp
             mbar_init(&a_empty[i], 1);
             mbar_init(&d_full[i], 1);
-            mbar_init(&d_empty[i], NPROD_WARPS * 32);
+            mbar_init(&d_empty[i], NPROD_WARPS);
         }
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -269,90 +322,85 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    const int64_t G = gridDim.x;
-    const int64_t W = args.tiles * args.n_chunks;
-    const int64_t u0 = W * (int64_t)blockIdx.x / G, u1 = W * ((int64_t)blockIdx.x + 1) / G;
+    const int n_items = args.tiles * args.slabs;
+    const int G = (int)gridDim.x;
     bool dead = false;
 
     if (warp == LOAD_WARP) {
         if (lane == 0) {
-            int64_t g = 0;
-            for (int64_t u = u0; u < u1 && !dead; ++u, ++g) {
-                const int64_t chunk = u % args.n_chunks;
-                const int stage = (int)(g % NSTAGE);
-                if (!mbar_wait(&empty[stage], (uint32_t)(((g / NSTAGE) + 1) & 1))) {
-                    atomicOr(args.err, 1u);
-                    dead = true;
-                    break;
+            int stage = 0;
+            uint32_t eph = 1;  // parity of empty[stage] that frees it (the first pass is free)
+            for (int i = blockIdx.x; i < n_items && !dead; i += G) {
+                const Item it = item_of(args, i);
+                for (int c = it.c0; c < it.c1; ++c) {
+                    if (!mbar_wait(&empty[stage], eph)) {
+                        atomicOr(args.err, 1u);
+                        dead = true;
+                        break;
+                    }
+                    mbar_expect_tx(&full[stage], (uint32_t)(BB + SPIN_BYTES));
+                    bulk_g2s(sB + (size_t)stage * BB, args.b_operand + (size_t)c * BB, (uint32_t)BB, &full[stage]);
+                    bulk_g2s(reinterpret_cast<uint8_t *>(sSpin) + (size_t)stage * SPIN_BYTES,
+                             reinterpret_cast<const uint8_t *>(args.spin_table) + (size_t)c * SPIN_BYTES,
+                             (uint32_t)SPIN_BYTES, &full[stage]);
+                    if (++stage == NSTAGE) {
+                        stage = 0;
+                        eph ^= 1u;
+                    }
                 }
-                mbar_expect_tx(&full[stage], (uint32_t)(BB + SPIN_BYTES));
-                bulk_g2s(sB + (size_t)stage * BB, args.b_operand + (size_t)chunk * BB, (uint32_t)BB, &full[stage]);
-                bulk_g2s(reinterpret_cast<uint8_t *>(sSpin) + (size_t)stage * SPIN_BYTES,
-                         reinterpret_cast<const uint8_t *>(args.spin_table) + (size_t)chunk * SPIN_BYTES,
-                         (uint32_t)SPIN_BYTES, &full[stage]);
             }
         }
         __syncwarp();
     } else if (warp == MMA_WARP) {
         if (lane == 0) {
-            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n_mma >> 3) << 17) |
-                                   ((uint32_t)(TM >> 4) << 24);
-            int64_t g = 0, grp = 0;
-            int64_t u = u0;
-            while (u < u1 && !dead) {
-                const int64_t k0 = u % args.n_chunks;
-                const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
-                int dbuf = 0;
-                uint32_t dcol = 0;
-                for (int64_t k = k0; k < k1; ++k, ++g) {
-                    const bool gstart = ((k - k0) % FLUSH) == 0;
-                    if (gstart) {
-                        dbuf = (int)(grp & 1);
-                        if (!mbar_wait(&d_empty[dbuf], (uint32_t)(((grp >> 1) + 1) & 1))) {
-                            atomicOr(args.err, 2u);
-                            dead = true;
-                            break;
-                        }
-                        tc_fence_after();
-                        dcol = tmem + (uint32_t)(dbuf * n_mma);
+            constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N_MMA >> 3) << 17) |
+                                       ((uint32_t)(TM >> 4) << 24);
+            int g = 0;  // chunks issued; chunk g uses A buffer and accumulator g % 2
+            int stage = 0;
+            uint32_t fph = 0;  // parity of full[stage] for chunk g
+            for (int i = blockIdx.x; i < n_items && !dead; i += G) {
+                const Item it = item_of(args, i);
+                for (int c = it.c0; c < it.c1; ++c, ++g) {
+                    const int buf = g & 1;
+                    if (!mbar_wait(&d_empty[buf], (uint32_t)(((g >> 1) + 1) & 1))) {
+                        atomicOr(args.err, 2u);
+                        dead = true;
+                        break;
                     }
-                    const int stage = (int)(g % NSTAGE);
-                    const int as = (int)(g & 1);
-                    if (!mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1)) ||
-                        !mbar_wait(&a_full[as], (uint32_t)((g >> 1) & 1))) {
+                    if (!mbar_wait(&full[stage], fph) || !mbar_wait(&a_full[buf], (uint32_t)((g >> 1) & 1))) {
                         atomicOr(args.err, 4u);
                         dead = true;
                         break;
                     }
                     tc_fence_after();
+                    const uint32_t dcol = tmem + (uint32_t)(buf * N_MMA);
                     const uint32_t sbase = smem_u32(sB + (size_t)stage * BB);
-                    const uint32_t a_hi = tmem + A_COL0 + (uint32_t)as * 128u;
+                    const uint32_t a_hi = tmem + A_COL0 + (uint32_t)buf * 128u;
                     const uint32_t a_lo = a_hi + 64u;
-                    // The accumulator add of each MMA rounds relative to |D|,
-                    // so the two small cross-term passes (hi*lo, lo*hi) go
-                    // first, while D is small, and hi*hi last.
+                    // Each chunk is its own accumulator generation.  The
+                    // accumulator add of each MMA rounds relative to |D|, so the
+                    // two small cross-term passes (hi*lo, lo*hi) go first, while
+                    // D is small, and hi*hi last.
 #pragma unroll
                     for (int ks = 0; ks < KSTEPS; ++ks) {
-                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * n_mma * 32));
-                        const uint64_t blo = bdesc(sbase + (uint32_t)((KSTEPS + ks) * n_mma * 32));
-                        const uint32_t first = (gstart && ks == 0) ? 0u : 1u;
-                        tc_mma_tf32(dcol, a_hi + ks * 8, blo, idesc, first);
+                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * N_MMA * 32));
+                        const uint64_t blo = bdesc(sbase + (uint32_t)((KSTEPS + ks) * N_MMA * 32));
+                        tc_mma_tf32(dcol, a_hi + ks * 8, blo, idesc, ks == 0 ? 0u : 1u);
                         tc_mma_tf32(dcol, a_lo + ks * 8, bhi, idesc, 1u);
                     }
 #pragma unroll
                     for (int ks = 0; ks < KSTEPS; ++ks) {
-                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * n_mma * 32));
+                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * N_MMA * 32));
                         tc_mma_tf32(dcol, a_hi + ks * 8, bhi, idesc, 1u);
                     }
                     tc_commit(&empty[stage]);
-                    tc_commit(&a_empty[as]);
-                    if ((k - k0) % FLUSH == FLUSH - 1 || k + 1 == k1) {
-                        tc_commit(&d_full[dbuf]);
-                        ++grp;
+                    tc_commit(&a_empty[buf]);
+                    tc_commit(&d_full[buf]);
+                    if (++stage == NSTAGE) {
+                        stage = 0;
+                        fph ^= 1u;
                     }
                 }
-                if (dead) break;
-                u += k1 - k0;
             }
             // Drain: wait for every issued MMA before TMEM is released.
             tc_commit(done);
@@ -360,49 +408,69 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         }
         __syncwarp();
     } else {
-        // Producers.  Warp w: lane quarter Q (tile rows 32Q..32Q+31), spin
-        // group P (8 spins of each chunk).  DMMA fragment coordinates:
-        // gq = groupID (row / spin of a fragment), tq = threadID_in_group.
-        const int Q = warp & 3, P = warp >> 2;
+        // Producers.  Warp w works in TMEM lane quarter Q = w % 4 (tile rows
+        // 32Q..32Q+31) with half H = w / 4.  For the phase/magnetisation tile
+        // it takes rows 32Q + 16H .. +15 and all 32 spins of each chunk: 2 x 4
+        // DMMA 8x8 tiles (gq = groupID, tq = threadID_in_group).  For the
+        // accumulator drain it takes thread <-> tile row 32Q + lane and
+        // column half H.
+        const int Q = warp & 3, H = warp >> 2;
         const int gq = lane >> 2, tq = lane & 3;
-        const uint32_t lane_base = (uint32_t)(Q * 32) << 16;
-        // Accumulator drain: thread <-> tile row (32x32b), columns [P*ncol, (P+1)*ncol).
+        const uint32_t q_base = (uint32_t)(Q * 32) << 16;
+        const uint32_t a_lane = (uint32_t)(Q * 32 + H * 16) << 16;
         const int row = Q * 32 + lane;
-        const int ncol = n_mma / 4;
-        float *arow = accf + (size_t)row * (n_mma + ACC_PAD) + P * ncol;
-        int64_t g = 0, grp = 0;
-        int64_t u = u0;
+        float *arow = accf + (size_t)row * (N_MMA + ACC_PAD) + H * NCOL;
+        int g = 0;  // chunks produced by this CTA
+        int stage = 0;
+        uint32_t fph = 0;  // parity of full[stage] for chunk g
         // Two-level drain of each chunk's accumulator generation: the FP32
         // TMEM result is added (round to nearest) into this thread's FP32 row
         // accumulator in shared memory; every WINDOW chunks, and at the end of
-        // a piece, that row is promoted into the FP64 split-K partial.
-        int64_t pend_grp = -1;
+        // an item, that row is promoted into the FP64 split-K partial.  The
+        // drain of chunk g runs after the A operand of chunk g+1 is written.
+        int pend = -1;  // chunk whose accumulator waits to be drained
         double *pend_dst = nullptr;
         bool pend_wfirst = false, pend_promote = false, pend_pfirst = false;
         auto drain = [&]() -> bool {
-            const int dbuf = (int)(pend_grp & 1);
-            const bool ok = mbar_wait(&d_full[dbuf], (uint32_t)((pend_grp >> 1) & 1));
+            const int buf = pend & 1;
+            const bool ok = mbar_wait(&d_full[buf], (uint32_t)((pend >> 1) & 1));
             __syncwarp();
             if (!__all_sync(0xffffffffu, ok)) {
                 if (lane == 0) atomicOr(args.err, 32u);
                 return false;
             }
             tc_fence_after();
-            for (int cc = 0; cc < ncol; cc += 4) {
-                float v[4];
-                tmem_ld_x4(tmem + lane_base + (uint32_t)(dbuf * n_mma + P * ncol + cc), v);
+            const uint32_t ta = tmem + q_base + (uint32_t)(buf * N_MMA + H * NCOL);
+#pragma unroll
+            for (int cb = 0; cb < NCOL; cb += 16) {
+                float v[16];
+                const int w = (NCOL - cb) >= 16 ? 16 : 8;
+                if (w == 16)
+                    tmem_ld_x16(ta + (uint32_t)cb, v);
+                else
+                    tmem_ld_x8(ta + (uint32_t)cb, v);
                 tmem_wait_ld();
-                float4 a = pend_wfirst ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<float4 *>(arow + cc);
-                a.x += v[0];
-                a.y += v[1];
-                a.z += v[2];
-                a.w += v[3];
-                *reinterpret_cast<float4 *>(arow + cc) = a;
+                if (cb + 16 >= NCOL) {
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&d_empty[buf]);
+                }
+#pragma unroll
+                for (int c4 = 0; c4 < 4; ++c4) {
+                    if (c4 * 4 < w) {
+                        float *ap = arow + cb + c4 * 4;
+                        float4 a = pend_wfirst ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<float4 *>(ap);
+                        a.x += v[c4 * 4 + 0];
+                        a.y += v[c4 * 4 + 1];
+                        a.z += v[c4 * 4 + 2];
+                        a.w += v[c4 * 4 + 3];
+                        *reinterpret_cast<float4 *>(ap) = a;
+                    }
+                }
             }
-            tc_fence_before();
-            mbar_arrive(&d_empty[dbuf]);
             if (pend_promote) {
-                for (int cc = 0; cc < ncol; cc += 2) {
+#pragma unroll 4
+                for (int cc = 0; cc < NCOL; cc += 2) {
                     const float2 a = *reinterpret_cast<const float2 *>(arow + cc);
                     double2 *d = reinterpret_cast<double2 *>(pend_dst + cc);
                     double2 o = pend_pfirst ? make_double2(0.0, 0.0) : *d;
@@ -411,103 +479,125 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     *d = o;
                 }
             }
-            pend_grp = -1;
+            pend = -1;
             return true;
         };
-        while (u < u1 && !dead) {
-            const int64_t tile = u / args.n_chunks;
-            const int64_t k0 = u % args.n_chunks;
-            const int64_t k1 = min(args.n_chunks, k0 + (u1 - u));
-            const int slot = (int)(blockIdx.x - cta_of(tile * args.n_chunks, G, W));
+        for (int i = blockIdx.x; i < n_items && !dead; i += G) {
+            const Item it = item_of(args, i);
             double *dst_piece =
-                args.partial + (((size_t)tile * args.maxp + slot) * TM + row) * (size_t)n_mma + P * ncol;
-            // A fragments of the phase GEMM: kappa[row 32Q + 8mt + gq][k = 4ks + tq].
-            double ka[4][5];
-            float tj[4];
+                args.partial + (((size_t)it.tile * args.slabs + it.z) * TM + row) * (size_t)N_MMA + H * NCOL;
+            // A fragments of the phase GEMM: kappa[row 32Q + 16H + 8mt + gq][k = 4ks + tq].
+            double ka[2][5];
+            float tj[2];
 #pragma unroll
-            for (int mt = 0; mt < 4; ++mt) {
-                int64_t j = tile * TM + Q * 32 + mt * 8 + gq;
+            for (int mt = 0; mt < 2; ++mt) {
+                int64_t j = (int64_t)it.tile * TM + Q * 32 + H * 16 + mt * 8 + gq;
                 if (j >= args.nsamples) j = args.nsamples - 1;
                 const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
 #pragma unroll
                 for (int ks = 0; ks < 5; ++ks) ka[mt][ks] = pr[4 * ks + tq];
                 tj[mt] = (float)pr[PREFIX_T];
             }
-            for (int64_t k = k0; k < k1; ++k, ++g) {
-                const int stage = (int)(g % NSTAGE);
-                const int as = (int)(g & 1);
-                bool ok = mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1));
-                ok = ok && mbar_wait(&a_empty[as], (uint32_t)(((g >> 1) + 1) & 1));
+            // One chunk: magnetisation of chunk c from thc (FP32 work), with the
+            // FP64 tensor work of chunk c+1 (into thn) issued in the same
+            // stretch of code so that both pipes run.
+            auto step = [&](double (&thc)[2][4][2], double (&thn)[2][4][2], int c) -> bool {
+                const bool has_next = c + 1 < it.c1;
+                int nstage = stage + 1;
+                uint32_t nfph = fph;
+                if (nstage == NSTAGE) {
+                    nstage = 0;
+                    nfph ^= 1u;
+                }
+                const int buf = g & 1;
+                bool ok = mbar_wait(&a_empty[buf], (uint32_t)(((g >> 1) + 1) & 1));
+                if (has_next) ok = ok && mbar_wait(&full[nstage], nfph);
+                __syncwarp();
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(args.err, 16u);
+                    return false;
+                }
+                tc_fence_after();
+                const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
+                // Past the last chunk of an item the look-ahead reads the
+                // current chunk again (its result is not used), so the code
+                // below stays free of branches.
+                const double *tabn = has_next ? sSpin + (size_t)nstage * (SPIN_BYTES / 8) : tab;
+                const uint32_t a_col = tmem + A_COL0 + (uint32_t)buf * 128u + a_lane;
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    chunk_phases(thn, ka, tabn, gq, tq, nt);
+                    // This thread's spins of group nt: 8nt + 2tq + i.
+                    const float4 rl = *reinterpret_cast<const float4 *>(tab + TAB_PACK + 8 * nt + 2 * tq);
+                    const float r2v[2] = {rl.x, rl.z};
+                    const float l2v[2] = {rl.y, rl.w};
+                    // 16x256b.x2 register order: [i*4 + mt*2 + comp] for
+                    // spin 2tq + i (column 8i + 2tq + comp), row 8mt + gq.
+                    uint32_t hi[8], lo[8];
+#pragma unroll
+                    for (int mt = 0; mt < 2; ++mt) {
+#pragma unroll
+                        for (int ii = 0; ii < 2; ++ii) {
+                            float mre, mim;
+                            magnetisation(thc[mt][nt][ii], tj[mt], r2v[ii], l2v[ii], mre, mim);
+                            const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
+                            const int e = ii * 4 + mt * 2;
+                            hi[e] = hr;
+                            hi[e + 1] = hm;
+                            lo[e] = tf32_rna(mre - __uint_as_float(hr));
+                            lo[e + 1] = tf32_rna(mim - __uint_as_float(hm));
+                        }
+                    }
+                    tmem_st_16x256b_x2(a_col + (uint32_t)nt * 16u, hi);
+                    tmem_st_16x256b_x2(a_col + 64u + (uint32_t)nt * 16u, lo);
+                }
+                tmem_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&a_full[buf]);
+                // The previous generation has had a whole chunk of producer
+                // time to finish: drain it now.
+                if (pend >= 0 && !drain()) return false;
+                const int ci = c - it.c0;
+                pend = g;
+                pend_dst = dst_piece;
+                pend_wfirst = (ci % WINDOW) == 0;
+                pend_promote = (ci % WINDOW) == WINDOW - 1 || c + 1 == it.c1;
+                pend_pfirst = ci < WINDOW;
+                ++g;
+                stage = nstage;
+                fph = nfph;
+                return true;
+            };
+            double thA[2][4][2], thB[2][4][2];
+            {
+                const bool ok = mbar_wait(&full[stage], fph);
                 __syncwarp();
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(args.err, 16u);
                     dead = true;
                     break;
                 }
-                tc_fence_after();
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                // B fragments: b[k = 4ks + tq][spin 8P + gq].
-                double bf[5];
 #pragma unroll
-                for (int ks = 0; ks < 5; ++ks) bf[ks] = tab[(4 * ks + tq) * KC + 8 * P + gq];
-                double th[4][2];
-#pragma unroll
-                for (int mt = 0; mt < 4; ++mt) {
-                    th[mt][0] = 0.0;
-                    th[mt][1] = 0.0;
-#pragma unroll
-                    for (int ks = 0; ks < 5; ++ks) dmma_8x8x4(th[mt][0], th[mt][1], ka[mt][ks], bf[ks]);
-                }
-                // This thread's spins: 8P + 2tq + i.
-                const float4 rl = *reinterpret_cast<const float4 *>(tab + SPIN_PACK * KC + 8 * P + 2 * tq);
-                const float r2v[2] = {rl.x, rl.z};
-                const float l2v[2] = {rl.y, rl.w};
-                // 16x256b.x2 register order per pair of row tiles (mt, mt+1):
-                // [i*4 + (mt&1)*2 + comp] for spin 2tq + i.
-                uint32_t hi[2][8], lo[2][8];
-#pragma unroll
-                for (int mt = 0; mt < 4; ++mt) {
-#pragma unroll
-                    for (int i = 0; i < 2; ++i) {
-                        float mre, mim;
-                        magnetisation(th[mt][i], tj[mt], r2v[i], l2v[i], mre, mim);
-                        const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
-                        const int e = i * 4 + (mt & 1) * 2;
-                        hi[mt >> 1][e] = hr;
-                        hi[mt >> 1][e + 1] = hm;
-                        lo[mt >> 1][e] = tf32_rna(mre - __uint_as_float(hr));
-                        lo[mt >> 1][e + 1] = tf32_rna(mim - __uint_as_float(hm));
-                    }
-                }
-                const uint32_t a_col = tmem + A_COL0 + (uint32_t)as * 128u + (uint32_t)P * 16u;
-                tmem_st_16x256b_x2(a_col + lane_base, hi[0]);
-                tmem_st_16x256b_x2(a_col + lane_base + (16u << 16), hi[1]);
-                tmem_st_16x256b_x2(a_col + 64u + lane_base, lo[0]);
-                tmem_st_16x256b_x2(a_col + 64u + lane_base + (16u << 16), lo[1]);
-                tmem_wait_st();
-                tc_fence_before();
-                mbar_arrive(&a_full[as]);
-                // The previous generation has had a whole chunk of producer
-                // time to finish: drain it now.
-                if (pend_grp >= 0 && !drain()) {
+                for (int nt = 0; nt < 4; ++nt) chunk_phases(thA, ka, tab, gq, tq, nt);
+            }
+            // Two chunks per trip so that the phase arrays swap roles without copies.
+            for (int c = it.c0; c < it.c1; c += 2) {
+                if (!step(thA, thB, c)) {
                     dead = true;
                     break;
                 }
-                if ((k - k0) % FLUSH == FLUSH - 1 || k + 1 == k1) {
-                    const int64_t i = k - k0;
-                    pend_grp = grp++;
-                    pend_dst = dst_piece;
-                    pend_wfirst = (i % WINDOW) == 0;
-                    pend_promote = (i % WINDOW) == WINDOW - 1 || k + 1 == k1;
-                    pend_pfirst = i < WINDOW;
+                if (c + 1 < it.c1 && !step(thB, thA, c + 1)) {
+                    dead = true;
+                    break;
                 }
             }
             if (dead) break;
-            if (pend_grp >= 0 && !drain()) {
+            if (pend >= 0 && !drain()) {
                 dead = true;
                 break;
             }
-            u += k1 - k0;
         }
     }
     tc_fence_before();
@@ -518,11 +608,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     }
 }
 
-// Sum split-K partials of each (sample, column) in piece order (FP64) and
+// Sum the split-K partials of each (sample, column) in slab order (FP64) and
 // write complex samples: column n < nc is Re S(j, n), nc <= n < 2nc is Im.
 template <typename T>
-__global__ void split_finalize_kernel(const double *partial, int64_t nsamples, int32_t nc, int n_mma, int maxp,
-                                      int64_t n_chunks, int64_t G, int64_t W, cplx<T> *sig, int64_t ldsig) {
+__global__ void split_finalize_kernel(const double *partial, int64_t nsamples, int32_t nc, int n_mma, int slabs,
+                                      cplx<T> *sig, int64_t ldsig) {
     const int64_t total = nsamples * nc;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -530,12 +620,9 @@ __global__ void split_finalize_kernel(const double *partial, int64_t nsamples, i
         const int32_t c = (int32_t)(i / nsamples);
         const int64_t tile = j / TM;
         const int row = (int)(j % TM);
-        const int64_t first = cta_of(tile * n_chunks, G, W);
-        const int64_t last = cta_of((tile + 1) * n_chunks - 1, G, W);
-        const int np = (int)(last - first + 1);
         double re = 0.0, im = 0.0;
-        for (int p = 0; p < np; ++p) {
-            const double *src = partial + (((size_t)tile * maxp + p) * TM + row) * (size_t)n_mma;
+        for (int z = 0; z < slabs; ++z) {
+            const double *src = partial + (((size_t)tile * slabs + z) * TM + row) * (size_t)n_mma;
             re += src[c];
             im += src[nc + c];
         }
@@ -605,37 +692,36 @@ __global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32
     }
 }
 
-// Spin table of a segment, from the state at its start (k-major per chunk):
-// rows 0..15 basis, 16 dw/(2 pi) (0 if dw is off in precession),
-// 17 theta0 = arg(m0)/(2 pi), 18..19 zero, 20 packed float2
-// (-log2(e)/T2, log2|m0|).  Also checks the phase range: |theta| must stay
-// below 2^18 turns for the fixed-point reduction (error bit 64 otherwise).
+// Spin table of a segment, from the state at its start (tab_index layout per
+// chunk): phase rows 0..15 basis, 16 dw/(2 pi) (0 if dw is off in
+// precession), 17 theta0 = arg(m0)/(2 pi), 18..19 zero, then the packed
+// float2 (-log2(e)/T2, log2|m0|).  Also checks the phase range: |theta| must
+// stay below 2^18 turns for the fixed-point reduction (error bit 64 otherwise).
 __global__ void spin_table_kernel(const double *basis, const double *dw, const double *T2, const cplx<double> *xy,
                                   int64_t ns, int64_t nchunks, uint32_t method, const double *colmax,
                                   unsigned int *err, double *table) {
     const int64_t total = nchunks * KC;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total;
          s += (int64_t)gridDim.x * blockDim.x) {
-        double *t = table + (s / KC) * (SPIN_ROWS * KC) + (s % KC);
+        double *t = table + (s / KC) * (SPIN_ROWS * KC);
+        const int sl = (int)(s % KC);
+        double row[NTERM];
+        for (int k = 0; k < NTERM; ++k) row[k] = 0.0;
+        float2 rl = make_float2(0.0f, -INFINITY);
         if (s < ns) {
-            for (int k = 0; k < 16; ++k) t[k * KC] = basis[s * 16 + k];
-            t[16 * KC] = (method & HOMS_DW_PRECESSION) ? dw[s] / (2.0 * 3.141592653589793) : 0.0;
+            for (int k = 0; k < 16; ++k) row[k] = basis[s * 16 + k];
+            row[16] = (method & HOMS_DW_PRECESSION) ? dw[s] / (2.0 * 3.141592653589793) : 0.0;
             const cplx<double> m0 = xy[s];
             const double mag = hypot(m0.re, m0.im);
-            t[17 * KC] = atan2(m0.im, m0.re) / (2.0 * 3.141592653589793);
-            double bound = fabs(t[17 * KC]);
-            for (int k = 0; k < 17; ++k) bound += fabs(t[k * KC]) * colmax[k];
+            row[17] = atan2(m0.im, m0.re) / (2.0 * 3.141592653589793);
+            double bound = fabs(row[17]);
+            for (int k = 0; k < 17; ++k) bound += fabs(row[k]) * colmax[k];
             if (!(bound < 262144.0)) atomicOr(err, 64u);
-            float2 rl;
             rl.x = (float)(-1.4426950408889634 / T2[s]);
             rl.y = mag > 0.0 ? (float)log2(mag) : -INFINITY;
-            *reinterpret_cast<float2 *>(&t[SPIN_PACK * KC]) = rl;
-        } else {
-            for (int k = 0; k < 18; ++k) t[k * KC] = 0.0;
-            *reinterpret_cast<float2 *>(&t[SPIN_PACK * KC]) = make_float2(0.0f, -INFINITY);
         }
-        t[18 * KC] = 0.0;
-        t[19 * KC] = 0.0;
+        for (int k = 0; k < NTERM; ++k) t[tab_index(k, sl)] = row[k];
+        *reinterpret_cast<float2 *>(&t[TAB_PACK + sl]) = rl;
     }
 }
 
@@ -724,9 +810,10 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
 __global__ void state_update_kernel(const double *table, const double *endrow, const double *T1, const double *T2,
                                     const double *rho, int64_t ns, cplx<double> *xy, double *mz) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns; s += (int64_t)gridDim.x * blockDim.x) {
-        const double *t = table + (s / KC) * (SPIN_ROWS * KC) + (s % KC);
-        double th = t[17 * KC];
-        for (int k = 0; k < 17; ++k) th = fma(t[k * KC], endrow[k], th);
+        const double *t = table + (s / KC) * (SPIN_ROWS * KC);
+        const int sl = (int)(s % KC);
+        double th = t[tab_index(17, sl)];
+        for (int k = 0; k < 17; ++k) th = fma(t[tab_index(k, sl)], endrow[k], th);
         const double T = endrow[PREFIX_T];
         const cplx<double> m0 = xy[s];
         const double mag = hypot(m0.re, m0.im);
@@ -806,6 +893,48 @@ static size_t kernel_smem(int n_mma) {
     return 1024 + (size_t)kernel_stages(n_mma) * (b_bytes(n_mma) + SPIN_BYTES) + acc_bytes(n_mma) + 32 * 8 + 64;
 }
 
+// Number of chunk slabs per tile: the smallest that keeps the busiest CTA's
+// work (items x (chunks per item + an allowance for the per-item start-up))
+// within reach of the best split.
+static int choose_slabs(int64_t tiles, int64_t nchunks, int64_t G) {
+    int best = 1;
+    double best_cost = 1e300;
+    const int64_t zmax = std::min<int64_t>(nchunks, 4096);
+    for (int64_t z = 1; z <= zmax; ++z) {
+        const int64_t per_cta = (tiles * z + G - 1) / G;
+        const double cost = (double)per_cta * (double)((nchunks + z - 1) / z + 2);
+        if (cost < best_cost * 0.995) {
+            best_cost = cost;
+            best = (int)z;
+        }
+    }
+    return best;
+}
+
+template <int N>
+static cudaError_t launch_precession(const KernelArgs &ka, unsigned grid, size_t smem, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(split_precession_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    split_precession_kernel<N><<<grid, THREADS, smem, stream>>>(ka);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_precession(int n_mma, const KernelArgs &ka, unsigned grid, size_t smem,
+                                     cudaStream_t stream) {
+    switch (n_mma) {
+        case 16: return launch_precession<16>(ka, grid, smem, stream);
+        case 32: return launch_precession<32>(ka, grid, smem, stream);
+        case 48: return launch_precession<48>(ka, grid, smem, stream);
+        case 64: return launch_precession<64>(ka, grid, smem, stream);
+        case 80: return launch_precession<80>(ka, grid, smem, stream);
+        case 96: return launch_precession<96>(ka, grid, smem, stream);
+        case 112: return launch_precession<112>(ka, grid, smem, stream);
+        case 128: return launch_precession<128>(ka, grid, smem, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 // One precession segment.
 static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi,
                                  int64_t sample0, int64_t nsamples, cudaStream_t stream, std::string *err) {
@@ -852,20 +981,16 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         int dev = 0, nsm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const int64_t W = tiles * nchunks;
-        const int64_t G = std::min<int64_t>(nsm, W);
-        int maxp = 1;
-        for (int64_t t = 0; t < tiles; ++t) {
-            const int64_t f = ((t * nchunks + 1) * G - 1) / W;
-            const int64_t l = (((t + 1) * nchunks) * G - 1) / W;
-            maxp = std::max<int>(maxp, (int)(l - f + 1));
+        const int slabs = choose_slabs(tiles, nchunks, nsm);
+        const int64_t n_items = tiles * slabs;
+        if (tiles > INT32_MAX / slabs || nchunks > INT32_MAX) {
+            *err = "split mode: segment too large for one launch";
+            return cudaSuccess;
         }
-        const size_t pbytes = sizeof(double) * (size_t)tiles * maxp * TM * r.n_mma;
+        const int64_t G = std::min<int64_t>(nsm, n_items);
+        const size_t pbytes = sizeof(double) * (size_t)tiles * slabs * TM * r.n_mma;
         if ((e = grow(r.partial, r.partial_bytes, pbytes)) != cudaSuccess) return e;
         const size_t smem = kernel_smem(r.n_mma);
-        if ((e = cudaFuncSetAttribute(split_precession_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-            cudaSuccess)
-            return e;
         KernelArgs ka;
         ka.prefix = (const double *)r.prefix;
         ka.b_operand = (const uint8_t *)r.b_operand;
@@ -873,21 +998,19 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         ka.partial = (double *)r.partial;
         ka.err = (unsigned int *)r.err;
         ka.nsamples = nsamples;
-        ka.n_chunks = nchunks;
-        ka.tiles = tiles;
-        ka.maxp = maxp;
-        ka.n_mma = r.n_mma;
+        ka.n_chunks = (int)nchunks;
+        ka.tiles = (int)tiles;
+        ka.slabs = slabs;
         ka.nstage = kernel_stages(r.n_mma);
         if (a.ev_start) cudaEventRecord(a.ev_start, stream);
-        split_precession_kernel<<<(unsigned)G, THREADS, smem, stream>>>(ka);
+        e = launch_precession(r.n_mma, ka, (unsigned)G, smem, stream);
         if (a.ev_stop) cudaEventRecord(a.ev_stop, stream);
         if (a.launches) *a.launches += 2;
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (e != cudaSuccess) return e;
         const int64_t total = nsamples * r.nc;
         if (a.sizeof_T == 8)
             split_finalize_kernel<double><<<grid_for(total), 256, 0, stream>>>(
-                (const double *)r.partial, nsamples, r.nc, r.n_mma, maxp, nchunks, G, W,
-                (cplx<double> *)a.sig + sample0, a.nadc);
+                (const double *)r.partial, nsamples, r.nc, r.n_mma, slabs, (cplx<double> *)a.sig + sample0, a.nadc);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if (a.launches) *a.launches += 3;
