@@ -56,17 +56,20 @@ constexpr int TM = 128;          // samples per tile (UMMA M)
 constexpr int KC = 32;           // spins per chunk
 constexpr int KSTEPS = 8;        // (2*KC real K values) / 8 per tf32 MMA
 constexpr int MAX_STAGE = 4;     // shared-memory stages (fewer for wide N)
-constexpr int NTERM = 20;        // phase GEMM depth: 16 basis + dw + theta0 + 2 zero
-constexpr int SPIN_ROWS = 21;    // k-major spin table rows per chunk: b_0..b_19, packed (r2, log2|m0|)
-constexpr int SPIN_BYTES = SPIN_ROWS * KC * 8;
+constexpr int NTERM = 16;        // phase GEMM depth (DMMA K): the 16 basis terms
 constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_19, t, pad
 constexpr int PREFIX_T = 20;
-// 8 producer warps (2 per TMEM lane quarter) + MMA issuer + loader: at most 3
-// warps per SM sub-partition, which leaves 168 registers per thread.
-constexpr int NPROD_WARPS = 8;
-constexpr int MMA_WARP = 8;
-constexpr int LOAD_WARP = 9;
-constexpr int THREADS = 320;
+// Warp roles: 4 phase warps (one per SM sub-partition), 8 magnetisation warps
+// (2 per TMEM lane quarter), MMA issuer, loader -- at most 4 warps per
+// sub-partition, which leaves 128 registers per thread.
+constexpr int NPHASE_WARPS = 4;
+constexpr int NMAG_WARPS = 8;
+constexpr int MMA_WARP = 12;
+constexpr int LOAD_WARP = 13;
+constexpr int THREADS = 448;
+// Turn fractions of one chunk for one lane quarter: [mt 4][nt 4][lane 32] uint2.
+constexpr int TURN_TILE = 16 * 32;
+constexpr int TURN_BYTES = 4 * TURN_TILE * 8;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr uint32_t A_COL0 = 256;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
@@ -84,12 +87,15 @@ constexpr float C1 = -0.5f, C2 = 0.04166662320494652f, C3 = -0.00138867634814232
 
 __host__ __device__ constexpr int b_bytes(int n_mma) { return 2 * KSTEPS * n_mma * 32; }
 
-// Spin table of a chunk, in doubles: phase row k (0..19) of local spin s at
+// Spin table of a chunk, in doubles: basis term k (0..15) of local spin s at
 // ((k/4)*KC + s)*4 + k%4, so that one DMMA B fragment (k = 4ks + tq, spin
-// base + gq) is 32 consecutive doubles; then one packed float2
-// (-log2(e)/T2, log2|m0|) per spin.
+// base + gq) is 32 consecutive doubles; then theta0 = arg(m0)/(2 pi) and
+// dw/(2 pi) per spin, and one packed float2 (-log2(e)/T2, log2|m0|) per spin.
 __host__ __device__ inline int tab_index(int k, int s) { return (((k >> 2) * KC + s) << 2) + (k & 3); }
-constexpr int TAB_PACK = NTERM * KC;
+constexpr int TAB_THETA0 = NTERM * KC;
+constexpr int TAB_DW = TAB_THETA0 + KC;
+constexpr int TAB_PACK = TAB_DW + KC;
+constexpr int SPIN_BYTES = (TAB_PACK + KC) * 8;
 
 // K order of a chunk's A/B operands: spins 8P..8P+7 (one DMMA n-tile) fill
 // the 16 columns 16P + j, where column j holds spin 8P + 2*((j%8)/2) + j/8
@@ -155,7 +161,7 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint32_t a, uint64_t bde
 // (a: row groupID, col threadID_in_group; b: row threadID_in_group, col
 // groupID; c: row groupID, cols 2*threadID_in_group + {0,1}).
 __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(c0), "+d"(c1)
                  : "d"(a), "d"(b));
 }
@@ -216,14 +222,15 @@ __device__ __forceinline__ uint64_t bdesc(uint32_t saddr) {
 struct KernelArgs {
     const double *prefix;      // [rows][PREFIX_STRIDE]
     const uint8_t *b_operand;  // [nchunks][b_bytes]
-    const double *spin_table;  // [nchunks][SPIN_ROWS * KC]
+    const double *spin_table;  // [nchunks][SPIN_BYTES / 8]
     double *partial;           // [tiles][slabs][TM][n_mma], FP64 split-K partials
     unsigned int *err;
     int64_t nsamples;
     int n_chunks;
     int tiles;
     int slabs;
-    int nstage;
+    int nstage;  // shared-memory stages of B operand + spin table
+    int nbuf;    // turn-fraction buffers between phase and magnetisation warps (1 or 2)
 };
 
 struct Item {
@@ -238,10 +245,14 @@ __device__ __forceinline__ Item item_of(const KernelArgs &a, int i) {
     return it;
 }
 
-// M(s,j) for one spin given the FP64 turn count; returns (re, im).
-__device__ __forceinline__ void magnetisation(double th, float tj, float r2, float l2m0, float &mre, float &mim) {
-    const double g = th + 1572864.0;  // 1.5 * 2^20: frac(th) * 2^32 lands in the low word
-    const uint32_t u = (uint32_t)__double2loint(g);
+// frac(th) * 2^32 of an FP64 turn count |th| < 2^18: adding 1.5 * 2^20 puts
+// the fraction's leading 32 bits in the low word (the mod-2pi reduction).
+__device__ __forceinline__ uint32_t turn_fraction(double th) {
+    return (uint32_t)__double2loint(th + 1572864.0);
+}
+
+// M(s,j) for one spin from its 32-bit turn fraction u; returns (re, im).
+__device__ __forceinline__ void magnetisation(uint32_t u, float tj, float r2, float l2m0, float &mre, float &mim) {
     // u = q' 2^30 + r: quadrant q = nearest quarter turn = (u + 2^29) >> 30, and
     // (int)(u << 2) = 4 * (r as a signed 30-bit offset from it), in [-2^31, 2^31).
     const uint32_t v = u + 0x20000000u;
@@ -260,40 +271,28 @@ __device__ __forceinline__ void magnetisation(double th, float tj, float r2, flo
     mim = a * s;
 }
 
-// Phases of one chunk for a producer thread: th[mt][nt][i] of spin
-// 8nt + 2tq + i at tile row 8mt + gq (rows relative to the warp's 16).
-__device__ __forceinline__ void chunk_phases(double (&th)[2][4][2], const double (&ka)[2][5], const double *tab,
-                                             int gq, int tq, int nt) {
-    double bf[5];
-#pragma unroll
-    for (int ks = 0; ks < 5; ++ks) bf[ks] = tab[tab_index(4 * ks + tq, 8 * nt + gq)];
-#pragma unroll
-    for (int mt = 0; mt < 2; ++mt) {
-        th[mt][nt][0] = 0.0;
-        th[mt][nt][1] = 0.0;
-#pragma unroll
-        for (int ks = 0; ks < 5; ++ks) dmma_8x8x4(th[mt][nt][0], th[mt][nt][1], ka[mt][ks], bf[ks]);
-    }
-}
-
 template <int N_MMA>
 __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
     constexpr int BB = b_bytes(N_MMA);
-    constexpr int NCOL = N_MMA / 2;  // accumulator columns drained per producer thread
+    constexpr int NCOL = N_MMA / 2;  // accumulator columns drained per magnetisation thread
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const int NSTAGE = args.nstage;
+    const int NB = args.nbuf;
     uint8_t *sB = smem;                                             // NSTAGE * BB
     double *sSpin = reinterpret_cast<double *>(sB + NSTAGE * BB);  // NSTAGE * SPIN_BYTES
-    float *accf = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);  // TM x (N_MMA+pad)
+    uint2 *sTurn = reinterpret_cast<uint2 *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);  // NB * TURN_BYTES
+    float *accf = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(sTurn) + NB * TURN_BYTES);  // TM x (N_MMA+pad)
     uint64_t *bars = reinterpret_cast<uint64_t *>(accf + (size_t)TM * (N_MMA + ACC_PAD));
     uint64_t *full = bars;                    // [NSTAGE] loader -> consumers (tx)
     uint64_t *empty = bars + MAX_STAGE;       // [NSTAGE] MMA commit -> loader
-    uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] producers -> MMA
-    uint64_t *a_empty = a_full + 2;           // [2] MMA commit -> producers
+    uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] magnetisation warps -> MMA
+    uint64_t *a_empty = a_full + 2;           // [2] MMA commit -> magnetisation warps
     uint64_t *d_full = a_empty + 2;           // [2] MMA commit -> drain
     uint64_t *d_empty = d_full + 2;           // [2] drain -> MMA
-    uint64_t *done = d_empty + 2;             // [1] final MMA commit
+    uint64_t *t_full = d_empty + 2;           // [4 quarters][2] phase warp -> magnetisation warps
+    uint64_t *t_empty = t_full + 8;           // [4 quarters][2] magnetisation warps -> phase warp
+    uint64_t *done = t_empty + 8;             // [1] final MMA commit
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -303,10 +302,14 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             mbar_init(&empty[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
-            mbar_init(&a_full[i], NPROD_WARPS);  // one elected arrive per producer warp
+            mbar_init(&a_full[i], NMAG_WARPS);  // one elected arrive per magnetisation warp
             mbar_init(&a_empty[i], 1);
             mbar_init(&d_full[i], 1);
-            mbar_init(&d_empty[i], NPROD_WARPS);
+            mbar_init(&d_empty[i], NMAG_WARPS);
+        }
+        for (int i = 0; i < 8; ++i) {
+            mbar_init(&t_full[i], 1);
+            mbar_init(&t_empty[i], NMAG_WARPS / 4);
         }
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -324,6 +327,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 
     const int n_items = args.tiles * args.slabs;
     const int G = (int)gridDim.x;
+    const int gq = lane >> 2, tq = lane & 3;
     bool dead = false;
 
     if (warp == LOAD_WARP) {
@@ -407,22 +411,95 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             if (!mbar_wait(done, 0)) atomicOr(args.err, 8u);
         }
         __syncwarp();
+    } else if (warp < NPHASE_WARPS) {
+        // Phase warp q: the FP64 phase tile of tile rows 32q..32q+31 (4 x 4 DMMA
+        // 8x8 tiles per chunk, K = 16), accumulators initialised with
+        // theta0 + (dw/2pi) * kappa_16, reduced to 32-bit turn fractions.
+        const int q = warp;
+        int stage = 0, tb = 0;
+        uint32_t fph = 0, tk = 0;  // parities of full[stage] and of this use of turn buffer tb
+        for (int i = blockIdx.x; i < n_items && !dead; i += G) {
+            const Item it = item_of(args, i);
+            // A fragments: kappa[row 32q + 8mt + gq][k = 4ks + tq], and kappa_16 of the row.
+            double ka[4][4], k16[4];
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) {
+                int64_t j = (int64_t)it.tile * TM + q * 32 + mt * 8 + gq;
+                if (j >= args.nsamples) j = args.nsamples - 1;
+                const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) ka[mt][ks] = pr[4 * ks + tq];
+                k16[mt] = pr[16];
+            }
+            for (int c = it.c0; c < it.c1; ++c) {
+                bool ok = mbar_wait(&full[stage], fph);
+                ok = ok && mbar_wait(&t_empty[q * 2 + tb], tk ^ 1u);
+                __syncwarp();
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(args.err, 128u);
+                    dead = true;
+                    break;
+                }
+                const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
+                uint2 *dst = sTurn + (size_t)(tb * 4 + q) * TURN_TILE;
+                // Two spin groups at a time: 8 independent accumulator chains,
+                // k-step outermost, so that consecutive DMMAs never depend on
+                // one another and the FP64 pipe, not the DMMA latency, sets the pace.
+#pragma unroll
+                for (int np = 0; np < 2; ++np) {
+                    double bf[2][4], th[2][4][2];
+#pragma unroll
+                    for (int n2 = 0; n2 < 2; ++n2) {
+                        const int nt = 2 * np + n2;
+#pragma unroll
+                        for (int ks = 0; ks < 4; ++ks) bf[n2][ks] = tab[tab_index(4 * ks + tq, 8 * nt + gq)];
+                        const double2 t0 = *reinterpret_cast<const double2 *>(tab + TAB_THETA0 + 8 * nt + 2 * tq);
+                        const double2 dw = *reinterpret_cast<const double2 *>(tab + TAB_DW + 8 * nt + 2 * tq);
+#pragma unroll
+                        for (int mt = 0; mt < 4; ++mt) {
+                            th[n2][mt][0] = fma(dw.x, k16[mt], t0.x);
+                            th[n2][mt][1] = fma(dw.y, k16[mt], t0.y);
+                        }
+                    }
+#pragma unroll
+                    for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+                        for (int n2 = 0; n2 < 2; ++n2)
+#pragma unroll
+                            for (int mt = 0; mt < 4; ++mt)
+                                dmma_8x8x4(th[n2][mt][0], th[n2][mt][1], ka[mt][ks], bf[n2][ks]);
+#pragma unroll
+                    for (int n2 = 0; n2 < 2; ++n2)
+#pragma unroll
+                        for (int mt = 0; mt < 4; ++mt)
+                            dst[(mt * 4 + 2 * np + n2) * 32 + lane] =
+                                make_uint2(turn_fraction(th[n2][mt][0]), turn_fraction(th[n2][mt][1]));
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&t_full[q * 2 + tb]);
+                if (++stage == NSTAGE) {
+                    stage = 0;
+                    fph ^= 1u;
+                }
+                if (++tb == NB) {
+                    tb = 0;
+                    tk ^= 1u;
+                }
+            }
+        }
     } else {
-        // Producers.  Warp w works in TMEM lane quarter Q = w % 4 (tile rows
-        // 32Q..32Q+31) with half H = w / 4.  For the phase/magnetisation tile
-        // it takes rows 32Q + 16H .. +15 and all 32 spins of each chunk: 2 x 4
-        // DMMA 8x8 tiles (gq = groupID, tq = threadID_in_group).  For the
-        // accumulator drain it takes thread <-> tile row 32Q + lane and
-        // column half H.
-        const int Q = warp & 3, H = warp >> 2;
-        const int gq = lane >> 2, tq = lane & 3;
-        const uint32_t q_base = (uint32_t)(Q * 32) << 16;
-        const uint32_t a_lane = (uint32_t)(Q * 32 + H * 16) << 16;
-        const int row = Q * 32 + lane;
-        float *arow = accf + (size_t)row * (N_MMA + ACC_PAD) + H * NCOL;
+        // Magnetisation warp w: TMEM lane quarter q = w % 4, half h: tile rows
+        // 32q + 16h .. +15 (phase tiles mt = 2h, 2h+1 of quarter q) and all 32
+        // spins of each chunk.  For the accumulator drain it takes thread <->
+        // tile row 32q + lane and column half h.
+        const int q = warp & 3, h = (warp - NPHASE_WARPS) >> 2;
+        const uint32_t q_base = (uint32_t)(q * 32) << 16;
+        const uint32_t a_lane = (uint32_t)(q * 32 + h * 16) << 16;
+        const int row = q * 32 + lane;
+        float *arow = accf + (size_t)row * (N_MMA + ACC_PAD) + h * NCOL;
         int g = 0;  // chunks produced by this CTA
-        int stage = 0;
-        uint32_t fph = 0;  // parity of full[stage] for chunk g
+        int stage = 0, tb = 0;
+        uint32_t tk = 0;
         // Two-level drain of each chunk's accumulator generation: the FP32
         // TMEM result is added (round to nearest) into this thread's FP32 row
         // accumulator in shared memory; every WINDOW chunks, and at the end of
@@ -440,7 +517,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 return false;
             }
             tc_fence_after();
-            const uint32_t ta = tmem + q_base + (uint32_t)(buf * N_MMA + H * NCOL);
+            const uint32_t ta = tmem + q_base + (uint32_t)(buf * N_MMA + h * NCOL);
 #pragma unroll
             for (int cb = 0; cb < NCOL; cb += 16) {
                 float v[16];
@@ -485,48 +562,38 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         for (int i = blockIdx.x; i < n_items && !dead; i += G) {
             const Item it = item_of(args, i);
             double *dst_piece =
-                args.partial + (((size_t)it.tile * args.slabs + it.z) * TM + row) * (size_t)N_MMA + H * NCOL;
-            // A fragments of the phase GEMM: kappa[row 32Q + 16H + 8mt + gq][k = 4ks + tq].
-            double ka[2][5];
+                args.partial + (((size_t)it.tile * args.slabs + it.z) * TM + row) * (size_t)N_MMA + h * NCOL;
             float tj[2];
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
-                int64_t j = (int64_t)it.tile * TM + Q * 32 + H * 16 + mt * 8 + gq;
+                int64_t j = (int64_t)it.tile * TM + q * 32 + h * 16 + mt * 8 + gq;
                 if (j >= args.nsamples) j = args.nsamples - 1;
-                const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
-#pragma unroll
-                for (int ks = 0; ks < 5; ++ks) ka[mt][ks] = pr[4 * ks + tq];
-                tj[mt] = (float)pr[PREFIX_T];
+                tj[mt] = (float)args.prefix[(size_t)j * PREFIX_STRIDE + PREFIX_T];
             }
-            // One chunk: magnetisation of chunk c from thc (FP32 work), with the
-            // FP64 tensor work of chunk c+1 (into thn) issued in the same
-            // stretch of code so that both pipes run.
-            auto step = [&](double (&thc)[2][4][2], double (&thn)[2][4][2], int c) -> bool {
-                const bool has_next = c + 1 < it.c1;
-                int nstage = stage + 1;
-                uint32_t nfph = fph;
-                if (nstage == NSTAGE) {
-                    nstage = 0;
-                    nfph ^= 1u;
-                }
+            for (int c = it.c0; c < it.c1; ++c) {
                 const int buf = g & 1;
-                bool ok = mbar_wait(&a_empty[buf], (uint32_t)(((g >> 1) + 1) & 1));
-                if (has_next) ok = ok && mbar_wait(&full[nstage], nfph);
+                bool ok = mbar_wait(&t_full[q * 2 + tb], tk);
+                ok = ok && mbar_wait(&a_empty[buf], (uint32_t)(((g >> 1) + 1) & 1));
                 __syncwarp();
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(args.err, 16u);
-                    return false;
+                    dead = true;
+                    break;
                 }
                 tc_fence_after();
+                // This thread's turn fractions: phase tile (2h + mt, nt).
+                const uint2 *src = sTurn + (size_t)(tb * 4 + q) * TURN_TILE;
+                uint2 tu[2][4];
+#pragma unroll
+                for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                    for (int nt = 0; nt < 4; ++nt) tu[mt][nt] = src[((2 * h + mt) * 4 + nt) * 32 + lane];
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&t_empty[q * 2 + tb]);
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                // Past the last chunk of an item the look-ahead reads the
-                // current chunk again (its result is not used), so the code
-                // below stays free of branches.
-                const double *tabn = has_next ? sSpin + (size_t)nstage * (SPIN_BYTES / 8) : tab;
                 const uint32_t a_col = tmem + A_COL0 + (uint32_t)buf * 128u + a_lane;
 #pragma unroll
                 for (int nt = 0; nt < 4; ++nt) {
-                    chunk_phases(thn, ka, tabn, gq, tq, nt);
                     // This thread's spins of group nt: 8nt + 2tq + i.
                     const float4 rl = *reinterpret_cast<const float4 *>(tab + TAB_PACK + 8 * nt + 2 * tq);
                     const float r2v[2] = {rl.x, rl.z};
@@ -539,7 +606,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 #pragma unroll
                         for (int ii = 0; ii < 2; ++ii) {
                             float mre, mim;
-                            magnetisation(thc[mt][nt][ii], tj[mt], r2v[ii], l2v[ii], mre, mim);
+                            magnetisation(ii ? tu[mt][nt].y : tu[mt][nt].x, tj[mt], r2v[ii], l2v[ii], mre, mim);
                             const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
                             const int e = ii * 4 + mt * 2;
                             hi[e] = hr;
@@ -555,9 +622,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&a_full[buf]);
-                // The previous generation has had a whole chunk of producer
-                // time to finish: drain it now.
-                if (pend >= 0 && !drain()) return false;
+                // The previous generation has had a whole chunk of time to
+                // finish: drain it now.
+                if (pend >= 0 && !drain()) {
+                    dead = true;
+                    break;
+                }
                 const int ci = c - it.c0;
                 pend = g;
                 pend_dst = dst_piece;
@@ -565,32 +635,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 pend_promote = (ci % WINDOW) == WINDOW - 1 || c + 1 == it.c1;
                 pend_pfirst = ci < WINDOW;
                 ++g;
-                stage = nstage;
-                fph = nfph;
-                return true;
-            };
-            double thA[2][4][2], thB[2][4][2];
-            {
-                const bool ok = mbar_wait(&full[stage], fph);
-                __syncwarp();
-                if (!__all_sync(0xffffffffu, ok)) {
-                    if (lane == 0) atomicOr(args.err, 16u);
-                    dead = true;
-                    break;
-                }
-                const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) chunk_phases(thA, ka, tab, gq, tq, nt);
-            }
-            // Two chunks per trip so that the phase arrays swap roles without copies.
-            for (int c = it.c0; c < it.c1; c += 2) {
-                if (!step(thA, thB, c)) {
-                    dead = true;
-                    break;
-                }
-                if (c + 1 < it.c1 && !step(thB, thA, c + 1)) {
-                    dead = true;
-                    break;
+                if (++stage == NSTAGE) stage = 0;
+                if (++tb == NB) {
+                    tb = 0;
+                    tk ^= 1u;
                 }
             }
             if (dead) break;
@@ -692,35 +740,38 @@ __global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32
     }
 }
 
-// Spin table of a segment, from the state at its start (tab_index layout per
-// chunk): phase rows 0..15 basis, 16 dw/(2 pi) (0 if dw is off in
-// precession), 17 theta0 = arg(m0)/(2 pi), 18..19 zero, then the packed
-// float2 (-log2(e)/T2, log2|m0|).  Also checks the phase range: |theta| must
-// stay below 2^18 turns for the fixed-point reduction (error bit 64 otherwise).
+// Spin table of a segment, from the state at its start (layout of
+// tab_index per chunk): the 16 basis terms, theta0 = arg(m0)/(2 pi), dw/(2 pi)
+// (0 if dw is off in precession) and the packed float2 (-log2(e)/T2,
+// log2|m0|).  Also checks the phase range: |theta| must stay below 2^18
+// turns for the fixed-point reduction (error bit 64 otherwise).
 __global__ void spin_table_kernel(const double *basis, const double *dw, const double *T2, const cplx<double> *xy,
                                   int64_t ns, int64_t nchunks, uint32_t method, const double *colmax,
                                   unsigned int *err, double *table) {
     const int64_t total = nchunks * KC;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total;
          s += (int64_t)gridDim.x * blockDim.x) {
-        double *t = table + (s / KC) * (SPIN_ROWS * KC);
+        double *t = table + (s / KC) * (SPIN_BYTES / 8);
         const int sl = (int)(s % KC);
-        double row[NTERM];
-        for (int k = 0; k < NTERM; ++k) row[k] = 0.0;
+        double row[17];
+        for (int k = 0; k < 17; ++k) row[k] = 0.0;
+        double theta0 = 0.0;
         float2 rl = make_float2(0.0f, -INFINITY);
         if (s < ns) {
             for (int k = 0; k < 16; ++k) row[k] = basis[s * 16 + k];
             row[16] = (method & HOMS_DW_PRECESSION) ? dw[s] / (2.0 * 3.141592653589793) : 0.0;
             const cplx<double> m0 = xy[s];
             const double mag = hypot(m0.re, m0.im);
-            row[17] = atan2(m0.im, m0.re) / (2.0 * 3.141592653589793);
-            double bound = fabs(row[17]);
+            theta0 = atan2(m0.im, m0.re) / (2.0 * 3.141592653589793);
+            double bound = fabs(theta0);
             for (int k = 0; k < 17; ++k) bound += fabs(row[k]) * colmax[k];
             if (!(bound < 262144.0)) atomicOr(err, 64u);
             rl.x = (float)(-1.4426950408889634 / T2[s]);
             rl.y = mag > 0.0 ? (float)log2(mag) : -INFINITY;
         }
         for (int k = 0; k < NTERM; ++k) t[tab_index(k, sl)] = row[k];
+        t[TAB_THETA0 + sl] = theta0;
+        t[TAB_DW + sl] = row[16];
         *reinterpret_cast<float2 *>(&t[TAB_PACK + sl]) = rl;
     }
 }
@@ -810,10 +861,10 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
 __global__ void state_update_kernel(const double *table, const double *endrow, const double *T1, const double *T2,
                                     const double *rho, int64_t ns, cplx<double> *xy, double *mz) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns; s += (int64_t)gridDim.x * blockDim.x) {
-        const double *t = table + (s / KC) * (SPIN_ROWS * KC);
+        const double *t = table + (s / KC) * (SPIN_BYTES / 8);
         const int sl = (int)(s % KC);
-        double th = t[tab_index(17, sl)];
-        for (int k = 0; k < 17; ++k) th = fma(t[tab_index(k, sl)], endrow[k], th);
+        double th = fma(t[TAB_DW + sl], endrow[16], t[TAB_THETA0 + sl]);
+        for (int k = 0; k < NTERM; ++k) th = fma(t[tab_index(k, sl)], endrow[k], th);
         const double T = endrow[PREFIX_T];
         const cplx<double> m0 = xy[s];
         const double mag = hypot(m0.re, m0.im);
@@ -883,14 +934,24 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
 
 static size_t acc_bytes(int n_mma) { return sizeof(float) * (size_t)TM * (n_mma + ACC_PAD); }
 
-static int kernel_stages(int n_mma) {
-    const size_t budget = 220 * 1024;
+// Shared memory: 1 KB alignment slack, NSTAGE x (B operand + spin table),
+// NB turn-fraction buffers, the FP32 row accumulator and the barriers.
+constexpr size_t SMEM_LIMIT = 227 * 1024;
+constexpr size_t SMEM_FIXED = 1024 + 512;
+
+static int kernel_stages(int n_mma, int nbuf) {
     const size_t per = (size_t)b_bytes(n_mma) + SPIN_BYTES;
-    return (int)std::max<size_t>(2, std::min<size_t>(MAX_STAGE, (budget - 2048 - acc_bytes(n_mma)) / per));
+    const size_t used = SMEM_FIXED + acc_bytes(n_mma) + (size_t)nbuf * TURN_BYTES;
+    if (used >= SMEM_LIMIT) return 0;
+    return (int)std::min<size_t>(MAX_STAGE, (SMEM_LIMIT - used) / per);
 }
 
+static int kernel_nbuf(int n_mma) { return kernel_stages(n_mma, 2) >= 2 ? 2 : 1; }
+
 static size_t kernel_smem(int n_mma) {
-    return 1024 + (size_t)kernel_stages(n_mma) * (b_bytes(n_mma) + SPIN_BYTES) + acc_bytes(n_mma) + 32 * 8 + 64;
+    const int nb = kernel_nbuf(n_mma);
+    return SMEM_FIXED + (size_t)kernel_stages(n_mma, nb) * (b_bytes(n_mma) + SPIN_BYTES) + (size_t)nb * TURN_BYTES +
+           acc_bytes(n_mma);
 }
 
 // Number of chunk slabs per tile: the smallest that keeps the busiest CTA's
@@ -1001,7 +1062,12 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         ka.n_chunks = (int)nchunks;
         ka.tiles = (int)tiles;
         ka.slabs = slabs;
-        ka.nstage = kernel_stages(r.n_mma);
+        ka.nbuf = kernel_nbuf(r.n_mma);
+        ka.nstage = kernel_stages(r.n_mma, ka.nbuf);
+        if (ka.nstage < 2) {
+            *err = "split mode: too many coils for the kernel's shared memory";
+            return cudaSuccess;
+        }
         if (a.ev_start) cudaEventRecord(a.ev_start, stream);
         e = launch_precession(r.n_mma, ka, (unsigned)G, smem, stream);
         if (a.ev_stop) cudaEventRecord(a.ev_stop, stream);
