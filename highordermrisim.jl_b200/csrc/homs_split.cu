@@ -1,42 +1,47 @@
 // Split-precision fused precession + coil contraction on sm_100a tensor cores.
 //
 // Math (one precession segment = a run of consecutive precession blocks):
-//   phase in turns   theta(s,j) = sum_k b_k(s) * kappa_k(j),  k = 0..19
+//   phase in turns   theta(s,j) = theta0(s) + w(s) kappa_16(j) + sum_k b_k(s) kappa_k(j),  k = 0..15
 //     b_0..15  : the 16 solid-harmonic basis values of spin s (FP64, resident)
-//     b_16     : dw/(2 pi)               kappa_16 = -t_j
-//     b_17     : theta0 = arg(m0)/(2 pi) kappa_17 = 1
+//     w        : dw/(2 pi) (0 when dw is off),  kappa_16 = -t_j
+//     theta0   : arg(m0)/(2 pi)
 //     kappa_k  : -gamma * trapezoid integral of field column k from the segment
-//                start to ADC sample j (FP64 prefix table, k < 16)
+//                start to ADC sample j (FP64 prefix table)
 //   M(s,j)   = |m0| 2^(t_j * r2(s)) * cis(2 pi theta)   (r2 = -log2(e)/T2)
 //   S(j,c)   = sum_s M(s,j) csm(s,c)                      (no conjugation)
 // This is the reference's phi = -2 pi gamma cumtrapz(dt, Bz) and
 // Mxy = M0 exp(i phi - t/T2) (src/simulation/Bloch/BlochHighOrderSimulatitonMethod.jl:76-92)
 // with the cumulative integral factored into per-spin x per-sample terms.
 //
-// Precision: theta(s,j) is a small FP64 GEMM (samples x 20) * (20 x spins),
-// computed with FP64 tensor-core MMAs (mma.sync m8n8k4.f64).  One FP64 add of
-// 1.5*2^20 leaves frac(theta) as a 32-bit fixed-point turn count in the low
-// mantissa word (the mod-2pi range reduction, exact to 2^-32 turn).  A
-// quadrant select plus float32 polynomials (coefficients fitted by
-// fit_sincos.py) give cos/sin; the decay is one ex2.approx.  M is split into
-// TF32 hi + lo and the coil contraction runs as three TF32 tcgen05 MMAs per
-// K-step (hi*lo and lo*hi first, hi*hi last) with FP32 accumulation in TMEM,
-// one accumulator generation per 32-spin chunk, drained through an FP32
-// shared-memory accumulator into FP64 split-K partials.
+// Precision.  theta(s,j) is a small FP64 GEMM (samples x 16) * (16 x spins)
+// on FP64 tensor-core MMAs (mma.sync m8n8k4.f64), its accumulator initialised
+// with theta0 + w kappa_16.  One FP64 add of 1.5*2^20 leaves frac(theta) as a
+// 32-bit fixed-point turn count in the low mantissa word: the mod-2pi range
+// reduction, exact to 2^-32 turn.  cos/sin of 2 pi frac(theta) in [-pi, pi)
+// and the decay come from the SFU (sin/cos/ex2.approx).  M and the
+// sensitivities are split into FP16 hi + lo pairs after exact power-of-two
+// scaling (per coil, and per segment for the amplitude), and the coil
+// contraction runs as two kind::f16 tcgen05 MMAs per 16-deep K-step, each with
+// N = 2 x columns: A_lo x [B_hi | B_lo] first, then A_hi x [B_hi | B_lo], so
+// one accumulator generation (per 32-spin chunk) holds A.B_hi and A.B_lo side
+// by side.  The drain adds the two halves in FP32 into a TMEM row accumulator
+// and every WINDOW chunks promotes it into FP64 split-K partials; the final
+// sum undoes the scaling exactly.
 //
-// Kernel organisation (one CTA per SM, persistent, stream-K over
-// (time tile of 128 samples) x (chunk of 32 spins) units):
-//   warps 0-7  producers: warp w owns 16 sample rows of TMEM lane quarter
-//              w%4 and all 32 spins of each chunk; DMMA gives the phases in
-//              the m8n8 accumulator layout, which tcgen05.st.16x256b writes
-//              to TMEM rows unchanged (A operand).  The DMMAs of chunk k+1
-//              are issued between the FP32 steps of chunk k.  The same warps
-//              drain the TMEM accumulator (tcgen05.ld.32x32b, thread <->
-//              sample row).
-//   warp 8     MMA issuer: tcgen05.mma.kind::tf32 with A in TMEM, B (the
-//              sensitivities, pre-split) in shared memory; tcgen05.commit
-//              releases shared-memory stages, A stages and accumulators.
-//   warp 9     loader: cp.async.bulk of each chunk's B operand and spin table.
+// Kernel organisation (one CTA per SM, persistent, slab-major work items of
+// (time tile of 128 samples) x (range of 32-spin chunks)):
+//   warps 0-3   phase: warp q computes the turn fractions of tile rows
+//               32q..32q+31 for each chunk (DMMA) and writes them to TMEM in
+//               the m8n8 fragment layout (tcgen05.st.16x256b).
+//   warps 4-11  magnetisation: 16 sample rows of lane quarter w%4 each; read
+//               the turn fractions, form M, split it into FP16 hi/lo and write
+//               the A operand to TMEM; drain the accumulator.
+//   warp 12     MMA issuer: tcgen05.mma.kind::f16, A in TMEM, B (the
+//               sensitivities, pre-split) in shared memory; tcgen05.commit
+//               releases shared-memory stages, A buffers and accumulators.
+//   warp 13     loader: cp.async.bulk of each chunk's B operand and spin table.
+// TMEM (512 columns for N <= 64 output columns): accumulators 2 x 2N, A
+// operands 2 x 64, turn fractions 2 x 32, FP32 row accumulator N.
 // Every wait is bounded: on time-out the kernel records the place in a device
 // error word and returns without hanging the GPU.
 #include <algorithm>
@@ -44,6 +49,8 @@
 #include <cstring>
 #include <string>
 #include <vector>
+
+#include <cuda_fp16.h>
 
 #include "homs_common.cuh"
 #include "homs_split.cuh"
@@ -54,11 +61,12 @@ namespace split {
 
 constexpr int TM = 128;          // samples per tile (UMMA M)
 constexpr int KC = 32;           // spins per chunk
-constexpr int KSTEPS = 8;        // (2*KC real K values) / 8 per tf32 MMA
-constexpr int MAX_STAGE = 4;     // shared-memory stages (fewer for wide N)
+constexpr int KSTEPS = 4;        // (2*KC real K values) / 16 per f16 MMA
+constexpr int MAX_STAGE = 6;     // shared-memory stages of B operand + spin table
 constexpr int NTERM = 16;        // phase GEMM depth (DMMA K): the 16 basis terms
-constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_19, t, pad
+constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_16, t at PREFIX_T
 constexpr int PREFIX_T = 20;
+constexpr int GROUP_COILS = 32;  // coils per kernel pass (N <= 64 output columns)
 // Warp roles: 4 phase warps (one per SM sub-partition), 8 magnetisation warps
 // (2 per TMEM lane quarter), MMA issuer, loader -- at most 4 warps per
 // sub-partition, which leaves 128 registers per thread.
@@ -67,25 +75,24 @@ constexpr int NMAG_WARPS = 8;
 constexpr int MMA_WARP = 12;
 constexpr int LOAD_WARP = 13;
 constexpr int THREADS = 448;
-// Turn fractions of one chunk for one lane quarter: [mt 4][nt 4][lane 32] uint2.
-constexpr int TURN_TILE = 16 * 32;
-constexpr int TURN_BYTES = 4 * TURN_TILE * 8;
 constexpr uint32_t TMEM_COLS = 512;
-constexpr uint32_t A_COL0 = 256;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
 // Each 32-spin chunk is its own FP32 TMEM accumulator generation: the tensor
 // core's accumulator add is not round-to-nearest, and its error is systematic
-// and grows with |D| and with the number of MMAs per generation.
-// Chunks summed (round to nearest, FP32) in shared memory before promotion to
-// the FP64 partials, and the row padding of that accumulator (bank spread).
+// and grows with |D| and with the number of MMAs per generation.  The drain
+// adds generations (round to nearest, FP32) in a TMEM row accumulator and
+// promotes it to the FP64 partials every WINDOW chunks.
 constexpr int WINDOW = 32;
-constexpr int ACC_PAD = 4;
 
-// Sine/cosine coefficients on [-pi/4, pi/4] (see fit_sincos.py).
-constexpr float S1 = -0.16666650772094727f, S2 = 0.00833197869360447f, S3 = -0.00019495606829877943f;
-constexpr float C1 = -0.5f, C2 = 0.04166662320494652f, C3 = -0.0013886763481423259f, C4 = 2.439039235468954e-05f;
+// TMEM column map for N output columns (N <= 64).
+__host__ __device__ constexpr uint32_t d_col(int n, int buf) { return (uint32_t)(buf * 2 * n); }
+__host__ __device__ constexpr uint32_t a_col(int n, int buf) { return (uint32_t)(4 * n + buf * 64); }
+__host__ __device__ constexpr uint32_t t_col(int n, int tb) { return (uint32_t)(4 * n + 128 + tb * 32); }
+__host__ __device__ constexpr uint32_t acc_col(int n) { return (uint32_t)(4 * n + 192); }
 
-__host__ __device__ constexpr int b_bytes(int n_mma) { return 2 * KSTEPS * n_mma * 32; }
+// B operand of one chunk: KSTEPS slabs of 2N rows ([B_hi | B_lo]) x 16 f16,
+// no-swizzle K-major (core matrices of 8 rows x 16 bytes).
+__host__ __device__ constexpr int b_bytes(int n) { return KSTEPS * 2 * n * 32; }
 
 // Spin table of a chunk, in doubles: basis term k (0..15) of local spin s at
 // ((k/4)*KC + s)*4 + k%4, so that one DMMA B fragment (k = 4ks + tq, spin
@@ -97,14 +104,12 @@ constexpr int TAB_DW = TAB_THETA0 + KC;
 constexpr int TAB_PACK = TAB_DW + KC;
 constexpr int SPIN_BYTES = (TAB_PACK + KC) * 8;
 
-// K order of a chunk's A/B operands: spins 8P..8P+7 (one DMMA n-tile) fill
-// the 16 columns 16P + j, where column j holds spin 8P + 2*((j%8)/2) + j/8
-// (re for even j, im for odd j) -- the column order of tcgen05.st.16x256b.x2
-// applied to the m8n8 accumulator fragments.
-__host__ __device__ inline void k_to_spin(int k, int &s_local, int &imag) {
-    const int P = k >> 4, r = k & 15;
-    s_local = 8 * P + 2 * ((r & 7) >> 1) + (r >> 3);
-    imag = r & 1;
+// Smallest e with 2^e >= x for a non-negative double given by its bits (0 for 0).
+__host__ __device__ inline int pow2_ceil_exp(unsigned long long bits) {
+    if (bits == 0) return 0;
+    int e = (int)((bits >> 52) & 0x7FF) - 1023;
+    if (bits & 0xFFFFFFFFFFFFFull) e += 1;
+    return e;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -149,11 +154,12 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
-__device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
+
+__device__ __forceinline__ void tc_mma_f16(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
         "r"(a), "l"(bdesc), "r"(idesc), "r"(accum)
         : "memory");
 }
@@ -162,27 +168,51 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t d, uint32_t a, uint64_t bde
 // groupID; c: row groupID, cols 2*threadID_in_group + {0,1}).
 __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
     asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
 }
-// Round to TF32 (10 stored mantissa bits), nearest with ties away from zero:
-// add half of the 13 dropped bits to the magnitude, then clear them.
-__device__ __forceinline__ uint32_t tf32_rna(float x) { return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u; }
 __device__ __forceinline__ float ex2_approx(float x) {
     float r;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+__device__ __forceinline__ float sin_approx(float x) {
+    float r;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float cos_approx(float x) {
+    float r;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
-// 16 TMEM lanes x 16 columns: thread t writes lanes t/4 and t/4+8, columns
-// 2*(t%4)+{0,1} (v[0..3]) and 8+2*(t%4)+{0,1} (v[4..7]).
+// 16 TMEM lanes x 8r columns (r = 2 or 4 repetitions): thread t writes lanes
+// t/4 (v[4i], v[4i+1]) and t/4+8 (v[4i+2], v[4i+3]), columns 8i + 2*(t%4) + {0,1}.
 __device__ __forceinline__ void tmem_st_16x256b_x2(uint32_t taddr, const uint32_t *v) {
     asm volatile("tcgen05.st.sync.aligned.16x256b.x2.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
                  "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
                  : "memory");
 }
+__device__ __forceinline__ void tmem_st_16x256b_x4(uint32_t taddr, const uint32_t *v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.16x256b.x4.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_ld_16x256b_x4(uint32_t taddr, uint32_t *v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr)
+        : "memory");
+}
 // 32 TMEM lanes (thread <-> lane) x 8 or 16 consecutive columns.
-__device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, float *v) {
+__device__ __forceinline__ void tmem_ld_32x32b_x8(uint32_t taddr, float *v) {
     uint32_t r[8];
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
@@ -191,7 +221,7 @@ __device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, float *v) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
-__device__ __forceinline__ void tmem_ld_x16(uint32_t taddr, float *v) {
+__device__ __forceinline__ void tmem_ld_32x32b_x16(uint32_t taddr, float *v) {
     uint32_t r[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -202,6 +232,19 @@ __device__ __forceinline__ void tmem_ld_x16(uint32_t taddr, float *v) {
         : "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_st_32x32b_x8(uint32_t taddr, const float *v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_st_32x32b_x16(uint32_t taddr, const float *v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16};" ::"r"(taddr),
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
+        "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
+        : "memory");
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -223,14 +266,14 @@ struct KernelArgs {
     const double *prefix;      // [rows][PREFIX_STRIDE]
     const uint8_t *b_operand;  // [nchunks][b_bytes]
     const double *spin_table;  // [nchunks][SPIN_BYTES / 8]
-    double *partial;           // [tiles][slabs][TM][n_mma], FP64 split-K partials
+    const unsigned long long *amp_max;  // bits of max |m0| over the segment's spins
+    double *partial;           // [tiles][slabs][TM][N], FP64 split-K partials
     unsigned int *err;
     int64_t nsamples;
     int n_chunks;
     int tiles;
     int slabs;
     int nstage;  // shared-memory stages of B operand + spin table
-    int nbuf;    // turn-fraction buffers between phase and magnetisation warps (1 or 2)
 };
 
 struct Item {
@@ -245,45 +288,36 @@ __device__ __forceinline__ Item item_of(const KernelArgs &a, int i) {
     return it;
 }
 
-// frac(th) * 2^32 of an FP64 turn count |th| < 2^18: adding 1.5 * 2^20 puts
-// the fraction's leading 32 bits in the low word (the mod-2pi reduction).
-__device__ __forceinline__ uint32_t turn_fraction(double th) {
-    return (uint32_t)__double2loint(th + 1572864.0);
+// The phase accumulator starts at TURN_BIAS + theta0 + w kappa_16: with
+// |theta| < 2^18, every partial sum stays in [2^20, 2^21), where the FP64
+// spacing is 2^-32, so the low mantissa word of the result is frac(theta)
+// * 2^32 (the mod-2pi range reduction) and each DMMA add rounds at 2^-33 turn.
+constexpr double TURN_BIAS = 1572864.0;  // 1.5 * 2^20
+__device__ __forceinline__ uint32_t turn_fraction(double biased_th) { return (uint32_t)__double2loint(biased_th); }
+
+// A operand words of one spin-sample: M = 2^(tj r2 + l2) cis(2 pi u / 2^32),
+// split into FP16 hi + lo, each packed as (re low half, im high half).
+__device__ __forceinline__ void magnetisation(uint32_t u, float tj, float r2, float l2, uint32_t &hi, uint32_t &lo) {
+    const float x = (float)(int32_t)u * 1.4629180792671596e-09f;  // 2 pi / 2^32, x in [-pi, pi)
+    const float a = ex2_approx(fmaf(tj, r2, l2));
+    const float mre = a * cos_approx(x), mim = a * sin_approx(x);
+    const __half2 h = __floats2half2_rn(mre, mim);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(mre - hf.x, mim - hf.y);
+    hi = *reinterpret_cast<const uint32_t *>(&h);
+    lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-// M(s,j) for one spin from its 32-bit turn fraction u; returns (re, im).
-__device__ __forceinline__ void magnetisation(uint32_t u, float tj, float r2, float l2m0, float &mre, float &mim) {
-    // u = q' 2^30 + r: quadrant q = nearest quarter turn = (u + 2^29) >> 30, and
-    // (int)(u << 2) = 4 * (r as a signed 30-bit offset from it), in [-2^31, 2^31).
-    const uint32_t v = u + 0x20000000u;
-    const float x = (float)(int32_t)(u << 2) * 3.6572951981678990e-10f;  // 2 pi / 2^34
-    const float x2 = x * x;
-    const float sp = fmaf(x * x2, fmaf(x2, fmaf(x2, S3, S2), S1), x);
-    const float cp = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, C4, C3), C2), C1), 1.0f);
-    // cis(x + q*pi/2): swap for odd q (bit 30 of v), negate cos for q in {1,2}
-    // (bit 31 of v + 2^30), negate sin for q in {2,3} (bit 31 of v).
-    const bool swap = (v & 0x40000000u) != 0;
-    const uint32_t cbits = __float_as_uint(swap ? sp : cp) ^ ((v + 0x40000000u) & 0x80000000u);
-    const uint32_t sbits = __float_as_uint(swap ? cp : sp) ^ (v & 0x80000000u);
-    const float c = __uint_as_float(cbits), s = __uint_as_float(sbits);
-    const float a = ex2_approx(fmaf(tj, r2, l2m0));
-    mre = a * c;
-    mim = a * s;
-}
-
-template <int N_MMA>
+template <int N>
 __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
-    constexpr int BB = b_bytes(N_MMA);
-    constexpr int NCOL = N_MMA / 2;  // accumulator columns drained per magnetisation thread
+    constexpr int BB = b_bytes(N);
+    constexpr int HALF = N / 2;  // accumulator columns drained per magnetisation thread
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const int NSTAGE = args.nstage;
-    const int NB = args.nbuf;
     uint8_t *sB = smem;                                             // NSTAGE * BB
     double *sSpin = reinterpret_cast<double *>(sB + NSTAGE * BB);  // NSTAGE * SPIN_BYTES
-    uint2 *sTurn = reinterpret_cast<uint2 *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);  // NB * TURN_BYTES
-    float *accf = reinterpret_cast<float *>(reinterpret_cast<uint8_t *>(sTurn) + NB * TURN_BYTES);  // TM x (N_MMA+pad)
-    uint64_t *bars = reinterpret_cast<uint64_t *>(accf + (size_t)TM * (N_MMA + ACC_PAD));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);
     uint64_t *full = bars;                    // [NSTAGE] loader -> consumers (tx)
     uint64_t *empty = bars + MAX_STAGE;       // [NSTAGE] MMA commit -> loader
     uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] magnetisation warps -> MMA
@@ -357,8 +391,8 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         __syncwarp();
     } else if (warp == MMA_WARP) {
         if (lane == 0) {
-            constexpr uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N_MMA >> 3) << 17) |
-                                       ((uint32_t)(TM >> 4) << 24);
+            // kind::f16: D f32 (bit 4), A and B f16 (format 0), both K-major; N = 2N columns.
+            constexpr uint32_t idesc = (1u << 4) | ((uint32_t)((2 * N) >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
             int g = 0;  // chunks issued; chunk g uses A buffer and accumulator g % 2
             int stage = 0;
             uint32_t fph = 0;  // parity of full[stage] for chunk g
@@ -377,26 +411,19 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t dcol = tmem + (uint32_t)(buf * N_MMA);
+                    const uint32_t dcol = tmem + d_col(N, buf);
+                    const uint32_t acol = tmem + a_col(N, buf);
                     const uint32_t sbase = smem_u32(sB + (size_t)stage * BB);
-                    const uint32_t a_hi = tmem + A_COL0 + (uint32_t)buf * 128u;
-                    const uint32_t a_lo = a_hi + 64u;
-                    // Each chunk is its own accumulator generation.  The
-                    // accumulator add of each MMA rounds relative to |D|, so the
-                    // two small cross-term passes (hi*lo, lo*hi) go first, while
-                    // D is small, and hi*hi last.
+                    // Each chunk is its own accumulator generation; the small
+                    // lo pass goes first, while D is small, then the hi pass.
 #pragma unroll
-                    for (int ks = 0; ks < KSTEPS; ++ks) {
-                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * N_MMA * 32));
-                        const uint64_t blo = bdesc(sbase + (uint32_t)((KSTEPS + ks) * N_MMA * 32));
-                        tc_mma_tf32(dcol, a_hi + ks * 8, blo, idesc, ks == 0 ? 0u : 1u);
-                        tc_mma_tf32(dcol, a_lo + ks * 8, bhi, idesc, 1u);
-                    }
+                    for (int ks = 0; ks < KSTEPS; ++ks)
+                        tc_mma_f16(dcol, acol + 32u + (uint32_t)ks * 8u, bdesc(sbase + (uint32_t)(ks * 2 * N * 32)),
+                                   idesc, ks == 0 ? 0u : 1u);
 #pragma unroll
-                    for (int ks = 0; ks < KSTEPS; ++ks) {
-                        const uint64_t bhi = bdesc(sbase + (uint32_t)(ks * N_MMA * 32));
-                        tc_mma_tf32(dcol, a_hi + ks * 8, bhi, idesc, 1u);
-                    }
+                    for (int ks = 0; ks < KSTEPS; ++ks)
+                        tc_mma_f16(dcol, acol + (uint32_t)ks * 8u, bdesc(sbase + (uint32_t)(ks * 2 * N * 32)), idesc,
+                                   1u);
                     tc_commit(&empty[stage]);
                     tc_commit(&a_empty[buf]);
                     tc_commit(&d_full[buf]);
@@ -412,10 +439,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         }
         __syncwarp();
     } else if (warp < NPHASE_WARPS) {
-        // Phase warp q: the FP64 phase tile of tile rows 32q..32q+31 (4 x 4 DMMA
+        // Phase warp q: turn fractions of tile rows 32q..32q+31 (4 x 4 DMMA
         // 8x8 tiles per chunk, K = 16), accumulators initialised with
-        // theta0 + (dw/2pi) * kappa_16, reduced to 32-bit turn fractions.
+        // theta0 + w kappa_16; written to TMEM columns t_col(tb) + spin.
         const int q = warp;
+        const uint32_t t_lane = (uint32_t)(q * 32) << 16;
         int stage = 0, tb = 0;
         uint32_t fph = 0, tk = 0;  // parities of full[stage] and of this use of turn buffer tb
         for (int i = blockIdx.x; i < n_items && !dead; i += G) {
@@ -440,11 +468,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     dead = true;
                     break;
                 }
+                tc_fence_after();
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                uint2 *dst = sTurn + (size_t)(tb * 4 + q) * TURN_TILE;
+                const uint32_t tcol = tmem + t_col(N, tb) + t_lane;
                 // Two spin groups at a time: 8 independent accumulator chains,
-                // k-step outermost, so that consecutive DMMAs never depend on
-                // one another and the FP64 pipe, not the DMMA latency, sets the pace.
+                // k-step outermost.
 #pragma unroll
                 for (int np = 0; np < 2; ++np) {
                     double bf[2][4], th[2][4][2];
@@ -455,10 +483,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                         for (int ks = 0; ks < 4; ++ks) bf[n2][ks] = tab[tab_index(4 * ks + tq, 8 * nt + gq)];
                         const double2 t0 = *reinterpret_cast<const double2 *>(tab + TAB_THETA0 + 8 * nt + 2 * tq);
                         const double2 dw = *reinterpret_cast<const double2 *>(tab + TAB_DW + 8 * nt + 2 * tq);
+                        const double b0 = t0.x + TURN_BIAS, b1 = t0.y + TURN_BIAS;
 #pragma unroll
                         for (int mt = 0; mt < 4; ++mt) {
-                            th[n2][mt][0] = fma(dw.x, k16[mt], t0.x);
-                            th[n2][mt][1] = fma(dw.y, k16[mt], t0.y);
+                            th[n2][mt][0] = fma(dw.x, k16[mt], b0);
+                            th[n2][mt][1] = fma(dw.y, k16[mt], b1);
                         }
                     }
 #pragma unroll
@@ -468,20 +497,30 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 #pragma unroll
                             for (int mt = 0; mt < 4; ++mt)
                                 dmma_8x8x4(th[n2][mt][0], th[n2][mt][1], ka[mt][ks], bf[n2][ks]);
+                    // Rows 16p..16p+15 (mt = 2p, 2p+1), spin groups 2np, 2np+1:
+                    // 16x256b.x2 register order [4 n2 + 2 (mt & 1) + i].
 #pragma unroll
-                    for (int n2 = 0; n2 < 2; ++n2)
+                    for (int p = 0; p < 2; ++p) {
+                        uint32_t v[8];
 #pragma unroll
-                        for (int mt = 0; mt < 4; ++mt)
-                            dst[(mt * 4 + 2 * np + n2) * 32 + lane] =
-                                make_uint2(turn_fraction(th[n2][mt][0]), turn_fraction(th[n2][mt][1]));
+                        for (int n2 = 0; n2 < 2; ++n2)
+#pragma unroll
+                            for (int m1 = 0; m1 < 2; ++m1)
+#pragma unroll
+                                for (int ii = 0; ii < 2; ++ii)
+                                    v[4 * n2 + 2 * m1 + ii] = turn_fraction(th[n2][2 * p + m1][ii]);
+                        tmem_st_16x256b_x2(tcol + ((uint32_t)(16 * p) << 16) + (uint32_t)(16 * np), v);
+                    }
                 }
+                tmem_wait_st();
+                tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&t_full[q * 2 + tb]);
                 if (++stage == NSTAGE) {
                     stage = 0;
                     fph ^= 1u;
                 }
-                if (++tb == NB) {
+                if (++tb == 2) {
                     tb = 0;
                     tk ^= 1u;
                 }
@@ -491,23 +530,22 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         // Magnetisation warp w: TMEM lane quarter q = w % 4, half h: tile rows
         // 32q + 16h .. +15 (phase tiles mt = 2h, 2h+1 of quarter q) and all 32
         // spins of each chunk.  For the accumulator drain it takes thread <->
-        // tile row 32q + lane and column half h.
+        // tile row 32q + lane and output columns [h N/2, (h+1) N/2).
         const int q = warp & 3, h = (warp - NPHASE_WARPS) >> 2;
-        const uint32_t q_base = (uint32_t)(q * 32) << 16;
-        const uint32_t a_lane = (uint32_t)(q * 32 + h * 16) << 16;
+        const uint32_t q_lane = (uint32_t)(q * 32) << 16;
+        const uint32_t m_lane = (uint32_t)(q * 32 + h * 16) << 16;
         const int row = q * 32 + lane;
-        float *arow = accf + (size_t)row * (N_MMA + ACC_PAD) + h * NCOL;
+        // Amplitude scale of the segment: M is formed as M / 2^eA (|M| <= 1).
+        const float l2off = (float)pow2_ceil_exp(*args.amp_max);
         int g = 0;  // chunks produced by this CTA
         int stage = 0, tb = 0;
         uint32_t tk = 0;
-        // Two-level drain of each chunk's accumulator generation: the FP32
-        // TMEM result is added (round to nearest) into this thread's FP32 row
-        // accumulator in shared memory; every WINDOW chunks, and at the end of
-        // an item, that row is promoted into the FP64 split-K partial.  The
-        // drain of chunk g runs after the A operand of chunk g+1 is written.
-        int pend = -1;  // chunk whose accumulator waits to be drained
+        int pend = -1;  // chunk whose accumulator generation waits to be drained
         double *pend_dst = nullptr;
         bool pend_wfirst = false, pend_promote = false, pend_pfirst = false;
+        // Drain: add the generation's two halves (A.B_hi, A.B_lo) into the
+        // FP32 row accumulator in TMEM; every WINDOW chunks, and at the end of
+        // an item, add the accumulator into the FP64 split-K partial instead.
         auto drain = [&]() -> bool {
             const int buf = pend & 1;
             const bool ok = mbar_wait(&d_full[buf], (uint32_t)((pend >> 1) & 1));
@@ -517,43 +555,47 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 return false;
             }
             tc_fence_after();
-            const uint32_t ta = tmem + q_base + (uint32_t)(buf * N_MMA + h * NCOL);
+            const uint32_t dsrc = tmem + q_lane + d_col(N, buf) + (uint32_t)(h * HALF);
+            const uint32_t asrc = tmem + q_lane + acc_col(N) + (uint32_t)(h * HALF);
 #pragma unroll
-            for (int cb = 0; cb < NCOL; cb += 16) {
-                float v[16];
-                const int w = (NCOL - cb) >= 16 ? 16 : 8;
-                if (w == 16)
-                    tmem_ld_x16(ta + (uint32_t)cb, v);
-                else
-                    tmem_ld_x8(ta + (uint32_t)cb, v);
+            for (int cb = 0; cb < HALF; cb += 16) {
+                constexpr int W0 = HALF >= 16 ? 16 : 8;
+                const int w = (HALF - cb) >= 16 ? 16 : 8;
+                (void)W0;
+                float d1[16], d2[16], ac[16];
+                if (w == 16) {
+                    tmem_ld_32x32b_x16(dsrc + (uint32_t)cb, d1);
+                    tmem_ld_32x32b_x16(dsrc + (uint32_t)(N + cb), d2);
+                    if (!pend_wfirst) tmem_ld_32x32b_x16(asrc + (uint32_t)cb, ac);
+                } else {
+                    tmem_ld_32x32b_x8(dsrc + (uint32_t)cb, d1);
+                    tmem_ld_32x32b_x8(dsrc + (uint32_t)(N + cb), d2);
+                    if (!pend_wfirst) tmem_ld_32x32b_x8(asrc + (uint32_t)cb, ac);
+                }
                 tmem_wait_ld();
-                if (cb + 16 >= NCOL) {
+                if (cb + 16 >= HALF) {
                     tc_fence_before();
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&d_empty[buf]);
                 }
 #pragma unroll
-                for (int c4 = 0; c4 < 4; ++c4) {
-                    if (c4 * 4 < w) {
-                        float *ap = arow + cb + c4 * 4;
-                        float4 a = pend_wfirst ? make_float4(0.f, 0.f, 0.f, 0.f) : *reinterpret_cast<float4 *>(ap);
-                        a.x += v[c4 * 4 + 0];
-                        a.y += v[c4 * 4 + 1];
-                        a.z += v[c4 * 4 + 2];
-                        a.w += v[c4 * 4 + 3];
-                        *reinterpret_cast<float4 *>(ap) = a;
+                for (int e = 0; e < 16; ++e)
+                    if (e < w) d1[e] = pend_wfirst ? d1[e] + d2[e] : (d1[e] + d2[e]) + ac[e];
+                if (pend_promote) {
+                    double *d = pend_dst + cb;
+#pragma unroll
+                    for (int e = 0; e < 16; e += 2) {
+                        if (e < w) {
+                            double2 o = pend_pfirst ? make_double2(0.0, 0.0) : *reinterpret_cast<double2 *>(d + e);
+                            o.x += (double)d1[e];
+                            o.y += (double)d1[e + 1];
+                            *reinterpret_cast<double2 *>(d + e) = o;
+                        }
                     }
-                }
-            }
-            if (pend_promote) {
-#pragma unroll 4
-                for (int cc = 0; cc < NCOL; cc += 2) {
-                    const float2 a = *reinterpret_cast<const float2 *>(arow + cc);
-                    double2 *d = reinterpret_cast<double2 *>(pend_dst + cc);
-                    double2 o = pend_pfirst ? make_double2(0.0, 0.0) : *d;
-                    o.x += (double)a.x;
-                    o.y += (double)a.y;
-                    *d = o;
+                } else if (w == 16) {
+                    tmem_st_32x32b_x16(asrc + (uint32_t)cb, d1);
+                } else {
+                    tmem_st_32x32b_x8(asrc + (uint32_t)cb, d1);
                 }
             }
             pend = -1;
@@ -562,7 +604,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         for (int i = blockIdx.x; i < n_items && !dead; i += G) {
             const Item it = item_of(args, i);
             double *dst_piece =
-                args.partial + (((size_t)it.tile * args.slabs + it.z) * TM + row) * (size_t)N_MMA + h * NCOL;
+                args.partial + (((size_t)it.tile * args.slabs + it.z) * TM + row) * (size_t)N + h * HALF;
             float tj[2];
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
@@ -581,43 +623,33 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     break;
                 }
                 tc_fence_after();
-                // This thread's turn fractions: phase tile (2h + mt, nt).
-                const uint2 *src = sTurn + (size_t)(tb * 4 + q) * TURN_TILE;
-                uint2 tu[2][4];
-#pragma unroll
-                for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                    for (int nt = 0; nt < 4; ++nt) tu[mt][nt] = src[((2 * h + mt) * 4 + nt) * 32 + lane];
+                // Turn fractions of rows 16h + 8mt + gq, spins 8nt + 2tq + i:
+                // 16x256b.x4 register order [4 nt + 2 mt + i].
+                uint32_t tu[16];
+                tmem_ld_16x256b_x4(tmem + t_col(N, tb) + m_lane, tu);
+                tmem_wait_ld();
+                tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&t_empty[q * 2 + tb]);
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                const uint32_t a_col = tmem + A_COL0 + (uint32_t)buf * 128u + a_lane;
+                uint32_t hi[16], lo[16];
 #pragma unroll
                 for (int nt = 0; nt < 4; ++nt) {
                     // This thread's spins of group nt: 8nt + 2tq + i.
                     const float4 rl = *reinterpret_cast<const float4 *>(tab + TAB_PACK + 8 * nt + 2 * tq);
                     const float r2v[2] = {rl.x, rl.z};
-                    const float l2v[2] = {rl.y, rl.w};
-                    // 16x256b.x2 register order: [i*4 + mt*2 + comp] for
-                    // spin 2tq + i (column 8i + 2tq + comp), row 8mt + gq.
-                    uint32_t hi[8], lo[8];
+                    const float l2v[2] = {rl.y - l2off, rl.w - l2off};
 #pragma unroll
-                    for (int mt = 0; mt < 2; ++mt) {
+                    for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
                         for (int ii = 0; ii < 2; ++ii) {
-                            float mre, mim;
-                            magnetisation(ii ? tu[mt][nt].y : tu[mt][nt].x, tj[mt], r2v[ii], l2v[ii], mre, mim);
-                            const uint32_t hr = tf32_rna(mre), hm = tf32_rna(mim);
-                            const int e = ii * 4 + mt * 2;
-                            hi[e] = hr;
-                            hi[e + 1] = hm;
-                            lo[e] = tf32_rna(mre - __uint_as_float(hr));
-                            lo[e + 1] = tf32_rna(mim - __uint_as_float(hm));
+                            const int e = 4 * nt + 2 * mt + ii;
+                            magnetisation(tu[e], tj[mt], r2v[ii], l2v[ii], hi[e], lo[e]);
                         }
-                    }
-                    tmem_st_16x256b_x2(a_col + (uint32_t)nt * 16u, hi);
-                    tmem_st_16x256b_x2(a_col + 64u + (uint32_t)nt * 16u, lo);
                 }
+                const uint32_t acol = tmem + a_col(N, buf) + m_lane;
+                tmem_st_16x256b_x4(acol, hi);
+                tmem_st_16x256b_x4(acol + 32u, lo);
                 tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
@@ -636,7 +668,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 pend_pfirst = ci < WINDOW;
                 ++g;
                 if (++stage == NSTAGE) stage = 0;
-                if (++tb == NB) {
+                if (++tb == 2) {
                     tb = 0;
                     tk ^= 1u;
                 }
@@ -656,12 +688,15 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     }
 }
 
-// Sum the split-K partials of each (sample, column) in slab order (FP64) and
-// write complex samples: column n < nc is Re S(j, n), nc <= n < 2nc is Im.
+// Sum the split-K partials of each (sample, column) in slab order (FP64),
+// undo the power-of-two scaling of the operands and write complex samples:
+// column n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
 template <typename T>
-__global__ void split_finalize_kernel(const double *partial, int64_t nsamples, int32_t nc, int n_mma, int slabs,
-                                      cplx<T> *sig, int64_t ldsig) {
-    const int64_t total = nsamples * nc;
+__global__ void split_finalize_kernel(const double *partial, int64_t nsamples, int32_t ncg, int n_cols, int slabs,
+                                      const int *coil_exp, const unsigned long long *amp_max, cplx<T> *sig,
+                                      int64_t ldsig) {
+    const int64_t total = nsamples * ncg;
+    const int ea = pow2_ceil_exp(*amp_max);
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t j = i % nsamples;
@@ -670,11 +705,12 @@ __global__ void split_finalize_kernel(const double *partial, int64_t nsamples, i
         const int row = (int)(j % TM);
         double re = 0.0, im = 0.0;
         for (int z = 0; z < slabs; ++z) {
-            const double *src = partial + (((size_t)tile * slabs + z) * TM + row) * (size_t)n_mma;
+            const double *src = partial + (((size_t)tile * slabs + z) * TM + row) * (size_t)n_cols;
             re += src[c];
-            im += src[nc + c];
+            im += src[ncg + c];
         }
-        sig[j + (int64_t)c * ldsig] = cplx<T>{T(re), T(im)};
+        const int e = coil_exp[c] + ea;
+        sig[j + (int64_t)c * ldsig] = cplx<T>{T(ldexp(re, e)), T(ldexp(im, e))};
     }
 }
 
@@ -705,49 +741,75 @@ __global__ void basis_kernel(const double *x, const double *y, const double *z, 
     }
 }
 
-// Sensitivities -> TF32 hi/lo B operand in the no-swizzle K-major layout, K
-// permuted as k_to_spin.  With real K index kk of spin s:
-//   B[n][kk] = (n < nc ? Re c(s,n) : Im c(s,n-nc))   for the re column,
-//   B[n][kk] = (n < nc ? -Im c(s,n) : Re c(s,n-nc))  for the im column.
-__global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_mma, int64_t nchunks,
-                                 float *out) {
-    const int64_t per_chunk = (int64_t)KSTEPS * n_mma * 8;
-    const int64_t total = nchunks * per_chunk;
+
+// Largest |Re| or |Im| of each coil's sensitivity (bits of a non-negative
+// double, combined with an unsigned max).
+__global__ void coil_max_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, unsigned long long *mx) {
+    const int64_t total = ns * nc;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t chunk = i / per_chunk;
+        const cplx<double> v = csm_rows[i];
+        const double m = fmax(fabs(v.re), fabs(v.im));
+        atomicMax(&mx[i % nc], (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__global__ void coil_exp_kernel(const unsigned long long *mx, int32_t nc, int *coil_exp) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x)
+        coil_exp[c] = pow2_ceil_exp(mx[c]);
+}
+
+// Sensitivities -> FP16 hi/lo B operand, per coil group of GROUP_COILS coils,
+// scaled by 2^-e(coil) so that every entry is at most 1 in magnitude.  Real
+// K index k = 2 s + comp of local spin s:
+//   B[n][k] = (n < ncg ? Re c(s,n) : Im c(s,n-ncg))   for comp = 0 (re of M),
+//   B[n][k] = (n < ncg ? -Im c(s,n) : Re c(s,n-ncg))  for comp = 1 (im of M);
+// rows 0..N-1 of each K-step slab hold the hi parts, rows N..2N-1 the lo parts.
+__global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_cols, int64_t nchunks,
+                                 int ngroups, const int *coil_exp, __half *out) {
+    const int64_t per_chunk = (int64_t)KSTEPS * 2 * n_cols * 16;
+    const int64_t total = (int64_t)ngroups * nchunks * per_chunk;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t gc = i / per_chunk;  // group * nchunks + chunk
+        const int grp = (int)(gc / nchunks);
+        const int64_t chunk = gc % nchunks;
         int64_t r = i % per_chunk;
-        const int ks = (int)(r / (n_mma * 8));
-        r %= (n_mma * 8);
-        const int n = (int)(r / 8), kk = (int)(r % 8);
-        int s_local, imrow;
-        k_to_spin(ks * 8 + kk, s_local, imrow);
-        const int64_t s = chunk * KC + s_local;
+        const int ks = (int)(r / (2 * n_cols * 16));
+        r %= (2 * n_cols * 16);
+        const int nn = (int)(r / 16), kk = (int)(r % 16);
+        const bool lopart = nn >= n_cols;
+        const int n = lopart ? nn - n_cols : nn;
+        const int k = 16 * ks + kk;
+        const int64_t s = chunk * KC + (k >> 1);
+        const int comp = k & 1;
+        const int coil0 = grp * GROUP_COILS;
+        const int ncg = min(GROUP_COILS, nc - coil0);
         double v = 0.0;
-        if (s < ns && n < 2 * nc) {
-            const cplx<double> c = csm_rows[s * nc + (n < nc ? n : n - nc)];
-            if (n < nc) v = imrow ? -c.im : c.re;
-            else v = imrow ? c.re : c.im;
+        if (s < ns && n < 2 * ncg) {
+            const int coil = coil0 + (n < ncg ? n : n - ncg);
+            const cplx<double> cv = csm_rows[s * nc + coil];
+            if (n < ncg) v = comp ? -cv.im : cv.re;
+            else v = comp ? cv.re : cv.im;
+            v = ldexp(v, -coil_exp[coil]);
         }
-        const float vf = (float)v;
-        const uint32_t hb = tf32_rna(vf);
-        // lo carries what the TF32 hi misses of the FP64 value.
-        const uint32_t lb = tf32_rna((float)(v - (double)__uint_as_float(hb)));
-        const size_t off = (size_t)(n / 8) * 256 + (size_t)(kk / 4) * 128 + (size_t)(n % 8) * 16 + (size_t)(kk % 4) * 4;
-        uint8_t *base = reinterpret_cast<uint8_t *>(out) + (size_t)chunk * b_bytes(n_mma);
-        *reinterpret_cast<uint32_t *>(base + (size_t)ks * n_mma * 32 + off) = hb;
-        *reinterpret_cast<uint32_t *>(base + (size_t)(KSTEPS + ks) * n_mma * 32 + off) = lb;
+        const __half hb = __double2half(v);
+        const __half lb = __double2half(v - (double)__half2float(hb));
+        const size_t off = (size_t)(nn / 8) * 256 + (size_t)(kk / 8) * 128 + (size_t)(nn % 8) * 16 + (size_t)(kk % 8) * 2;
+        uint8_t *base = reinterpret_cast<uint8_t *>(out) + (size_t)gc * b_bytes(n_cols) + (size_t)ks * 2 * n_cols * 32;
+        *reinterpret_cast<__half *>(base + off) = lopart ? lb : hb;
     }
 }
 
 // Spin table of a segment, from the state at its start (layout of
 // tab_index per chunk): the 16 basis terms, theta0 = arg(m0)/(2 pi), dw/(2 pi)
 // (0 if dw is off in precession) and the packed float2 (-log2(e)/T2,
-// log2|m0|).  Also checks the phase range: |theta| must stay below 2^18
-// turns for the fixed-point reduction (error bit 64 otherwise).
+// log2|m0|).  Also records the largest |m0| (amplitude scale of the FP16
+// operand) and checks the phase range: |theta| must stay below 2^18 turns for
+// the fixed-point reduction (error bit 64 otherwise).
 __global__ void spin_table_kernel(const double *basis, const double *dw, const double *T2, const cplx<double> *xy,
                                   int64_t ns, int64_t nchunks, uint32_t method, const double *colmax,
-                                  unsigned int *err, double *table) {
+                                  unsigned int *err, unsigned long long *amp_max, double *table) {
     const int64_t total = nchunks * KC;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total;
          s += (int64_t)gridDim.x * blockDim.x) {
@@ -768,6 +830,7 @@ __global__ void spin_table_kernel(const double *basis, const double *dw, const d
             if (!(bound < 262144.0)) atomicOr(err, 64u);
             rl.x = (float)(-1.4426950408889634 / T2[s]);
             rl.y = mag > 0.0 ? (float)log2(mag) : -INFINITY;
+            if (mag > 0.0) atomicMax(amp_max, (unsigned long long)__double_as_longlong(mag));
         }
         for (int k = 0; k < NTERM; ++k) t[tab_index(k, sl)] = row[k];
         t[TAB_THETA0 + sl] = theta0;
@@ -880,12 +943,13 @@ __global__ void state_update_kernel(const double *table, const double *endrow, c
 
 inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
 
+
 }  // namespace split
 
 using namespace split;
 
 SplitResident::~SplitResident() {
-    for (void *p : {basis, b_operand, spin_table, prefix, tvec, partial, tile_map, err})
+    for (void *p : {basis, b_operand, spin_table, prefix, tvec, partial, coil_exp, amp, err})
         if (p) cudaFree(p);
 }
 
@@ -908,50 +972,53 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
             "split path's error budget";
         return cudaSuccess;
     }
-    const int n_mma = std::max(16, ((2 * nc + 15) / 16) * 16);
-    if (n_mma > 128) {
-        *err = "split mode supports at most 64 coils per run";
-        return cudaSuccess;
-    }
+    const int ngroups = (nc + GROUP_COILS - 1) / GROUP_COILS;
+    const int ncg_max = std::min<int32_t>(nc, GROUP_COILS);
+    const int n_cols = std::max(16, ((2 * ncg_max + 15) / 16) * 16);
     r.ns = ns;
     r.nc = nc;
-    r.n_mma = n_mma;
+    r.n_mma = n_cols;
+    r.ngroups = ngroups;
     const int64_t nchunks = (ns + KC - 1) / KC;
     r.ns_pad = nchunks * KC;
     cudaError_t e;
     if ((e = grow(r.basis, r.basis_bytes, sizeof(double) * 16 * (size_t)ns)) != cudaSuccess) return e;
-    if ((e = grow(r.b_operand, r.b_bytes, (size_t)b_bytes(n_mma) * (size_t)nchunks)) != cudaSuccess) return e;
+    if ((e = grow(r.b_operand, r.b_bytes, (size_t)b_bytes(n_cols) * (size_t)nchunks * ngroups)) != cudaSuccess)
+        return e;
+    // Per-coil scale exponents, preceded by the per-coil maxima they come from.
+    if ((e = grow(r.coil_exp, r.coil_exp_bytes, (sizeof(unsigned long long) + sizeof(int)) * (size_t)nc)) !=
+        cudaSuccess)
+        return e;
+    if (!r.amp) {
+        if ((e = cudaMalloc(&r.amp, sizeof(unsigned long long))) != cudaSuccess) return e;
+    }
     if (!r.err) {
         if ((e = cudaMalloc(&r.err, sizeof(unsigned int))) != cudaSuccess) return e;
     }
+    unsigned long long *cmax = reinterpret_cast<unsigned long long *>(r.coil_exp);
+    int *cexp = reinterpret_cast<int *>(cmax + nc);
     basis_kernel<<<grid_for(ns), 256, 0, stream>>>((const double *)x, (const double *)y, (const double *)z, ns,
                                                    (double *)r.basis);
-    const int64_t total = nchunks * KSTEPS * n_mma * 8;
-    b_operand_kernel<<<grid_for(total), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_mma, nchunks,
-                                                          (float *)r.b_operand);
+    if ((e = cudaMemsetAsync(cmax, 0, sizeof(unsigned long long) * (size_t)nc, stream)) != cudaSuccess) return e;
+    coil_max_kernel<<<grid_for(ns * nc), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, cmax);
+    coil_exp_kernel<<<1, 128, 0, stream>>>(cmax, nc, cexp);
+    const int64_t total = (int64_t)ngroups * nchunks * KSTEPS * 2 * n_cols * 16;
+    b_operand_kernel<<<grid_for(total), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_cols, nchunks,
+                                                          ngroups, cexp, (__half *)r.b_operand);
     return cudaGetLastError();
 }
 
-static size_t acc_bytes(int n_mma) { return sizeof(float) * (size_t)TM * (n_mma + ACC_PAD); }
-
-// Shared memory: 1 KB alignment slack, NSTAGE x (B operand + spin table),
-// NB turn-fraction buffers, the FP32 row accumulator and the barriers.
+// Shared memory: 1 KB alignment slack, NSTAGE x (B operand + spin table), the barriers.
 constexpr size_t SMEM_LIMIT = 227 * 1024;
 constexpr size_t SMEM_FIXED = 1024 + 512;
 
-static int kernel_stages(int n_mma, int nbuf) {
-    const size_t per = (size_t)b_bytes(n_mma) + SPIN_BYTES;
-    const size_t used = SMEM_FIXED + acc_bytes(n_mma) + (size_t)nbuf * TURN_BYTES;
-    if (used >= SMEM_LIMIT) return 0;
-    return (int)std::min<size_t>(MAX_STAGE, (SMEM_LIMIT - used) / per);
+static int kernel_stages(int n_cols) {
+    const size_t per = (size_t)b_bytes(n_cols) + SPIN_BYTES;
+    return (int)std::min<size_t>(MAX_STAGE, (SMEM_LIMIT - SMEM_FIXED) / per);
 }
 
-static int kernel_nbuf(int n_mma) { return kernel_stages(n_mma, 2) >= 2 ? 2 : 1; }
-
-static size_t kernel_smem(int n_mma) {
-    const int nb = kernel_nbuf(n_mma);
-    return SMEM_FIXED + (size_t)kernel_stages(n_mma, nb) * (b_bytes(n_mma) + SPIN_BYTES) + (size_t)nb * TURN_BYTES +
-           acc_bytes(n_mma);
+static size_t kernel_smem(int n_cols) {
+    return SMEM_FIXED + (size_t)kernel_stages(n_cols) * (b_bytes(n_cols) + SPIN_BYTES);
 }
 
 // Number of chunk slabs per tile: the smallest that keeps the busiest CTA's
@@ -981,17 +1048,13 @@ static cudaError_t launch_precession(const KernelArgs &ka, unsigned grid, size_t
     return cudaGetLastError();
 }
 
-static cudaError_t launch_precession(int n_mma, const KernelArgs &ka, unsigned grid, size_t smem,
+static cudaError_t launch_precession(int n_cols, const KernelArgs &ka, unsigned grid, size_t smem,
                                      cudaStream_t stream) {
-    switch (n_mma) {
+    switch (n_cols) {
         case 16: return launch_precession<16>(ka, grid, smem, stream);
         case 32: return launch_precession<32>(ka, grid, smem, stream);
         case 48: return launch_precession<48>(ka, grid, smem, stream);
         case 64: return launch_precession<64>(ka, grid, smem, stream);
-        case 80: return launch_precession<80>(ka, grid, smem, stream);
-        case 96: return launch_precession<96>(ka, grid, smem, stream);
-        case 112: return launch_precession<112>(ka, grid, smem, stream);
-        case 128: return launch_precession<128>(ka, grid, smem, stream);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -1033,10 +1096,11 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
     prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(tv + rank_bytes),
                                           (const uint8_t *)a.adc, reinterpret_cast<const int32_t *>(tv), n_lo, n_hi,
                                           nsamples, a.gamma, (double *)r.prefix);
+    if ((e = cudaMemsetAsync(r.amp, 0, sizeof(unsigned long long), stream)) != cudaSuccess) return e;
     spin_table_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>(
         (const double *)r.basis, (const double *)a.dw, (const double *)a.T2, (const cplx<double> *)a.xy, r.ns, nchunks,
         m, (const double *)r.prefix + (size_t)(nsamples + 1) * PREFIX_STRIDE, (unsigned int *)r.err,
-        (double *)r.spin_table);
+        (unsigned long long *)r.amp, (double *)r.spin_table);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (nsamples > 0) {
         int dev = 0, nsm = 148;
@@ -1052,32 +1116,36 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         const size_t pbytes = sizeof(double) * (size_t)tiles * slabs * TM * r.n_mma;
         if ((e = grow(r.partial, r.partial_bytes, pbytes)) != cudaSuccess) return e;
         const size_t smem = kernel_smem(r.n_mma);
+        const int *cexp = reinterpret_cast<const int *>(reinterpret_cast<const unsigned long long *>(r.coil_exp) + r.nc);
         KernelArgs ka;
         ka.prefix = (const double *)r.prefix;
-        ka.b_operand = (const uint8_t *)r.b_operand;
         ka.spin_table = (const double *)r.spin_table;
+        ka.amp_max = (const unsigned long long *)r.amp;
         ka.partial = (double *)r.partial;
         ka.err = (unsigned int *)r.err;
         ka.nsamples = nsamples;
         ka.n_chunks = (int)nchunks;
         ka.tiles = (int)tiles;
         ka.slabs = slabs;
-        ka.nbuf = kernel_nbuf(r.n_mma);
-        ka.nstage = kernel_stages(r.n_mma, ka.nbuf);
-        if (ka.nstage < 2) {
-            *err = "split mode: too many coils for the kernel's shared memory";
-            return cudaSuccess;
-        }
+        ka.nstage = kernel_stages(r.n_mma);
         if (a.ev_start) cudaEventRecord(a.ev_start, stream);
-        e = launch_precession(r.n_mma, ka, (unsigned)G, smem, stream);
-        if (a.ev_stop) cudaEventRecord(a.ev_stop, stream);
-        if (a.launches) *a.launches += 2;
-        if (e != cudaSuccess) return e;
-        const int64_t total = nsamples * r.nc;
-        if (a.sizeof_T == 8)
-            split_finalize_kernel<double><<<grid_for(total), 256, 0, stream>>>(
-                (const double *)r.partial, nsamples, r.nc, r.n_mma, slabs, (cplx<double> *)a.sig + sample0, a.nadc);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        // One pass per group of GROUP_COILS coils.
+        for (int grp = 0; grp < r.ngroups; ++grp) {
+            const int coil0 = grp * GROUP_COILS;
+            const int ncg = std::min<int>(GROUP_COILS, r.nc - coil0);
+            ka.b_operand = (const uint8_t *)r.b_operand + (size_t)grp * nchunks * b_bytes(r.n_mma);
+            e = launch_precession(r.n_mma, ka, (unsigned)G, smem, stream);
+            if (a.ev_stop && grp + 1 == r.ngroups) cudaEventRecord(a.ev_stop, stream);
+            if (a.launches) *a.launches += 2;
+            if (e != cudaSuccess) return e;
+            const int64_t total = nsamples * ncg;
+            if (a.sizeof_T == 8)
+                split_finalize_kernel<double><<<grid_for(total), 256, 0, stream>>>(
+                    (const double *)r.partial, nsamples, ncg, r.n_mma, slabs, cexp + coil0,
+                    (const unsigned long long *)r.amp, (cplx<double> *)a.sig + sample0 + (int64_t)coil0 * a.nadc,
+                    a.nadc);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
     }
     if (a.launches) *a.launches += 3;
     state_update_kernel<<<grid_for(r.ns), 256, 0, stream>>>(

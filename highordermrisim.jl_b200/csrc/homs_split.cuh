@@ -10,27 +10,29 @@
 namespace homs {
 
 // Device operands that depend only on the phantom (built once per plan):
-// per-spin FP64 basis rows and the receive sensitivities split into TF32
-// hi/lo pairs, laid out in the canonical no-swizzle K-major UMMA layout.
+// per-spin FP64 basis rows and the receive sensitivities, scaled per coil by a
+// power of two and split into FP16 hi/lo pairs, laid out in the canonical
+// no-swizzle K-major UMMA layout, one operand per group of 32 coils.
 struct SplitResident {
     void *basis = nullptr;     // [ns_pad][16] double
-    void *b_operand = nullptr; // [nchunks][2 (hi,lo)][8 ksteps][N rows][8 tf32]
-    void *spin_table = nullptr;  // per-run spin parameters, [ns_pad][SPIN_STRIDE] double
-    void *prefix = nullptr;    // per-segment phase table, [nadc_seg_pad][PREFIX_STRIDE] double
-    void *tvec = nullptr;      // per-segment sample times, float
-    void *partial = nullptr;   // split-K partials, float
-    void *tile_map = nullptr;  // per time tile: (first cta, npieces)
+    void *b_operand = nullptr; // [groups][nchunks][4 ksteps][2N rows (hi, lo)][16 f16]
+    void *spin_table = nullptr;  // per-segment spin parameters, [nchunks][608] double
+    void *prefix = nullptr;    // per-segment phase table, [nadc_seg_pad][24] double
+    void *tvec = nullptr;      // per-segment ADC ranks and field-column pointers
+    void *partial = nullptr;   // FP64 split-K partials, [tiles][slabs][128][N]
+    void *coil_exp = nullptr;  // per coil: max |Re|,|Im| (u64 bits), then the scale exponent (int)
+    void *amp = nullptr;       // per segment: bits of the largest |m0| (u64)
     void *err = nullptr;       // device error word
     size_t basis_bytes = 0, b_bytes = 0, spin_bytes = 0, prefix_bytes = 0, tvec_bytes = 0, partial_bytes = 0,
-           tile_map_bytes = 0;
+           coil_exp_bytes = 0;
     int64_t ns = 0, ns_pad = 0;
-    int32_t nc = 0, n_mma = 0;
+    int32_t nc = 0, n_mma = 0, ngroups = 1;
     SplitResident() = default;
     SplitResident(const SplitResident &) = delete;
     SplitResident &operator=(const SplitResident &) = delete;
     ~SplitResident();
     size_t device_bytes() const {
-        return basis_bytes + b_bytes + spin_bytes + prefix_bytes + tvec_bytes + partial_bytes + tile_map_bytes;
+        return basis_bytes + b_bytes + spin_bytes + prefix_bytes + tvec_bytes + partial_bytes + coil_exp_bytes;
     }
 };
 
