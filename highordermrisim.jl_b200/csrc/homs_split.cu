@@ -30,16 +30,16 @@
 //
 // Kernel organisation (one CTA per SM, persistent, slab-major work items of
 // (time tile of 128 samples) x (range of 32-spin chunks)):
-//   warps 0-3   phase: warp q computes the turn fractions of tile rows
-//               32q..32q+31 for each chunk (DMMA) and writes them to TMEM in
-//               the m8n8 fragment layout (tcgen05.st.16x256b).
-//   warps 4-11  magnetisation: 16 sample rows of lane quarter w%4 each; read
-//               the turn fractions, form M, split it into FP16 hi/lo and write
-//               the A operand to TMEM; drain the accumulator.
-//   warp 12     MMA issuer: tcgen05.mma.kind::f16, A in TMEM, B (the
+//   warps 0-7   phase: warp w computes the turn fractions of the 16 tile rows
+//               32(w%4) + 16(w/4) .. +15 for each chunk (DMMA) and writes them
+//               to TMEM in the m8n8 fragment layout (tcgen05.st.16x256b).
+//   warps 8-15  magnetisation: the same 16 rows for warp w-8; read the turn
+//               fractions, form M, split it into FP16 hi/lo and write the A
+//               operand to TMEM; drain the accumulator.
+//   warp 16     MMA issuer: tcgen05.mma.kind::f16, A in TMEM, B (the
 //               sensitivities, pre-split) in shared memory; tcgen05.commit
 //               releases shared-memory stages, A buffers and accumulators.
-//   warp 13     loader: cp.async.bulk of each chunk's B operand and spin table.
+//   warp 17     loader: cp.async.bulk of each chunk's B operand and spin table.
 // TMEM (512 columns for N <= 64 output columns): accumulators 2 x 2N, A
 // operands 2 x 64, turn fractions 2 x 32, FP32 row accumulator N.
 // Every wait is bounded: on time-out the kernel records the place in a device
@@ -67,14 +67,13 @@ constexpr int NTERM = 16;        // phase GEMM depth (DMMA K): the 16 basis term
 constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_16, t at PREFIX_T
 constexpr int PREFIX_T = 20;
 constexpr int GROUP_COILS = 32;  // coils per kernel pass (N <= 64 output columns)
-// Warp roles: 4 phase warps (one per SM sub-partition), 8 magnetisation warps
-// (2 per TMEM lane quarter), MMA issuer, loader -- at most 4 warps per
-// sub-partition, which leaves 128 registers per thread.
-constexpr int NPHASE_WARPS = 4;
+// Warp roles: 8 phase warps and 8 magnetisation warps (2 of each per TMEM
+// lane quarter, paired by the 16 rows they share), MMA issuer, loader.
+constexpr int NPHASE_WARPS = 8;
 constexpr int NMAG_WARPS = 8;
-constexpr int MMA_WARP = 12;
-constexpr int LOAD_WARP = 13;
-constexpr int THREADS = 448;
+constexpr int MMA_WARP = 16;
+constexpr int LOAD_WARP = 17;
+constexpr int THREADS = 576;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
 // Each 32-spin chunk is its own FP32 TMEM accumulator generation: the tensor
@@ -324,9 +323,9 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     uint64_t *a_empty = a_full + 2;           // [2] MMA commit -> magnetisation warps
     uint64_t *d_full = a_empty + 2;           // [2] MMA commit -> drain
     uint64_t *d_empty = d_full + 2;           // [2] drain -> MMA
-    uint64_t *t_full = d_empty + 2;           // [4 quarters][2] phase warp -> magnetisation warps
-    uint64_t *t_empty = t_full + 8;           // [4 quarters][2] magnetisation warps -> phase warp
-    uint64_t *done = t_empty + 8;             // [1] final MMA commit
+    uint64_t *t_full = d_empty + 2;           // [8 row groups][2] phase warp -> magnetisation warp
+    uint64_t *t_empty = t_full + 16;          // [8 row groups][2] magnetisation warp -> phase warp
+    uint64_t *done = t_empty + 16;            // [1] final MMA commit
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -341,9 +340,9 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             mbar_init(&d_full[i], 1);
             mbar_init(&d_empty[i], NMAG_WARPS);
         }
-        for (int i = 0; i < 8; ++i) {
+        for (int i = 0; i < 16; ++i) {
             mbar_init(&t_full[i], 1);
-            mbar_init(&t_empty[i], NMAG_WARPS / 4);
+            mbar_init(&t_empty[i], 1);
         }
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -439,20 +438,22 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         }
         __syncwarp();
     } else if (warp < NPHASE_WARPS) {
-        // Phase warp q: turn fractions of tile rows 32q..32q+31 (4 x 4 DMMA
-        // 8x8 tiles per chunk, K = 16), accumulators initialised with
-        // theta0 + w kappa_16; written to TMEM columns t_col(tb) + spin.
-        const int q = warp;
-        const uint32_t t_lane = (uint32_t)(q * 32) << 16;
+        // Phase warp w: turn fractions of tile rows 32q + 16p .. +15 (q = w % 4,
+        // p = w / 4): 2 x 4 DMMA 8x8 tiles per chunk, K = 16, accumulators
+        // initialised with TURN_BIAS + theta0 + w kappa_16; written to TMEM
+        // columns t_col(tb) + spin of those rows.
+        const int q = warp & 3, p = warp >> 2;
+        const int grp = q * 2 + p;  // row group shared with magnetisation warp 8 + warp
+        const uint32_t t_lane = (uint32_t)(q * 32 + p * 16) << 16;
         int stage = 0, tb = 0;
         uint32_t fph = 0, tk = 0;  // parities of full[stage] and of this use of turn buffer tb
         for (int i = blockIdx.x; i < n_items && !dead; i += G) {
             const Item it = item_of(args, i);
-            // A fragments: kappa[row 32q + 8mt + gq][k = 4ks + tq], and kappa_16 of the row.
-            double ka[4][4], k16[4];
+            // A fragments: kappa[row 32q + 16p + 8mt + gq][k = 4ks + tq], and kappa_16 of the row.
+            double ka[2][4], k16[2];
 #pragma unroll
-            for (int mt = 0; mt < 4; ++mt) {
-                int64_t j = (int64_t)it.tile * TM + q * 32 + mt * 8 + gq;
+            for (int mt = 0; mt < 2; ++mt) {
+                int64_t j = (int64_t)it.tile * TM + q * 32 + p * 16 + mt * 8 + gq;
                 if (j >= args.nsamples) j = args.nsamples - 1;
                 const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
 #pragma unroll
@@ -461,7 +462,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             }
             for (int c = it.c0; c < it.c1; ++c) {
                 bool ok = mbar_wait(&full[stage], fph);
-                ok = ok && mbar_wait(&t_empty[q * 2 + tb], tk ^ 1u);
+                ok = ok && mbar_wait(&t_empty[grp * 2 + tb], tk ^ 1u);
                 __syncwarp();
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(args.err, 128u);
@@ -471,11 +472,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 tc_fence_after();
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
                 const uint32_t tcol = tmem + t_col(N, tb) + t_lane;
-                // Two spin groups at a time: 8 independent accumulator chains,
+                // Two spin groups at a time: 4 independent accumulator chains,
                 // k-step outermost.
 #pragma unroll
                 for (int np = 0; np < 2; ++np) {
-                    double bf[2][4], th[2][4][2];
+                    double bf[2][4], th[2][2][2];
 #pragma unroll
                     for (int n2 = 0; n2 < 2; ++n2) {
                         const int nt = 2 * np + n2;
@@ -485,7 +486,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                         const double2 dw = *reinterpret_cast<const double2 *>(tab + TAB_DW + 8 * nt + 2 * tq);
                         const double b0 = t0.x + TURN_BIAS, b1 = t0.y + TURN_BIAS;
 #pragma unroll
-                        for (int mt = 0; mt < 4; ++mt) {
+                        for (int mt = 0; mt < 2; ++mt) {
                             th[n2][mt][0] = fma(dw.x, k16[mt], b0);
                             th[n2][mt][1] = fma(dw.y, k16[mt], b1);
                         }
@@ -495,27 +496,22 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 #pragma unroll
                         for (int n2 = 0; n2 < 2; ++n2)
 #pragma unroll
-                            for (int mt = 0; mt < 4; ++mt)
+                            for (int mt = 0; mt < 2; ++mt)
                                 dmma_8x8x4(th[n2][mt][0], th[n2][mt][1], ka[mt][ks], bf[n2][ks]);
-                    // Rows 16p..16p+15 (mt = 2p, 2p+1), spin groups 2np, 2np+1:
-                    // 16x256b.x2 register order [4 n2 + 2 (mt & 1) + i].
+                    // Spin groups 2np, 2np+1: 16x256b.x2 register order [4 n2 + 2 mt + i].
+                    uint32_t v[8];
 #pragma unroll
-                    for (int p = 0; p < 2; ++p) {
-                        uint32_t v[8];
+                    for (int n2 = 0; n2 < 2; ++n2)
 #pragma unroll
-                        for (int n2 = 0; n2 < 2; ++n2)
+                        for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
-                            for (int m1 = 0; m1 < 2; ++m1)
-#pragma unroll
-                                for (int ii = 0; ii < 2; ++ii)
-                                    v[4 * n2 + 2 * m1 + ii] = turn_fraction(th[n2][2 * p + m1][ii]);
-                        tmem_st_16x256b_x2(tcol + ((uint32_t)(16 * p) << 16) + (uint32_t)(16 * np), v);
-                    }
+                            for (int ii = 0; ii < 2; ++ii) v[4 * n2 + 2 * mt + ii] = turn_fraction(th[n2][mt][ii]);
+                    tmem_st_16x256b_x2(tcol + (uint32_t)(16 * np), v);
                 }
                 tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&t_full[q * 2 + tb]);
+                if (lane == 0) mbar_arrive(&t_full[grp * 2 + tb]);
                 if (++stage == NSTAGE) {
                     stage = 0;
                     fph ^= 1u;
@@ -528,10 +524,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         }
     } else {
         // Magnetisation warp w: TMEM lane quarter q = w % 4, half h: tile rows
-        // 32q + 16h .. +15 (phase tiles mt = 2h, 2h+1 of quarter q) and all 32
-        // spins of each chunk.  For the accumulator drain it takes thread <->
-        // tile row 32q + lane and output columns [h N/2, (h+1) N/2).
+        // 32q + 16h .. +15 (the rows of phase warp w - 8) and all 32 spins of
+        // each chunk.  For the accumulator drain it takes thread <-> tile row
+        // 32q + lane and output columns [h N/2, (h+1) N/2).
         const int q = warp & 3, h = (warp - NPHASE_WARPS) >> 2;
+        const int grp = q * 2 + h;
         const uint32_t q_lane = (uint32_t)(q * 32) << 16;
         const uint32_t m_lane = (uint32_t)(q * 32 + h * 16) << 16;
         const int row = q * 32 + lane;
@@ -614,7 +611,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             }
             for (int c = it.c0; c < it.c1; ++c) {
                 const int buf = g & 1;
-                bool ok = mbar_wait(&t_full[q * 2 + tb], tk);
+                bool ok = mbar_wait(&t_full[grp * 2 + tb], tk);
                 ok = ok && mbar_wait(&a_empty[buf], (uint32_t)(((g >> 1) + 1) & 1));
                 __syncwarp();
                 if (!__all_sync(0xffffffffu, ok)) {
@@ -630,26 +627,31 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 tmem_wait_ld();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&t_empty[q * 2 + tb]);
+                if (lane == 0) mbar_arrive(&t_empty[grp * 2 + tb]);
                 const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                uint32_t hi[16], lo[16];
-#pragma unroll
-                for (int nt = 0; nt < 4; ++nt) {
-                    // This thread's spins of group nt: 8nt + 2tq + i.
-                    const float4 rl = *reinterpret_cast<const float4 *>(tab + TAB_PACK + 8 * nt + 2 * tq);
-                    const float r2v[2] = {rl.x, rl.z};
-                    const float l2v[2] = {rl.y - l2off, rl.w - l2off};
-#pragma unroll
-                    for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                        for (int ii = 0; ii < 2; ++ii) {
-                            const int e = 4 * nt + 2 * mt + ii;
-                            magnetisation(tu[e], tj[mt], r2v[ii], l2v[ii], hi[e], lo[e]);
-                        }
-                }
                 const uint32_t acol = tmem + a_col(N, buf) + m_lane;
-                tmem_st_16x256b_x4(acol, hi);
-                tmem_st_16x256b_x4(acol + 32u, lo);
+#pragma unroll
+                for (int np = 0; np < 2; ++np) {
+                    // Spin groups 2np, 2np+1: 16x256b.x2 register order [4 n2 + 2 mt + i].
+                    uint32_t hi[8], lo[8];
+#pragma unroll
+                    for (int n2 = 0; n2 < 2; ++n2) {
+                        // This thread's spins of group nt: 8nt + 2tq + i.
+                        const int nt = 2 * np + n2;
+                        const float4 rl = *reinterpret_cast<const float4 *>(tab + TAB_PACK + 8 * nt + 2 * tq);
+                        const float r2v[2] = {rl.x, rl.z};
+                        const float l2v[2] = {rl.y - l2off, rl.w - l2off};
+#pragma unroll
+                        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                            for (int ii = 0; ii < 2; ++ii) {
+                                const int e = 4 * n2 + 2 * mt + ii;
+                                magnetisation(tu[4 * nt + 2 * mt + ii], tj[mt], r2v[ii], l2v[ii], hi[e], lo[e]);
+                            }
+                    }
+                    tmem_st_16x256b_x2(acol + (uint32_t)(16 * np), hi);
+                    tmem_st_16x256b_x2(acol + 32u + (uint32_t)(16 * np), lo);
+                }
                 tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
