@@ -76,12 +76,15 @@ constexpr int LOAD_WARP = 17;
 constexpr int THREADS = 576;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
-// Each 32-spin chunk is its own FP32 TMEM accumulator generation: the tensor
-// core's accumulator add is not round-to-nearest, and its error is systematic
-// and grows with |D| and with the number of MMAs per generation.  The drain
-// adds generations (round to nearest, FP32) in a TMEM row accumulator and
-// promotes it to the FP64 partials every WINDOW chunks.
-constexpr int WINDOW = 32;
+// FLUSH chunks (8 MMAs each) form one FP32 TMEM accumulator generation: the
+// tensor core's accumulator add is not round-to-nearest, and its error is
+// systematic and grows with |D| and with the number of MMAs per generation
+// (two chunks per generation raised the signal NRMSE from 4.6e-7 to 5.2e-7 on
+// the 3D workload for a 1% gain, so each chunk keeps its own).
+// The drain adds generations (round to nearest, FP32) in a TMEM row
+// accumulator and promotes it to the FP64 partials every WINDOW chunks.
+constexpr int FLUSH = 1;
+constexpr int WINDOW = 32;  // a multiple of FLUSH
 
 // TMEM column map for N output columns (N <= 64).
 __host__ __device__ constexpr uint32_t d_col(int n, int buf) { return (uint32_t)(buf * 2 * n); }
@@ -392,14 +395,18 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         if (lane == 0) {
             // kind::f16: D f32 (bit 4), A and B f16 (format 0), both K-major; N = 2N columns.
             constexpr uint32_t idesc = (1u << 4) | ((uint32_t)((2 * N) >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-            int g = 0;  // chunks issued; chunk g uses A buffer and accumulator g % 2
+            int g = 0;    // chunks issued; chunk g uses A buffer g % 2
+            int gen = 0;  // accumulator generations issued; generation gen uses accumulator gen % 2
             int stage = 0;
             uint32_t fph = 0;  // parity of full[stage] for chunk g
             for (int i = blockIdx.x; i < n_items && !dead; i += G) {
                 const Item it = item_of(args, i);
                 for (int c = it.c0; c < it.c1; ++c, ++g) {
-                    const int buf = g & 1;
-                    if (!mbar_wait(&d_empty[buf], (uint32_t)(((g >> 1) + 1) & 1))) {
+                    const int buf = g & 1, dbuf = gen & 1;
+                    const int ci = c - it.c0;
+                    const bool gen_first = (ci % FLUSH) == 0;
+                    const bool gen_last = (ci % FLUSH) == FLUSH - 1 || c + 1 == it.c1;
+                    if (gen_first && !mbar_wait(&d_empty[dbuf], (uint32_t)(((gen >> 1) + 1) & 1))) {
                         atomicOr(args.err, 2u);
                         dead = true;
                         break;
@@ -410,22 +417,24 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t dcol = tmem + d_col(N, buf);
+                    const uint32_t dcol = tmem + d_col(N, dbuf);
                     const uint32_t acol = tmem + a_col(N, buf);
                     const uint32_t sbase = smem_u32(sB + (size_t)stage * BB);
-                    // Each chunk is its own accumulator generation; the small
-                    // lo pass goes first, while D is small, then the hi pass.
+                    // The small lo pass goes first, while D is small, then the hi pass.
 #pragma unroll
                     for (int ks = 0; ks < KSTEPS; ++ks)
                         tc_mma_f16(dcol, acol + 32u + (uint32_t)ks * 8u, bdesc(sbase + (uint32_t)(ks * 2 * N * 32)),
-                                   idesc, ks == 0 ? 0u : 1u);
+                                   idesc, (gen_first && ks == 0) ? 0u : 1u);
 #pragma unroll
                     for (int ks = 0; ks < KSTEPS; ++ks)
                         tc_mma_f16(dcol, acol + (uint32_t)ks * 8u, bdesc(sbase + (uint32_t)(ks * 2 * N * 32)), idesc,
                                    1u);
                     tc_commit(&empty[stage]);
                     tc_commit(&a_empty[buf]);
-                    tc_commit(&d_full[buf]);
+                    if (gen_last) {
+                        tc_commit(&d_full[dbuf]);
+                        ++gen;
+                    }
                     if (++stage == NSTAGE) {
                         stage = 0;
                         fph ^= 1u;
@@ -534,10 +543,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         const int row = q * 32 + lane;
         // Amplitude scale of the segment: M is formed as M / 2^eA (|M| <= 1).
         const float l2off = (float)pow2_ceil_exp(*args.amp_max);
-        int g = 0;  // chunks produced by this CTA
+        int g = 0;    // chunks produced by this CTA
+        int gen = 0;  // accumulator generations completed
         int stage = 0, tb = 0;
         uint32_t tk = 0;
-        int pend = -1;  // chunk whose accumulator generation waits to be drained
+        int pend = -1;  // accumulator generation waiting to be drained
         double *pend_dst = nullptr;
         bool pend_wfirst = false, pend_promote = false, pend_pfirst = false;
         // Drain: add the generation's two halves (A.B_hi, A.B_lo) into the
@@ -663,11 +673,14 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     break;
                 }
                 const int ci = c - it.c0;
-                pend = g;
-                pend_dst = dst_piece;
-                pend_wfirst = (ci % WINDOW) == 0;
-                pend_promote = (ci % WINDOW) == WINDOW - 1 || c + 1 == it.c1;
-                pend_pfirst = ci < WINDOW;
+                if ((ci % FLUSH) == FLUSH - 1 || c + 1 == it.c1) {
+                    const int gstart = ci - ci % FLUSH;  // first chunk of this generation
+                    pend = gen++;
+                    pend_dst = dst_piece;
+                    pend_wfirst = (gstart % WINDOW) == 0;
+                    pend_promote = (ci % WINDOW) == WINDOW - 1 || c + 1 == it.c1;
+                    pend_pfirst = gstart < WINDOW;
+                }
                 ++g;
                 if (++stage == NSTAGE) stage = 0;
                 if (++tb == 2) {
