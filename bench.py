@@ -131,7 +131,7 @@ def _units(w):
     return len(w.obj) * sum(count_block_adc(w.seq.adc, w.parts)) * w.obj.ncoils
 
 
-def cpu_baseline(seconds_target=15.0, threads=None):
+def cpu_baseline(seconds_target=20.0, threads=None):
     """Time the CPU oracle (a port of the reference's CPU Float64 path) on a
     deterministic spin subsample of the workload, on all host threads."""
     from homs.model import BlochHighOrder
@@ -140,7 +140,7 @@ def cpu_baseline(seconds_target=15.0, threads=None):
     if threads is None:
         threads = max(1, len(os.sched_getaffinity(0)))
     # The oracle's cost is linear in the spin count; grow the subsample until
-    # one run takes at least a third of the target time.
+    # one run takes at least half of the target time.
     stride = 400
     while True:
         w = _workload(stride=stride)
@@ -148,7 +148,7 @@ def cpu_baseline(seconds_target=15.0, threads=None):
         t0 = time.perf_counter()
         orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)
         dt = time.perf_counter() - t0
-        if dt >= seconds_target / 3 or stride == 1:
+        if dt >= seconds_target / 2 or stride == 1:
             break
         stride = max(1, int(stride * dt / seconds_target))
     return {"value": _units(w) / dt, "unit": UNIT, "cores": threads, "kind": "port",

@@ -118,6 +118,9 @@ struct homs_context {
     std::mutex mu;
     // reusable scratch
     DevBuf scratch_csm, scratch_partial, scratch_acc, scratch_bnd, scratch_sig, scratch_conv;
+    // Device workspace of homs_simulate, kept between calls (per dtype) so that
+    // repeated simulations reuse their buffers instead of reallocating them.
+    std::unique_ptr<struct ResidentBase> cache[2];
 };
 
 namespace {
@@ -179,12 +182,12 @@ void upload_csm_rows(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype
     if (total == 0) return;
     HOMS_REQUIRE(src != nullptr, "csm is NULL");
     const void *dsrc = src;
-    DevBuf staging;
     if (mem == HOMS_HOST) {
+        // Staged through the context's scratch buffer (kept between calls).
         const size_t bytes = 2 * dsize(src_dt) * (size_t)(ld * (nc - 1) + ns);
-        HOMS_CUDA(staging.ensure(bytes));
-        HOMS_CUDA(cudaMemcpyAsync(staging.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
-        dsrc = staging.p;
+        HOMS_CUDA(ctx->scratch_csm.ensure(bytes));
+        HOMS_CUDA(cudaMemcpyAsync(ctx->scratch_csm.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        dsrc = ctx->scratch_csm.p;
     }
     if (src_dt == HOMS_F64)
         transpose_csm_kernel<T, double><<<grid_for(total), 256, 0, ctx->stream>>>(
@@ -193,7 +196,6 @@ void upload_csm_rows(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype
         transpose_csm_kernel<T, float><<<grid_for(total), 256, 0, ctx->stream>>>(
             reinterpret_cast<cplx<T> *>(dst.p), static_cast<const float *>(dsrc), ns, nc, ld);
     HOMS_CUDA(cudaGetLastError());
-    if (mem == HOMS_HOST) HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
 void validate_phantom(const homs_phantom *p) {
@@ -346,9 +348,12 @@ struct Resident : ResidentBase {
 
 namespace {
 
+// Upload a phantom and a sampled sequence into `r` (fresh or reused: device
+// buffers only grow).  Host arrays may be released when this returns: copies
+// from pageable memory are staged before cudaMemcpyAsync returns.
 template <typename T>
-std::unique_ptr<Resident<T>> make_resident(homs_context *ctx, const homs_phantom *p, const homs_sequence *q) {
-    auto r = std::make_unique<Resident<T>>();
+void fill_resident(homs_context *ctx, Resident<T> *r, const homs_phantom *p, const homs_sequence *q) {
+    r->split_ready = false;
     r->dtype = sizeof(T) == 8 ? HOMS_F64 : HOMS_F32;
     r->ns = p->nspins;
     r->nc = p->ncoils;
@@ -391,7 +396,23 @@ std::unique_ptr<Resident<T>> make_resident(homs_context *ctx, const homs_phantom
     HOMS_CUDA(r->mz.ensure(sizeof(T) * (size_t)ns));
     HOMS_CUDA(r->acc.ensure(sizeof(T) * (size_t)ns));
     HOMS_CUDA(r->sig.ensure(sizeof(cplx<T>) * (size_t)std::max<int64_t>(nadc * p->ncoils, 1)));
+}
+
+template <typename T>
+std::unique_ptr<Resident<T>> make_resident(homs_context *ctx, const homs_phantom *p, const homs_sequence *q) {
+    auto r = std::make_unique<Resident<T>>();
+    fill_resident<T>(ctx, r.get(), p, q);
     HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return r;
+}
+
+// The context's cached workspace for dtype T, refilled with this phantom and sequence.
+template <typename T>
+Resident<T> *cached_resident(homs_context *ctx, const homs_phantom *p, const homs_sequence *q) {
+    auto &slot = ctx->cache[sizeof(T) == 8 ? 1 : 0];
+    if (!slot) slot = std::make_unique<Resident<T>>();
+    Resident<T> *r = static_cast<Resident<T> *>(slot.get());
+    fill_resident<T>(ctx, r, p, q);
     return r;
 }
 
@@ -721,6 +742,8 @@ homs_status homs_context_destroy(homs_context *ctx) {
         ctx->scratch_bnd.release();
         ctx->scratch_sig.release();
         ctx->scratch_conv.release();
+        ctx->cache[0].reset();
+        ctx->cache[1].reset();
         if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     }
     delete ctx;
@@ -757,12 +780,12 @@ homs_status homs_simulate(homs_context *ctx, const homs_phantom *phantom, const 
         validate_sequence(seq);
         HOMS_REQUIRE(sig_memory == HOMS_HOST || sig_memory == HOMS_DEVICE, "invalid signal memory kind");
         if (phantom->dtype == HOMS_F64) {
-            auto r = make_resident<double>(ctx, phantom, seq);
+            Resident<double> *r = cached_resident<double>(ctx, phantom, seq);
             init_state<double>(ctx, *r, state, phantom->dtype);
             run_resident<double>(ctx, *r, opts);
             copy_out<double>(ctx, *r, sig, sig_memory, state);
         } else {
-            auto r = make_resident<float>(ctx, phantom, seq);
+            Resident<float> *r = cached_resident<float>(ctx, phantom, seq);
             init_state<float>(ctx, *r, state, phantom->dtype);
             run_resident<float>(ctx, *r, opts);
             copy_out<float>(ctx, *r, sig, sig_memory, state);
@@ -770,8 +793,13 @@ homs_status homs_simulate(homs_context *ctx, const homs_phantom *phantom, const 
         return HOMS_OK;
     } catch (const Failure &f) {
         cudaStreamSynchronize(ctx->stream);
+        ctx->cache[0].reset();
+        ctx->cache[1].reset();
         return fail(ctx, f);
     } catch (const std::bad_alloc &) {
+        cudaStreamSynchronize(ctx->stream);
+        ctx->cache[0].reset();
+        ctx->cache[1].reset();
         return fail(ctx, Failure{HOMS_ENOMEM, "host allocation failed"});
     }
 }

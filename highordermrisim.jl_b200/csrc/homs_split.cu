@@ -1105,9 +1105,9 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
     src[16] = (m & HOMS_DW_PRECESSION) ? reinterpret_cast<const double *>(1) : nullptr;
     uint8_t *tv = (uint8_t *)r.tvec;
     if ((e = cudaMemcpyAsync(tv, rank.data(), rank_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
+    // Copies from pageable host memory are staged before cudaMemcpyAsync
+    // returns, so the host arrays above may go away without a synchronisation.
     if ((e = cudaMemcpyAsync(tv + rank_bytes, src, src_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
-    // The host arrays above are stack/vector memory: finish the copies before they go away.
-    if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(tv + rank_bytes),
                                           (const uint8_t *)a.adc, reinterpret_cast<const int32_t *>(tv), n_lo, n_hi,
                                           nsamples, a.gamma, (double *)r.prefix);
