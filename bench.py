@@ -121,9 +121,14 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def _workload(stride=1):
+def _workload(stride=1, k=CONFIG_INDEX):
     from homs import workloads as W
-    return W.config(CONFIG_INDEX, spins_stride=stride)
+    return W.config(k, spins_stride=stride)
+
+
+def _workload_name(k, stride):
+    from homs import workloads as W
+    return W.CONFIG_NAMES[k] + (f"_every{stride}thspin" if stride > 1 else "")
 
 
 def _units(w):
@@ -204,14 +209,15 @@ def run_homs(args):
     stream = torch.cuda.current_stream()
     ctx = _lib.Context(local, stream.cuda_stream)
     lib = _lib.load()
-    w = _workload(args.spin_stride)
+    w = _workload(args.spin_stride, args.config)
     units = _units(w)
     method = BlochHighOrder(w.mask)
-    params = {"sim_method": method, "precision": "f64", "homs_precision": args.mode}
+    params = {"sim_method": method, "precision": args.precision, "homs_precision": args.mode}
     plan = homs.prepare_simulation(w.obj, w.seq, sim_params=params, parts=w.parts, excitation=w.excitation,
                                    context=ctx)
     nadc, nc = plan.nadc, plan.nc
-    sig_dev = torch.empty((nc, nadc), dtype=torch.complex128, device="cuda")
+    sig_dev = torch.empty((nc, nadc), dtype=torch.complex128 if args.precision == "f64" else torch.complex64,
+                          device="cuda")
 
     def device_step():
         _lib.check(lib.homs_plan_run(plan.handle, ctypes.c_void_p(sig_dev.data_ptr()), _lib.HOMS_DEVICE, None),
@@ -252,25 +258,28 @@ def run_homs(args):
         keep = _lib._Keep()
         pin = lambda a: _pinned(torch, a)  # noqa: E731
         obj, seq = w.obj, w.seq
-        ph = _lib.Phantom(len(obj), nc, _lib.HOMS_F64, _lib.HOMS_HOST,
-                          *[keep.ptr(pin(np.asarray(v, np.float64))) for v in
+        rt = np.float64 if args.precision == "f64" else np.float32
+        ct = np.complex128 if args.precision == "f64" else np.complex64
+        dcode = _lib.HOMS_F64 if args.precision == "f64" else _lib.HOMS_F32
+        ph = _lib.Phantom(len(obj), nc, dcode, _lib.HOMS_HOST,
+                          *[keep.ptr(pin(np.asarray(v, rt))) for v in
                             (obj.x, obj.y, obj.z, obj.rho, obj.T1, obj.T2, obj.dw)],
-                          keep.ptr(pin(np.asfortranarray(obj.csm.astype(np.complex128)))))
-        hp = [pin(np.ascontiguousarray(seq.h[k], np.float64)) for k in range(16)]
+                          keep.ptr(pin(np.asfortranarray(obj.csm.astype(ct)))))
+        hp = [pin(np.ascontiguousarray(seq.h[k], rt)) for k in range(16)]
         keep.items.extend(hp)
         first = np.array([p[0] for p in w.parts], np.int64)
         last = np.array([p[1] for p in w.parts], np.int64)
         exc = np.array(w.excitation, np.uint8)
-        sq = _lib.Sequence(len(seq.t), _lib.HOMS_F64, _lib.HOMS_HOST,
-                           *[keep.ptr(pin(np.asarray(v, np.float64))) for v in (seq.t, seq.dt, seq.gx, seq.gy, seq.gz)],
-                           keep.ptr(pin(np.asarray(seq.b1, np.complex128))), keep.ptr(pin(np.asarray(seq.df, np.float64))),
-                           keep.ptr(pin(np.asarray(seq.psi, np.float64))),
+        sq = _lib.Sequence(len(seq.t), dcode, _lib.HOMS_HOST,
+                           *[keep.ptr(pin(np.asarray(v, rt))) for v in (seq.t, seq.dt, seq.gx, seq.gy, seq.gz)],
+                           keep.ptr(pin(np.asarray(seq.b1, ct))), keep.ptr(pin(np.asarray(seq.df, rt))),
+                           keep.ptr(pin(np.asarray(seq.psi, rt))),
                            keep.ptr(pin(np.asarray(seq.adc, np.uint8))),
                            (ctypes.c_void_p * 16)(*[a.ctypes.data for a in hp]), len(w.parts), keep.ptr(first),
                            keep.ptr(last), keep.ptr(exc), homs.GAMMA)
-        sig_h = pin(np.zeros((nc, nadc), np.complex128))
-        xy_h = pin(np.zeros(len(obj), np.complex128))
-        z_h = pin(np.asarray(obj.rho, np.float64).copy())
+        sig_h = pin(np.zeros((nc, nadc), ct))
+        xy_h = pin(np.zeros(len(obj), ct))
+        z_h = pin(np.asarray(obj.rho, rt).copy())
         st = _lib.State(xy_h.ctypes.data, z_h.ctypes.data, _lib.HOMS_HOST)
         opts = _lib.RunOptions()
         opts.method = method.flags
@@ -306,10 +315,11 @@ def run_homs(args):
         return 0
 
     bf16_peak, hbm_peak, peak_kind = _peaks()
-    seg_units = len(w.obj) * 9500 * nc
+    seg_units = units * args.steps / max(fused_n, 1)  # units per fused launch
     avg_launch_ms = fused_ms / max(fused_n, 1)
     achieved_tflops = FLOPS_PER_UNIT * seg_units / (avg_launch_ms / 1e3) / 1e12 if avg_launch_ms > 0 else None
-    traffic = _traffic_per_launch()
+    traffic = _traffic_per_launch() if (args.config == CONFIG_INDEX and args.mode == "split"
+                                        and args.spin_stride == 1) else None
     roof = {"bound": "tensor", "achieved": achieved_tflops, "peak": bf16_peak, "unit": "TFLOP/s",
             "frac": (achieved_tflops / bf16_peak) if achieved_tflops else None, "traffic": traffic,
             "peak_source": f"{peak_kind} dense bf16 (MEASURED_PEAKS.json)" if peak_kind == "measured" else
@@ -317,16 +327,20 @@ def run_homs(args):
             "segment_kernel", "kernel_ms_per_launch": avg_launch_ms,
             "units_per_launch": seg_units, "flops_per_unit": FLOPS_PER_UNIT}
     base = None
-    if ws == 1 and not args.no_cpu_baseline:
+    if ws == 1 and not args.no_cpu_baseline and args.config == CONFIG_INDEX:
         base, _ = cpu_baseline()
+    nchunks = -(-len(w.obj) // 32)
+    op_mb = nchunks * 16384 * -(-nc // 32) / 1e6 if args.mode == "split" else 0.0
+    csm_mb = len(w.obj) * nc * 16 / 1e6
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f64 phase / f32 trig / tf32x3 tensor" if args.mode == "split" else "f64",
+           "dtype": "f64 phase / f32 sfu trig / f16x3 tensor" if args.mode == "split" else args.precision,
            "data": "synthetic",
-           "config": {"workload": "3d_stack_of_spirals_100x100x35_350000spins_32coils_4x9500adc" +
-                                  (f"_every{args.spin_stride}thspin" if args.spin_stride > 1 else ""), "spins": len(w.obj),
+           "config": {"workload": _workload_name(args.config, args.spin_stride), "spins": len(w.obj),
                       "samples": nadc, "coils": nc, "mask": w.mask, "mode": args.mode,
-                      "l2": "inputs larger than L2 (split operand 358 MB, csm 179 MB)", "parallelism": f"replicas{ws}"},
+                      "l2": (f"inputs larger than L2 (csm {csm_mb:.0f} MB" +
+                             (f", split operand {op_mb:.0f} MB)" if op_mb else ")")) if csm_mb > 126 else
+                      f"inputs smaller than L2 (csm {csm_mb:.0f} MB)", "parallelism": f"replicas{ws}"},
            "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
            "clocks": clocks.summary()}
     print(json.dumps(out))
@@ -351,6 +365,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="homs", choices=["homs", "reference"])
     ap.add_argument("--mode", default="split", choices=["split", "plain"])
+    ap.add_argument("--config", type=int, default=CONFIG_INDEX, choices=[0, 1, 2, 3],
+                    help="benchmark configuration (2: the 3D 32-coil workload, the default bench line)")
+    ap.add_argument("--precision", default="f64", choices=["f64", "f32"],
+                    help="arithmetic of the plain kernel (split mode needs f64 inputs)")
     ap.add_argument("--spin-stride", type=int, default=1,
                     help="run every k-th spin of the workload (small cases for profiling; bench lines use 1)")
     ap.add_argument("--no-e2e", action="store_true")

@@ -78,6 +78,8 @@ struct NodeCache {
     T df[NODE_CHUNK + 1];
     T psi[NODE_CHUNK + 1];
     cplx<T> b1[NODE_CHUNK + 1];
+    T ab1[NODE_CHUNK + 1];  // |B1| of the node (RF segments)
+    T dfg[NODE_CHUNK + 1];  // df / gamma of the node (RF segments)
     uint8_t adc[NODE_CHUNK + 1];
     uint8_t bnd[NODE_CHUNK + 1];
 };
@@ -106,7 +108,7 @@ __device__ __forceinline__ T field_cached(const NodeCache<T> &nc, int i, const T
 }
 
 template <typename T, bool RF>
-__device__ void load_nodes(NodeCache<T> &nc, const SeqDev<T> &q, int64_t c0, int64_t c_end, uint32_t m) {
+__device__ void load_nodes(NodeCache<T> &nc, const SeqDev<T> &q, int64_t c0, int64_t c_end, uint32_t m, T gamma) {
     // nodes c0 .. min(c0 + NODE_CHUNK, c_end) inclusive
     const int n = (int)imin64(NODE_CHUNK, c_end - c0) + 1;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -118,9 +120,14 @@ __device__ void load_nodes(NodeCache<T> &nc, const SeqDev<T> &q, int64_t c0, int
             nc.g[0][i] = q.gx[g];
             nc.g[1][i] = q.gy[g];
             nc.g[2][i] = q.gz[g];
-            nc.b1[i] = q.b1[g];
+            const cplx<T> b1 = q.b1[g];
+            nc.b1[i] = b1;
             nc.df[i] = q.df[g];
             nc.psi[i] = q.psi[g];
+            // Spin-independent parts of the RF step, computed once per node
+            // with the same operations as the per-spin code used.
+            nc.ab1[i] = Math<T>::hyp(b1.re, b1.im);
+            nc.dfg[i] = nc.df[i] / gamma;
         } else {
             if (!(m & HOMS_HO1)) {
                 nc.g[0][i] = q.gx[g];
@@ -252,13 +259,14 @@ __global__ void __launch_bounds__(PLAIN_THREADS)
         off = (m & HOMS_DW_EXCITATION) ? p.dw[si] / c_twopig : T(0);
     }
 
+    T dt_rel = T(-1), e1_rel = T(0), e2_rel = T(0);  // RF relaxation factors of the last dt
     int staged = 0;
     int64_t sample = 0;
     cplx<T> *out_base = a.partial + (int64_t)blockIdx.x * a.nsamples * ncoil;
 
     for (int64_t c0 = a.n_lo; c0 < a.n_hi; c0 += NODE_CHUNK) {
         __syncthreads();
-        load_nodes<T, RF>(nc, q, c0, a.n_hi, m);
+        load_nodes<T, RF>(nc, q, c0, a.n_hi, m, gamma);
         __syncthreads();
         const int nint = (int)imin64(NODE_CHUNK, a.n_hi - c0);
         if (c0 == a.n_lo) {
@@ -289,16 +297,18 @@ __global__ void __launch_bounds__(PLAIN_THREADS)
                     have = true;
                 }
             } else {
-                const T dbz = off - nc.df[i] / gamma;
+                const T dbz = off - nc.dfg[i];
                 const T bz = ((nc.g[0][i] * px + nc.g[1][i] * py) + nc.g[2][i] * pz) + dbz;
                 const cplx<T> b1 = nc.b1[i];
-                const T ab1 = Math<T>::hyp(b1.re, b1.im);
+                const T ab1 = nc.ab1[i];
                 T B = Math<T>::sq(ab1 * ab1 + bz * bz);
                 if (B == T(0)) B = Math<T>::eps();
                 const T phi = c_neg * (B * dt);
                 T sh, ch;
                 Math<T>::sc(phi / T(2), &sh, &ch);
-                const T nz = bz / B, nxr = b1.re / B, nxi = b1.im / B;
+                // Unit field direction (one reciprocal; within an ulp of three divisions).
+                const T rB = T(1) / B;
+                const T nz = bz * rB, nxr = b1.re * rB, nxi = b1.im * rB;
                 const cplx<T> al{ch, -(nz * sh)};
                 const cplx<T> be{nxi * sh, -(nxr * sh)};
                 cplx<T> t1 = cmul(cplx<T>{T(2) * al.re, -(T(2) * al.im)}, be);
@@ -308,13 +318,19 @@ __global__ void __launch_bounds__(PLAIN_THREADS)
                 const cplx<T> t2 = cmul(cmul(ca, ca), xy);
                 const cplx<T> t3 = cmul(cmul(be, be), cplx<T>{xy.re, -xy.im});
                 const cplx<T> nxy{(t1.re + t2.re) - t3.re, (t1.im + t2.im) - t3.im};
-                const T aa = Math<T>::hyp(al.re, al.im), bb = Math<T>::hyp(be.re, be.im);
+                // |alpha|^2 - |beta|^2 as sums of squares (the reference's abs2;
+                // within an ulp of hypot()^2).
+                const T aa2 = al.re * al.re + al.im * al.im, bb2 = be.re * be.re + be.im * be.im;
                 const cplx<T> pr = cmul(cmul(al, be), cplx<T>{xy.re, -xy.im});
-                const T nz2 = (aa * aa - bb * bb) * mz - T(2) * pr.re;
-                const T e2 = Math<T>::ex(-dt / T2);
-                xy = cplx<T>{nxy.re * e2, nxy.im * e2};
-                const T e1 = Math<T>::ex(-dt / T1);
-                mz = nz2 * e1 + rho * (T(1) - e1);
+                const T nz2 = (aa2 - bb2) * mz - T(2) * pr.re;
+                // Relaxation factors depend on dt only: reuse them while dt repeats.
+                if (!(dt == dt_rel)) {
+                    e2_rel = Math<T>::ex(-dt / T2);
+                    e1_rel = Math<T>::ex(-dt / T1);
+                    dt_rel = dt;
+                }
+                xy = cplx<T>{nxy.re * e2_rel, nxy.im * e2_rel};
+                mz = nz2 * e1_rel + rho * (T(1) - e1_rel);
                 if (nc.adc[i + 1]) {
                     T sn, cs;
                     Math<T>::sc(nc.psi[i + 1], &sn, &cs);

@@ -180,6 +180,20 @@ def test_config0_full_fp64(oracle, gpu_context):
     assert nrmse(got[1], ref[1]) <= 1e-12
 
 
+@pytest.mark.parametrize("cfg,stride", [(1, 41), (2, 401), (3, 2003)])
+def test_config_subsample_fp64(oracle, gpu_context, cfg, stride):
+    # Deterministic spin subsamples of the 2D 8-coil, 3D 32-coil and 3D
+    # TR-loop workloads (windowed-sinc RF, 35 repetitions): plain FP64 <= 1e-12.
+    w = W.config(cfg, spins_stride=stride)
+    method = BlochHighOrder(w.mask)
+    ref = oracle_run(oracle, w.obj, w.seq, w.parts, w.excitation, method)
+    assert np.linalg.norm(ref[0]) > 0
+    got = gpu_run(w.obj, w.seq, w.parts, w.excitation, method, "f64")
+    assert nrmse(got[0], ref[0]) <= 1e-12
+    assert nrmse(got[1], ref[1]) <= 1e-12
+    assert nrmse(got[2], ref[2]) <= 1e-12
+
+
 def _dev(t):
     return ctypes.c_void_p(t.data_ptr())
 

@@ -62,7 +62,7 @@ def test_split_config0_full(oracle, gpu_context):
     assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
 
 
-@pytest.mark.parametrize("cfg,stride", [(1, 41), (2, 401), (2, 97)])
+@pytest.mark.parametrize("cfg,stride", [(1, 41), (2, 401), (2, 97), (3, 2003)])
 def test_split_config_subsample(oracle, gpu_context, cfg, stride):
     w = W.config(cfg, spins_stride=stride)
     assert np.count_nonzero(w.obj.rho) > len(w.obj) // 4
@@ -71,6 +71,19 @@ def test_split_config_subsample(oracle, gpu_context, cfg, stride):
     assert np.linalg.norm(ref[0]) > 0
     got = split_run(w.obj, w.seq, w.parts, w.excitation, method)
     assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+    # The state leaves the split path through the FP64 segment-end update.
+    assert nrmse(got[1], ref[1]) <= 1e-10
+
+
+def test_split_more_coils_than_one_group(oracle, gpu_context):
+    # 40 coils run as two coil groups (32 + 8) of the tcgen05 kernel.
+    obj, seq, st = W.high_order_workload(nspins=700, nsteps=64, ncoils=40)
+    method = BlochHighOrder("1111")
+    ref = oracle_run(oracle, obj, seq, [(0, 64)], [False], method, st)
+    got = split_run(obj, seq, [(0, 64)], [False], method, st)
+    assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+    for c in (0, 31, 32, 39):
+        assert nrmse(got[0][:, c], ref[0][:, c]) <= 10 * SPLIT_NRMSE
 
 
 def test_split_deterministic_and_plan(gpu_context):
