@@ -1,0 +1,261 @@
+// Serving loop of libhoms: continuous batching of independent simulations.
+//
+// The reference keeps one persistent worker per device and runs prepared
+// simulations one after another (src/simulation/PreparedSimulation.jl:144-258).
+// Here a server owns `slots` contexts -- each with its own CUDA stream and its
+// own cached device workspace -- and one worker thread per slot.  Requests
+// wait in submission order; the request at the head of the queue is admitted
+// as soon as a worker is free and its estimated device footprint fits in the
+// byte budget beside the requests already in flight.  Admitted requests run
+// homs_simulate on their worker's context, so requests that arrive while
+// others are on the GPU start as slots and memory free up, and their kernels
+// overlap on the device.  A request computes exactly what homs_simulate
+// computes for it: its result does not depend on what runs beside it.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/homs.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    homs_phantom phantom;
+    homs_sequence seq;
+    homs_run_options opts;
+    homs_state state;
+    bool has_state = false;
+    void *sig = nullptr;
+    homs_memory sig_memory = HOMS_HOST;
+    size_t bytes = 0;  // admission estimate of the device footprint
+    bool done = false;
+    homs_status status = HOMS_EBUSY;
+    std::string error;
+    double t_submit = 0, t_start = 0, t_finish = 0;
+};
+
+// Upper estimate of the device memory one simulation needs (inputs, state,
+// signal, staging of host sensitivities, and the path's work buffers).
+size_t estimate_bytes(const homs_phantom &p, const homs_sequence &q, const homs_run_options &o) {
+    const double es = p.dtype == HOMS_F64 ? 8.0 : 4.0;
+    const double ns = (double)p.nspins, nc = (double)p.ncoils, nt = (double)q.nnodes;
+    int64_t nadc = q.nnodes;
+    if (q.memory == HOMS_HOST) homs_count_adc(&q, &nadc);
+    double b = ns * (7 * es + 4 * es * nc + 3 * es);  // phantom, csm rows + staging, state
+    b += nt * (26 * es + 2);                          // sampled sequence
+    b += (double)nadc * nc * 2 * es;                  // signal
+    if (o.mode == HOMS_SPLIT) {
+        const double groups = std::ceil(nc / 32.0);
+        b += ns * (128.0 + 512.0 * groups + 152.0);   // basis, pre-split sensitivities, spin table
+        b += 4500.0 * 128 * 64 * 8 + (double)nadc * 192.0;  // split-K partials, phase prefix
+    } else {
+        const double grid = std::ceil(ns / 256.0);
+        b += std::min(768.0 * (1 << 20), grid * nc * 2 * es * (double)nadc);  // split-K partials
+    }
+    return (size_t)(b + (64 << 20));
+}
+
+}  // namespace
+
+struct homs_server {
+    int device = 0;
+    size_t budget = 0;
+    size_t inflight_bytes = 0;
+    Clock::time_point t0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Request *> queue;
+    std::map<int64_t, std::unique_ptr<Request>> requests;
+    int64_t next_ticket = 1;
+    bool stopping = false;
+    std::vector<homs_context *> contexts;
+    std::vector<std::thread> workers;
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+
+    // The head of the queue may start: a worker is asking, and it fits.
+    bool head_fits() const {
+        return !queue.empty() && (inflight_bytes == 0 || inflight_bytes + queue.front()->bytes <= budget);
+    }
+
+    void work(homs_context *ctx) {
+        for (;;) {
+            Request *r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_work.wait(lk, [&] { return head_fits() || (stopping && queue.empty()); });
+                if (queue.empty()) return;  // stopping
+                r = queue.front();
+                queue.pop_front();
+                inflight_bytes += r->bytes;
+                r->t_start = now();
+            }
+            const homs_status s = homs_simulate(ctx, &r->phantom, &r->seq, &r->opts, r->has_state ? &r->state : nullptr,
+                                                r->sig, r->sig_memory);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                r->status = s;
+                if (s != HOMS_OK) r->error = homs_last_error(ctx);
+                r->t_finish = now();
+                r->done = true;
+                inflight_bytes -= r->bytes;
+            }
+            cv_done.notify_all();
+            cv_work.notify_all();
+        }
+    }
+};
+
+extern "C" {
+
+homs_status homs_server_create(const homs_server_options *opts, homs_server **out) {
+    if (!opts || !out) return HOMS_EINVAL;
+    *out = nullptr;
+    const int slots = opts->slots > 0 ? opts->slots : 4;
+    if (slots > 64 || opts->max_device_bytes < 0) return HOMS_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return HOMS_EUNSUPPORTED;
+    }
+    if (opts->device < 0 || opts->device >= ndev) return HOMS_EINVAL;
+    auto srv = std::make_unique<homs_server>();
+    srv->device = opts->device;
+    srv->t0 = Clock::now();
+    if (opts->max_device_bytes > 0) {
+        srv->budget = (size_t)opts->max_device_bytes;
+    } else {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(opts->device);
+        size_t free_b = 0, total_b = 0;
+        const cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+        cudaSetDevice(prev);
+        if (e != cudaSuccess) return HOMS_ECUDA;
+        srv->budget = free_b / 4 * 3;
+    }
+    for (int k = 0; k < slots; ++k) {
+        homs_context *ctx = nullptr;
+        const homs_status s = homs_context_create(opts->device, nullptr, &ctx);
+        if (s != HOMS_OK) {
+            for (homs_context *c : srv->contexts) homs_context_destroy(c);
+            return s;
+        }
+        srv->contexts.push_back(ctx);
+    }
+    homs_server *raw = srv.get();
+    for (homs_context *ctx : srv->contexts) srv->workers.emplace_back([raw, ctx] { raw->work(ctx); });
+    *out = srv.release();
+    return HOMS_OK;
+}
+
+homs_status homs_server_submit(homs_server *srv, const homs_phantom *phantom, const homs_sequence *seq,
+                               const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory,
+                               int64_t *ticket) {
+    if (!srv || !phantom || !seq || !opts || !ticket) return HOMS_EINVAL;
+    auto r = std::make_unique<Request>();
+    r->phantom = *phantom;
+    r->seq = *seq;
+    r->opts = *opts;
+    if (state) {
+        r->state = *state;
+        r->has_state = true;
+    }
+    r->sig = sig;
+    r->sig_memory = sig_memory;
+    r->bytes = estimate_bytes(*phantom, *seq, *opts);
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stopping) return HOMS_ECLOSED;
+    r->t_submit = srv->now();
+    const int64_t id = srv->next_ticket++;
+    Request *rp = r.get();
+    srv->requests.emplace(id, std::move(r));
+    if (rp->bytes > srv->budget) {
+        // Larger than the whole admission budget: fail it here rather than block the queue.
+        rp->status = HOMS_ENOMEM;
+        rp->error = "the request's estimated device footprint exceeds the server's admission budget";
+        rp->done = true;
+        rp->t_start = rp->t_finish = rp->t_submit;
+    } else {
+        srv->queue.push_back(rp);
+    }
+    *ticket = id;
+    srv->cv_work.notify_all();
+    return HOMS_OK;
+}
+
+homs_status homs_server_poll(homs_server *srv, int64_t ticket) {
+    if (!srv) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) return HOMS_EINVAL;
+    return it->second->done ? it->second->status : HOMS_EBUSY;
+}
+
+homs_status homs_server_wait(homs_server *srv, int64_t ticket, double timeout_seconds) {
+    if (!srv || !(timeout_seconds >= 0)) return HOMS_EINVAL;
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) return HOMS_EINVAL;
+    Request *r = it->second.get();
+    const auto limit = std::chrono::duration<double>(std::min(timeout_seconds, 1e7));
+    if (!srv->cv_done.wait_for(lk, limit, [r] { return r->done; })) return HOMS_ETIMEDOUT;
+    return r->status;
+}
+
+homs_status homs_server_times(homs_server *srv, int64_t ticket, homs_request_times *out) {
+    if (!srv || !out) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) return HOMS_EINVAL;
+    out->submitted = it->second->t_submit;
+    out->started = it->second->t_start;
+    out->finished = it->second->t_finish;
+    return it->second->done ? HOMS_OK : HOMS_EBUSY;
+}
+
+const char *homs_server_error(homs_server *srv, int64_t ticket) {
+    if (!srv) return "no server";
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) return "unknown ticket";
+    return it->second->error.c_str();
+}
+
+homs_status homs_server_release(homs_server *srv, int64_t ticket) {
+    if (!srv) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) return HOMS_EINVAL;
+    if (!it->second->done) return HOMS_EBUSY;
+    srv->requests.erase(it);
+    return HOMS_OK;
+}
+
+homs_status homs_server_destroy(homs_server *srv) {
+    if (!srv) return HOMS_EINVAL;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stopping = true;
+    }
+    srv->cv_work.notify_all();
+    for (std::thread &t : srv->workers) t.join();
+    for (homs_context *c : srv->contexts) homs_context_destroy(c);
+    delete srv;
+    return HOMS_OK;
+}
+
+}  // extern "C"

@@ -28,7 +28,7 @@ from .model import (GAMMA, ArgumentError, BlochHighOrder, DimensionMismatch, HO_
                     count_block_adc, get_sim_ranges, initialize_spins_state)
 
 __all__ = [
-    "simulate", "prepare_simulation", "Plan", "Context", "HomsError", "ArgumentError", "DimensionMismatch",
+    "simulate", "prepare_simulation", "Plan", "Server", "Context", "HomsError", "ArgumentError", "DimensionMismatch",
     "BlochHighOrder", "HO_Phantom", "HO_DiscreteSequence", "Mag", "get_sim_ranges", "count_block_adc",
     "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks",
 ]
@@ -302,3 +302,107 @@ class Plan:
 def prepare_simulation(obj, seqd, sys=None, *, sim_params=None, parts=None, excitation=None, context=None):
     """Create a ``Plan`` (use as a context manager or call ``close()``)."""
     return Plan(obj, seqd, sys, sim_params, parts, excitation, context)
+
+
+@dataclass
+class _Request:
+    keep: Any
+    sig: np.ndarray
+    xy: np.ndarray
+    z: np.ndarray
+    params: Dict[str, Any]
+    parts: Any
+    excitation: Any
+    seqd: Any
+    structs: Tuple[Any, ...]
+
+
+class Server:
+    """Continuous-batching simulation server (``homs_server_*``).
+
+    Requests run as ``simulate`` would run them, on ``slots`` concurrent
+    contexts of one device; a request is admitted in submission order as soon
+    as a slot is free and its device footprint fits in ``max_device_bytes``
+    (0: three quarters of the free device memory) beside the requests in
+    flight.  ``submit`` returns a ticket; ``result`` waits for it and returns
+    what ``simulate`` returns.  The serving counterpart of the reference's
+    persistent worker (src/simulation/PreparedSimulation.jl:2-287).
+    """
+
+    def __init__(self, device: int = 0, slots: int = 4, max_device_bytes: int = 0):
+        self._lib = _lib.load()
+        opts = _lib.ServerOptions()
+        opts.device = int(device)
+        opts.slots = int(slots)
+        opts.max_device_bytes = int(max_device_bytes)
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.homs_server_create(ctypes.byref(opts), ctypes.byref(h)))
+        self.handle = h
+        self._requests: Dict[int, _Request] = {}
+
+    def submit(self, obj: HO_Phantom, seqd: HO_DiscreteSequence, *, sim_params=None, parts=None, excitation=None,
+               state: Optional[Mag] = None) -> int:
+        """Queue one simulation; the arguments are those of ``simulate``."""
+        if self.handle is None:
+            raise HomsError(6, "server is closed")
+        params, parts, excitation = _setup(obj, seqd, dict(sim_params or {}), parts, excitation)
+        dt = _dtype(params)
+        keep = _lib._Keep()
+        ph = _lib.host_phantom(obj, keep, dt)
+        sq = _lib.host_sequence(seqd, parts, excitation, keep, dt, params["gamma"])
+        nadc = sum(count_block_adc(seqd.adc, parts))
+        cdt = np.complex128 if dt == _lib.HOMS_F64 else np.complex64
+        fdt = np.float64 if dt == _lib.HOMS_F64 else np.float32
+        sig = np.zeros((nadc, obj.ncoils), dtype=cdt, order="F")
+        if state is None:
+            xy = np.zeros(len(obj), dtype=cdt)
+            z = np.ascontiguousarray(np.asarray(obj.rho, dtype=fdt)).copy()
+        else:
+            xy = np.ascontiguousarray(np.asarray(state.xy, dtype=cdt)).copy()
+            z = np.ascontiguousarray(np.asarray(state.z, dtype=fdt)).copy()
+        st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+        opts = _run_options(params)
+        ticket = ctypes.c_int64()
+        _lib.check(self._lib.homs_server_submit(self.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
+                                                ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST,
+                                                ctypes.byref(ticket)))
+        self._requests[ticket.value] = _Request(keep, sig, xy, z, params, parts, excitation, seqd, (ph, sq, st, opts))
+        return ticket.value
+
+    def done(self, ticket: int) -> bool:
+        """True once the request has finished (successfully or not)."""
+        return self._lib.homs_server_poll(self.handle, int(ticket)) != 7
+
+    def times(self, ticket: int) -> Tuple[float, float, float]:
+        """(submitted, started, finished) in seconds since the server started."""
+        t = _lib.RequestTimes()
+        self._lib.homs_server_times(self.handle, int(ticket), ctypes.byref(t))
+        return t.submitted, t.started, t.finished
+
+    def result(self, ticket: int, timeout: float = 600.0):
+        """Wait for a request and return what ``simulate`` returns for it."""
+        req = self._requests[int(ticket)]
+        status = self._lib.homs_server_wait(self.handle, int(ticket), float(timeout))
+        if status != 0:
+            msg = self._lib.homs_server_error(self.handle, int(ticket))
+            raise HomsError(status, (msg or b"").decode() or _lib.load().homs_status_string(status).decode())
+        t0, t1, t2 = self.times(ticket)
+        return _finalize(req.params, np.asarray(req.sig), req.xy, req.z, req.parts, req.excitation, req.seqd, t2 - t1)
+
+    def release(self, ticket: int) -> None:
+        """Forget a finished request (its buffers are released)."""
+        if self._lib.homs_server_release(self.handle, int(ticket)) == 0:
+            self._requests.pop(int(ticket), None)
+
+    def close(self) -> None:
+        """Finish every queued request and free the server."""
+        if self.handle is not None:
+            self._lib.homs_server_destroy(self.handle)
+            self.handle = None
+            self._requests.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -25,7 +25,8 @@ EXPORTED = [
     "homs_abi_version", "homs_status_string", "homs_context_create", "homs_context_destroy", "homs_last_error",
     "homs_synchronize", "homs_precession_block", "homs_excitation_block", "homs_coil_reduce", "homs_simulate",
     "homs_count_adc", "homs_plan_create", "homs_plan_run", "homs_plan_device_bytes", "homs_plan_timing",
-    "homs_plan_destroy", "homs_coil_reduce_noalloc",
+    "homs_plan_destroy", "homs_coil_reduce_noalloc", "homs_server_create", "homs_server_submit", "homs_server_poll",
+    "homs_server_wait", "homs_server_times", "homs_server_error", "homs_server_release", "homs_server_destroy",
 ]
 
 
@@ -69,6 +70,15 @@ class State(ctypes.Structure):
     _fields_ = [("xy", ctypes.c_void_p), ("z", ctypes.c_void_p), ("memory", ctypes.c_int)]
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("slots", ctypes.c_int32), ("max_device_bytes", ctypes.c_int64),
+                ("reserved", ctypes.c_int32 * 4)]
+
+
+class RequestTimes(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_double), ("started", ctypes.c_double), ("finished", ctypes.c_double)]
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 
@@ -104,6 +114,16 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_plan_timing": (ctypes.c_int, [vp, ctypes.POINTER(Timing)]),
         "homs_plan_destroy": (ctypes.c_int, [vp]),
         "homs_coil_reduce_noalloc": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i32, vp, i64, vp, i64, vp, i64]),
+        "homs_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOptions), ctypes.POINTER(vp)]),
+        "homs_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Phantom), ctypes.POINTER(Sequence),
+                                              ctypes.POINTER(RunOptions), ctypes.POINTER(State), vp, ctypes.c_int,
+                                              ctypes.POINTER(i64)]),
+        "homs_server_poll": (ctypes.c_int, [vp, i64]),
+        "homs_server_wait": (ctypes.c_int, [vp, i64, ctypes.c_double]),
+        "homs_server_times": (ctypes.c_int, [vp, i64, ctypes.POINTER(RequestTimes)]),
+        "homs_server_error": (ctypes.c_char_p, [vp, i64]),
+        "homs_server_release": (ctypes.c_int, [vp, i64]),
+        "homs_server_destroy": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -213,6 +213,48 @@ typedef struct homs_timing {
 homs_status homs_plan_timing(const homs_plan *plan, homs_timing *out);
 homs_status homs_plan_destroy(homs_plan *plan);
 
+/* ---- serving: continuous batching of independent simulations --------------
+ * The serving counterpart of the reference's persistent per-device worker
+ * (src/simulation/PreparedSimulation.jl:2-287), which runs one simulation at a
+ * time.  A server owns `slots` contexts (each with its own stream and cached
+ * device workspace) and one worker thread per slot.  Requests are admitted in
+ * submission order as soon as a slot is free and their estimated device
+ * footprint fits in `max_device_bytes` together with the requests already in
+ * flight; admitted requests run concurrently, so their kernels overlap on the
+ * device.  Each request computes exactly what homs_simulate computes for it,
+ * whatever else runs beside it.
+ * Submission copies nothing: the phantom, sequence (including the block
+ * arrays), state and signal buffers must stay valid and unchanged until the
+ * request completes. */
+typedef struct homs_server_options {
+    int device;
+    int32_t slots;            /* concurrent requests (0: 4) */
+    int64_t max_device_bytes; /* admission budget for in-flight requests (0: 3/4 of free device memory) */
+    int32_t reserved[4];
+} homs_server_options;
+
+/* Seconds since the server was created. */
+typedef struct homs_request_times {
+    double submitted, started, finished;
+} homs_request_times;
+
+homs_status homs_server_create(const homs_server_options *opts, homs_server **out);
+/* Queue a simulation (the arguments of homs_simulate); *ticket identifies it. */
+homs_status homs_server_submit(homs_server *srv, const homs_phantom *phantom, const homs_sequence *seq,
+                               const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory,
+                               int64_t *ticket);
+/* HOMS_OK when the request has finished, HOMS_EBUSY while it is queued or
+ * running, otherwise the status it failed with (message: homs_server_error). */
+homs_status homs_server_poll(homs_server *srv, int64_t ticket);
+/* Block until the request finishes or `timeout_seconds` pass (HOMS_ETIMEDOUT). */
+homs_status homs_server_wait(homs_server *srv, int64_t ticket, double timeout_seconds);
+homs_status homs_server_times(homs_server *srv, int64_t ticket, homs_request_times *out);
+const char *homs_server_error(homs_server *srv, int64_t ticket);
+/* Forget a finished request. */
+homs_status homs_server_release(homs_server *srv, int64_t ticket);
+/* Finish every admitted and queued request, then free the server. */
+homs_status homs_server_destroy(homs_server *srv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,3 +64,24 @@ def test_context_without_gpu_fails_loudly(homs_lib):
     assert st == _lib.HOMS_EUNSUPPORTED
     with pytest.raises(_lib.HomsError):
         _lib.Context(0)
+
+
+def test_server_arguments_and_no_gpu(homs_lib):
+    # Argument checks need no device; creation without a GPU fails loudly.
+    assert homs_lib.homs_server_create(None, None) == _lib.HOMS_EINVAL
+    assert homs_lib.homs_server_poll(None, 1) == _lib.HOMS_EINVAL
+    assert homs_lib.homs_server_wait(None, 1, 1.0) == _lib.HOMS_EINVAL
+    assert homs_lib.homs_server_destroy(None) == _lib.HOMS_EINVAL
+    assert homs_lib.homs_server_error(None, 1) == b"no server"
+    opts = _lib.ServerOptions()
+    opts.slots = 100
+    h = ctypes.c_void_p()
+    assert homs_lib.homs_server_create(ctypes.byref(opts), ctypes.byref(h)) == _lib.HOMS_EINVAL
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if not has_gpu:
+        opts.slots = 2
+        assert homs_lib.homs_server_create(ctypes.byref(opts), ctypes.byref(h)) == _lib.HOMS_EUNSUPPORTED
