@@ -161,6 +161,58 @@ def cpu_baseline(seconds_target=20.0, threads=None):
                       f"{dt:.1f} s"}, stride
 
 
+def serving_benchmark(n_pool=16, passes=6, load=0.9, slots=4):
+    """Serving stream of mixed simulations through homs.Server.
+
+    Batch mode submits every request at once (the server's capacity);
+    serving mode submits the same requests with Poisson arrivals at ``load``
+    times the batch request rate.  Latency is finish - submit per request;
+    sustained throughput is total units over first submit to last finish."""
+    import homs
+    from homs import workloads as W
+    pool = W.serving_pool(n_pool)
+    reqs = [pool[i % n_pool] for i in range(n_pool * passes)]
+    units = float(sum(r.units for r in reqs))
+
+    def submit(srv, r):
+        return srv.submit(r.obj, r.seq, sim_params=r.params, parts=r.parts, excitation=r.excitation)
+
+    with homs.Server(slots=slots) as srv:
+        for t in [submit(srv, r) for r in pool]:  # warm-up: every request once
+            srv.result(t)
+            srv.release(t)
+        t0 = time.perf_counter()
+        tickets = [submit(srv, r) for r in reqs]
+        for t in tickets:
+            srv.result(t)
+        batch_s = time.perf_counter() - t0
+        for t in tickets:
+            srv.release(t)
+        rate = len(reqs) / batch_s * load
+        rng = np.random.default_rng(7)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+        tickets = []
+        t0 = time.perf_counter()
+        for r, at in zip(reqs, arrivals):
+            wait = at - (time.perf_counter() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            tickets.append(submit(srv, r))
+        for t in tickets:
+            srv.result(t)
+        spans = [srv.times(t) for t in tickets]
+    lat = np.array([f - s for s, _, f in spans]) * 1e3
+    makespan = max(f for _, _, f in spans) - min(s for s, _, _ in spans)
+    sustained = units / makespan
+    batch = units / batch_s
+    return {"requests": len(reqs), "distinct": n_pool, "slots": slots, "load": load,
+            "arrival_rate_per_s": rate, "batch_units_per_s": batch, "sustained_units_per_s": sustained,
+            "fraction_of_batch": sustained / batch, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
+            "mix": "spins log-uniform 1e3-1e6, 2D/3D, ADC U[1k,20k] at 1-5 us, coils {1,8,16,32}, random masks, "
+                   "f64 on the split kernel / f32 on the plain kernel"}
+
+
 def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -343,6 +395,8 @@ def run_homs(args):
                       f"inputs smaller than L2 (csm {csm_mb:.0f} MB)", "parallelism": f"replicas{ws}"},
            "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
            "clocks": clocks.summary()}
+    if ws == 1 and not args.no_serve:
+        out["serving"] = serving_benchmark()
     print(json.dumps(out))
     if ws > 1:
         dist.barrier()
@@ -372,6 +426,7 @@ def main():
     ap.add_argument("--spin-stride", type=int, default=1,
                     help="run every k-th spin of the workload (small cases for profiling; bench lines use 1)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -85,4 +85,16 @@ cudaError_t launch_coil_reduce(int64_t ns, int64_t nadc, int32_t nc, const cplx<
 template <typename T>
 size_t segment_smem_bytes(int32_t nc);
 
+// Allow `func` the device's largest opt-in dynamic shared memory.  The
+// attribute belongs to the function, not to a launch: every caller sets the
+// same value, so launches from concurrent host threads (each sizing its own
+// shared memory below that limit) never see it lowered under them.
+inline cudaError_t allow_max_dynamic_smem(const void *func) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    return e;
+}
+
 }  // namespace homs

@@ -456,12 +456,11 @@ cudaError_t launch_segment(bool rf, const PhantomDev<T> &p, const SeqDev<T> &q, 
     const size_t smem = segment_smem_bytes<T>(p.nc);
     cudaError_t e;
     if (rf) {
-        e = cudaFuncSetAttribute(segment_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        e = allow_max_dynamic_smem((const void *)segment_kernel<T, true>);
         if (e != cudaSuccess) return e;
         segment_kernel<T, true><<<grid, PLAIN_THREADS, smem, stream>>>(p, q, st, a);
     } else {
-        e = cudaFuncSetAttribute(segment_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
+        e = allow_max_dynamic_smem((const void *)segment_kernel<T, false>);
         if (e != cudaSuccess) return e;
         segment_kernel<T, false><<<grid, PLAIN_THREADS, smem, stream>>>(p, q, st, a);
     }
@@ -487,7 +486,7 @@ cudaError_t launch_coil_reduce(int64_t ns, int64_t nadc, int32_t nc, const cplx<
     if (tiles == 0 || chunks == 0) return cudaSuccess;
     size_t smem = 2 * sizeof(cplx<T>) * PLAIN_STAGE * PLAIN_THREADS;
     if (sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS <= 96 * 1024) smem += sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS;
-    cudaError_t e = cudaFuncSetAttribute(coil_reduce_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_max_dynamic_smem((const void *)coil_reduce_kernel<T>);
     if (e != cudaSuccess) return e;
     dim3 grid((unsigned)tiles, (unsigned)chunks);
     coil_reduce_kernel<T><<<grid, PLAIN_THREADS, smem, stream>>>(ns, nadc, nc, states, ldstates, csm, ldcsm, partial);

@@ -1056,8 +1056,7 @@ static int choose_slabs(int64_t tiles, int64_t nchunks, int64_t G) {
 
 template <int N>
 static cudaError_t launch_precession(const KernelArgs &ka, unsigned grid, size_t smem, cudaStream_t stream) {
-    cudaError_t e = cudaFuncSetAttribute(split_precession_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = allow_max_dynamic_smem((const void *)split_precession_kernel<N>);
     if (e != cudaSuccess) return e;
     split_precession_kernel<N><<<grid, THREADS, smem, stream>>>(ka);
     return cudaGetLastError();

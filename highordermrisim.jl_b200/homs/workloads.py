@@ -20,7 +20,7 @@ from typing import List, Tuple
 
 import numpy as np
 
-from .model import GAMMA, HO_DiscreteSequence, HO_Phantom, Mag, get_sim_ranges
+from .model import GAMMA, BlochHighOrder, HO_DiscreteSequence, HO_Phantom, Mag, get_sim_ranges
 
 
 @dataclass
@@ -343,6 +343,73 @@ def config(k: int, max_block_length=math.inf, spins_stride: int = 1) -> Workload
     parts, exc = get_sim_ranges(seq, max_block_length, max_block_length)
     state = Mag(np.zeros(len(obj), np.complex128), obj.rho.copy())
     return Workload(obj, seq, parts, exc, state, mask, CONFIG_NAMES[k])
+
+
+@dataclass
+class ServingRequest:
+    obj: HO_Phantom
+    seq: HO_DiscreteSequence
+    parts: list
+    excitation: list
+    params: dict
+    units: int  # spins x ADC samples x coils
+
+
+def serving_request(rng) -> ServingRequest:
+    """One request of the serving stream: spin count log-uniform in [1e3, 1e6]
+    on a 2D or 3D grid over a 0.2 m FOV (ellipsoidal support), tissue as the
+    2D single-coil configuration, a 90 degree hard pulse then a single-shot
+    spiral of U[1k, 20k] ADC samples at 1-5 us dwell, 1/8/16/32 Gaussian
+    coils, a random order mask, FP32 (plain kernel) or FP64 (split kernel)."""
+    ns_target = 10 ** rng.uniform(3.0, 6.0)
+    fov = 0.2
+    if rng.random() < 0.5:
+        nx = ny = max(2, int(round(math.sqrt(ns_target))))
+        nz = 1
+    else:
+        nz = max(2, int(round(ns_target ** (1.0 / 3.0) / 2)))
+        nx = ny = max(2, int(round(math.sqrt(ns_target / nz))))
+    d = fov / nx
+    x, y, z = grid(nx, ny, nz, d, d, d)
+    if nz == 1:
+        z = np.zeros_like(x)
+    rho, T1, T2, dw = tissue(rng, x.shape[0], 20.0)
+    az = max(0.45 * nz * d, 1e-9)
+    rho = rho * (((x / 0.09) ** 2 + (y / 0.09) ** 2 + (z / az) ** 2 if nz > 1 else (x / 0.09) ** 2 + (y / 0.09) ** 2)
+                 <= 1.0)
+    nc = int(rng.choice([1, 8, 16, 32]))
+    if nc == 1:
+        csm = np.ones((x.shape[0], 1), np.complex128)
+    else:
+        csm = gaussian_coils(rng, x, y, z, fibonacci_hemisphere(nc, 0.14), 0.08)
+    nadc = int(rng.integers(1000, 20001))
+    dwell = float(rng.integers(1, 6)) * 1e-6
+    b = _SeqBuilder()
+    b.hard_rf(90.0)
+    gx, gy = spiral_gradients(nadc, dwell, nx / (2 * fov), 30e-3, rotation=rng.uniform(0, 2 * np.pi))
+    b.add(np.full(nadc, dwell), gx=gx, gy=gy, adc=np.ones(nadc, bool))
+
+    def h_fn(t):
+        h = field_waveforms(rng, t, (1e-6, 1e-3, 5e-3, 20e-3))
+        h[1] += np.asarray(b.gx)
+        h[2] += np.asarray(b.gy)
+        h[3] += np.asarray(b.gz)
+        return h
+
+    seq = b.build(h_fn)
+    obj = HO_Phantom(x=x, y=y, z=z, rho=rho, T1=T1, T2=T2, dw=dw, csm=csm, name="serving")
+    parts, exc = get_sim_ranges(seq, math.inf, math.inf)
+    mask = format(int(rng.integers(0, 16)), "04b")
+    f64 = bool(rng.random() < 0.5)
+    params = {"sim_method": BlochHighOrder(mask), "precision": "f64" if f64 else "f32",
+              "homs_precision": "split" if f64 else "plain"}
+    return ServingRequest(obj, seq, parts, exc, params, x.shape[0] * nadc * nc)
+
+
+def serving_pool(n: int, seed: int = 1004) -> List[ServingRequest]:
+    """``n`` seeded requests of the serving stream."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [serving_request(rng) for _ in range(n)]
 
 
 def _windowed_sinc_rf(b: _SeqBuilder, flip_deg, dur, nsteps, slab):
