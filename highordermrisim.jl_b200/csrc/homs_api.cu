@@ -3,7 +3,7 @@
 // A context owns one device and one stream; calls on a context are serialised
 // by a mutex (the reference serialises runs of a prepared plan with plan.lock,
 // src/simulation/PreparedSimulation.jl:224).  Inputs are copied into resident
-// device buffers in the phantom's precision; the block loop of
+// device buffers in the phantom's precision (FP64 in split mode); the block loop of
 // src/simulation/SimulatorCore.jl:96-152 is planned on the host into launches
 // of the fused segment kernels.
 #include <algorithm>
@@ -155,17 +155,13 @@ void upload(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype src_dt, 
         return;
     }
     if (mem == HOMS_HOST) {
-        std::vector<T> tmp((size_t)n);
-        if (src_dt == HOMS_F64) {
-            const double *s = static_cast<const double *>(src);
-            for (int64_t i = 0; i < n; ++i) tmp[i] = T(s[i]);
-        } else {
-            const float *s = static_cast<const float *>(src);
-            for (int64_t i = 0; i < n; ++i) tmp[i] = T(s[i]);
-        }
-        HOMS_CUDA(cudaMemcpyAsync(dst.p, tmp.data(), sizeof(T) * (size_t)n, cudaMemcpyHostToDevice, ctx->stream));
-        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
-        return;
+        // Staged as-is through the context's conversion buffer and converted on
+        // the device; the next upload reuses the buffer only after this
+        // conversion, in stream order.
+        const size_t raw = dsize(src_dt) * (size_t)n;
+        HOMS_CUDA(ctx->scratch_conv.ensure(raw));
+        HOMS_CUDA(cudaMemcpyAsync(ctx->scratch_conv.p, src, raw, cudaMemcpyHostToDevice, ctx->stream));
+        src = ctx->scratch_conv.p;
     }
     if (src_dt == HOMS_F64)
         convert_kernel<T, double><<<grid_for(n), 256, 0, ctx->stream>>>(reinterpret_cast<T *>(dst.p), static_cast<const double *>(src), n);
@@ -533,10 +529,7 @@ void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opt
     if (mode == HOMS_PLAIN) {
         run_plain<T>(ctx, r, method);
     } else if (mode == HOMS_SPLIT) {
-        if (sizeof(T) != 8)
-            throw Failure{HOMS_EUNSUPPORTED,
-                          "split mode takes FP64 phantom and sequence arrays: FP32 positions alone carry phase "
-                          "errors above the split path's error budget"};
+        if (sizeof(T) != 8) throw Failure{HOMS_EUNSUPPORTED, "internal: split mode runs on FP64 resident arrays"};
         if (!r.split_ready) {
             std::string err;
             cudaError_t e = split_prepare(r.split, r.ns, r.nc, r.x.p, r.y.p, r.z.p, r.dw.p, r.csm_rows.p, true,
@@ -650,21 +643,49 @@ void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opt
     }
 }
 
+// Copy `n` device elements of type T to `dst` (host or device) as `out_dt`.
+// Narrowing FP64 -> FP32 runs on the device, through the conversion buffer
+// when the destination is host memory.
 template <typename T>
-void copy_out(homs_context *ctx, Resident<T> &r, void *sig, homs_memory sig_memory, homs_state *state) {
-    const size_t sig_bytes = sizeof(cplx<T>) * (size_t)(r.nadc * r.nc);
-    if (sig_bytes > 0) {
+void download(homs_context *ctx, void *dst, homs_memory mem, const void *src, int64_t n, homs_dtype out_dt) {
+    if (n == 0) return;
+    const cudaMemcpyKind kind = mem == HOMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if ((out_dt == HOMS_F64) == (sizeof(T) == 8)) {
+        HOMS_CUDA(cudaMemcpyAsync(dst, src, sizeof(T) * (size_t)n, kind, ctx->stream));
+        return;
+    }
+    HOMS_REQUIRE(sizeof(T) == 8 && out_dt == HOMS_F32, "internal: unsupported output conversion");
+    float *narrow = static_cast<float *>(dst);
+    if (mem == HOMS_HOST) {
+        HOMS_CUDA(ctx->scratch_conv.ensure(sizeof(float) * (size_t)n));
+        narrow = ctx->scratch_conv.as<float>();
+    }
+    convert_kernel<float, double><<<grid_for(n), 256, 0, ctx->stream>>>(narrow, static_cast<const double *>(src), n);
+    HOMS_CUDA(cudaGetLastError());
+    if (mem == HOMS_HOST)
+        HOMS_CUDA(cudaMemcpyAsync(dst, narrow, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+}
+
+// Signal and final state out, in the caller's dtype `out_dt`.
+template <typename T>
+void copy_out(homs_context *ctx, Resident<T> &r, void *sig, homs_memory sig_memory, homs_state *state,
+              homs_dtype out_dt) {
+    if (r.nadc * r.nc > 0) {
         HOMS_REQUIRE(sig != nullptr, "sig is NULL");
-        HOMS_CUDA(cudaMemcpyAsync(sig, r.sig.p, sig_bytes,
-                                  sig_memory == HOMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
-                                  ctx->stream));
+        download<T>(ctx, sig, sig_memory, r.sig.p, 2 * r.nadc * r.nc, out_dt);
     }
     if (state && state->xy && state->z) {
-        const cudaMemcpyKind kind = state->memory == HOMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-        HOMS_CUDA(cudaMemcpyAsync(state->xy, r.xy.p, sizeof(cplx<T>) * (size_t)r.ns, kind, ctx->stream));
-        HOMS_CUDA(cudaMemcpyAsync(state->z, r.mz.p, sizeof(T) * (size_t)r.ns, kind, ctx->stream));
+        download<T>(ctx, state->xy, state->memory, r.xy.p, 2 * r.ns, out_dt);
+        download<T>(ctx, state->z, state->memory, r.mz.p, r.ns, out_dt);
     }
     HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+// Split mode computes in FP64 whatever the caller's dtype: FP32 phantom and
+// sequence arrays are widened on upload, and the signal and state are
+// narrowed on the way out.
+inline bool compute_f64(const homs_phantom *p, const homs_run_options *opts) {
+    return p->dtype == HOMS_F64 || (opts && opts->mode == HOMS_SPLIT);
 }
 
 }  // namespace
@@ -677,7 +698,7 @@ struct homs_plan {
     homs_context *ctx = nullptr;
     homs_run_options opts{};
     std::unique_ptr<ResidentBase> res;
-    std::vector<unsigned char> state_snapshot;  // unused: runs restart from Mxy=0, Mz=rho
+    homs_dtype out_dtype = HOMS_F64;  // the caller's dtype (the resident copy may be wider)
 };
 
 // ---------------------------------------------------------------------------
@@ -779,16 +800,16 @@ homs_status homs_simulate(homs_context *ctx, const homs_phantom *phantom, const 
         validate_phantom(phantom);
         validate_sequence(seq);
         HOMS_REQUIRE(sig_memory == HOMS_HOST || sig_memory == HOMS_DEVICE, "invalid signal memory kind");
-        if (phantom->dtype == HOMS_F64) {
+        if (compute_f64(phantom, opts)) {
             Resident<double> *r = cached_resident<double>(ctx, phantom, seq);
             init_state<double>(ctx, *r, state, phantom->dtype);
             run_resident<double>(ctx, *r, opts);
-            copy_out<double>(ctx, *r, sig, sig_memory, state);
+            copy_out<double>(ctx, *r, sig, sig_memory, state, phantom->dtype);
         } else {
             Resident<float> *r = cached_resident<float>(ctx, phantom, seq);
             init_state<float>(ctx, *r, state, phantom->dtype);
             run_resident<float>(ctx, *r, opts);
-            copy_out<float>(ctx, *r, sig, sig_memory, state);
+            copy_out<float>(ctx, *r, sig, sig_memory, state, phantom->dtype);
         }
         return HOMS_OK;
     } catch (const Failure &f) {
@@ -817,7 +838,8 @@ homs_status homs_plan_create(homs_context *ctx, const homs_phantom *phantom, con
         plan->ctx = ctx;
         if (opts) plan->opts = *opts;
         else plan->opts.method = 0x3Fu;
-        if (phantom->dtype == HOMS_F64) plan->res = make_resident<double>(ctx, phantom, seq);
+        plan->out_dtype = phantom->dtype;
+        if (compute_f64(phantom, &plan->opts)) plan->res = make_resident<double>(ctx, phantom, seq);
         else plan->res = make_resident<float>(ctx, phantom, seq);
         *out = plan.release();
         return HOMS_OK;
@@ -840,12 +862,12 @@ homs_status homs_plan_run(homs_plan *plan, void *sig, homs_memory sig_memory, ho
             auto &r = static_cast<Resident<double> &>(*plan->res);
             init_state<double>(ctx, r, nullptr, HOMS_F64);
             run_resident<double>(ctx, r, &plan->opts);
-            copy_out<double>(ctx, r, sig, sig_memory, state_out);
+            copy_out<double>(ctx, r, sig, sig_memory, state_out, plan->out_dtype);
         } else {
             auto &r = static_cast<Resident<float> &>(*plan->res);
             init_state<float>(ctx, r, nullptr, HOMS_F32);
             run_resident<float>(ctx, r, &plan->opts);
-            copy_out<float>(ctx, r, sig, sig_memory, state_out);
+            copy_out<float>(ctx, r, sig, sig_memory, state_out, plan->out_dtype);
         }
         return HOMS_OK;
     } catch (const Failure &f) {

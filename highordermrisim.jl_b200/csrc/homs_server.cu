@@ -50,7 +50,7 @@ struct Request {
 // Upper estimate of the device memory one simulation needs (inputs, state,
 // signal, staging of host sensitivities, and the path's work buffers).
 size_t estimate_bytes(const homs_phantom &p, const homs_sequence &q, const homs_run_options &o) {
-    const double es = p.dtype == HOMS_F64 ? 8.0 : 4.0;
+    const double es = (p.dtype == HOMS_F64 || o.mode == HOMS_SPLIT) ? 8.0 : 4.0;  // split mode is resident in FP64
     const double ns = (double)p.nspins, nc = (double)p.ncoils, nt = (double)q.nnodes;
     int64_t nadc = q.nnodes;
     if (q.memory == HOMS_HOST) homs_count_adc(&q, &nadc);

@@ -105,11 +105,13 @@ class HO_Phantom:
         self.T2s = _vec(T2s, n, 1_000_000.0, dtype)
         self.dw = _vec(dw, n, 0.0, dtype)
         cdt = np.complex64 if np.dtype(dtype) == np.float32 else np.complex128
+        # Column-major, as the reference's Julia arrays and the C ABI: the
+        # array crosses to libhoms without a per-call transpose.
         if csm is None:
-            self.csm = np.ones((n, 1), dtype=cdt)
+            self.csm = np.ones((n, 1), dtype=cdt, order="F")
         else:
             c = np.asarray(csm, dtype=cdt)
-            self.csm = c.reshape(c.shape[0], -1) if c.ndim == 1 else c
+            self.csm = np.asfortranarray(c.reshape(c.shape[0], -1) if c.ndim == 1 else c)
 
     def __len__(self):
         return int(self.rho.shape[0])
@@ -142,7 +144,7 @@ class HO_Phantom:
         out.name = self.name
         for k in ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw"):
             setattr(out, k, np.asarray(getattr(self, k), dtype=dtype))
-        out.csm = np.asarray(self.csm, dtype=np.complex64 if np.dtype(dtype) == np.float32 else np.complex128)
+        out.csm = np.asfortranarray(self.csm, dtype=np.complex64 if np.dtype(dtype) == np.float32 else np.complex128)
         return out
 
 

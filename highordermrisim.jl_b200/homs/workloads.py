@@ -360,7 +360,9 @@ def serving_request(rng) -> ServingRequest:
     on a 2D or 3D grid over a 0.2 m FOV (ellipsoidal support), tissue as the
     2D single-coil configuration, a 90 degree hard pulse then a single-shot
     spiral of U[1k, 20k] ADC samples at 1-5 us dwell, 1/8/16/32 Gaussian
-    coils, a random order mask, FP32 (plain kernel) or FP64 (split kernel)."""
+    coils, a random order mask, FP32 or FP64 arrays; every request runs on
+    the split kernel (FP32 arrays are widened on the device and the results
+    returned in FP32)."""
     ns_target = 10 ** rng.uniform(3.0, 6.0)
     fov = 0.2
     if rng.random() < 0.5:
@@ -401,8 +403,10 @@ def serving_request(rng) -> ServingRequest:
     parts, exc = get_sim_ranges(seq, math.inf, math.inf)
     mask = format(int(rng.integers(0, 16)), "04b")
     f64 = bool(rng.random() < 0.5)
+    if not f64:  # an FP32 caller holds FP32 arrays
+        obj, seq = obj.astype(np.float32), seq.astype(np.float32)
     params = {"sim_method": BlochHighOrder(mask), "precision": "f64" if f64 else "f32",
-              "homs_precision": "split" if f64 else "plain"}
+              "homs_precision": "split"}
     return ServingRequest(obj, seq, parts, exc, params, x.shape[0] * nadc * nc)
 
 

@@ -49,10 +49,14 @@ typedef enum homs_memory { HOMS_HOST = 0, HOMS_DEVICE = 1 } homs_memory;
 /* Arithmetic of a run.
  *   HOMS_PLAIN  -- the reference's per-spin sequential trapezoid and fused coil
  *                  sum in the phantom's dtype (CUDA cores only);
- *   HOMS_SPLIT  -- FP64 phase (prefix-integrated field table, FP64 mod-2pi
- *                  reduction), FP32 trigonometry/relaxation, and the coil
- *                  contraction on tcgen05 tensor cores with TF32 hi/lo split
- *                  operands and FP32 accumulation; RF blocks in FP64. */
+ *   HOMS_SPLIT  -- FP64 phase (prefix-integrated field table, FP64 tensor-core
+ *                  phase tile, exact mod-2pi reduction), FP32 trigonometry and
+ *                  decay, and the coil contraction on tcgen05 tensor cores with
+ *                  FP16 hi/lo split operands and FP32 accumulation; RF blocks
+ *                  in FP64.  Always computes in FP64: FP32 phantom and sequence
+ *                  arrays are widened on upload and the signal and state are
+ *                  returned in FP32 (signal NRMSE <= 1e-6 against an FP64
+ *                  computation on the same FP32 inputs). */
 typedef enum homs_mode { HOMS_PLAIN = 0, HOMS_SPLIT = 1 } homs_mode;
 
 /* BlochHighOrder flags (src/simulation/BlochHighOrder.jl:21-43). */

@@ -96,9 +96,11 @@ def test_failures_stay_on_their_ticket(gpu_context):
         with pytest.raises(homs.HomsError) as e:
             srv.result(big)
         assert e.value.status == 2
+    far, _, _ = W.high_order_workload(nspins=100, nsteps=16, ncoils=2)
+    far.x[7] = 1000.0
     with homs.Server(slots=2) as srv:
-        # Split mode takes FP64 inputs only.
-        bad = srv.submit(obj, seq, sim_params={"sim_method": BlochHighOrder("1111"), "precision": "f32",
+        # A spin 1 km off-centre: its phase leaves the split path's fixed-point range.
+        bad = srv.submit(far, seq, sim_params={"sim_method": BlochHighOrder("1111"), "precision": "f32",
                                                "homs_precision": "split"}, parts=[(0, 16)], excitation=[False])
         good = srv.submit(obj, seq, sim_params={"sim_method": BlochHighOrder("1111")}, parts=[(0, 16)],
                           excitation=[False])

@@ -100,8 +100,60 @@ def test_split_deterministic_and_plan(gpu_context):
     assert np.array_equal(r1[:, :, 0], a[0])
 
 
-def test_split_rejects_fp32_inputs(gpu_context):
+@pytest.mark.parametrize("scenario", ["fixture", "rf", "config1"])
+def test_split_fp32_inputs(oracle, gpu_context, scenario):
+    # FP32 arrays run on the split path in FP64 and come back as FP32: the
+    # signal matches an FP64 computation on the same FP32-rounded inputs to the
+    # split bound, and the reference's own FP32 path to its 3e-5 tolerance.
+    if scenario == "fixture":
+        obj, seq, st = W.high_order_workload(nspins=2000, nsteps=300, ncoils=8)
+        parts, exc = [(0, 300)], [False]
+    elif scenario == "rf":
+        obj, seq, _, _ = W.rf_acquisition_workload(3, 2, 11)
+        parts, exc = get_sim_ranges(seq, 4, 5)
+        st = None
+    else:
+        w = W.config(1, spins_stride=41)
+        obj, seq, parts, exc, st = w.obj, w.seq, w.parts, w.excitation, None
+    method = BlochHighOrder("1111")
+    obj32, seq32 = obj.astype(np.float32), seq.astype(np.float32)
+    st32 = None if st is None else type(st)(st.xy.astype(np.complex64), st.z.astype(np.float32))
+    ref = oracle_run(oracle, obj32.astype(np.float64), seq32.astype(np.float64), parts, exc, method,
+                     None if st32 is None else type(st)(st32.xy.astype(np.complex128), st32.z.astype(np.float64)))
+    got = homs.run_blocks(obj32, seq32, parts, exc, method, "f32", "split", st32)
+    assert got[0].dtype == np.complex64 and got[1].dtype == np.complex64 and got[2].dtype == np.float32
+    assert nrmse(got[0], ref[0]) <= SPLIT_NRMSE
+    assert nrmse(got[1], ref[1]) <= 1e-6
+    assert nrmse(got[2], ref[2]) <= 1e-6
+    plain = homs.run_blocks(obj32, seq32, parts, exc, method, "f32", "plain", st32)
+    # The plain FP32 kernel accumulates phase in FP32: on the reference's own
+    # short fixture it stays within the reference's 3e-5, and over the 10,000
+    # samples of a 2D readout it drifts further from the FP64 result than the
+    # split path does.
+    if scenario == "fixture":
+        assert nrmse(got[0], plain[0]) <= 3e-5
+    if scenario == "config1":
+        assert nrmse(got[0], ref[0]) < nrmse(plain[0], ref[0])
+
+
+def test_split_fp32_plan_matches_simulate(gpu_context):
+    w = W.config(2, spins_stride=400)
+    obj32, seq32 = w.obj.astype(np.float32), w.seq.astype(np.float32)
+    method = BlochHighOrder(w.mask)
+    direct = homs.run_blocks(obj32, seq32, w.parts, w.excitation, method, "f32", "split")
+    params = {"sim_method": method, "precision": "f32", "homs_precision": "split"}
+    with homs.prepare_simulation(obj32, seq32, sim_params=params, parts=w.parts, excitation=w.excitation) as plan:
+        r = plan.run()
+    assert r.dtype == np.complex64
+    assert np.array_equal(r[:, :, 0], direct[0])
+
+
+def test_split_phase_range_is_reported(gpu_context):
+    # A spin 1 km from the isocentre accumulates more than 2^18 turns in a
+    # segment: the split path refuses it with HOMS_EUNSUPPORTED and a message.
     obj, seq, st = W.high_order_workload(nspins=33, nsteps=8, ncoils=2)
+    obj.x[5] = 1000.0
     with pytest.raises(homs.HomsError) as e:
-        homs.run_blocks(obj, seq, [(0, 8)], [False], BlochHighOrder("1111"), "f32", "split", st)
+        homs.run_blocks(obj, seq, [(0, 8)], [False], BlochHighOrder("1111"), "f64", "split", st)
     assert e.value.status == 3
+    assert "2^18" in str(e.value)
