@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "homs_common.cuh"
+#include "homs_kspace.cuh"
 #include "homs_split.cuh"
 
 using namespace homs;
@@ -118,6 +119,11 @@ struct homs_context {
     std::mutex mu;
     // reusable scratch
     DevBuf scratch_csm, scratch_partial, scratch_acc, scratch_bnd, scratch_sig, scratch_conv;
+    // encoding export (homs_kspace): staged inputs, metadata, work and outputs,
+    // and the events around its kernels
+    DevBuf kspace_in, kspace_meta, kspace_work, kspace_out;
+    cudaEvent_t kspace_ev[2] = {nullptr, nullptr};
+    bool kspace_timed = false;
     // Device workspace of homs_simulate, kept between calls (per dtype) so that
     // repeated simulations reuse their buffers instead of reallocating them.
     std::unique_ptr<struct ResidentBase> cache[2];
@@ -763,6 +769,12 @@ homs_status homs_context_destroy(homs_context *ctx) {
         ctx->scratch_bnd.release();
         ctx->scratch_sig.release();
         ctx->scratch_conv.release();
+        ctx->kspace_in.release();
+        ctx->kspace_meta.release();
+        ctx->kspace_work.release();
+        ctx->kspace_out.release();
+        for (cudaEvent_t &e : ctx->kspace_ev)
+            if (e) cudaEventDestroy(e);
         ctx->cache[0].reset();
         ctx->cache[1].reset();
         if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
@@ -1045,6 +1057,127 @@ homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins
     } catch (const Failure &f) {
         return fail(ctx, f);
     }
+}
+
+homs_status homs_kspace(homs_context *ctx, const homs_sequence *seq, int32_t nrf, const int64_t *rf_start,
+                        const int8_t *rf_sign, int64_t nq, const double *q_times, double *k, double *k_q,
+                        homs_memory out_memory) {
+    if (!ctx) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    ctx->kspace_timed = false;
+    try {
+        HOMS_REQUIRE(seq != nullptr, "sequence is NULL");
+        HOMS_REQUIRE(seq->nnodes >= 2, "Cannot integrate an empty sequence.");
+        HOMS_REQUIRE(seq->dtype == HOMS_F32 || seq->dtype == HOMS_F64, "sequence dtype must be f32 or f64");
+        HOMS_REQUIRE(seq->memory == HOMS_HOST || seq->memory == HOMS_DEVICE, "invalid sequence memory kind");
+        HOMS_REQUIRE(seq->t && seq->dt && seq->gx && seq->gy && seq->gz, "t, dt, gx, gy and gz must be provided");
+        for (int c = 0; c < 16; ++c) HOMS_REQUIRE(seq->h[c] != nullptr, "every field coefficient array must be provided");
+        HOMS_REQUIRE(std::isfinite(seq->gamma) && seq->gamma > 0, "gamma must be finite and positive");
+        HOMS_REQUIRE(out_memory == HOMS_HOST || out_memory == HOMS_DEVICE, "invalid output memory kind");
+        HOMS_REQUIRE(k != nullptr, "k is NULL");
+        HOMS_REQUIRE(nrf >= 0 && (nrf == 0 || (rf_start && rf_sign)), "RF break arrays are NULL");
+        HOMS_REQUIRE(nq >= 0 && (nq == 0 || (q_times && k_q)), "query times or k_q is NULL");
+        const int64_t nn = seq->nnodes, m = nn - 1;
+        for (int32_t i = 0; i < nrf; ++i) {
+            HOMS_REQUIRE(rf_start[i] >= 1 && rf_start[i] < m, "RF breaks must lie inside the sequence's intervals");
+            HOMS_REQUIRE(i == 0 || rf_start[i] > rf_start[i - 1], "RF breaks must be strictly increasing");
+            HOMS_REQUIRE(rf_sign[i] >= -1 && rf_sign[i] <= 1, "RF signs must be -1, 0 or 1");
+        }
+        for (int64_t j = 0; j < nq; ++j) HOMS_REQUIRE(std::isfinite(q_times[j]), "query times must be finite");
+        constexpr int32_t NCOLS = 19;  // gx, gy, gz, h0 .. h15
+        const int32_t nparts = nrf + 1;
+        const size_t es = dsize(seq->dtype);
+        // Device inputs: the caller's arrays, or a staged copy of host arrays.
+        const void *dev_t = seq->t, *dev_dt = seq->dt;
+        const void *cols[NCOLS] = {seq->gx, seq->gy, seq->gz};
+        for (int c = 0; c < 16; ++c) cols[3 + c] = seq->h[c];
+        if (seq->memory == HOMS_HOST) {
+            const size_t col_bytes = (es * (size_t)nn + 255) & ~size_t(255);
+            HOMS_CUDA(ctx->kspace_in.ensure(col_bytes * (NCOLS + 2)));
+            uint8_t *base = ctx->kspace_in.as<uint8_t>();
+            HOMS_CUDA(cudaMemcpyAsync(base, seq->t, es * (size_t)nn, cudaMemcpyHostToDevice, ctx->stream));
+            HOMS_CUDA(cudaMemcpyAsync(base + col_bytes, seq->dt, es * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
+            dev_t = base;
+            dev_dt = base + col_bytes;
+            for (int c = 0; c < NCOLS; ++c) {
+                uint8_t *dst = base + (size_t)(2 + c) * col_bytes;
+                HOMS_CUDA(cudaMemcpyAsync(dst, cols[c], es * (size_t)nn, cudaMemcpyHostToDevice, ctx->stream));
+                cols[c] = dst;
+            }
+        }
+        // Metadata: column pointers, part starts, query times, part signs.
+        std::vector<uint8_t> meta;
+        const size_t off_starts = sizeof(void *) * NCOLS;
+        const size_t off_q = off_starts + sizeof(int64_t) * (size_t)nparts;
+        const size_t off_signs = off_q + sizeof(double) * (size_t)nq;
+        meta.resize(off_signs + (size_t)nparts);
+        std::memcpy(meta.data(), cols, sizeof(void *) * NCOLS);
+        int64_t *st = reinterpret_cast<int64_t *>(meta.data() + off_starts);
+        int8_t *sg = reinterpret_cast<int8_t *>(meta.data() + off_signs);
+        st[0] = 0;
+        sg[0] = 0;
+        for (int32_t i = 0; i < nrf; ++i) {
+            st[i + 1] = rf_start[i];
+            sg[i + 1] = rf_sign[i];
+        }
+        if (nq > 0) std::memcpy(meta.data() + off_q, q_times, sizeof(double) * (size_t)nq);
+        HOMS_CUDA(ctx->kspace_meta.ensure(meta.size()));
+        uint8_t *dmeta = ctx->kspace_meta.as<uint8_t>();
+        HOMS_CUDA(cudaMemcpyAsync(dmeta, meta.data(), meta.size(), cudaMemcpyHostToDevice, ctx->stream));
+        // Outputs: the caller's device arrays or a staging buffer.
+        double *dk = k, *dkq = k_q;
+        const size_t k_bytes = sizeof(double) * (size_t)m * NCOLS, kq_bytes = sizeof(double) * (size_t)nq * NCOLS;
+        if (out_memory == HOMS_HOST) {
+            const size_t k_pad = (k_bytes + 255) & ~size_t(255);
+            HOMS_CUDA(ctx->kspace_out.ensure(k_pad + kq_bytes));
+            dk = ctx->kspace_out.as<double>();
+            dkq = reinterpret_cast<double *>(ctx->kspace_out.as<uint8_t>() + k_pad);
+        }
+        HOMS_CUDA(ctx->kspace_work.ensure(kspace_work_bytes(nn, NCOLS, nparts)));
+        KspaceArgs a;
+        a.nnodes = nn;
+        a.f64 = seq->dtype == HOMS_F64;
+        a.t = dev_t;
+        a.dt = dev_dt;
+        a.ncols = NCOLS;
+        a.cols = reinterpret_cast<const void *const *>(dmeta);
+        a.nparts = nparts;
+        a.starts = reinterpret_cast<const int64_t *>(dmeta + off_starts);
+        a.signs = reinterpret_cast<const int8_t *>(dmeta + off_signs);
+        a.gamma = seq->gamma;
+        a.nq = nq;
+        a.q = reinterpret_cast<const double *>(dmeta + off_q);
+        a.k = dk;
+        a.kq = dkq;
+        a.work = ctx->kspace_work.p;
+        for (cudaEvent_t &e : ctx->kspace_ev)
+            if (!e) HOMS_CUDA(cudaEventCreate(&e));
+        HOMS_CUDA(cudaEventRecord(ctx->kspace_ev[0], ctx->stream));
+        HOMS_CUDA(kspace_launch(a, ctx->stream));
+        HOMS_CUDA(cudaEventRecord(ctx->kspace_ev[1], ctx->stream));
+        if (out_memory == HOMS_HOST) {
+            HOMS_CUDA(cudaMemcpyAsync(k, dk, k_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+            if (nq > 0) HOMS_CUDA(cudaMemcpyAsync(k_q, dkq, kq_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->kspace_timed = true;
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    }
+}
+
+homs_status homs_kspace_timing(homs_context *ctx, double *ms) {
+    if (!ctx || !ms) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->kspace_timed) return fail(ctx, Failure{HOMS_EINVAL, "no completed homs_kspace call on this context"});
+    float t = 0.f;
+    cudaError_t e = cudaEventElapsedTime(&t, ctx->kspace_ev[0], ctx->kspace_ev[1]);
+    if (e != cudaSuccess) return fail(ctx, Failure{HOMS_ECUDA, cudaGetErrorString(e)});
+    *ms = (double)t;
+    return HOMS_OK;
 }
 
 }  // extern "C"

@@ -25,12 +25,13 @@ import numpy as np
 from . import _lib
 from ._lib import Context, HomsError
 from .model import (GAMMA, ArgumentError, BlochHighOrder, DimensionMismatch, HO_DiscreteSequence, HO_Phantom, Mag,
-                    count_block_adc, get_sim_ranges, initialize_spins_state)
+                    count_block_adc, get_sim_ranges, initialize_spins_state, rf_events)
 
 __all__ = [
     "simulate", "prepare_simulation", "Plan", "Server", "Context", "HomsError", "ArgumentError", "DimensionMismatch",
     "BlochHighOrder", "HO_Phantom", "HO_DiscreteSequence", "Mag", "get_sim_ranges", "count_block_adc",
-    "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks",
+    "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks", "get_kspace",
+    "rf_events",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -234,6 +235,48 @@ def run_blocks(obj: HO_Phantom, seqd: HO_DiscreteSequence, parts, excitation, me
                                          ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST),
                ctx.handle)
     return np.asarray(sig), xy, z
+
+
+def get_kspace(seqd: HO_DiscreteSequence, rf_start=None, rf_sign=None, skip_rf=None, adc_times=None,
+               gamma: float = GAMMA, context: Optional[Context] = None, precision: str = "f64"):
+    """``K_nominal, K_nominal_adc, K_dfc, K_dfc_adc`` of a sampled sequence on
+    the GPU (``get_kspace``, src/datatypes/HO_Sequence.jl:236-255).
+
+    ``K_nominal`` (Nt-1 x 3) integrates the nominal gradients and ``K_dfc``
+    (Nt-1 x 16) the sixteen field coefficients, with KomaMRICore's cumtrapz,
+    restarted or negated at the RF breaks; the ``_adc`` copies interpolate them
+    at ``adc_times`` (default: the times of the ADC nodes).  The RF breaks are
+    ``rf_start`` / ``rf_sign`` (0-based interval indices; 0 excitation, -1
+    refocusing, +1 kept) or, by default, ``rf_events(seqd, gamma, skip_rf)``.
+    ``precision`` is the dtype the sequence arrays cross the ABI in; the
+    integral is FP64 either way."""
+    seqd.validate()
+    if rf_start is None:
+        if rf_sign is not None:
+            raise ArgumentError("rf_sign needs rf_start")
+        rf_start, rf_sign = rf_events(seqd, gamma, skip_rf)
+    elif rf_sign is None or len(rf_sign) != len(rf_start):
+        raise DimensionMismatch("rf_sign must contain one value per RF break.")
+    if precision not in ("f32", "f64"):
+        raise ArgumentError("precision must be f32 or f64")
+    if adc_times is None:
+        adc_times = np.asarray(seqd.t, dtype=np.float64)[np.asarray(seqd.adc, dtype=bool)]
+    ctx = context or _context(0)
+    dt = _lib.HOMS_F64 if precision == "f64" else _lib.HOMS_F32
+    keep = _lib._Keep()
+    nt = seqd.nnodes
+    sq = _lib.host_sequence(seqd, [(0, nt - 1)], [False], keep, dt, gamma)
+    starts = np.ascontiguousarray(rf_start, dtype=np.int64)
+    signs = np.ascontiguousarray(rf_sign, dtype=np.int8)
+    q = np.ascontiguousarray(adc_times, dtype=np.float64)
+    k = np.zeros((nt - 1, 19), order="F")
+    kq = np.zeros((q.shape[0], 19), order="F")
+    _lib.check(_lib.load().homs_kspace(ctx.handle, ctypes.byref(sq), len(starts),
+                                       starts.ctypes.data if len(starts) else None,
+                                       signs.ctypes.data if len(signs) else None, q.shape[0],
+                                       q.ctypes.data if q.shape[0] else None, k.ctypes.data,
+                                       kq.ctypes.data if q.shape[0] else None, _lib.HOMS_HOST), ctx.handle)
+    return k[:, :3], kq[:, :3], k[:, 3:], kq[:, 3:]
 
 
 class Plan:

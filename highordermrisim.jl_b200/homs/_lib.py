@@ -27,6 +27,7 @@ EXPORTED = [
     "homs_count_adc", "homs_plan_create", "homs_plan_run", "homs_plan_device_bytes", "homs_plan_timing",
     "homs_plan_destroy", "homs_coil_reduce_noalloc", "homs_server_create", "homs_server_submit", "homs_server_poll",
     "homs_server_wait", "homs_server_times", "homs_server_error", "homs_server_release", "homs_server_destroy",
+    "homs_kspace", "homs_kspace_timing",
 ]
 
 
@@ -124,6 +125,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_server_error": (ctypes.c_char_p, [vp, i64]),
         "homs_server_release": (ctypes.c_int, [vp, i64]),
         "homs_server_destroy": (ctypes.c_int, [vp]),
+        "homs_kspace": (ctypes.c_int, [vp, ctypes.POINTER(Sequence), i32, vp, vp, i64, vp, vp, vp, ctypes.c_int]),
+        "homs_kspace_timing": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

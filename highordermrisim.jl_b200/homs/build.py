@@ -27,6 +27,7 @@ UNITS = {
     "homs_plain.cu": ["-fmad=false"],
     "homs_split.cu": [],
     "homs_api.cu": [],
+    "homs_kspace.cu": [],
     "homs_noalloc.cu": [],
     "homs_server.cu": [],
 }

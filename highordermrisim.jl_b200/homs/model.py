@@ -274,3 +274,50 @@ def initialize_spins_state(obj: HO_Phantom) -> Mag:
     """Mxy = 0, Mz = rho (``BlochHighOrderSimulatitonMethod.jl:9-15``)."""
     cdt = np.complex64 if obj.rho.dtype == np.float32 else np.complex128
     return Mag(np.zeros(len(obj), dtype=cdt), obj.rho.copy())
+
+
+def rf_events(seqd: HO_DiscreteSequence, gamma: float = GAMMA, skip_rf=None):
+    """RF breaks of a sampled sequence for the encoding export.
+
+    The reference takes them from KomaMRIBase.get_RF_types on the unsampled
+    sequence (``src/datatypes/HO_Sequence.jl:263``): every RF pulse cuts the
+    k-space integral at its centre and is an excitation (flip angle up to
+    90.01 degrees; the integral restarts) or a refocusing pulse (the integral
+    changes sign).  Here a pulse is a run of consecutive excitation intervals
+    with nonzero B1; its flip angle is 360 gamma sum |B1[n]| dt[n] degrees, its
+    centre the |B1|-weighted mean interval midpoint, and its break the first
+    interval of the run that starts at or after that centre.  ``skip_rf``
+    (one flag per pulse) keeps the integral running through a pulse, as in
+    the reference (:272).  Returns 0-based ``(rf_start, rf_sign)`` lists.
+    """
+    exc = np.asarray(seqd.excitation, dtype=bool)
+    t = np.asarray(seqd.t, dtype=np.float64)
+    dt = np.asarray(seqd.dt, dtype=np.float64)
+    b1 = np.abs(np.asarray(seqd.b1, dtype=np.complex128))
+    m = exc.shape[0]
+    pulses = []
+    i = 0
+    while i < m:
+        if not (exc[i] and b1[i] > 0):
+            i += 1
+            continue
+        j = i
+        while j < m and exc[j] and b1[j] > 0:
+            j += 1
+        w = b1[i:j] * dt[i:j]
+        area = float(w.sum())
+        centre = float((w * (t[i:j] + dt[i:j] / 2)).sum() / area) if area > 0 else float(t[i])
+        start = next((n for n in range(i, j) if t[n] >= centre), j - 1)
+        pulses.append((start, 360.0 * gamma * area))
+        i = j
+    if skip_rf is None:
+        skip_rf = [False] * len(pulses)
+    if len(skip_rf) != len(pulses):
+        raise DimensionMismatch("skip_rf must contain one flag per RF event.")
+    # As in the reference, part r + 1 takes the type of the r-th pulse
+    # whichever break opened it; a break at the first interval opens no part
+    # (kfoldperm's breaks are part starts).
+    signs = [1 if skip else (0 if flip <= 90.01 else -1) for (_, flip), skip in zip(pulses, skip_rf)]
+    rf_start = sorted({start for start, _ in pulses if 1 <= start < m})
+    return rf_start, signs[:len(rf_start)]
+

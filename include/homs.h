@@ -179,6 +179,31 @@ homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, int64_t nsp
                                      const void *states, int64_t ldstates, const void *csm, int64_t ldcsm, void *sig,
                                      int64_t ldsig);
 
+/* ---- encoding export ------------------------------------------------------------
+ * Generalised k-space of a sampled sequence: replaces get_kspace / grad2kspace
+ * (src/datatypes/HO_Sequence.jl:236-287).  Columns 0..2 integrate the nominal
+ * gradients gx, gy, gz (K_nominal) and columns 3..18 the field coefficients
+ * h0..h15 (K_dfc).  Over the intervals n = 0 .. nnodes-2 of `seq`, each column
+ * is KomaMRICore's cumtrapz of its node values, restarted at every RF break:
+ * rf_start[i] (0-based interval index, strictly increasing, 1 <= rf_start[i] <
+ * nnodes-1) begins part i+1, whose values then add rf_sign[i] times the value
+ * at the end of part i (0 after an excitation, -1 after a refocusing pulse, +1
+ * otherwise or when the pulse is skipped).  All values are multiplied by
+ * seq->gamma (cycles/m^order).  k is (nnodes-1) x 19 FP64, column-major.
+ * k_q (nq x 19, column-major) holds k at the times q_times by linear
+ * interpolation over the knots t[n] + dt[n], 0 outside them (the ADC-sampled
+ * K_nominal_adc / K_dfc_adc with q_times = the ADC times).
+ * The RF breaks and their signs come from the caller: the reference derives
+ * them from the unsampled sequence (KomaMRIBase.get_RF_types), which does not
+ * cross this ABI.  seq's arrays may be host or device memory (seq->memory);
+ * rf_start, rf_sign and q_times are host memory; k and k_q are in out_memory.
+ * The block-plan fields of seq are not used.  Returns when k and k_q are ready. */
+homs_status homs_kspace(homs_context *ctx, const homs_sequence *seq, int32_t nrf, const int64_t *rf_start,
+                        const int8_t *rf_sign, int64_t nq, const double *q_times, double *k, double *k_q,
+                        homs_memory out_memory);
+/* Device time (CUDA events) of the kernels of the last homs_kspace call on ctx. */
+homs_status homs_kspace_timing(homs_context *ctx, double *ms);
+
 /* ---- whole simulation ---------------------------------------------------------- */
 
 /* Run every block of `seq` on `phantom` (host or device arrays).

@@ -279,3 +279,62 @@ def simulate_np(phantom, seq, parts, excitation, method_flags, mxy0=None, mz0=No
     nc = np.asarray(phantom.csm).reshape(ns, -1).shape[1]
     sig = np.concatenate(blocks, axis=0) if blocks else np.zeros((0, nc), np.complex128)
     return sig, mxy, mz
+
+
+# ---------------------------------------------------------------------------
+# Encoding export: grad2kspace (src/datatypes/HO_Sequence.jl:257-287).
+# ---------------------------------------------------------------------------
+
+def cumtrapz_np(dt, x):
+    """KomaMRICore's cumtrapz for vectors: cumsum((x[2:end] + x[1:end-1]) .* (dt / 2))
+    (third-party, KomaMRICore 0.14.0; used at HO_Sequence.jl:268)."""
+    x = np.asarray(x, dtype=np.float64)
+    return np.cumsum((x[1:] + x[:-1]) * (np.asarray(dt, dtype=np.float64) / 2))
+
+
+def kfoldperm_parts(n, breaks):
+    """Parts of 1:n cut at 1-based ``breaks``, as KomaMRIBase's
+    kfoldperm(n, 1; breaks) builds them (HO_Sequence.jl:264): each break
+    starts a new part; returned 0-based as (first, last_exclusive)."""
+    b = sorted(set([1, n + 1] + [int(v) for v in breaks]))
+    return [(b[i] - 1, b[i + 1] - 1) for i in range(len(b) - 1)]
+
+
+def grad2kspace_np(seq, rf_start, rf_sign, gamma=GAMMA, q_times=None):
+    """k-space of the 19 columns gx, gy, gz, h0..h15 of a sampled sequence
+    (grad2kspace, HO_Sequence.jl:261-287), part by part exactly as the loop at
+    :266-278, with the RF breaks given as 0-based interval indices
+    ``rf_start`` and their signs (0 excitation, -1 refocusing, +1 other or
+    skipped; :272-274).  Returns (k (m x 19), k at ``q_times`` (nq x 19)),
+    the latter by linear interpolation over the knots t[n] + dt[n] with 0
+    outside them (:279-286)."""
+    t = np.asarray(seq.t, dtype=np.float64)
+    dt = np.asarray(seq.dt, dtype=np.float64)
+    m = t.shape[0] - 1
+    cols = [seq.gx, seq.gy, seq.gz] + [seq.h[i] for i in range(16)]
+    parts = kfoldperm_parts(m, [s + 1 for s in rf_start])
+    k = np.zeros((m, len(cols)))
+    for term, g in enumerate(cols):
+        g = np.asarray(g, dtype=np.float64)
+        previous = 0.0
+        for r, (a, b) in enumerate(parts):
+            k[a:b, term] = cumtrapz_np(dt[a:b], g[a:b + 1])
+            if r > 0:
+                k[a:b, term] += rf_sign[r - 1] * previous
+            previous = k[b - 1, term]
+    kspace = gamma * k
+    if q_times is None:
+        return kspace, np.zeros((0, len(cols)))
+    knots = t[:-1] + dt
+    q = np.asarray(q_times, dtype=np.float64)
+    kq = np.zeros((q.shape[0], len(cols)))
+    for j, tau in enumerate(q):
+        if tau < knots[0] or tau > knots[-1]:
+            continue
+        n = int(np.searchsorted(knots, tau, side="right")) - 1
+        if n == m - 1:
+            kq[j] = kspace[n]
+        else:
+            w = (tau - knots[n]) / (knots[n + 1] - knots[n])
+            kq[j] = kspace[n] + w * (kspace[n + 1] - kspace[n])
+    return kspace, kq
