@@ -15,13 +15,13 @@
 //           carry-in; the tile's (has-part-start, sum since the last start)
 //           and, for every part starting inside the tile, the sum of the
 //           tile's elements before it (that part's predecessor's tail);
-//   pass 2  per column, sequential over tiles and parts: carry into every
-//           tile, the local sum of every part and the part offsets
-//           sign_p * (end value of part p-1);
+//   pass 2  one warp per column: carry into every tile (segmented scan of
+//           the tile aggregates), the local sum of every part and the part
+//           offsets sign_p * (end value of part p-1) (an affine scan);
 //   pass 3  per tile: the same block scan with the tile's carry-in, plus the
 //           part offset, times gamma, written column-major;
-//   query   per (ADC time, column): binary search over the knots, linear
-//           interpolation.
+//   query   per ADC time: binary search over the knots, then linear
+//           interpolation of every column.
 // The traffic is one read of every column in passes 1 and 3 (the second read
 // hits L2 at the sizes of a sequence) and one write of k: an HBM-bound scan.
 #include <algorithm>
@@ -49,8 +49,13 @@ __device__ __forceinline__ double trap(const S *g, const S *dt, int64_t n) {
     return ((double)g[n] + (double)g[n + 1]) * ((double)dt[n] * 0.5);
 }
 
+// Shared tile of trapezoid terms, one double of padding after every ITEMS
+// (thread t's items t*ITEMS .. +ITEMS-1 then start 72 bytes apart: two-way
+// bank use, the minimum for 8-byte words, where 64 bytes would be 16-way).
+__device__ __forceinline__ int pad(int i) { return i + i / ITEMS; }
+
 struct Shared {
-    double y[TILE];
+    double y[TILE + TILE / ITEMS];
     uint32_t flag[TILE / 32];
     Seg warp_total[NWARPS];
     Seg warp_prefix[NWARPS + 1];
@@ -69,7 +74,7 @@ __device__ void tile_scan(const S *g, const S *dt, int64_t m, int64_t t0, const 
     for (int j = 0; j < ITEMS; ++j) {
         const int i = j * THREADS + tid;
         const int64_t n = t0 + i;
-        sh.y[i] = n < m ? trap(g, dt, n) : 0.0;
+        sh.y[pad(i)] = n < m ? trap(g, dt, n) : 0.0;
     }
     __syncthreads();
     for (int p = tid; p < nparts; p += THREADS) {
@@ -82,7 +87,7 @@ __device__ void tile_scan(const S *g, const S *dt, int64_t m, int64_t t0, const 
     Seg agg{false, 0.0};
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const double y = sh.y[base + j];
+        const double y = sh.y[pad(base + j)];
         if ((bits >> j) & 1u) {
             agg.f = true;
             agg.v = y;
@@ -137,7 +142,7 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(const S *dt, const void
     tile_scan<S>(g, dt, m, t0, starts, nparts, 0.0, sh, v, bits);
     const int base = threadIdx.x * ITEMS;
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) sh.y[base + j] = v[j];
+    for (int j = 0; j < ITEMS; ++j) sh.y[pad(base + j)] = v[j];
     __syncthreads();
     if (threadIdx.x == 0) {
         any[(size_t)col * ntiles + tile] = sh.warp_prefix[NWARPS].f ? 1 : 0;
@@ -147,43 +152,81 @@ __global__ void __launch_bounds__(THREADS) reduce_kernel(const S *dt, const void
         const int64_t s = starts[p];
         if (p > 0 && s >= t0 && s < t0 + TILE && s < m) {
             const int i = (int)(s - t0);
-            head[(size_t)col * nparts + p] = i > 0 ? sh.y[i - 1] : 0.0;
+            head[(size_t)col * nparts + p] = i > 0 ? sh.y[pad(i - 1)] : 0.0;
         }
     }
 }
 
-// Pass 2: carry into each tile, part sums and part offsets, per column.
-__global__ void carry_kernel(int64_t m, int ntiles, const int64_t *starts, const int8_t *signs, int nparts,
-                             const uint8_t *any, const double *tail, const double *head, double *carry_in,
-                             double *part_sum, double *offset) {
-    const int col = blockIdx.x;
-    if (threadIdx.x != 0) return;
+// Pass 2, one warp per column: the carry into every tile (a segmented scan
+// of the tile aggregates, 32 tiles at a time), the local sum of every part
+// (the carry into its first tile plus its head in that tile, or its head
+// alone when an earlier part starts in the same tile), and the part offsets
+// sign_p * (end value of part p-1), an affine scan prev_p = sign_p prev_{p-1}
+// + S_p over the parts.
+struct Affine {
+    double a, b;  // x -> a x + b
+};
+__device__ __forceinline__ Affine then(const Affine &first, const Affine &second) {
+    return Affine{second.a * first.a, second.a * first.b + second.b};
+}
+
+__global__ void __launch_bounds__(32) carry_kernel(int ntiles, const int64_t *starts, const int8_t *signs,
+                                                   int nparts, const uint8_t *any, const double *tail,
+                                                   const double *head, double *carry_in, double *part_sum,
+                                                   double *offset) {
+    const int col = blockIdx.x, lane = threadIdx.x;
     const uint8_t *a = any + (size_t)col * ntiles;
     const double *tl = tail + (size_t)col * ntiles;
     const double *hd = head + (size_t)col * nparts;
     double *ci = carry_in + (size_t)col * ntiles;
     double *ps = part_sum + (size_t)col * nparts;
     double *off = offset + (size_t)col * nparts;
-    double carry = 0.0;
-    int p = 1;
-    for (int i = 0; i < ntiles; ++i) {
-        ci[i] = carry;
-        bool first = true;
-        while (p < nparts && starts[p] / TILE == i) {
-            ps[p - 1] = (first ? carry : 0.0) + hd[p];
-            first = false;
-            ++p;
+    Seg run{false, 0.0};
+    for (int base = 0; base < ntiles; base += 32) {
+        const int i = base + lane;
+        Seg x = i < ntiles ? Seg{a[i] != 0, tl[i]} : Seg{false, 0.0};
+        Seg inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int uf = __shfl_up_sync(0xffffffffu, (int)inc.f, o);
+            const double uv = __shfl_up_sync(0xffffffffu, inc.v, o);
+            if (lane >= o) inc = combine(Seg{uf != 0, uv}, inc);
         }
-        carry = a[i] ? tl[i] : carry + tl[i];
+        const int ef = __shfl_up_sync(0xffffffffu, (int)inc.f, 1);
+        const double ev = __shfl_up_sync(0xffffffffu, inc.v, 1);
+        const Seg excl = lane == 0 ? Seg{false, 0.0} : Seg{ef != 0, ev};
+        if (i < ntiles) ci[i] = combine(run, excl).v;
+        const int lf = __shfl_sync(0xffffffffu, (int)inc.f, 31);
+        const double lv = __shfl_sync(0xffffffffu, inc.v, 31);
+        run = combine(run, Seg{lf != 0, lv});
     }
-    ps[nparts - 1] = carry;
-    double prev = 0.0;
-    for (int q = 0; q < nparts; ++q) {
-        const double o = q == 0 ? 0.0 : (double)signs[q] * prev;
-        off[q] = o;
-        prev = ps[q] + o;
+    __syncwarp();
+    for (int p = 1 + lane; p < nparts; p += 32) {
+        const int64_t tile = starts[p] / TILE;
+        const bool first = starts[p - 1] / TILE != tile;
+        ps[p - 1] = (first ? ci[tile] : 0.0) + hd[p];
     }
-    (void)m;
+    if (lane == 0) ps[nparts - 1] = run.v;
+    __syncwarp();
+    Affine acc{0.0, 0.0};  // prev_{-1} = 0 for every input
+    for (int base = 0; base < nparts; base += 32) {
+        const int p = base + lane;
+        Affine f = p < nparts ? Affine{p == 0 ? 0.0 : (double)signs[p], ps[p]} : Affine{1.0, 0.0};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double ua = __shfl_up_sync(0xffffffffu, f.a, o);
+            const double ub = __shfl_up_sync(0xffffffffu, f.b, o);
+            if (lane >= o) f = then(Affine{ua, ub}, f);
+        }
+        // prev_{p-1}: the composed map of the parts before p applied to 0.
+        const double ea = __shfl_up_sync(0xffffffffu, f.a, 1);
+        const double eb = __shfl_up_sync(0xffffffffu, f.b, 1);
+        const Affine before = lane == 0 ? acc : then(acc, Affine{ea, eb});
+        if (p < nparts) off[p] = p == 0 ? 0.0 : (double)signs[p] * before.b;
+        const double la = __shfl_sync(0xffffffffu, f.a, 31);
+        const double lb = __shfl_sync(0xffffffffu, f.b, 31);
+        acc = then(acc, Affine{la, lb});
+    }
 }
 
 // Pass 3: k = gamma * (part-local prefix + part offset), column-major.
@@ -214,48 +257,65 @@ __global__ void __launch_bounds__(THREADS) write_kernel(const S *dt, const void 
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         if (j > 0 && ((bits >> j) & 1u)) ++p;
-        sh.y[base + j] = gamma * (v[j] + off[p]);
+        sh.y[pad(base + j)] = gamma * (v[j] + off[p]);
     }
     __syncthreads();
     double *kc = k + (size_t)col * m;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const int i = j * THREADS + threadIdx.x;
-        if (t0 + i < m) kc[t0 + i] = sh.y[i];
+        if (t0 + i < m) kc[t0 + i] = sh.y[pad(i)];
     }
 }
 
 // Query: k at the times q by linear interpolation over the knots
-// t[n] + dt[n] (n < m), 0 outside [knot 0, knot m-1].
+// t[n] + dt[n] (n < m), 0 outside [knot 0, knot m-1].  Each block first
+// stages every stride-th knot in shared memory; a time's search runs there,
+// then over one stride of global knots, and serves all columns.
+constexpr int QTABLE = 1024;
+
 template <typename S>
-__global__ void query_kernel(const S *t, const S *dt, int64_t m, const double *k, int32_t ncols, const double *q,
-                             int64_t nq, double *kq) {
-    const int64_t total = nq * ncols;
-    for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
-         idx += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t j = idx % nq;
-        const int64_t col = idx / nq;
+__global__ void __launch_bounds__(256) query_kernel(const S *t, const S *dt, int64_t m, const double *k,
+                                                    int32_t ncols, const double *q, int64_t nq, double *kq) {
+    __shared__ double table[QTABLE];
+    auto knot = [&](int64_t n) { return (double)t[n] + (double)dt[n]; };
+    const int64_t stride = (m + QTABLE - 1) / QTABLE;
+    const int nrows = (int)((m + stride - 1) / stride);  // rows r: knot(r * stride), r * stride < m
+    for (int r = threadIdx.x; r < nrows; r += blockDim.x) table[r] = knot((int64_t)r * stride);
+    __syncthreads();
+    const double last = knot(m - 1);
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nq; j += (int64_t)gridDim.x * blockDim.x) {
         const double tau = q[j];
-        auto knot = [&](int64_t n) { return (double)t[n] + (double)dt[n]; };
-        double out = 0.0;
-        if (tau >= knot(0) && tau <= knot(m - 1)) {
-            int64_t lo = 0, hi = m;  // first n with knot(n) > tau
+        int64_t n = -1;
+        double w = 0.0;
+        if (tau >= table[0] && tau <= last) {
+            int lo = 0, hi = nrows;  // first row whose knot exceeds tau (lo >= 1 here)
             while (lo < hi) {
-                const int64_t mid = (lo + hi) >> 1;
-                if (knot(mid) <= tau) lo = mid + 1;
+                const int mid = (lo + hi) >> 1;
+                if (table[mid] <= tau) lo = mid + 1;
                 else hi = mid;
             }
-            const int64_t n = lo - 1;
-            const double *kc = k + (size_t)col * m;
-            if (n == m - 1) {
-                out = kc[n];
-            } else {
+            // knot((lo-1) stride) <= tau < knot(lo stride) (or lo stride >= m):
+            // the last knot <= tau lies in [(lo-1) stride, min(lo stride, m)).
+            int64_t glo = (int64_t)(lo - 1) * stride + 1, ghi = std::min<int64_t>((int64_t)lo * stride, m);
+            while (glo < ghi) {
+                const int64_t mid = (glo + ghi) >> 1;
+                if (knot(mid) <= tau) glo = mid + 1;
+                else ghi = mid;
+            }
+            n = glo - 1;
+            if (n < m - 1) {
                 const double s0 = knot(n), s1 = knot(n + 1);
-                const double w = (tau - s0) / (s1 - s0);
-                out = kc[n] + w * (kc[n + 1] - kc[n]);
+                w = (tau - s0) / (s1 - s0);
             }
         }
-        kq[idx] = out;
+        for (int32_t col = 0; col < ncols; ++col) {
+            const double *kc = k + (size_t)col * m;
+            double out = 0.0;
+            if (n == m - 1) out = kc[n];
+            else if (n >= 0) out = kc[n] + w * (kc[n + 1] - kc[n]);
+            kq[(size_t)col * nq + j] = out;
+        }
     }
 }
 
@@ -292,13 +352,12 @@ cudaError_t launch_typed(const KspaceArgs &a, cudaStream_t stream) {
     const S *dt = static_cast<const S *>(a.dt);
     const dim3 grid((unsigned)ntiles, (unsigned)a.ncols);
     reduce_kernel<S><<<grid, THREADS, 0, stream>>>(dt, a.cols, m, a.starts, a.nparts, ntiles, w.any, w.tail, w.head);
-    carry_kernel<<<a.ncols, 32, 0, stream>>>(m, ntiles, a.starts, a.signs, a.nparts, w.any, w.tail, w.head, w.carry,
+    carry_kernel<<<a.ncols, 32, 0, stream>>>(ntiles, a.starts, a.signs, a.nparts, w.any, w.tail, w.head, w.carry,
                                              w.part_sum, w.offset);
     write_kernel<S><<<grid, THREADS, 0, stream>>>(dt, a.cols, m, a.starts, a.nparts, ntiles, w.carry, w.offset,
                                                   a.gamma, a.k);
     if (a.nq > 0) {
-        const int64_t total = a.nq * a.ncols;
-        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, 148 * 16));
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((a.nq + 255) / 256, 148 * 4));
         query_kernel<S><<<blocks, 256, 0, stream>>>(t, dt, m, a.k, a.ncols, a.q, a.nq, a.kq);
     }
     return cudaGetLastError();

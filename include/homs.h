@@ -192,7 +192,9 @@ homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, int64_t nsp
  * seq->gamma (cycles/m^order).  k is (nnodes-1) x 19 FP64, column-major.
  * k_q (nq x 19, column-major) holds k at the times q_times by linear
  * interpolation over the knots t[n] + dt[n], 0 outside them (the ADC-sampled
- * K_nominal_adc / K_dfc_adc with q_times = the ADC times).
+ * K_nominal_adc / K_dfc_adc with q_times = the ADC times).  The knots must be
+ * non-decreasing, as they are when dt is the difference of consecutive t;
+ * otherwise k_q is unspecified (every access stays inside the arrays).
  * The RF breaks and their signs come from the caller: the reference derives
  * them from the unsampled sequence (KomaMRIBase.get_RF_types), which does not
  * cross this ABI.  seq's arrays may be host or device memory (seq->memory);

@@ -76,8 +76,13 @@ def test_kspace_tails_and_tile_boundaries(gpu_context, nt):
 
 
 def test_kspace_fp32_sequence_arrays(gpu_context):
+    # FP32 times accumulated from positive FP32 steps, as a sampled sequence
+    # holds them: the knots t[n] + dt[n] are non-decreasing.
     rng = np.random.default_rng(5)
-    seq32 = _random_seq(rng, 9000).astype(np.float32)
+    seq32 = _random_seq(rng, 9000, zero_dt=0.0).astype(np.float32)
+    seq32.t = np.concatenate([[np.float32(0)], np.cumsum(seq32.dt, dtype=np.float32)])
+    knots = seq32.t[:-1].astype(np.float64) + seq32.dt.astype(np.float64)
+    assert np.all(np.diff(knots) >= 0)
     starts, signs = [1000, 5000], [0, -1]
     q = np.asarray(seq32.t, dtype=np.float64)[::7]
     want_k, want_q = orc.grad2kspace_np(seq32.astype(np.float64), starts, signs, GAMMA, q)
