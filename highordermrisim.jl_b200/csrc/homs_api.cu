@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "homs_common.cuh"
+#include "homs_internal.cuh"
 #include "homs_kspace.cuh"
 #include "homs_split.cuh"
 
@@ -26,31 +27,44 @@ using namespace homs;
 
 namespace {
 
+// Device buffer that grows on demand.  It owns its memory, or is a
+// read-only view of another buffer (a device-resident phantom's arrays):
+// ensure() never writes through a view, it replaces it with owned memory.
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    bool owned = true;
     DevBuf() = default;
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
-    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes), owned(o.owned) { o.p = nullptr; o.bytes = 0; o.owned = true; }
     DevBuf &operator=(DevBuf &&o) noexcept {
         if (this != &o) {
             release();
             p = o.p;
             bytes = o.bytes;
+            owned = o.owned;
             o.p = nullptr;
             o.bytes = 0;
+            o.owned = true;
         }
         return *this;
     }
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
         p = nullptr;
         bytes = 0;
+        owned = true;
+    }
+    void view(const DevBuf &src) {
+        release();
+        p = src.p;
+        bytes = src.bytes;
+        owned = false;
     }
     cudaError_t ensure(size_t n) {
-        if (n <= bytes && p) return cudaSuccess;
+        if (n <= bytes && p && owned) return cudaSuccess;
         release();
         if (n == 0) n = 16;
         cudaError_t e = cudaMalloc(&p, n);
@@ -350,18 +364,16 @@ struct Resident : ResidentBase {
 
 namespace {
 
-// Upload a phantom and a sampled sequence into `r` (fresh or reused: device
-// buffers only grow).  Host arrays may be released when this returns: copies
-// from pageable memory are staged before cudaMemcpyAsync returns.
+// Upload a phantom into `r` (fresh or reused: device buffers only grow).
+// Host arrays may be released when this returns: copies from pageable memory
+// are staged before cudaMemcpyAsync returns.
 template <typename T>
-void fill_resident(homs_context *ctx, Resident<T> *r, const homs_phantom *p, const homs_sequence *q) {
+void fill_phantom(homs_context *ctx, Resident<T> *r, const homs_phantom *p) {
     r->split_ready = false;
     r->dtype = sizeof(T) == 8 ? HOMS_F64 : HOMS_F32;
     r->ns = p->nspins;
     r->nc = p->ncoils;
-    r->nt = q->nnodes;
-    r->gamma = q->gamma;
-    const int64_t ns = p->nspins, nt = q->nnodes;
+    const int64_t ns = p->nspins;
     upload<T>(ctx, r->x, p->x, p->dtype, p->memory, ns);
     upload<T>(ctx, r->y, p->y, p->dtype, p->memory, ns);
     upload<T>(ctx, r->z, p->z, p->dtype, p->memory, ns);
@@ -370,6 +382,37 @@ void fill_resident(homs_context *ctx, Resident<T> *r, const homs_phantom *p, con
     upload<T>(ctx, r->T2, p->T2, p->dtype, p->memory, ns);
     upload<T>(ctx, r->dw, p->dw, p->dtype, p->memory, ns);
     upload_csm_rows<T>(ctx, r->csm_rows, p->csm, p->dtype, p->memory, ns, p->ncoils, ns);
+}
+
+// Make `r`'s phantom a read-only view of `src`'s (a device-resident phantom
+// that outlives the run), split operands included when `src` has them.
+template <typename T>
+void attach_phantom(Resident<T> *r, const Resident<T> &src) {
+    r->dtype = src.dtype;
+    r->ns = src.ns;
+    r->nc = src.nc;
+    r->x.view(src.x);
+    r->y.view(src.y);
+    r->z.view(src.z);
+    r->rho.view(src.rho);
+    r->T1.view(src.T1);
+    r->T2.view(src.T2);
+    r->dw.view(src.dw);
+    r->csm_rows.view(src.csm_rows);
+    r->split_ready = false;
+    if (src.split_ready) {
+        HOMS_CUDA(split_attach(r->split, src.split));
+        r->split_ready = true;
+    }
+}
+
+// Upload a sampled sequence and size the run's state and signal buffers for
+// the phantom already in `r`.
+template <typename T>
+void fill_sequence(homs_context *ctx, Resident<T> *r, const homs_sequence *q) {
+    r->nt = q->nnodes;
+    r->gamma = q->gamma;
+    const int64_t ns = r->ns, nt = q->nnodes;
     upload<T>(ctx, r->t, q->t, q->dtype, q->memory, nt);
     upload<T>(ctx, r->dt, q->dt, q->dtype, q->memory, nt - 1);
     upload<T>(ctx, r->gx, q->gx, q->dtype, q->memory, nt);
@@ -397,7 +440,13 @@ void fill_resident(homs_context *ctx, Resident<T> *r, const homs_phantom *p, con
     HOMS_CUDA(r->xy.ensure(sizeof(cplx<T>) * (size_t)ns));
     HOMS_CUDA(r->mz.ensure(sizeof(T) * (size_t)ns));
     HOMS_CUDA(r->acc.ensure(sizeof(T) * (size_t)ns));
-    HOMS_CUDA(r->sig.ensure(sizeof(cplx<T>) * (size_t)std::max<int64_t>(nadc * p->ncoils, 1)));
+    HOMS_CUDA(r->sig.ensure(sizeof(cplx<T>) * (size_t)std::max<int64_t>(nadc * r->nc, 1)));
+}
+
+template <typename T>
+void fill_resident(homs_context *ctx, Resident<T> *r, const homs_phantom *p, const homs_sequence *q) {
+    fill_phantom<T>(ctx, r, p);
+    fill_sequence<T>(ctx, r, q);
 }
 
 template <typename T>
@@ -525,6 +574,20 @@ void init_state(homs_context *ctx, Resident<T> &r, const homs_state *state, homs
     HOMS_CUDA(cudaMemsetAsync(r.acc.p, 0, sizeof(T) * (size_t)r.ns, ctx->stream));
 }
 
+// Build the split path's phantom operands (basis table, pre-split
+// sensitivities) unless `r` has them, its own or a resident phantom's.
+template <typename T>
+void ensure_split(homs_context *ctx, Resident<T> &r) {
+    if (r.split_ready) return;
+    std::string err;
+    cudaError_t e = split_prepare(r.split, r.ns, r.nc, r.x.p, r.y.p, r.z.p, r.dw.p, r.csm_rows.p, sizeof(T) == 8,
+                                  ctx->stream, &err);
+    if (e != cudaSuccess) throw Failure{e == cudaErrorMemoryAllocation ? HOMS_ENOMEM : HOMS_ECUDA,
+                                        std::string("split_prepare: ") + cudaGetErrorString(e)};
+    if (!err.empty()) throw Failure{HOMS_EUNSUPPORTED, err};
+    r.split_ready = true;
+}
+
 template <typename T>
 void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opts) {
     r.events_used = 0;
@@ -536,15 +599,7 @@ void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opt
         run_plain<T>(ctx, r, method);
     } else if (mode == HOMS_SPLIT) {
         if (sizeof(T) != 8) throw Failure{HOMS_EUNSUPPORTED, "internal: split mode runs on FP64 resident arrays"};
-        if (!r.split_ready) {
-            std::string err;
-            cudaError_t e = split_prepare(r.split, r.ns, r.nc, r.x.p, r.y.p, r.z.p, r.dw.p, r.csm_rows.p, true,
-                                          ctx->stream, &err);
-            if (e != cudaSuccess) throw Failure{e == cudaErrorMemoryAllocation ? HOMS_ENOMEM : HOMS_ECUDA,
-                                                std::string("split_prepare: ") + cudaGetErrorString(e)};
-            if (!err.empty()) throw Failure{HOMS_EUNSUPPORTED, err};
-            r.split_ready = true;
-        }
+        ensure_split<T>(ctx, r);
         HOMS_CUDA(split_reset_error(r.split, ctx->stream));
         SplitRunArgs sa;
         sa.sizeof_T = sizeof(T);
@@ -706,6 +761,53 @@ struct homs_plan {
     std::unique_ptr<ResidentBase> res;
     homs_dtype out_dtype = HOMS_F64;  // the caller's dtype (the resident copy may be wider)
 };
+
+// A phantom kept on one device for many simulations: its arrays in the
+// arithmetic's precision and, for split mode, its basis table and pre-split
+// sensitivity operand.  Immutable after creation, so runs on any number of
+// contexts of that device may read it at once.
+struct homs_resident {
+    int device = 0;
+    homs_mode mode = HOMS_PLAIN;
+    homs_dtype in_dtype = HOMS_F64;  // the caller's dtype: results come back in it
+    std::unique_ptr<ResidentBase> res;
+};
+
+namespace homs {
+bool resident_shape(const homs_resident *r, ResidentShape *out) {
+    if (!r || !r->res || !out) return false;
+    out->nspins = r->res->ns;
+    out->ncoils = r->res->nc;
+    out->compute = r->res->dtype;
+    out->mode = r->mode;
+    out->device = r->device;
+    return true;
+}
+}  // namespace homs
+
+namespace {
+
+// The context's cached workspace for dtype T, created empty if needed.
+template <typename T>
+Resident<T> *cache_slot(homs_context *ctx) {
+    auto &slot = ctx->cache[sizeof(T) == 8 ? 1 : 0];
+    if (!slot) slot = std::make_unique<Resident<T>>();
+    return static_cast<Resident<T> *>(slot.get());
+}
+
+template <typename T>
+void simulate_on_resident(homs_context *ctx, const homs_resident *res, const homs_sequence *seq,
+                          const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory) {
+    const auto &src = static_cast<const Resident<T> &>(*res->res);
+    Resident<T> *r = cache_slot<T>(ctx);
+    attach_phantom<T>(r, src);
+    fill_sequence<T>(ctx, r, seq);
+    init_state<T>(ctx, *r, state, res->in_dtype);
+    run_resident<T>(ctx, *r, opts);
+    copy_out<T>(ctx, *r, sig, sig_memory, state, res->in_dtype);
+}
+
+}  // namespace
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -1056,6 +1158,89 @@ homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins
         return HOMS_OK;
     } catch (const Failure &f) {
         return fail(ctx, f);
+    }
+}
+
+homs_status homs_resident_create(homs_context *ctx, const homs_phantom *phantom, homs_mode mode,
+                                 homs_resident **out) {
+    if (!ctx || !out) return HOMS_EINVAL;
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        validate_phantom(phantom);
+        HOMS_REQUIRE(mode == HOMS_PLAIN || mode == HOMS_SPLIT, "unknown run mode");
+        auto h = std::make_unique<homs_resident>();
+        h->device = ctx->device;
+        h->mode = mode;
+        h->in_dtype = phantom->dtype;
+        homs_run_options o{};
+        o.mode = mode;
+        if (compute_f64(phantom, &o)) {
+            auto r = std::make_unique<Resident<double>>();
+            fill_phantom<double>(ctx, r.get(), phantom);
+            if (mode == HOMS_SPLIT) ensure_split<double>(ctx, *r);
+            h->res = std::move(r);
+        } else {
+            auto r = std::make_unique<Resident<float>>();
+            fill_phantom<float>(ctx, r.get(), phantom);
+            h->res = std::move(r);
+        }
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+        *out = h.release();
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, Failure{HOMS_ENOMEM, "host allocation failed"});
+    }
+}
+
+homs_status homs_resident_device_bytes(const homs_resident *res, size_t *bytes) {
+    if (!res || !res->res || !bytes) return HOMS_EINVAL;
+    *bytes = res->res->device_bytes();
+    return HOMS_OK;
+}
+
+homs_status homs_resident_destroy(homs_resident *res) {
+    if (!res) return HOMS_EINVAL;
+    {
+        DeviceGuard g(res->device);
+        res->res.reset();
+    }
+    delete res;
+    return HOMS_OK;
+}
+
+homs_status homs_simulate_resident(homs_context *ctx, const homs_resident *res, const homs_sequence *seq,
+                                   const homs_run_options *opts, homs_state *state, void *sig,
+                                   homs_memory sig_memory) {
+    if (!ctx || !res || !res->res) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        HOMS_REQUIRE(res->device == ctx->device, "the resident phantom lives on another device than the context");
+        validate_sequence(seq);
+        HOMS_REQUIRE(sig_memory == HOMS_HOST || sig_memory == HOMS_DEVICE, "invalid signal memory kind");
+        homs_run_options o{};
+        o.method = 0x3Fu;
+        o.mode = res->mode;
+        if (opts) o = *opts;
+        HOMS_REQUIRE(o.mode == res->mode, "the run mode must be the one the resident phantom was prepared for");
+        if (res->res->dtype == HOMS_F64) simulate_on_resident<double>(ctx, res, seq, &o, state, sig, sig_memory);
+        else simulate_on_resident<float>(ctx, res, seq, &o, state, sig, sig_memory);
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        ctx->cache[0].reset();
+        ctx->cache[1].reset();
+        return fail(ctx, f);
+    } catch (const std::bad_alloc &) {
+        cudaStreamSynchronize(ctx->stream);
+        ctx->cache[0].reset();
+        ctx->cache[1].reset();
+        return fail(ctx, Failure{HOMS_ENOMEM, "host allocation failed"});
     }
 }
 

@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/homs.h"
+#include "homs_internal.cuh"
 
 namespace {
 
@@ -34,6 +35,7 @@ using Clock = std::chrono::steady_clock;
 
 struct Request {
     homs_phantom phantom;
+    const homs_resident *resident = nullptr;  // set: run on this device-resident phantom
     homs_sequence seq;
     homs_run_options opts;
     homs_state state;
@@ -49,17 +51,22 @@ struct Request {
 
 // Upper estimate of the device memory one simulation needs (inputs, state,
 // signal, staging of host sensitivities, and the path's work buffers).
-size_t estimate_bytes(const homs_phantom &p, const homs_sequence &q, const homs_run_options &o) {
-    const double es = (p.dtype == HOMS_F64 || o.mode == HOMS_SPLIT) ? 8.0 : 4.0;  // split mode is resident in FP64
-    const double ns = (double)p.nspins, nc = (double)p.ncoils, nt = (double)q.nnodes;
+// With `resident` the phantom's arrays, basis and pre-split sensitivities are
+// already on the device and are left out.
+size_t estimate_bytes(int64_t nspins, int32_t ncoils, homs_dtype dtype, const homs_sequence &q,
+                      const homs_run_options &o, bool resident) {
+    const double es = (dtype == HOMS_F64 || o.mode == HOMS_SPLIT) ? 8.0 : 4.0;  // split mode is resident in FP64
+    const double ns = (double)nspins, nc = (double)ncoils, nt = (double)q.nnodes;
     int64_t nadc = q.nnodes;
     if (q.memory == HOMS_HOST) homs_count_adc(&q, &nadc);
-    double b = ns * (7 * es + 4 * es * nc + 3 * es);  // phantom, csm rows + staging, state
-    b += nt * (26 * es + 2);                          // sampled sequence
-    b += (double)nadc * nc * 2 * es;                  // signal
+    double b = ns * 3 * es;                                // state
+    if (!resident) b += ns * (7 * es + 4 * es * nc);       // phantom, csm rows + staging
+    b += nt * (26 * es + 2);                               // sampled sequence
+    b += (double)nadc * nc * 2 * es;                       // signal
     if (o.mode == HOMS_SPLIT) {
         const double groups = std::ceil(nc / 32.0);
-        b += ns * (128.0 + 512.0 * groups + 152.0);   // basis, pre-split sensitivities, spin table
+        if (!resident) b += ns * (128.0 + 512.0 * groups);  // basis, pre-split sensitivities
+        b += ns * 152.0;                                    // spin table
         b += 4500.0 * 128 * 64 * 8 + (double)nadc * 192.0;  // split-K partials, phase prefix
     } else {
         const double grid = std::ceil(ns / 256.0);
@@ -103,8 +110,10 @@ struct homs_server {
                 inflight_bytes += r->bytes;
                 r->t_start = now();
             }
-            const homs_status s = homs_simulate(ctx, &r->phantom, &r->seq, &r->opts, r->has_state ? &r->state : nullptr,
-                                                r->sig, r->sig_memory);
+            homs_state *st = r->has_state ? &r->state : nullptr;
+            const homs_status s =
+                r->resident ? homs_simulate_resident(ctx, r->resident, &r->seq, &r->opts, st, r->sig, r->sig_memory)
+                            : homs_simulate(ctx, &r->phantom, &r->seq, &r->opts, st, r->sig, r->sig_memory);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 r->status = s;
@@ -118,6 +127,31 @@ struct homs_server {
         }
     }
 };
+
+namespace {
+
+homs_status enqueue(homs_server *srv, std::unique_ptr<Request> r, int64_t *ticket) {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stopping) return HOMS_ECLOSED;
+    r->t_submit = srv->now();
+    const int64_t id = srv->next_ticket++;
+    Request *rp = r.get();
+    srv->requests.emplace(id, std::move(r));
+    if (rp->bytes > srv->budget) {
+        // Larger than the whole admission budget: fail it here rather than block the queue.
+        rp->status = HOMS_ENOMEM;
+        rp->error = "the request's estimated device footprint exceeds the server's admission budget";
+        rp->done = true;
+        rp->t_start = rp->t_finish = rp->t_submit;
+    } else {
+        srv->queue.push_back(rp);
+    }
+    *ticket = id;
+    srv->cv_work.notify_all();
+    return HOMS_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -162,6 +196,7 @@ homs_status homs_server_create(const homs_server_options *opts, homs_server **ou
     return HOMS_OK;
 }
 
+
 homs_status homs_server_submit(homs_server *srv, const homs_phantom *phantom, const homs_sequence *seq,
                                const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory,
                                int64_t *ticket) {
@@ -176,25 +211,28 @@ homs_status homs_server_submit(homs_server *srv, const homs_phantom *phantom, co
     }
     r->sig = sig;
     r->sig_memory = sig_memory;
-    r->bytes = estimate_bytes(*phantom, *seq, *opts);
-    std::lock_guard<std::mutex> lk(srv->mu);
-    if (srv->stopping) return HOMS_ECLOSED;
-    r->t_submit = srv->now();
-    const int64_t id = srv->next_ticket++;
-    Request *rp = r.get();
-    srv->requests.emplace(id, std::move(r));
-    if (rp->bytes > srv->budget) {
-        // Larger than the whole admission budget: fail it here rather than block the queue.
-        rp->status = HOMS_ENOMEM;
-        rp->error = "the request's estimated device footprint exceeds the server's admission budget";
-        rp->done = true;
-        rp->t_start = rp->t_finish = rp->t_submit;
-    } else {
-        srv->queue.push_back(rp);
+    r->bytes = estimate_bytes(phantom->nspins, phantom->ncoils, phantom->dtype, *seq, *opts, false);
+    return enqueue(srv, std::move(r), ticket);
+}
+
+homs_status homs_server_submit_resident(homs_server *srv, const homs_resident *res, const homs_sequence *seq,
+                                        const homs_run_options *opts, homs_state *state, void *sig,
+                                        homs_memory sig_memory, int64_t *ticket) {
+    homs::ResidentShape shape;
+    if (!srv || !seq || !opts || !ticket || !homs::resident_shape(res, &shape)) return HOMS_EINVAL;
+    if (shape.device != srv->device) return HOMS_EINVAL;
+    auto r = std::make_unique<Request>();
+    r->resident = res;
+    r->seq = *seq;
+    r->opts = *opts;
+    if (state) {
+        r->state = *state;
+        r->has_state = true;
     }
-    *ticket = id;
-    srv->cv_work.notify_all();
-    return HOMS_OK;
+    r->sig = sig;
+    r->sig_memory = sig_memory;
+    r->bytes = estimate_bytes(shape.nspins, shape.ncoils, shape.compute, *seq, *opts, true);
+    return enqueue(srv, std::move(r), ticket);
 }
 
 homs_status homs_server_poll(homs_server *srv, int64_t ticket) {

@@ -964,8 +964,19 @@ inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64
 using namespace split;
 
 SplitResident::~SplitResident() {
-    for (void *p : {basis, b_operand, spin_table, prefix, tvec, partial, coil_exp, amp, err})
+    for (void *p : {spin_table, prefix, tvec, partial, amp, err})
         if (p) cudaFree(p);
+    if (!phantom_view)
+        for (void *p : {basis, b_operand, coil_exp})
+            if (p) cudaFree(p);
+}
+
+// Forget shared phantom operands (owned elsewhere) so that they are rebuilt.
+static void split_detach(SplitResident &r) {
+    if (!r.phantom_view) return;
+    r.basis = r.b_operand = r.coil_exp = nullptr;
+    r.basis_bytes = r.b_bytes = r.coil_exp_bytes = 0;
+    r.phantom_view = false;
 }
 
 static cudaError_t grow(void *&p, size_t &have, size_t need) {
@@ -987,6 +998,7 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
             "split path's error budget";
         return cudaSuccess;
     }
+    split_detach(r);
     const int ngroups = (nc + GROUP_COILS - 1) / GROUP_COILS;
     const int ncg_max = std::min<int32_t>(nc, GROUP_COILS);
     const int n_cols = std::max(16, ((2 * ncg_max + 15) / 16) * 16);
@@ -1166,6 +1178,32 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         (const double *)r.spin_table, (const double *)r.prefix + (size_t)nsamples * PREFIX_STRIDE, (const double *)a.T1,
         (const double *)a.T2, (const double *)a.rho, r.ns, (cplx<double> *)a.xy, (double *)a.mz);
     return cudaGetLastError();
+}
+
+cudaError_t split_attach(SplitResident &r, const SplitResident &src) {
+    if (&r == &src) return cudaSuccess;
+    if (!r.phantom_view) {
+        for (void **p : {&r.basis, &r.b_operand, &r.coil_exp}) {
+            if (*p) cudaFree(*p);
+            *p = nullptr;
+        }
+    }
+    r.basis = src.basis;
+    r.b_operand = src.b_operand;
+    r.coil_exp = src.coil_exp;
+    r.basis_bytes = src.basis_bytes;
+    r.b_bytes = src.b_bytes;
+    r.coil_exp_bytes = src.coil_exp_bytes;
+    r.ns = src.ns;
+    r.ns_pad = src.ns_pad;
+    r.nc = src.nc;
+    r.n_mma = src.n_mma;
+    r.ngroups = src.ngroups;
+    r.phantom_view = true;
+    cudaError_t e;
+    if (!r.amp && (e = cudaMalloc(&r.amp, sizeof(unsigned long long))) != cudaSuccess) return e;
+    if (!r.err && (e = cudaMalloc(&r.err, sizeof(unsigned int))) != cudaSuccess) return e;
+    return cudaSuccess;
 }
 
 cudaError_t split_reset_error(SplitResident &r, cudaStream_t stream) {

@@ -27,12 +27,16 @@ struct SplitResident {
            coil_exp_bytes = 0;
     int64_t ns = 0, ns_pad = 0;
     int32_t nc = 0, n_mma = 0, ngroups = 1;
+    // basis, b_operand and coil_exp belong to another SplitResident (a
+    // device-resident phantom shared by many runs); the rest is this one's.
+    bool phantom_view = false;
     SplitResident() = default;
     SplitResident(const SplitResident &) = delete;
     SplitResident &operator=(const SplitResident &) = delete;
     ~SplitResident();
     size_t device_bytes() const {
-        return basis_bytes + b_bytes + spin_bytes + prefix_bytes + tvec_bytes + partial_bytes + coil_exp_bytes;
+        return (phantom_view ? 0 : basis_bytes + b_bytes + coil_exp_bytes) + spin_bytes + prefix_bytes + tvec_bytes +
+               partial_bytes;
     }
 };
 
@@ -60,6 +64,12 @@ struct SplitRunArgs {
 // for valid requests the split path does not serve.
 cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *x, const void *y, const void *z,
                           const void *dw, const void *csm_rows, bool is_f64, cudaStream_t stream, std::string *err);
+
+// Use the phantom operands of `src` (built by split_prepare, never written
+// again) in runs of `r`; `src` keeps owning them and must outlive those runs.
+// r's per-run buffers stay its own, so runs of different SplitResidents that
+// share one `src` may overlap on the device.
+cudaError_t split_attach(SplitResident &r, const SplitResident &src);
 
 // Clear the device error word before a run.
 cudaError_t split_reset_error(SplitResident &r, cudaStream_t stream);

@@ -31,7 +31,7 @@ __all__ = [
     "simulate", "prepare_simulation", "Plan", "Server", "Context", "HomsError", "ArgumentError", "DimensionMismatch",
     "BlochHighOrder", "HO_Phantom", "HO_DiscreteSequence", "Mag", "get_sim_ranges", "count_block_adc",
     "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks", "get_kspace",
-    "rf_events",
+    "rf_events", "ResidentPhantom",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -153,6 +153,70 @@ def _context(device: int) -> Context:
     return ctx
 
 
+class ResidentPhantom:
+    """A phantom kept on the device for many simulations (``homs_resident_*``).
+
+    Its arrays are copied once, in the arithmetic's precision, and for
+    ``homs_precision="split"`` its basis table and pre-split sensitivity
+    operand are built once.  Pass it to ``simulate`` or ``Server.submit`` in
+    place of the ``HO_Phantom``: only the sequence, the state and the signal
+    move per simulation.  ``precision`` is the dtype the phantom arrives in
+    and the results come back in.  Keep it open until every simulation that
+    uses it has finished."""
+
+    def __init__(self, obj: HO_Phantom, precision: str = "f64", homs_precision: str = "plain",
+                 context: Optional[Context] = None):
+        if not isinstance(obj, HO_Phantom):
+            raise ArgumentError("obj must be an HO_Phantom.")
+        if precision not in ("f32", "f64"):
+            raise ArgumentError("The legacy high-order path supports f32 and f64 precision.")
+        if homs_precision not in ("plain", "split"):
+            raise ArgumentError("homs_precision must be plain or split.")
+        obj.validate()
+        self.obj, self.precision, self.homs_precision = obj, precision, homs_precision
+        ctx = context or _context(0)
+        self.device = ctx.device
+        keep = _lib._Keep()
+        ph = _lib.host_phantom(obj, keep, _lib.HOMS_F64 if precision == "f64" else _lib.HOMS_F32)
+        mode = _lib.HOMS_SPLIT if homs_precision == "split" else _lib.HOMS_PLAIN
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().homs_resident_create(ctx.handle, ctypes.byref(ph), mode, ctypes.byref(h)), ctx.handle)
+        self.handle = h
+
+    def __len__(self):
+        return len(self.obj)
+
+    def device_bytes(self) -> int:
+        n = ctypes.c_size_t()
+        _lib.check(_lib.load().homs_resident_device_bytes(self.handle, ctypes.byref(n)))
+        return int(n.value)
+
+    def close(self):
+        if self.handle is not None:
+            _lib.load().homs_resident_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _resident_args(obj, sim_params):
+    """(HO_Phantom, ResidentPhantom or None, sim_params) for a call given an
+    HO_Phantom or a ResidentPhantom; a resident fixes precision and homs_precision."""
+    sim_params = dict(sim_params or {})
+    if not isinstance(obj, ResidentPhantom):
+        return obj, None, sim_params
+    if obj.handle is None:
+        raise ArgumentError("The resident phantom is closed.")
+    for key, val in (("precision", obj.precision), ("homs_precision", obj.homs_precision)):
+        if sim_params.setdefault(key, val) != val:
+            raise ArgumentError(f"{key} must be the resident phantom's ({val}).")
+    return obj.obj, obj, sim_params
+
+
 def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params=None, parts=None, excitation=None,
              state: Optional[Mag] = None, context: Optional[Context] = None, gpus=None, callbacks=(), verbose=False):
     """Simulate ``obj`` under the sampled sequence ``seqd``.
@@ -170,16 +234,19 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params
     if callbacks:
         raise ArgumentError("callbacks run between blocks on the reference's Julia side; use the block entry points "
                             "(homs_precession_block / homs_excitation_block) for per-block access.")
-    params, parts, excitation = _setup(obj, seqd, dict(sim_params or {}), parts, excitation)
+    obj, resident, sim_params = _resident_args(obj, sim_params)
+    params, parts, excitation = _setup(obj, seqd, sim_params, parts, excitation)
     if gpus is not None:
         if not isinstance(gpus, (list, tuple)) or len(gpus) != 1 or not isinstance(gpus[0], (int, np.integer)) \
                 or isinstance(gpus[0], bool) or gpus[0] < 0:
             raise ArgumentError("gpus must name exactly one visible device on this engine.")
         params["gpu_device"] = int(gpus[0])
+    if resident is not None and gpus is None:
+        params["gpu_device"] = resident.device
     ctx = context or _context(int(params["gpu_device"]))
     dt = _dtype(params)
     keep = _lib._Keep()
-    ph = _lib.host_phantom(obj, keep, dt)
+    ph = _lib.host_phantom(obj, keep, dt) if resident is None else None
     sq = _lib.host_sequence(seqd, parts, excitation, keep, dt, params["gamma"])
     nadc = sum(count_block_adc(seqd.adc, parts))
     cdt = np.complex128 if dt == _lib.HOMS_F64 else np.complex64
@@ -195,8 +262,13 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params
     opts = _run_options(params)
     t0 = time.perf_counter()
     lib = _lib.load()
-    _lib.check(lib.homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
-                                 ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST), ctx.handle)
+    if resident is None:
+        _lib.check(lib.homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
+                                     ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST), ctx.handle)
+    else:
+        _lib.check(lib.homs_simulate_resident(ctx.handle, resident.handle, ctypes.byref(sq), ctypes.byref(opts),
+                                              ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST),
+                   ctx.handle)
     seconds = time.perf_counter() - t0
     return _finalize(params, np.asarray(sig), xy, z, parts, excitation, seqd, seconds)
 
@@ -385,13 +457,15 @@ class Server:
 
     def submit(self, obj: HO_Phantom, seqd: HO_DiscreteSequence, *, sim_params=None, parts=None, excitation=None,
                state: Optional[Mag] = None) -> int:
-        """Queue one simulation; the arguments are those of ``simulate``."""
+        """Queue one simulation; the arguments are those of ``simulate`` (``obj``
+        an ``HO_Phantom`` or a ``ResidentPhantom`` of the server's device)."""
         if self.handle is None:
             raise HomsError(6, "server is closed")
-        params, parts, excitation = _setup(obj, seqd, dict(sim_params or {}), parts, excitation)
+        obj, resident, sim_params = _resident_args(obj, sim_params)
+        params, parts, excitation = _setup(obj, seqd, sim_params, parts, excitation)
         dt = _dtype(params)
         keep = _lib._Keep()
-        ph = _lib.host_phantom(obj, keep, dt)
+        ph = _lib.host_phantom(obj, keep, dt) if resident is None else None
         sq = _lib.host_sequence(seqd, parts, excitation, keep, dt, params["gamma"])
         nadc = sum(count_block_adc(seqd.adc, parts))
         cdt = np.complex128 if dt == _lib.HOMS_F64 else np.complex64
@@ -406,10 +480,18 @@ class Server:
         st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
         opts = _run_options(params)
         ticket = ctypes.c_int64()
-        _lib.check(self._lib.homs_server_submit(self.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
-                                                ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST,
-                                                ctypes.byref(ticket)))
-        self._requests[ticket.value] = _Request(keep, sig, xy, z, params, parts, excitation, seqd, (ph, sq, st, opts))
+        if resident is None:
+            _lib.check(self._lib.homs_server_submit(self.handle, ctypes.byref(ph), ctypes.byref(sq),
+                                                    ctypes.byref(opts), ctypes.byref(st),
+                                                    sig.ctypes.data if nadc else None, _lib.HOMS_HOST,
+                                                    ctypes.byref(ticket)))
+        else:
+            _lib.check(self._lib.homs_server_submit_resident(self.handle, resident.handle, ctypes.byref(sq),
+                                                             ctypes.byref(opts), ctypes.byref(st),
+                                                             sig.ctypes.data if nadc else None, _lib.HOMS_HOST,
+                                                             ctypes.byref(ticket)))
+        self._requests[ticket.value] = _Request(keep, sig, xy, z, params, parts, excitation, seqd,
+                                                (ph, sq, st, opts, resident))
         return ticket.value
 
     def done(self, ticket: int) -> bool:

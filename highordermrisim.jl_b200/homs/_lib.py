@@ -27,7 +27,8 @@ EXPORTED = [
     "homs_count_adc", "homs_plan_create", "homs_plan_run", "homs_plan_device_bytes", "homs_plan_timing",
     "homs_plan_destroy", "homs_coil_reduce_noalloc", "homs_server_create", "homs_server_submit", "homs_server_poll",
     "homs_server_wait", "homs_server_times", "homs_server_error", "homs_server_release", "homs_server_destroy",
-    "homs_kspace", "homs_kspace_timing",
+    "homs_kspace", "homs_kspace_timing", "homs_resident_create", "homs_resident_device_bytes",
+    "homs_resident_destroy", "homs_simulate_resident", "homs_server_submit_resident",
 ]
 
 
@@ -127,6 +128,14 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_server_destroy": (ctypes.c_int, [vp]),
         "homs_kspace": (ctypes.c_int, [vp, ctypes.POINTER(Sequence), i32, vp, vp, i64, vp, vp, vp, ctypes.c_int]),
         "homs_kspace_timing": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
+        "homs_resident_create": (ctypes.c_int, [vp, ctypes.POINTER(Phantom), ctypes.c_int, ctypes.POINTER(vp)]),
+        "homs_resident_device_bytes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
+        "homs_resident_destroy": (ctypes.c_int, [vp]),
+        "homs_simulate_resident": (ctypes.c_int, [vp, vp, ctypes.POINTER(Sequence), ctypes.POINTER(RunOptions),
+                                                  ctypes.POINTER(State), vp, ctypes.c_int]),
+        "homs_server_submit_resident": (ctypes.c_int, [vp, vp, ctypes.POINTER(Sequence), ctypes.POINTER(RunOptions),
+                                                       ctypes.POINTER(State), vp, ctypes.c_int,
+                                                       ctypes.POINTER(i64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -117,6 +117,7 @@ typedef struct homs_state {
 typedef struct homs_context homs_context;
 typedef struct homs_plan homs_plan;
 typedef struct homs_server homs_server;
+typedef struct homs_resident homs_resident;
 
 /* ---- library --------------------------------------------------------------- */
 
@@ -218,6 +219,29 @@ homs_status homs_kspace_timing(homs_context *ctx, double *ms);
 homs_status homs_simulate(homs_context *ctx, const homs_phantom *phantom, const homs_sequence *seq,
                           const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory);
 
+/* ---- device-resident phantoms ---------------------------------------------------
+ * A phantom copied to the device once and reused by many simulations: its
+ * arrays in the arithmetic's precision (FP64 for HOMS_SPLIT, the phantom's
+ * dtype for HOMS_PLAIN) and, for HOMS_SPLIT, its spherical-harmonic basis table
+ * and pre-split sensitivity operand.  The serving counterpart of the
+ * reference's resident per-device simulation state
+ * (src/simulation/PreparedSimulation.jl:144-212), kept per phantom so that
+ * simulations of different sequences share it.  Immutable after creation:
+ * simulations on any contexts of the same device may use it at once.  Keep it
+ * alive until every simulation using it has returned (or, for the server, its
+ * ticket has completed). */
+homs_status homs_resident_create(homs_context *ctx, const homs_phantom *phantom, homs_mode mode,
+                                 homs_resident **out);
+homs_status homs_resident_device_bytes(const homs_resident *res, size_t *bytes);
+homs_status homs_resident_destroy(homs_resident *res);
+/* homs_simulate on a device-resident phantom: only the sequence, the state
+ * and the signal move.  opts->mode must be the resident's mode (opts NULL: all
+ * terms of the resident's mode).  state and sig are in the phantom's dtype as
+ * given to homs_resident_create. */
+homs_status homs_simulate_resident(homs_context *ctx, const homs_resident *res, const homs_sequence *seq,
+                                   const homs_run_options *opts, homs_state *state, void *sig,
+                                   homs_memory sig_memory);
+
 /* Number of ADC samples the blocks of `seq` own (sum of ADC[first+1..last]). */
 homs_status homs_count_adc(const homs_sequence *seq, int64_t *nadc);
 
@@ -274,6 +298,12 @@ homs_status homs_server_create(const homs_server_options *opts, homs_server **ou
 homs_status homs_server_submit(homs_server *srv, const homs_phantom *phantom, const homs_sequence *seq,
                                const homs_run_options *opts, homs_state *state, void *sig, homs_memory sig_memory,
                                int64_t *ticket);
+/* Queue a simulation on a device-resident phantom of the server's device
+ * (the arguments of homs_simulate_resident).  Its admission estimate leaves
+ * out the phantom, which is already on the device. */
+homs_status homs_server_submit_resident(homs_server *srv, const homs_resident *res, const homs_sequence *seq,
+                                        const homs_run_options *opts, homs_state *state, void *sig,
+                                        homs_memory sig_memory, int64_t *ticket);
 /* HOMS_OK when the request has finished, HOMS_EBUSY while it is queued or
  * running, otherwise the status it failed with (message: homs_server_error). */
 homs_status homs_server_poll(homs_server *srv, int64_t ticket);
