@@ -299,6 +299,11 @@ struct Resident : ResidentBase {
     double gamma = 0;
     SplitResident split;  // split-precision operands (built on demand)
     bool split_ready = false;
+    // Split-path tables of the sequence: the global ADC sample index of every
+    // node, and the 17 prefix-table column sources of `src_method`.
+    DevBuf grank, src_table;
+    bool grank_ready = false;
+    uint32_t src_method = ~0u;
     // Instrumentation of the last run: events around every launch of the
     // dominant fused kernel, and a count of all kernels launched.
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -412,6 +417,8 @@ template <typename T>
 void fill_sequence(homs_context *ctx, Resident<T> *r, const homs_sequence *q) {
     r->nt = q->nnodes;
     r->gamma = q->gamma;
+    r->grank_ready = false;
+    r->src_method = ~0u;
     const int64_t ns = r->ns, nt = q->nnodes;
     upload<T>(ctx, r->t, q->t, q->dtype, q->memory, nt);
     upload<T>(ctx, r->dt, q->dt, q->dtype, q->memory, nt - 1);
@@ -523,7 +530,8 @@ std::vector<std::pair<Launch, T>> plan_plain(const Resident<T> &r, int64_t max_s
 }
 
 template <typename T>
-void run_plain(homs_context *ctx, Resident<T> &r, uint32_t method) {
+void run_plain(homs_context *ctx, Resident<T> &r, uint32_t method, bool capture) {
+    const unsigned ev_flags = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
     const int grid = (int)((r.ns + PLAIN_THREADS - 1) / PLAIN_THREADS);
     const size_t row_bytes = sizeof(cplx<T>) * (size_t)r.nc * (size_t)grid;
     const size_t budget = size_t(768) << 20;
@@ -549,9 +557,9 @@ void run_plain(homs_context *ctx, Resident<T> &r, uint32_t method) {
         a.gamma_d = r.gamma;
         a.partial = reinterpret_cast<cplx<T> *>(r.partial.p);
         auto ev = r.next_events();
-        HOMS_CUDA(cudaEventRecord(ev.first, ctx->stream));
+        HOMS_CUDA(cudaEventRecordWithFlags(ev.first, ctx->stream, ev_flags));
         HOMS_CUDA(launch_segment<T>(L.rf, p, q, st, a, grid, ctx->stream));
-        HOMS_CUDA(cudaEventRecord(ev.second, ctx->stream));
+        HOMS_CUDA(cudaEventRecordWithFlags(ev.second, ctx->stream, ev_flags));
         r.launches += 1;
         if (L.nsamples > 0) {
             HOMS_CUDA(launch_partial_finalize<T>(a.partial, grid, L.nsamples, r.nc,
@@ -588,18 +596,71 @@ void ensure_split(homs_context *ctx, Resident<T> &r) {
     r.split_ready = true;
 }
 
+// Read the split kernel's device error word (synchronises the stream).
 template <typename T>
-void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opts) {
+void check_split(homs_context *ctx, Resident<T> &r) {
+    std::string err;
+    HOMS_CUDA(split_check(r.split, ctx->stream, &err));
+    if (!err.empty())
+        throw Failure{err.find("timed out") != std::string::npos ? HOMS_ETIMEDOUT : HOMS_EUNSUPPORTED, err};
+}
+
+// The split path's sequence tables: the global ADC sample index of every
+// owned node (blocks share boundary nodes; a node belongs to the block that
+// ends on it) and the prefix-table column sources of `method`.  Uploaded
+// from the host only when the sequence or the method changed.
+template <typename T>
+void ensure_split_tables(homs_context *ctx, Resident<T> &r, uint32_t method) {
+    if (!r.grank_ready) {
+        std::vector<int32_t> g((size_t)r.nt, 0);
+        int64_t c = 0;
+        for (size_t k = 0; k < r.first.size(); ++k)
+            for (int64_t n = r.first[k] + 1; n <= r.last[k]; ++n) {
+                g[(size_t)n] = (int32_t)c;
+                if (r.adc_host[(size_t)n]) ++c;
+            }
+        HOMS_REQUIRE(c <= INT32_MAX, "too many ADC samples for the split path");
+        HOMS_CUDA(r.grank.ensure(sizeof(int32_t) * (size_t)r.nt));
+        HOMS_CUDA(cudaMemcpyAsync(r.grank.p, g.data(), sizeof(int32_t) * (size_t)r.nt, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+        r.grank_ready = true;
+    }
+    if (r.src_method != method) {
+        const void *h[16];
+        for (int k = 0; k < 16; ++k) h[k] = r.h[k].p;
+        const void *src[17];
+        split_column_sources(method, h, r.gx.p, r.gy.p, r.gz.p, src);
+        HOMS_CUDA(r.src_table.ensure(sizeof(src)));
+        HOMS_CUDA(cudaMemcpyAsync(r.src_table.p, src, sizeof(src), cudaMemcpyHostToDevice, ctx->stream));
+        r.src_method = method;
+    }
+}
+
+// Issue one run of the block plan on ctx's stream.  With `capture` the
+// stream is being captured into a CUDA graph: every host-side table and
+// buffer must already be in place (an earlier run of the same plan built
+// them), and only kernels, memsets, device copies and graph-external event
+// records are issued.  `check` reads the split kernel's error word
+// afterwards (a synchronisation; not possible under capture).
+template <typename T>
+void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opts, bool capture = false,
+                  bool check = true) {
     r.events_used = 0;
     r.launches = 0;
     const uint32_t method = opts ? opts->method : 0x3Fu;
     const homs_mode mode = opts ? opts->mode : HOMS_PLAIN;
     HOMS_REQUIRE((method & ~0x3Fu) == 0, "unknown method flag bits");
     if (mode == HOMS_PLAIN) {
-        run_plain<T>(ctx, r, method);
+        run_plain<T>(ctx, r, method, capture);
     } else if (mode == HOMS_SPLIT) {
         if (sizeof(T) != 8) throw Failure{HOMS_EUNSUPPORTED, "internal: split mode runs on FP64 resident arrays"};
-        ensure_split<T>(ctx, r);
+        if (capture) {
+            HOMS_REQUIRE(r.split_ready && r.grank_ready && r.src_method == method,
+                         "internal: split tables missing under capture");
+        } else {
+            ensure_split<T>(ctx, r);
+            ensure_split_tables<T>(ctx, r, method);
+        }
         HOMS_CUDA(split_reset_error(r.split, ctx->stream));
         SplitRunArgs sa;
         sa.sizeof_T = sizeof(T);
@@ -614,6 +675,9 @@ void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opt
         sa.exc = r.exc.data();
         sa.nblocks = (int32_t)r.first.size();
         sa.adc_host = r.adc_host.data();
+        sa.grank = reinterpret_cast<const int32_t *>(r.grank.p);
+        sa.src_dev = reinterpret_cast<const void *const *>(r.src_table.p);
+        sa.capture = capture;
         sa.t = r.t.p;
         sa.dt = r.dt.p;
         sa.gx = r.gx.p;
@@ -695,10 +759,7 @@ void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opt
             if (!err.empty()) throw Failure{HOMS_EUNSUPPORTED, err};
             i = j;
         }
-        std::string err;
-        HOMS_CUDA(split_check(r.split, ctx->stream, &err));
-        if (!err.empty())
-            throw Failure{err.find("timed out") != std::string::npos ? HOMS_ETIMEDOUT : HOMS_EUNSUPPORTED, err};
+        if (check) check_split<T>(ctx, r);
     } else {
         throw Failure{HOMS_EINVAL, "unknown run mode"};
     }
@@ -755,11 +816,22 @@ inline bool compute_f64(const homs_phantom *p, const homs_run_options *opts) {
 // Plans
 // ---------------------------------------------------------------------------
 
+// A plan's runs are identical launch sequences on the same device buffers:
+// the first run is issued directly (it builds every table and sizes every
+// buffer), the second is captured into a CUDA graph, and later runs replay
+// that graph.  If capture fails, the plan keeps issuing its runs directly.
 struct homs_plan {
     homs_context *ctx = nullptr;
     homs_run_options opts{};
     std::unique_ptr<ResidentBase> res;
     homs_dtype out_dtype = HOMS_F64;  // the caller's dtype (the resident copy may be wider)
+    cudaGraphExec_t exec = nullptr;
+    int64_t runs = 0;
+    bool graph_failed = false;
+    std::string graph_error;
+    ~homs_plan() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
 };
 
 // A phantom kept on one device for many simulations: its arrays in the
@@ -805,6 +877,64 @@ void simulate_on_resident(homs_context *ctx, const homs_resident *res, const hom
     init_state<T>(ctx, *r, state, res->in_dtype);
     run_resident<T>(ctx, *r, opts);
     copy_out<T>(ctx, *r, sig, sig_memory, state, res->in_dtype);
+}
+
+}  // namespace
+
+namespace {
+
+// One run of a prepared plan: directly, by capturing it into the plan's CUDA
+// graph, or by replaying that graph (see homs_plan).
+template <typename T>
+void plan_run_typed(homs_plan *plan, void *sig, homs_memory sig_memory, homs_state *state_out) {
+    homs_context *ctx = plan->ctx;
+    auto &r = static_cast<Resident<T> &>(*plan->res);
+    const homs_dtype rdt = sizeof(T) == 8 ? HOMS_F64 : HOMS_F32;
+    bool issued = false;
+    if (!plan->exec && plan->runs >= 1 && !plan->graph_failed) {
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            std::string why;
+            try {
+                init_state<T>(ctx, r, nullptr, rdt);
+                run_resident<T>(ctx, r, &plan->opts, /*capture=*/true, /*check=*/false);
+            } catch (const Failure &f) {
+                why = f.msg;
+            }
+            cudaGraph_t graph = nullptr;
+            e = cudaStreamEndCapture(ctx->stream, &graph);
+            if (why.empty() && e == cudaSuccess && graph) {
+                e = cudaGraphInstantiate(&plan->exec, graph, 0);
+                if (e != cudaSuccess) {
+                    plan->exec = nullptr;
+                    why = std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e);
+                }
+            } else if (why.empty()) {
+                why = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+            }
+            if (graph) cudaGraphDestroy(graph);
+            if (!why.empty()) {
+                cudaGetLastError();
+                plan->graph_failed = true;
+                plan->graph_error = why;
+            }
+        } else {
+            cudaGetLastError();
+            plan->graph_failed = true;
+            plan->graph_error = std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e);
+        }
+    }
+    if (plan->exec) {
+        HOMS_CUDA(cudaGraphLaunch(plan->exec, ctx->stream));
+        issued = true;
+    }
+    if (!issued) {
+        init_state<T>(ctx, r, nullptr, rdt);
+        run_resident<T>(ctx, r, &plan->opts, /*capture=*/false, /*check=*/false);
+    }
+    if (plan->opts.mode == HOMS_SPLIT) check_split<T>(ctx, r);
+    copy_out<T>(ctx, r, sig, sig_memory, state_out, plan->out_dtype);
+    ++plan->runs;
 }
 
 }  // namespace
@@ -972,17 +1102,8 @@ homs_status homs_plan_run(homs_plan *plan, void *sig, homs_memory sig_memory, ho
     DeviceGuard g(ctx->device);
     try {
         HOMS_REQUIRE(sig_memory == HOMS_HOST || sig_memory == HOMS_DEVICE, "invalid signal memory kind");
-        if (plan->res->dtype == HOMS_F64) {
-            auto &r = static_cast<Resident<double> &>(*plan->res);
-            init_state<double>(ctx, r, nullptr, HOMS_F64);
-            run_resident<double>(ctx, r, &plan->opts);
-            copy_out<double>(ctx, r, sig, sig_memory, state_out, plan->out_dtype);
-        } else {
-            auto &r = static_cast<Resident<float> &>(*plan->res);
-            init_state<float>(ctx, r, nullptr, HOMS_F32);
-            run_resident<float>(ctx, r, &plan->opts);
-            copy_out<float>(ctx, r, sig, sig_memory, state_out, plan->out_dtype);
-        }
+        if (plan->res->dtype == HOMS_F64) plan_run_typed<double>(plan, sig, sig_memory, state_out);
+        else plan_run_typed<float>(plan, sig, sig_memory, state_out);
         return HOMS_OK;
     } catch (const Failure &f) {
         cudaStreamSynchronize(ctx->stream);
@@ -1004,12 +1125,22 @@ homs_status homs_plan_timing(const homs_plan *plan, homs_timing *out) {
     return HOMS_OK;
 }
 
+homs_status homs_plan_graph(const homs_plan *plan, int32_t *state, const char **why) {
+    if (!plan || !state) return HOMS_EINVAL;
+    if (!plan->res) return HOMS_ECLOSED;
+    *state = plan->exec ? 1 : (plan->graph_failed ? -1 : 0);
+    if (why) *why = plan->graph_error.c_str();
+    return HOMS_OK;
+}
+
 homs_status homs_plan_destroy(homs_plan *plan) {
     if (!plan) return HOMS_EINVAL;
     if (plan->ctx) {
         std::lock_guard<std::mutex> lock(plan->ctx->mu);
         DeviceGuard g(plan->ctx->device);
         cudaStreamSynchronize(plan->ctx->stream);
+        if (plan->exec) cudaGraphExecDestroy(plan->exec);
+        plan->exec = nullptr;
         plan->res.reset();
     }
     delete plan;

@@ -860,7 +860,8 @@ __global__ void spin_table_kernel(const double *basis, const double *dw, const d
 // column's largest |value| at row nsamples+1.  Block 17: elapsed time t
 // (entry PREFIX_T) and the constant columns 17 (= 1) and 18, 19 (= 0).
 __global__ void prefix_kernel(const double *dt, const double *const *src, const uint8_t *adc, const int32_t *rank,
-                              int64_t n_lo, int64_t n_hi, int64_t nsamples, double gamma, double *prefix) {
+                              int64_t rank_base, int64_t n_lo, int64_t n_hi, int64_t nsamples, double gamma,
+                              double *prefix) {
     __shared__ double part[256];
     const int col = blockIdx.x;
     const double *f = col < 17 ? src[col] : reinterpret_cast<const double *>(1);  // nullptr: zero; 1: constant one
@@ -896,7 +897,7 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
         cum += term;
         peak = fmax(peak, fabs(scale * cum));
         if (adc[n + 1]) {
-            double *pr = prefix + (size_t)rank[n + 1] * PREFIX_STRIDE;
+            double *pr = prefix + (size_t)(rank[n + 1] - rank_base) * PREFIX_STRIDE;
             pr[out_col] = scale * cum;
             if (col == 17) {
                 pr[17] = 1.0;
@@ -1091,37 +1092,18 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
     cudaError_t e;
     const int64_t nchunks = r.ns_pad / KC;
     const int64_t tiles = (nsamples + TM - 1) / TM;
-    // ADC rank per node of the segment (host), uploaded with the column sources.
-    std::vector<int32_t> rank((size_t)a.nt, 0);
-    int64_t c = 0;
-    for (int64_t n = n_lo + 1; n <= n_hi; ++n)
-        if (a.adc_host[n]) rank[(size_t)n] = (int32_t)c++;
-    if (c != nsamples) {
-        *err = "internal: segment sample count mismatch";
+    if (!a.grank || !a.src_dev) {
+        *err = "internal: split segment without its ADC rank and column tables";
         return cudaSuccess;
     }
-    const size_t rank_bytes = (sizeof(int32_t) * (size_t)a.nt + 255) & ~size_t(255);  // keeps the pointer table aligned
-    const size_t src_bytes = sizeof(void *) * 17;
+    const uint32_t m = a.method;
     const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2);
     if ((e = grow(r.prefix, r.prefix_bytes, prefix_rows * PREFIX_STRIDE * sizeof(double))) != cudaSuccess) return e;
-    if ((e = grow(r.tvec, r.tvec_bytes, rank_bytes + src_bytes)) != cudaSuccess) return e;
     if ((e = grow(r.spin_table, r.spin_bytes, (size_t)nchunks * SPIN_BYTES)) != cudaSuccess) return e;
-    const double *src[17];
-    const uint32_t m = a.method;
-    src[0] = (m & HOMS_HO0) ? (const double *)a.h[0] : nullptr;
-    for (int k = 1; k <= 3; ++k)
-        src[k] = (m & HOMS_HO1) ? (const double *)a.h[k] : (const double *)(k == 1 ? a.gx : k == 2 ? a.gy : a.gz);
-    for (int k = 4; k <= 8; ++k) src[k] = (m & HOMS_HO2) ? (const double *)a.h[k] : nullptr;
-    for (int k = 9; k <= 15; ++k) src[k] = (m & HOMS_HO3) ? (const double *)a.h[k] : nullptr;
-    src[16] = (m & HOMS_DW_PRECESSION) ? reinterpret_cast<const double *>(1) : nullptr;
-    uint8_t *tv = (uint8_t *)r.tvec;
-    if ((e = cudaMemcpyAsync(tv, rank.data(), rank_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
-    // Copies from pageable host memory are staged before cudaMemcpyAsync
-    // returns, so the host arrays above may go away without a synchronisation.
-    if ((e = cudaMemcpyAsync(tv + rank_bytes, src, src_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
-    prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(tv + rank_bytes),
-                                          (const uint8_t *)a.adc, reinterpret_cast<const int32_t *>(tv), n_lo, n_hi,
-                                          nsamples, a.gamma, (double *)r.prefix);
+    // The segment's samples are the global ADC indices sample0 .. sample0 + nsamples - 1.
+    prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(a.src_dev),
+                                          (const uint8_t *)a.adc, a.grank, sample0, n_lo, n_hi, nsamples, a.gamma,
+                                          (double *)r.prefix);
     if ((e = cudaMemsetAsync(r.amp, 0, sizeof(unsigned long long), stream)) != cudaSuccess) return e;
     spin_table_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>(
         (const double *)r.basis, (const double *)a.dw, (const double *)a.T2, (const cplx<double> *)a.xy, r.ns, nchunks,
@@ -1154,14 +1136,15 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         ka.tiles = (int)tiles;
         ka.slabs = slabs;
         ka.nstage = kernel_stages(r.n_mma);
-        if (a.ev_start) cudaEventRecord(a.ev_start, stream);
+        const unsigned ev_flags = a.capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+        if (a.ev_start) cudaEventRecordWithFlags(a.ev_start, stream, ev_flags);
         // One pass per group of GROUP_COILS coils.
         for (int grp = 0; grp < r.ngroups; ++grp) {
             const int coil0 = grp * GROUP_COILS;
             const int ncg = std::min<int>(GROUP_COILS, r.nc - coil0);
             ka.b_operand = (const uint8_t *)r.b_operand + (size_t)grp * nchunks * b_bytes(r.n_mma);
             e = launch_precession(r.n_mma, ka, (unsigned)G, smem, stream);
-            if (a.ev_stop && grp + 1 == r.ngroups) cudaEventRecord(a.ev_stop, stream);
+            if (a.ev_stop && grp + 1 == r.ngroups) cudaEventRecordWithFlags(a.ev_stop, stream, ev_flags);
             if (a.launches) *a.launches += 2;
             if (e != cudaSuccess) return e;
             const int64_t total = nsamples * ncg;
@@ -1204,6 +1187,15 @@ cudaError_t split_attach(SplitResident &r, const SplitResident &src) {
     if (!r.amp && (e = cudaMalloc(&r.amp, sizeof(unsigned long long))) != cudaSuccess) return e;
     if (!r.err && (e = cudaMalloc(&r.err, sizeof(unsigned int))) != cudaSuccess) return e;
     return cudaSuccess;
+}
+
+void split_column_sources(uint32_t m, const void *const h[16], const void *gx, const void *gy, const void *gz,
+                          const void *out[17]) {
+    out[0] = (m & HOMS_HO0) ? h[0] : nullptr;
+    for (int k = 1; k <= 3; ++k) out[k] = (m & HOMS_HO1) ? h[k] : (k == 1 ? gx : k == 2 ? gy : gz);
+    for (int k = 4; k <= 8; ++k) out[k] = (m & HOMS_HO2) ? h[k] : nullptr;
+    for (int k = 9; k <= 15; ++k) out[k] = (m & HOMS_HO3) ? h[k] : nullptr;
+    out[16] = (m & HOMS_DW_PRECESSION) ? reinterpret_cast<const void *>(1) : nullptr;
 }
 
 cudaError_t split_reset_error(SplitResident &r, cudaStream_t stream) {

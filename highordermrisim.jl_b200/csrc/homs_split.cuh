@@ -18,7 +18,7 @@ struct SplitResident {
     void *b_operand = nullptr; // [groups][nchunks][4 ksteps][2N rows (hi, lo)][16 f16]
     void *spin_table = nullptr;  // per-segment spin parameters, [nchunks][608] double
     void *prefix = nullptr;    // per-segment phase table, [nadc_seg_pad][24] double
-    void *tvec = nullptr;      // per-segment ADC ranks and field-column pointers
+    void *tvec = nullptr;      // unused (the ADC ranks and column pointers come with SplitRunArgs)
     void *partial = nullptr;   // FP64 split-K partials, [tiles][slabs][128][N]
     void *coil_exp = nullptr;  // per coil: max |Re|,|Im| (u64 bits), then the scale exponent (int)
     void *amp = nullptr;       // per segment: bits of the largest |m0| (u64)
@@ -50,6 +50,12 @@ struct SplitRunArgs {
     const uint8_t *exc;
     int32_t nblocks;
     const uint8_t *adc_host;
+    // device tables built once per sequence and method: the global ADC
+    // sample index of every node (0-based, ownership as in the block plan)
+    // and the 17 field-column pointers of the prefix table
+    const int32_t *grank = nullptr;
+    const void *const *src_dev = nullptr;
+    bool capture = false;  // the stream is being captured into a CUDA graph
     // resident device arrays (type T = double or float per sizeof_T)
     const void *t, *dt, *gx, *gy, *gz, *b1, *df, *psi, *adc, *bnd, *h[16];
     const void *x, *y, *z, *rho, *T1, *T2, *dw, *csm_rows;
@@ -74,9 +80,17 @@ cudaError_t split_attach(SplitResident &r, const SplitResident &src);
 // Clear the device error word before a run.
 cudaError_t split_reset_error(SplitResident &r, cudaStream_t stream);
 
+// The 17 prefix-table column sources for a method mask: h_k when its order
+// is on, the nominal gradient for k = 1..3 when the first order is off,
+// NULL (zero) otherwise, and the constant-one marker for the dw column.
+void split_column_sources(uint32_t method, const void *const h[16], const void *gx, const void *gy, const void *gz,
+                          const void *out[17]);
+
 // One precession segment (a run of consecutive precession blocks, nodes
 // [n_lo, n_hi]) on the split tcgen05 kernel; its samples go to sig rows
-// sample0 .. sample0+nsamples-1.  Updates the FP64 state.
+// sample0 .. sample0+nsamples-1.  Updates the FP64 state.  Issues only
+// kernels, memsets and (with a.capture, graph-external) event records, so it
+// may run under stream capture once its buffers have their sizes.
 cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
                               int64_t nsamples, cudaStream_t stream, std::string *err);
 

@@ -401,6 +401,14 @@ class Plan:
         _lib.check(_lib.load().homs_plan_device_bytes(self.handle, ctypes.byref(n)))
         return int(n.value)
 
+    def graph_state(self) -> Tuple[int, str]:
+        """(1, "") while runs replay the plan's captured CUDA graph, (0, "")
+        before the capture (the second run), (-1, reason) if capture failed
+        and runs are issued kernel by kernel."""
+        st, why = ctypes.c_int32(), ctypes.c_char_p()
+        _lib.check(_lib.load().homs_plan_graph(self.handle, ctypes.byref(st), ctypes.byref(why)))
+        return int(st.value), (why.value or b"").decode()
+
     def close(self):
         if not self.closed:
             _lib.load().homs_plan_destroy(self.handle)

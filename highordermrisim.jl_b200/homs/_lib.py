@@ -28,7 +28,7 @@ EXPORTED = [
     "homs_plan_destroy", "homs_coil_reduce_noalloc", "homs_server_create", "homs_server_submit", "homs_server_poll",
     "homs_server_wait", "homs_server_times", "homs_server_error", "homs_server_release", "homs_server_destroy",
     "homs_kspace", "homs_kspace_timing", "homs_resident_create", "homs_resident_device_bytes",
-    "homs_resident_destroy", "homs_simulate_resident", "homs_server_submit_resident",
+    "homs_resident_destroy", "homs_simulate_resident", "homs_server_submit_resident", "homs_plan_graph",
 ]
 
 
@@ -115,6 +115,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_plan_device_bytes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_size_t)]),
         "homs_plan_timing": (ctypes.c_int, [vp, ctypes.POINTER(Timing)]),
         "homs_plan_destroy": (ctypes.c_int, [vp]),
+        "homs_plan_graph": (ctypes.c_int, [vp, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_char_p)]),
         "homs_coil_reduce_noalloc": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i32, vp, i64, vp, i64, vp, i64]),
         "homs_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOptions), ctypes.POINTER(vp)]),
         "homs_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Phantom), ctypes.POINTER(Sequence),

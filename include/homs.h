@@ -266,6 +266,14 @@ typedef struct homs_timing {
     int64_t kernel_launches;
 } homs_timing;
 homs_status homs_plan_timing(const homs_plan *plan, homs_timing *out);
+/* How a plan's runs are issued.  The first run issues its kernels directly and
+ * sizes every buffer; the second is captured into a CUDA graph, which later
+ * runs replay (one launch of the whole block plan).  *state: 0 before the
+ * capture, 1 while runs replay the graph, -1 if capture failed and runs are
+ * issued directly (*why, if not NULL, then holds the reason; it stays valid
+ * until the plan is destroyed).  Not in the reference, which relaunches its
+ * kernels block by block (src/simulation/PreparedSimulation.jl:214-258). */
+homs_status homs_plan_graph(const homs_plan *plan, int32_t *state, const char **why);
 homs_status homs_plan_destroy(homs_plan *plan);
 
 /* ---- serving: continuous batching of independent simulations --------------
