@@ -707,25 +707,49 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 // undo the power-of-two scaling of the operands and write complex samples:
 // column n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
 template <typename T>
-__global__ void split_finalize_kernel(const double *partial, int64_t nsamples, int32_t ncg, int n_cols, int slabs,
-                                      const int *coil_exp, const unsigned long long *amp_max, cplx<T> *sig,
-                                      int64_t ldsig) {
-    const int64_t total = nsamples * ncg;
+__global__ void __launch_bounds__(256) split_finalize_kernel(const double *partial, int64_t nsamples, int32_t ncg,
+                                                             int n_cols, int slabs, const int *coil_exp,
+                                                             const unsigned long long *amp_max, cplx<T> *sig,
+                                                             int64_t ldsig) {
+    // A block sums FIN_ROWS rows x n_cols columns of one time tile over the
+    // slabs (each slab's rows are contiguous: coalesced reads), in slab order,
+    // then writes every coil's samples of those rows from shared memory.
+    constexpr int FIN_ROWS = 32, PER = FIN_ROWS * 64 / 256;
+    __shared__ double sacc[FIN_ROWS * 64];
     const int ea = pow2_ceil_exp(*amp_max);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t j = i % nsamples;
-        const int32_t c = (int32_t)(i / nsamples);
-        const int64_t tile = j / TM;
-        const int row = (int)(j % TM);
-        double re = 0.0, im = 0.0;
+    const int64_t tiles = (nsamples + TM - 1) / TM;
+    const int64_t units = tiles * (TM / FIN_ROWS);
+    const int elems = FIN_ROWS * n_cols;  // n_cols <= 64
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+        const int64_t tile = u / (TM / FIN_ROWS);
+        const int r0 = (int)(u % (TM / FIN_ROWS)) * FIN_ROWS;
+        double acc[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) acc[k] = 0.0;
         for (int z = 0; z < slabs; ++z) {
-            const double *src = partial + (((size_t)tile * slabs + z) * TM + row) * (size_t)n_cols;
-            re += src[c];
-            im += src[ncg + c];
+            const double *src = partial + (((size_t)tile * slabs + z) * TM + r0) * (size_t)n_cols;
+#pragma unroll
+            for (int k = 0; k < PER; ++k) {
+                const int e = threadIdx.x + k * 256;
+                if (e < elems) acc[k] += src[e];
+            }
         }
-        const int e = coil_exp[c] + ea;
-        sig[j + (int64_t)c * ldsig] = cplx<T>{T(ldexp(re, e)), T(ldexp(im, e))};
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int e = threadIdx.x + k * 256;
+            if (e < elems) sacc[e] = acc[k];
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < FIN_ROWS * ncg; q += blockDim.x) {
+            const int c = q / FIN_ROWS, row = q % FIN_ROWS;
+            const int64_t j = tile * TM + r0 + row;
+            if (j < nsamples) {
+                const int e = coil_exp[c] + ea;
+                sig[j + (int64_t)c * ldsig] =
+                    cplx<T>{T(ldexp(sacc[row * n_cols + c], e)), T(ldexp(sacc[row * n_cols + ncg + c], e))};
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -759,14 +783,33 @@ __global__ void basis_kernel(const double *x, const double *y, const double *z, 
 
 // Largest |Re| or |Im| of each coil's sensitivity (bits of a non-negative
 // double, combined with an unsigned max).
+// Per coil: the largest |Re| or |Im| of its sensitivities, as the bits of a
+// non-negative double (which order like the values).  Each block reduces a
+// range of whole spin rows in shared memory first (blockDim a multiple of nc
+// when nc <= 256, so a thread always sees the same coil), then merges one
+// value per coil into `mx`.
 __global__ void coil_max_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, unsigned long long *mx) {
-    const int64_t total = ns * nc;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const cplx<double> v = csm_rows[i];
-        const double m = fmax(fabs(v.re), fabs(v.im));
-        atomicMax(&mx[i % nc], (unsigned long long)__double_as_longlong(m));
+    extern __shared__ unsigned long long smax[];  // nc entries
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) smax[c] = 0ull;
+    __syncthreads();
+    const int64_t rows_per_block = (ns + gridDim.x - 1) / gridDim.x;
+    const int64_t i0 = min(ns, rows_per_block * blockIdx.x) * nc, i1 = min(ns, rows_per_block * (blockIdx.x + 1)) * nc;
+    if ((int)blockDim.x % nc == 0) {
+        unsigned long long local = 0ull;
+        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            const cplx<double> v = csm_rows[i];
+            local = max(local, (unsigned long long)__double_as_longlong(fmax(fabs(v.re), fabs(v.im))));
+        }
+        atomicMax(&smax[threadIdx.x % nc], local);
+    } else {
+        for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+            const cplx<double> v = csm_rows[i];
+            atomicMax(&smax[i % nc], (unsigned long long)__double_as_longlong(fmax(fabs(v.re), fabs(v.im))));
+        }
     }
+    __syncthreads();
+    for (int c = threadIdx.x; c < nc; c += blockDim.x)
+        if (smax[c]) atomicMax(&mx[c], smax[c]);
 }
 
 __global__ void coil_exp_kernel(const unsigned long long *mx, int32_t nc, int *coil_exp) {
@@ -782,37 +825,47 @@ __global__ void coil_exp_kernel(const unsigned long long *mx, int32_t nc, int *c
 // rows 0..N-1 of each K-step slab hold the hi parts, rows N..2N-1 the lo parts.
 __global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_cols, int64_t nchunks,
                                  int ngroups, const int *coil_exp, __half *out) {
-    const int64_t per_chunk = (int64_t)KSTEPS * 2 * n_cols * 16;
-    const int64_t total = (int64_t)ngroups * nchunks * per_chunk;
+    // One thread per 16-byte core-matrix row: operand row nn (hi rows
+    // 0..n_cols-1, lo rows n_cols..2 n_cols-1) of K-step ks, K-half kb (8
+    // consecutive K = 4 spins x (re, im)).
+    const int64_t total = (int64_t)ngroups * nchunks * KSTEPS * (2 * n_cols) * 2;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t gc = i / per_chunk;  // group * nchunks + chunk
+        int64_t r = i;
+        const int kb = (int)(r & 1);
+        r >>= 1;
+        const int nn = (int)(r % (2 * n_cols));
+        r /= 2 * n_cols;
+        const int ks = (int)(r % KSTEPS);
+        const int64_t gc = r / KSTEPS;  // group * nchunks + chunk
         const int grp = (int)(gc / nchunks);
         const int64_t chunk = gc % nchunks;
-        int64_t r = i % per_chunk;
-        const int ks = (int)(r / (2 * n_cols * 16));
-        r %= (2 * n_cols * 16);
-        const int nn = (int)(r / 16), kk = (int)(r % 16);
         const bool lopart = nn >= n_cols;
         const int n = lopart ? nn - n_cols : nn;
-        const int k = 16 * ks + kk;
-        const int64_t s = chunk * KC + (k >> 1);
-        const int comp = k & 1;
         const int coil0 = grp * GROUP_COILS;
         const int ncg = min(GROUP_COILS, nc - coil0);
-        double v = 0.0;
-        if (s < ns && n < 2 * ncg) {
-            const int coil = coil0 + (n < ncg ? n : n - ncg);
-            const cplx<double> cv = csm_rows[s * nc + coil];
-            if (n < ncg) v = comp ? -cv.im : cv.re;
-            else v = comp ? cv.re : cv.im;
-            v = ldexp(v, -coil_exp[coil]);
+        const bool live = n < 2 * ncg;
+        const int coil = coil0 + (n < ncg ? n : n - ncg);
+        const int e = live ? coil_exp[coil] : 0;
+        __align__(16) __half row[8];
+#pragma unroll
+        for (int j = 0; j < 8; j += 2) {
+            const int k = 16 * ks + 8 * kb + j;  // even: this spin's (re, im) pair is K = k, k + 1
+            const int64_t sp = chunk * KC + (k >> 1);
+            double v0 = 0.0, v1 = 0.0;
+            if (live && sp < ns) {
+                const cplx<double> cv = csm_rows[sp * nc + coil];
+                // Column n < ncg holds Re S: (re, -im); column ncg + n holds Im S: (im, re).
+                v0 = ldexp(n < ncg ? cv.re : cv.im, -e);
+                v1 = ldexp(n < ncg ? -cv.im : cv.re, -e);
+            }
+            const __half h0 = __double2half(v0), h1 = __double2half(v1);
+            row[j] = lopart ? __double2half(v0 - (double)__half2float(h0)) : h0;
+            row[j + 1] = lopart ? __double2half(v1 - (double)__half2float(h1)) : h1;
         }
-        const __half hb = __double2half(v);
-        const __half lb = __double2half(v - (double)__half2float(hb));
-        const size_t off = (size_t)(nn / 8) * 256 + (size_t)(kk / 8) * 128 + (size_t)(nn % 8) * 16 + (size_t)(kk % 8) * 2;
         uint8_t *base = reinterpret_cast<uint8_t *>(out) + (size_t)gc * b_bytes(n_cols) + (size_t)ks * 2 * n_cols * 32;
-        *reinterpret_cast<__half *>(base + off) = lopart ? lb : hb;
+        const size_t off = (size_t)(nn / 8) * 256 + (size_t)kb * 128 + (size_t)(nn % 8) * 16;
+        *reinterpret_cast<uint4 *>(base + off) = *reinterpret_cast<const uint4 *>(row);
     }
 }
 
@@ -834,6 +887,7 @@ __global__ void spin_table_kernel(const double *basis, const double *dw, const d
         for (int k = 0; k < 17; ++k) row[k] = 0.0;
         double theta0 = 0.0;
         float2 rl = make_float2(0.0f, -INFINITY);
+        unsigned long long amp = 0ull;
         if (s < ns) {
             for (int k = 0; k < 16; ++k) row[k] = basis[s * 16 + k];
             row[16] = (method & HOMS_DW_PRECESSION) ? dw[s] / (2.0 * 3.141592653589793) : 0.0;
@@ -845,8 +899,16 @@ __global__ void spin_table_kernel(const double *basis, const double *dw, const d
             if (!(bound < 262144.0)) atomicOr(err, 64u);
             rl.x = (float)(-1.4426950408889634 / T2[s]);
             rl.y = mag > 0.0 ? (float)log2(mag) : -INFINITY;
-            if (mag > 0.0) atomicMax(amp_max, (unsigned long long)__double_as_longlong(mag));
+            amp = (unsigned long long)__double_as_longlong(mag);
         }
+        // One atomic per warp for the amplitude maximum (bits of non-negative doubles order like the values).
+        const unsigned active = __activemask();
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(active, amp, o);
+            if ((active >> ((threadIdx.x & 31) ^ o)) & 1u) amp = max(amp, other);
+        }
+        if ((threadIdx.x & 31) == __ffs(active) - 1 && amp) atomicMax(amp_max, amp);
         for (int k = 0; k < NTERM; ++k) t[tab_index(k, sl)] = row[k];
         t[TAB_THETA0 + sl] = theta0;
         t[TAB_DW + sl] = row[16];
@@ -1028,9 +1090,18 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
     basis_kernel<<<grid_for(ns), 256, 0, stream>>>((const double *)x, (const double *)y, (const double *)z, ns,
                                                    (double *)r.basis);
     if ((e = cudaMemsetAsync(cmax, 0, sizeof(unsigned long long) * (size_t)nc, stream)) != cudaSuccess) return e;
-    coil_max_kernel<<<grid_for(ns * nc), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, cmax);
+    {
+        const int threads = nc <= 256 ? nc * (256 / nc) : 256;
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ns, 148 * 8));
+        const size_t smem = sizeof(unsigned long long) * (size_t)nc;
+        if (smem > 48 * 1024) {
+            *err = "split mode: more coils than the sensitivity-scale reduction supports (6144)";
+            return cudaSuccess;
+        }
+        coil_max_kernel<<<blocks, threads, smem, stream>>>((const cplx<double> *)csm_rows, ns, nc, cmax);
+    }
     coil_exp_kernel<<<1, 128, 0, stream>>>(cmax, nc, cexp);
-    const int64_t total = (int64_t)ngroups * nchunks * KSTEPS * 2 * n_cols * 16;
+    const int64_t total = (int64_t)ngroups * nchunks * KSTEPS * 2 * n_cols * 2;
     b_operand_kernel<<<grid_for(total), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_cols, nchunks,
                                                           ngroups, cexp, (__half *)r.b_operand);
     return cudaGetLastError();
@@ -1147,9 +1218,9 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
             if (a.ev_stop && grp + 1 == r.ngroups) cudaEventRecordWithFlags(a.ev_stop, stream, ev_flags);
             if (a.launches) *a.launches += 2;
             if (e != cudaSuccess) return e;
-            const int64_t total = nsamples * ncg;
+            const int fin_blocks = (int)std::min<int64_t>(tiles * (TM / 32), 148 * 8);
             if (a.sizeof_T == 8)
-                split_finalize_kernel<double><<<grid_for(total), 256, 0, stream>>>(
+                split_finalize_kernel<double><<<fin_blocks, 256, 0, stream>>>(
                     (const double *)r.partial, nsamples, ncg, r.n_mma, slabs, cexp + coil0,
                     (const unsigned long long *)r.amp, (cplx<double> *)a.sig + sample0 + (int64_t)coil0 * a.nadc,
                     a.nadc);
