@@ -17,6 +17,7 @@
 #include "homs_common.cuh"
 #include "homs_internal.cuh"
 #include "homs_kspace.cuh"
+#include "homs_phantom.cuh"
 #include "homs_split.cuh"
 
 using namespace homs;
@@ -136,6 +137,8 @@ struct homs_context {
     // encoding export (homs_kspace): staged inputs, metadata, work and outputs,
     // and the events around its kernels
     DevBuf kspace_in, kspace_meta, kspace_work, kspace_out;
+    // phantom builders: staged inputs, work area, staged outputs
+    DevBuf build_in, build_work, build_out;
     cudaEvent_t kspace_ev[2] = {nullptr, nullptr};
     bool kspace_timed = false;
     // Device workspace of homs_simulate, kept between calls (per dtype) so that
@@ -1005,6 +1008,9 @@ homs_status homs_context_destroy(homs_context *ctx) {
         ctx->kspace_meta.release();
         ctx->kspace_work.release();
         ctx->kspace_out.release();
+        ctx->build_in.release();
+        ctx->build_work.release();
+        ctx->build_out.release();
         for (cudaEvent_t &e : ctx->kspace_ev)
             if (e) cudaEventDestroy(e);
         ctx->cache[0].reset();
@@ -1372,6 +1378,171 @@ homs_status homs_simulate_resident(homs_context *ctx, const homs_resident *res, 
         ctx->cache[0].reset();
         ctx->cache[1].reset();
         return fail(ctx, Failure{HOMS_ENOMEM, "host allocation failed"});
+    }
+}
+
+}  // extern "C"
+
+namespace {
+
+// Device view of a brain spec: host inputs are staged into ctx->build_in.
+BrainArgs brain_args(homs_context *ctx, const homs_brain_spec *spec) {
+    HOMS_REQUIRE(spec != nullptr, "spec is NULL");
+    HOMS_REQUIRE(spec->nx >= 1 && spec->ny >= 1 && spec->nz >= 1, "Target matrix dimensions must be positive.");
+    for (int k = 0; k < 3; ++k) {
+        HOMS_REQUIRE(std::isfinite(spec->res[k]) && spec->res[k] > 0, "Target voxel sizes must be finite and positive.");
+        HOMS_REQUIRE(std::isfinite(spec->offcenter[k]), "The off-centre shift must be finite.");
+    }
+    HOMS_REQUIRE(spec->fieldstrength == 0 || spec->fieldstrength == 1, "Field strength available: 1.5T, 7T");
+    HOMS_REQUIRE(spec->ncoils >= 0 && (spec->ncoils == 0 || spec->csm), "csm is NULL for ncoils > 0");
+    HOMS_REQUIRE(spec->labels != nullptr, "labels is NULL");
+    HOMS_REQUIRE(spec->memory == HOMS_HOST || spec->memory == HOMS_DEVICE, "invalid memory kind");
+    const int64_t nvox = spec->nx * spec->ny * spec->nz;
+    HOMS_REQUIRE(nvox / spec->nx / spec->ny == spec->nz, "target matrix too large");
+    BrainArgs a;
+    a.nx = spec->nx;
+    a.ny = spec->ny;
+    a.nz = spec->nz;
+    for (int k = 0; k < 3; ++k) {
+        a.res[k] = spec->res[k];
+        a.offcenter[k] = spec->offcenter[k];
+    }
+    a.fieldstrength = spec->fieldstrength;
+    a.ncoils = spec->ncoils;
+    a.labels = spec->labels;
+    a.fieldmap = spec->fieldmap;
+    a.csm = spec->ncoils > 0 ? spec->csm : nullptr;
+    if (spec->memory == HOMS_HOST) {
+        // Every staged array starts on a 256-byte boundary (the kernel reads
+        // the sensitivities as 16-byte pairs).
+        const size_t lab = ((size_t)nvox + 255) & ~size_t(255);
+        const size_t fm = spec->fieldmap ? ((sizeof(double) * (size_t)nvox + 255) & ~size_t(255)) : 0;
+        const size_t cs = a.csm ? 2 * sizeof(double) * (size_t)nvox * (size_t)spec->ncoils : 0;
+        HOMS_CUDA(ctx->build_in.ensure(lab + fm + cs));
+        uint8_t *b = ctx->build_in.as<uint8_t>();
+        HOMS_CUDA(cudaMemcpyAsync(b, spec->labels, (size_t)nvox, cudaMemcpyHostToDevice, ctx->stream));
+        a.labels = b;
+        if (fm) {
+            HOMS_CUDA(cudaMemcpyAsync(b + lab, spec->fieldmap, sizeof(double) * (size_t)nvox, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+            a.fieldmap = reinterpret_cast<const double *>(b + lab);
+        }
+        if (cs) {
+            HOMS_CUDA(cudaMemcpyAsync(b + lab + fm, a.csm, cs, cudaMemcpyHostToDevice, ctx->stream));
+            a.csm = reinterpret_cast<const double *>(b + lab + fm);
+        }
+    }
+    HOMS_REQUIRE(!a.csm || (reinterpret_cast<uintptr_t>(a.csm) & 15) == 0, "csm must be 16-byte aligned");
+    HOMS_CUDA(ctx->build_work.ensure(brain_work_bytes(nvox) + sizeof(int64_t)));
+    return a;
+}
+
+int64_t brain_count_sync(homs_context *ctx, const BrainArgs &a) {
+    int64_t *dcount = reinterpret_cast<int64_t *>(ctx->build_work.as<uint8_t>() + brain_work_bytes(a.nx * a.ny * a.nz));
+    HOMS_CUDA(brain_count(a, ctx->build_work.p, dcount, ctx->stream));
+    int64_t n = 0;
+    HOMS_CUDA(cudaMemcpyAsync(&n, dcount, sizeof(n), cudaMemcpyDeviceToHost, ctx->stream));
+    HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+    return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+homs_status homs_brain_phantom_count(homs_context *ctx, const homs_brain_spec *spec, int64_t *nspins) {
+    if (!ctx || !nspins) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        const BrainArgs a = brain_args(ctx, spec);
+        *nspins = brain_count_sync(ctx, a);
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    }
+}
+
+homs_status homs_brain_phantom_fill(homs_context *ctx, const homs_brain_spec *spec, const homs_brain_out *out) {
+    if (!ctx || !out) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        const BrainArgs a = brain_args(ctx, spec);
+        HOMS_REQUIRE(out->memory == HOMS_HOST || out->memory == HOMS_DEVICE, "invalid output memory kind");
+        HOMS_REQUIRE(out->x && out->y && out->z && out->rho && out->T1 && out->T2 && out->dw && out->csm,
+                     "every output array but T2s must be provided");
+        const int64_t n = brain_count_sync(ctx, a);
+        HOMS_REQUIRE(out->nspins == n, "out->nspins must be the spin count of the phantom");
+        const int64_t nc = std::max<int32_t>(spec->ncoils, 1);
+        BrainOut o;
+        o.nspins = n;
+        double *host[9] = {out->x, out->y, out->z, out->rho, out->T1, out->T2, out->T2s, out->dw, out->csm};
+        const size_t len[9] = {1, 1, 1, 1, 1, 1, 1, 1, 2 * (size_t)nc};
+        double *dev[9];
+        if (out->memory == HOMS_DEVICE) {
+            for (int k = 0; k < 9; ++k) dev[k] = host[k];
+            HOMS_REQUIRE((reinterpret_cast<uintptr_t>(out->csm) & 15) == 0, "out->csm must be 16-byte aligned");
+        } else {
+            auto padded = [&](int k) {
+                return (sizeof(double) * len[k] * (size_t)std::max<int64_t>(n, 1) + 255) & ~size_t(255);
+            };
+            size_t total = 0;
+            for (int k = 0; k < 9; ++k) total += padded(k);
+            HOMS_CUDA(ctx->build_out.ensure(total));
+            uint8_t *p = ctx->build_out.as<uint8_t>();
+            for (int k = 0; k < 9; ++k) {
+                dev[k] = host[k] ? reinterpret_cast<double *>(p) : nullptr;
+                p += padded(k);
+            }
+        }
+        o.x = dev[0];
+        o.y = dev[1];
+        o.z = dev[2];
+        o.rho = dev[3];
+        o.T1 = dev[4];
+        o.T2 = dev[5];
+        o.T2s = dev[6];
+        o.dw = dev[7];
+        o.csm = dev[8];
+        if (n > 0) HOMS_CUDA(brain_fill(a, ctx->build_work.p, o, ctx->stream));
+        if (out->memory == HOMS_HOST && n > 0)
+            for (int k = 0; k < 9; ++k)
+                if (host[k])
+                    HOMS_CUDA(cudaMemcpyAsync(host[k], dev[k], sizeof(double) * len[k] * (size_t)n,
+                                              cudaMemcpyDeviceToHost, ctx->stream));
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    }
+}
+
+homs_status homs_csm_birdcage(homs_context *ctx, int64_t nx, int64_t ny, int32_t ncoils, double relative_radius,
+                              double *out, homs_memory out_memory) {
+    if (!ctx) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        HOMS_REQUIRE(nx >= 1 && ny >= 1 && ncoils >= 1, "nX, nY and nCoil must be positive");
+        HOMS_REQUIRE(std::isfinite(relative_radius), "relative_radius must be finite");
+        HOMS_REQUIRE(out != nullptr, "out is NULL");
+        HOMS_REQUIRE(out_memory == HOMS_HOST || out_memory == HOMS_DEVICE, "invalid output memory kind");
+        const size_t bytes = 2 * sizeof(double) * (size_t)nx * (size_t)ny * (size_t)ncoils;
+        double *dst = out;
+        if (out_memory == HOMS_HOST) {
+            HOMS_CUDA(ctx->build_out.ensure(bytes));
+            dst = ctx->build_out.as<double>();
+        }
+        HOMS_CUDA(birdcage(nx, ny, ncoils, relative_radius, dst, ctx->stream));
+        if (out_memory == HOMS_HOST) HOMS_CUDA(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
     }
 }
 

@@ -29,6 +29,7 @@ EXPORTED = [
     "homs_server_wait", "homs_server_times", "homs_server_error", "homs_server_release", "homs_server_destroy",
     "homs_kspace", "homs_kspace_timing", "homs_resident_create", "homs_resident_device_bytes",
     "homs_resident_destroy", "homs_simulate_resident", "homs_server_submit_resident", "homs_plan_graph",
+    "homs_brain_phantom_count", "homs_brain_phantom_fill", "homs_csm_birdcage",
 ]
 
 
@@ -70,6 +71,18 @@ class Timing(ctypes.Structure):
 
 class State(ctypes.Structure):
     _fields_ = [("xy", ctypes.c_void_p), ("z", ctypes.c_void_p), ("memory", ctypes.c_int)]
+
+
+class BrainSpec(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int64), ("ny", ctypes.c_int64), ("nz", ctypes.c_int64),
+                ("res", ctypes.c_double * 3), ("offcenter", ctypes.c_double * 3), ("fieldstrength", ctypes.c_int32),
+                ("ncoils", ctypes.c_int32), ("memory", ctypes.c_int), ("labels", ctypes.c_void_p),
+                ("fieldmap", ctypes.c_void_p), ("csm", ctypes.c_void_p)]
+
+
+class BrainOut(ctypes.Structure):
+    _fields_ = [("nspins", ctypes.c_int64), ("memory", ctypes.c_int)] + [
+        (name, ctypes.c_void_p) for name in ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw", "csm")]
 
 
 class ServerOptions(ctypes.Structure):
@@ -116,6 +129,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_plan_timing": (ctypes.c_int, [vp, ctypes.POINTER(Timing)]),
         "homs_plan_destroy": (ctypes.c_int, [vp]),
         "homs_plan_graph": (ctypes.c_int, [vp, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_char_p)]),
+        "homs_brain_phantom_count": (ctypes.c_int, [vp, ctypes.POINTER(BrainSpec), ctypes.POINTER(i64)]),
+        "homs_brain_phantom_fill": (ctypes.c_int, [vp, ctypes.POINTER(BrainSpec), ctypes.POINTER(BrainOut)]),
+        "homs_csm_birdcage": (ctypes.c_int, [vp, i64, i64, i32, ctypes.c_double, vp, ctypes.c_int]),
         "homs_coil_reduce_noalloc": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i32, vp, i64, vp, i64, vp, i64]),
         "homs_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOptions), ctypes.POINTER(vp)]),
         "homs_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Phantom), ctypes.POINTER(Sequence),

@@ -28,6 +28,7 @@ UNITS = {
     "homs_split.cu": [],
     "homs_api.cu": [],
     "homs_kspace.cu": [],
+    "homs_phantom.cu": [],
     "homs_noalloc.cu": [],
     "homs_server.cu": [],
 }

@@ -180,6 +180,46 @@ homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, int64_t nsp
                                      const void *states, int64_t ldstates, const void *csm, int64_t ldcsm, void *sig,
                                      int64_t ldsig);
 
+/* ---- phantom builders -------------------------------------------------------------
+ * The brain phantom of hophantom_brain (src/phantom/hophantom_brain.jl:2-58) built
+ * on the device from a volume of tissue classes: the voxel-centre grid of
+ * generate_grid (src/grid/Grid.jl:78-108) for fov = matrix .* res, plus
+ * `offcenter`; T1, T2, T2s and rho per class from SpinProperty's 1.5 T or 7 T
+ * tables (src/phantom/SpinProperty.jl:1-118); dw = 2 pi * field map, or the
+ * fat shift -220 * 2 pi rad/s on the fat classes 93 and 209 (b0_type = :fat);
+ * the caller's receive map, or one unit coil.  Only voxels with nonzero rho
+ * are kept, in column-major voxel order (the reference's x[rho .!= 0]).
+ * The volume is what load_phantom_mat returns: the reference reads and
+ * resamples its .mat files in Julia, and those stay on the caller's side. */
+typedef struct homs_brain_spec {
+    int64_t nx, ny, nz;        /* target matrix */
+    double res[3];             /* target resolution, m */
+    double offcenter[3];       /* grid shift, m */
+    int32_t fieldstrength;     /* 0: "1.5T", 1: "7T" */
+    int32_t ncoils;            /* columns of csm; 0: one unit coil */
+    homs_memory memory;        /* where labels, fieldmap and csm live */
+    const uint8_t *labels;     /* nx*ny*nz tissue classes, column-major */
+    const double *fieldmap;    /* nx*ny*nz off-resonance in Hz, or NULL for the fat shift */
+    const double *csm;         /* nx*ny*nz*ncoils complex (re, im), column-major, or NULL */
+} homs_brain_spec;
+
+/* Output arrays of homs_brain_phantom_fill: nspins doubles each (T2s may be
+ * NULL) and csm nspins x max(ncoils, 1) complex doubles, column-major. */
+typedef struct homs_brain_out {
+    int64_t nspins;            /* from homs_brain_phantom_count */
+    homs_memory memory;
+    double *x, *y, *z, *rho, *T1, *T2, *T2s, *dw, *csm;
+} homs_brain_out;
+
+/* Number of spins of the phantom (voxels with nonzero rho). */
+homs_status homs_brain_phantom_count(homs_context *ctx, const homs_brain_spec *spec, int64_t *nspins);
+/* Write the phantom's spin arrays; out->nspins must be the count above. */
+homs_status homs_brain_phantom_fill(homs_context *ctx, const homs_brain_spec *spec, const homs_brain_out *out);
+/* Birdcage receive map of csm_Birdcage (src/phantom/csm/Birdcage.jl:21-42):
+ * nx x ny x ncoils complex doubles, column-major, in out_memory. */
+homs_status homs_csm_birdcage(homs_context *ctx, int64_t nx, int64_t ny, int32_t ncoils, double relative_radius,
+                              double *out, homs_memory out_memory);
+
 /* ---- encoding export ------------------------------------------------------------
  * Generalised k-space of a sampled sequence: replaces get_kspace / grad2kspace
  * (src/datatypes/HO_Sequence.jl:236-287).  Columns 0..2 integrate the nominal

@@ -338,3 +338,88 @@ def grad2kspace_np(seq, rf_start, rf_sign, gamma=GAMMA, q_times=None):
             w = (tau - knots[n]) / (knots[n + 1] - knots[n])
             kq[j] = kspace[n] + w * (kspace[n + 1] - kspace[n])
     return kspace, kq
+
+
+# ---------------------------------------------------------------------------
+# Phantom builders: hophantom_brain (src/phantom/hophantom_brain.jl:2-58),
+# SpinProperty (src/phantom/SpinProperty.jl:1-118), generate_grid
+# (src/grid/Grid.jl:78-108), csm_Birdcage (src/phantom/csm/Birdcage.jl:21-42).
+# ---------------------------------------------------------------------------
+
+# class: (rho, T1 ms, T2 ms, T2s ms) at 1.5 T (SpinProperty.jl:12-59) and 7 T (:62-118)
+_TISSUE_1P5T = {23: (1, 2569, 329, 58), 46: (.86, 833, 83, 69), 70: (.77, 500, 70, 61), 93: (1, 350, 70, 58),
+                116: (1, 900, 47, 30), 139: (.7, 569, 329, 58), 162: (0, 0, 0, 0), 185: (0, 0, 0, 0),
+                209: (.77, 500, 70, 61), 232: (1, 2569, 329, 58), 255: (.77, 500, 70, 61)}
+_TISSUE_7T = {23: (1, 4400, 329, 58), 46: (.86, 2100, 50, 33), 70: (.77, 1200, 40, 27), 93: (1, 580, 46, 25),
+              116: (1, 1700, 30, 23), 139: (.7, 1700, 30, 23), 162: (0, 0, 0, 0), 185: (0, 0, 0, 0),
+              209: (.77, 1200, 40, 27), 232: (1, 4400, 329, 58), 255: (.77, 1200, 40, 27)}
+
+
+def spin_property_np(labels, fieldstrength="1.5T"):
+    """T1, T2, T2s (s) and rho per voxel: the class tables times 1e-3."""
+    table = {"1.5T": _TISSUE_1P5T, "7T": _TISSUE_7T}[fieldstrength]
+    lab = np.asarray(labels)
+    rho, t1, t2, t2s = (np.zeros(lab.shape) for _ in range(4))
+    for c, (r, a, b, d) in table.items():
+        sel = lab == c
+        rho[sel], t1[sel], t2[sel], t2s[sel] = float(r), float(a), float(b), float(d)
+    return t1 * 1e-3, t2 * 1e-3, t2s * 1e-3, rho
+
+
+def generate_grid_np(fov, matrix_size):
+    """Voxel centres (n1, n2, n3, 3): ((0:n-1) - (n-1)/2) * fov/n per axis."""
+    fov = np.asarray(fov, dtype=np.float64)
+    n = [int(v) for v in matrix_size]
+    spacing = fov / np.asarray(n, dtype=np.float64)
+    axes = [(np.arange(n[k], dtype=np.float64) - (n[k] - 1) / 2) * spacing[k] for k in range(3)]
+    grid = np.empty((n[0], n[1], n[2], 3))
+    grid[..., 0] = axes[0][:, None, None]
+    grid[..., 1] = axes[1][None, :, None]
+    grid[..., 2] = axes[2][None, None, :]
+    return grid
+
+
+def brain_phantom_np(labels, target_res, offcenter=(0.0, 0.0, 0.0), fieldstrength="1.5T", fieldmap=None, csm=None):
+    """Spin arrays of hophantom_brain for a resampled class volume: dict of
+    x, y, z, rho, T1, T2, T2s, dw (Ns) and csm (Ns x Nc, Nc = 1 unit coil
+    when csm is None), voxels with rho != 0 in column-major order."""
+    lab = np.asarray(labels)
+    matrix = lab.shape
+    fov = np.asarray(matrix, dtype=np.float64) * np.asarray(target_res, dtype=np.float64)
+    xyz = generate_grid_np(fov, matrix)
+    x = xyz[..., 0] + offcenter[0]
+    y = xyz[..., 1] + offcenter[1]
+    z = xyz[..., 2] + offcenter[2]
+    t1, t2, t2s, rho = spin_property_np(lab, fieldstrength)
+    if fieldmap is None:
+        dw_fat = -220 * (2 * np.pi)
+        dw = np.where((lab == 93) | (lab == 209), dw_fat, -0.0)
+    else:
+        dw = np.asarray(fieldmap, dtype=np.float64) * (2 * np.pi)
+    keep = (rho != 0).ravel(order="F")
+    f = lambda a: np.asarray(a).ravel(order="F")[keep]  # noqa: E731
+    out = {"x": f(x), "y": f(y), "z": f(z), "rho": f(rho), "T1": f(t1), "T2": f(t2), "T2s": f(t2s), "dw": f(dw)}
+    if csm is None:
+        out["csm"] = np.ones((int(keep.sum()), 1), np.complex128)
+    else:
+        c = np.asarray(csm, dtype=np.complex128)
+        out["csm"] = c.reshape(-1, c.shape[-1], order="F")[keep]
+    return out
+
+
+def csm_birdcage_np(nx, ny, ncoils, relative_radius=1.5):
+    """csm_Birdcage: (nx, ny, ncoils) complex, 1/r cis(phi) per coil, RSS-normalised."""
+    out = np.zeros((nx, ny, ncoils), np.complex128)
+    xs = np.arange(nx, dtype=np.float64)[:, None]
+    ys = np.arange(ny, dtype=np.float64)[None, :]
+    for c in range(ncoils):
+        ang = c * (2 * np.pi / ncoils)
+        coilx = relative_radius * np.cos(ang)
+        coily = relative_radius * np.sin(ang)
+        y_co = (ys - ny / 2) / (ny / 2) - coily
+        x_co = (xs - nx / 2) / (nx / 2) - coilx
+        rr = np.sqrt(x_co * x_co + y_co * y_co)
+        phi = np.arctan2(x_co, -y_co) + (-ang)
+        out[:, :, c] = (1 / rr) * (np.cos(phi) + 1j * np.sin(phi))
+    norm = np.sqrt(np.sum(np.abs(out) ** 2, axis=2, keepdims=True))
+    return out / norm
