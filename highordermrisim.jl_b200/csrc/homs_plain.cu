@@ -162,12 +162,14 @@ __device__ void reduce_stage(const cplx<T> *X, cplx<T> *P, int na, const cplx<T>
                 const int s = split * cw + i;
                 if (s >= nvalid) break;
                 const cplx<T> w = csm_rows[(int64_t)s * csm_ld + c];
+                // Complex multiply-accumulate as four fused multiply-adds: the
+                // reference's coil sum is a BLAS product, which fuses them too.
 #pragma unroll
                 for (int a = 0; a < PLAIN_STAGE; ++a) {
                     if (a < na) {
-                        cplx<T> v = cmul(X[a * PLAIN_THREADS + s], w);
-                        acc[a].re = acc[a].re + v.re;
-                        acc[a].im = acc[a].im + v.im;
+                        const cplx<T> x = X[a * PLAIN_THREADS + s];
+                        acc[a].re = fma(x.re, w.re, fma(-x.im, w.im, acc[a].re));
+                        acc[a].im = fma(x.re, w.im, fma(x.im, w.re, acc[a].im));
                     }
                 }
             }
