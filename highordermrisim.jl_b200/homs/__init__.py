@@ -31,7 +31,7 @@ __all__ = [
     "simulate", "prepare_simulation", "Plan", "Server", "Context", "HomsError", "ArgumentError", "DimensionMismatch",
     "BlochHighOrder", "HO_Phantom", "HO_DiscreteSequence", "Mag", "get_sim_ranges", "count_block_adc",
     "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks", "get_kspace",
-    "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage",
+    "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage", "grad2traj", "traj2grad", "InterpTrajTime",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -542,3 +542,4 @@ class Server:
 
 
 from .phantom import brain_phantom, csm_birdcage  # noqa: E402
+from .trajectory import InterpTrajTime, grad2traj, traj2grad  # noqa: E402
