@@ -132,6 +132,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def replica_throughput(ms_local: float, units_per_rank: float, ws: int, device: str = "cuda"):
+    """Whole-job throughput of N independent replicas: every rank processed
+    `units_per_rank` in its own `ms_local`; the job's time is the slowest
+    rank's (an all-reduce MAX over the process group when ws > 1).  Returns
+    (units/s for all ranks together, max ms)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms_local)], dtype=torch.float64, device=device)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return ws * units_per_rank / (ms_max / 1e3), ms_max
+
+
 def _workload(stride=1, k=CONFIG_INDEX):
     from homs import workloads as W
     return W.config(k, spins_stride=stride)
@@ -444,11 +458,7 @@ def run_homs(args):
         stop.record(stream)
         barrier()
     ms = start.elapsed_time(stop) / args.steps
-    ms_t = torch.tensor([ms], device="cuda")
-    if ws > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = ws * units / (ms_max / 1e3)
+    value, ms_max = replica_throughput(ms, units, ws)
     plan.close()
 
     # End to end through the C ABI from pinned host memory.
@@ -501,11 +511,9 @@ def run_homs(args):
             e2e_step()
         barrier()
         e_ms = (time.perf_counter() - t0) * 1e3 / n_e2e
-        e_t = torch.tensor([e_ms], device="cuda")
-        if ws > 1:
-            dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
-        e2e = {"value": ws * units / (float(e_t.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e_t.item())}
+        e_value, e_max = replica_throughput(e_ms, units, ws)
+        e2e = {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "ms_per_step": e_max}
 
     if rank != 0:
         if ws > 1:
