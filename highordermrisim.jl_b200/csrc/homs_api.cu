@@ -139,6 +139,7 @@ struct homs_context {
     DevBuf kspace_in, kspace_meta, kspace_work, kspace_out;
     // phantom builders: staged inputs, work area, staged outputs
     DevBuf build_in, build_work, build_out;
+    DevBuf selftest_err;  // error word of homs_selftest_wait_timeout
     cudaEvent_t kspace_ev[2] = {nullptr, nullptr};
     bool kspace_timed = false;
     // Device workspace of homs_simulate, kept between calls (per dtype) so that
@@ -1011,6 +1012,7 @@ homs_status homs_context_destroy(homs_context *ctx) {
         ctx->build_in.release();
         ctx->build_work.release();
         ctx->build_out.release();
+        ctx->selftest_err.release();
         for (cudaEvent_t &e : ctx->kspace_ev)
             if (e) cudaEventDestroy(e);
         ctx->cache[0].reset();
@@ -1649,6 +1651,26 @@ homs_status homs_kspace(homs_context *ctx, const homs_sequence *seq, int32_t nrf
         }
         HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->kspace_timed = true;
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        return fail(ctx, f);
+    }
+}
+
+homs_status homs_selftest_wait_timeout(homs_context *ctx, int64_t budget_cycles) {
+    if (!ctx) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        HOMS_REQUIRE(budget_cycles >= 1000 && budget_cycles <= 4000000000LL,
+                     "budget_cycles must lie in [1e3, 4e9]");
+        HOMS_CUDA(ctx->selftest_err.ensure(sizeof(unsigned int)));
+        HOMS_CUDA(wait_selftest(ctx->selftest_err.as<unsigned int>(), (long long)budget_cycles, ctx->stream));
+        unsigned int h = 0;
+        HOMS_CUDA(cudaMemcpyAsync(&h, ctx->selftest_err.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (h & 256u) throw Failure{HOMS_ETIMEDOUT, "self-test: the bounded device wait timed out (code 256)"};
         return HOMS_OK;
     } catch (const Failure &f) {
         cudaStreamSynchronize(ctx->stream);

@@ -130,13 +130,16 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_budget(uint64_t *bar, uint32_t parity, long long budget) {
     if (mbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try(bar, parity)) {
-        if (clock64() - t0 > WAIT_BUDGET) return false;
+        if (clock64() - t0 > budget) return false;
     }
     return true;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    return mbar_wait_budget(bar, parity, WAIT_BUDGET);
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -1022,9 +1025,29 @@ __global__ void state_update_kernel(const double *table, const double *endrow, c
 inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
 
 
+// Self-test of the bounded-wait path: one thread waits, with `budget`
+// cycles, on an mbarrier that nothing arrives at; when the wait runs out it
+// records code 256 in the error word and returns, as the split kernel's
+// waits do.
+__global__ void wait_selftest_kernel(unsigned int *err, long long budget) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (!mbar_wait_budget(&bar, 0u, budget)) atomicOr(err, 256u);
+    }
+}
+
 }  // namespace split
 
 using namespace split;
+
+cudaError_t wait_selftest(unsigned int *err, long long budget_cycles, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(err, 0, sizeof(unsigned int), stream);
+    if (e != cudaSuccess) return e;
+    wait_selftest_kernel<<<1, 32, 0, stream>>>(err, budget_cycles);
+    return cudaGetLastError();
+}
 
 SplitResident::~SplitResident() {
     for (void *p : {spin_table, prefix, tvec, partial, amp, err})

@@ -94,6 +94,10 @@ void split_column_sources(uint32_t method, const void *const h[16], const void *
 cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
                               int64_t nsamples, cudaStream_t stream, std::string *err);
 
+// Launch the bounded-wait self-test: a wait that nothing completes runs out
+// after `budget_cycles` and sets code 256 in *err (device word, cleared first).
+cudaError_t wait_selftest(unsigned int *err, long long budget_cycles, cudaStream_t stream);
+
 // Read the device error word (synchronises the stream).  Sets *err if a
 // bounded wait timed out or the phase range check failed.
 cudaError_t split_check(SplitResident &r, cudaStream_t stream, std::string *err);

@@ -29,7 +29,7 @@ EXPORTED = [
     "homs_server_wait", "homs_server_times", "homs_server_error", "homs_server_release", "homs_server_destroy",
     "homs_kspace", "homs_kspace_timing", "homs_resident_create", "homs_resident_device_bytes",
     "homs_resident_destroy", "homs_simulate_resident", "homs_server_submit_resident", "homs_plan_graph",
-    "homs_brain_phantom_count", "homs_brain_phantom_fill", "homs_csm_birdcage",
+    "homs_brain_phantom_count", "homs_brain_phantom_fill", "homs_csm_birdcage", "homs_selftest_wait_timeout",
 ]
 
 
@@ -132,6 +132,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_brain_phantom_count": (ctypes.c_int, [vp, ctypes.POINTER(BrainSpec), ctypes.POINTER(i64)]),
         "homs_brain_phantom_fill": (ctypes.c_int, [vp, ctypes.POINTER(BrainSpec), ctypes.POINTER(BrainOut)]),
         "homs_csm_birdcage": (ctypes.c_int, [vp, i64, i64, i32, ctypes.c_double, vp, ctypes.c_int]),
+        "homs_selftest_wait_timeout": (ctypes.c_int, [vp, i64]),
         "homs_coil_reduce_noalloc": (ctypes.c_int, [vp, ctypes.c_int, i64, i64, i32, vp, i64, vp, i64, vp, i64]),
         "homs_server_create": (ctypes.c_int, [ctypes.POINTER(ServerOptions), ctypes.POINTER(vp)]),
         "homs_server_submit": (ctypes.c_int, [vp, ctypes.POINTER(Phantom), ctypes.POINTER(Sequence),

@@ -244,6 +244,14 @@ homs_status homs_csm_birdcage(homs_context *ctx, int64_t nx, int64_t ny, int32_t
 homs_status homs_kspace(homs_context *ctx, const homs_sequence *seq, int32_t nrf, const int64_t *rf_start,
                         const int8_t *rf_sign, int64_t nq, const double *q_times, double *k, double *k_q,
                         homs_memory out_memory);
+/* Self-test of failure detection, with no counterpart in the reference: one
+ * device thread waits, with a budget of `budget_cycles` (1e3 .. 4e9), on an
+ * mbarrier that nothing arrives at, through the same bounded-wait code the
+ * split kernel uses.  The wait runs out, the kernel records it in a device
+ * error word and returns, and the call returns HOMS_ETIMEDOUT with the
+ * context still usable (no trap, no fault, no hang). */
+homs_status homs_selftest_wait_timeout(homs_context *ctx, int64_t budget_cycles);
+
 /* Device time (CUDA events) of the kernels of the last homs_kspace call on ctx. */
 homs_status homs_kspace_timing(homs_context *ctx, double *ms);
 
