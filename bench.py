@@ -186,7 +186,7 @@ def cpu_baseline(seconds_target=20.0, threads=None):
                       f"{dt:.1f} s"}, stride
 
 
-def serving_benchmark(n_pool=16, passes=6, load=0.9, slots=4, resident=False):
+def serving_benchmark(n_pool=16, passes=10, load=0.9, slots=4, resident=False):
     """Serving stream of mixed simulations through homs.Server.
 
     Batch mode submits every request at once (the server's capacity);
@@ -211,7 +211,10 @@ def serving_benchmark(n_pool=16, passes=6, load=0.9, slots=4, resident=False):
         return srv.submit(obj, r.seq, sim_params=r.params, parts=r.parts, excitation=r.excitation)
 
     with homs.Server(slots=slots) as srv:
-        for t in [submit(srv, r) for r in pool]:  # warm-up: every request once
+        # Warm-up: the whole batch once, so that every slot's device workspace
+        # has grown to the requests it may get (a growth frees device memory,
+        # which waits for the whole device) before anything is timed.
+        for t in [submit(srv, r) for r in reqs]:
             srv.result(t)
             srv.release(t)
         t0 = time.perf_counter()

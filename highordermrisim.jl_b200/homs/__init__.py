@@ -135,6 +135,22 @@ def _finalize(params, sig, state_xy, state_z, parts, excitation, seqd, seconds):
     return RawData(profiles, raw_params)
 
 
+def _state_arrays(obj, state, params, cdt, fdt):
+    """(xy, z, pointer to the homs_state or None).  With no initial state and a
+    return type that does not need the final one, no state crosses the ABI:
+    the device starts from Mxy = 0, Mz = rho itself and keeps the result."""
+    if state is None and params["return_type"] != "state":
+        return None, None, None
+    if state is None:
+        xy = np.zeros(len(obj), dtype=cdt)
+        z = np.ascontiguousarray(np.asarray(obj.rho, dtype=fdt)).copy()
+    else:
+        xy = np.ascontiguousarray(np.asarray(state.xy, dtype=cdt)).copy()
+        z = np.ascontiguousarray(np.asarray(state.z, dtype=fdt)).copy()
+    st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+    return xy, z, st
+
+
 def _run_options(params) -> _lib.RunOptions:
     opts = _lib.RunOptions()
     opts.method = params["sim_method"].flags
@@ -252,22 +268,17 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params
     cdt = np.complex128 if dt == _lib.HOMS_F64 else np.complex64
     fdt = np.float64 if dt == _lib.HOMS_F64 else np.float32
     sig = np.zeros((nadc, obj.ncoils), dtype=cdt, order="F")
-    if state is None:
-        xy = np.zeros(len(obj), dtype=cdt)
-        z = np.ascontiguousarray(np.asarray(obj.rho, dtype=fdt)).copy()
-    else:
-        xy = np.ascontiguousarray(np.asarray(state.xy, dtype=cdt)).copy()
-        z = np.ascontiguousarray(np.asarray(state.z, dtype=fdt)).copy()
-    st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+    xy, z, st = _state_arrays(obj, state, params, cdt, fdt)
+    st_ref = ctypes.byref(st) if st is not None else None
     opts = _run_options(params)
     t0 = time.perf_counter()
     lib = _lib.load()
     if resident is None:
         _lib.check(lib.homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
-                                     ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST), ctx.handle)
+                                     st_ref, sig.ctypes.data if nadc else None, _lib.HOMS_HOST), ctx.handle)
     else:
         _lib.check(lib.homs_simulate_resident(ctx.handle, resident.handle, ctypes.byref(sq), ctypes.byref(opts),
-                                              ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST),
+                                              st_ref, sig.ctypes.data if nadc else None, _lib.HOMS_HOST),
                    ctx.handle)
     seconds = time.perf_counter() - t0
     return _finalize(params, np.asarray(sig), xy, z, parts, excitation, seqd, seconds)
@@ -385,12 +396,14 @@ class Plan:
         cdt = np.complex128 if self.dtype == _lib.HOMS_F64 else np.complex64
         fdt = np.float64 if self.dtype == _lib.HOMS_F64 else np.float32
         sig = np.zeros((self.nadc, self.nc), dtype=cdt, order="F")
-        xy = np.zeros(self.ns, dtype=cdt)
-        z = np.zeros(self.ns, dtype=fdt)
-        st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+        xy = z = st = None
+        if return_type == "state":  # the final state is copied back only when it is returned
+            xy = np.zeros(self.ns, dtype=cdt)
+            z = np.zeros(self.ns, dtype=fdt)
+            st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
         t0 = time.perf_counter()
         _lib.check(_lib.load().homs_plan_run(self.handle, sig.ctypes.data if self.nadc else None, _lib.HOMS_HOST,
-                                             ctypes.byref(st)), self.ctx.handle)
+                                             ctypes.byref(st) if st is not None else None), self.ctx.handle)
         params = dict(self.params)
         params["return_type"] = return_type
         return _finalize(params, np.asarray(sig), xy, z, self.parts, self.excitation, self.seqd,
@@ -479,23 +492,18 @@ class Server:
         cdt = np.complex128 if dt == _lib.HOMS_F64 else np.complex64
         fdt = np.float64 if dt == _lib.HOMS_F64 else np.float32
         sig = np.zeros((nadc, obj.ncoils), dtype=cdt, order="F")
-        if state is None:
-            xy = np.zeros(len(obj), dtype=cdt)
-            z = np.ascontiguousarray(np.asarray(obj.rho, dtype=fdt)).copy()
-        else:
-            xy = np.ascontiguousarray(np.asarray(state.xy, dtype=cdt)).copy()
-            z = np.ascontiguousarray(np.asarray(state.z, dtype=fdt)).copy()
-        st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
+        xy, z, st = _state_arrays(obj, state, params, cdt, fdt)
+        st_ref = ctypes.byref(st) if st is not None else None
         opts = _run_options(params)
         ticket = ctypes.c_int64()
         if resident is None:
             _lib.check(self._lib.homs_server_submit(self.handle, ctypes.byref(ph), ctypes.byref(sq),
-                                                    ctypes.byref(opts), ctypes.byref(st),
+                                                    ctypes.byref(opts), st_ref,
                                                     sig.ctypes.data if nadc else None, _lib.HOMS_HOST,
                                                     ctypes.byref(ticket)))
         else:
             _lib.check(self._lib.homs_server_submit_resident(self.handle, resident.handle, ctypes.byref(sq),
-                                                             ctypes.byref(opts), ctypes.byref(st),
+                                                             ctypes.byref(opts), st_ref,
                                                              sig.ctypes.data if nadc else None, _lib.HOMS_HOST,
                                                              ctypes.byref(ticket)))
         self._requests[ticket.value] = _Request(keep, sig, xy, z, params, parts, excitation, seqd,
