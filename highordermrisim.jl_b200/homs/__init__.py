@@ -25,13 +25,17 @@ import numpy as np
 from . import _lib
 from ._lib import Context, HomsError
 from .model import (GAMMA, ArgumentError, BlochHighOrder, DimensionMismatch, HO_DiscreteSequence, HO_Phantom, Mag,
-                    count_block_adc, get_sim_ranges, initialize_spins_state, rf_events)
+                    count_block_adc, get_sim_ranges, initialize_spins_state, rf_break_lists, rf_events)
+from .sequence import (ADC, RF, Grad, HO_Sequence, MaxStepSizeRule, Sequence, discretize, get_adc_phase_compensation,
+                       get_adc_sampling_times, get_block_start_times, rf_pulses)
 
 __all__ = [
     "simulate", "prepare_simulation", "Plan", "Server", "Context", "HomsError", "ArgumentError", "DimensionMismatch",
     "BlochHighOrder", "HO_Phantom", "HO_DiscreteSequence", "Mag", "get_sim_ranges", "count_block_adc",
     "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks", "get_kspace",
     "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage", "grad2traj", "traj2grad", "InterpTrajTime",
+    "Grad", "RF", "ADC", "Sequence", "HO_Sequence", "MaxStepSizeRule", "discretize", "get_adc_sampling_times",
+    "get_adc_phase_compensation", "get_block_start_times",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -53,7 +57,25 @@ class RawData:
     params: Dict[str, Any] = field(default_factory=dict)
 
 
-def _setup(obj: HO_Phantom, seqd: HO_DiscreteSequence, sim_params, parts=None, excitation=None):
+def _sampled(seq, sim_params):
+    """(sampled sequence, ADC phase compensation or None, native ADC count or
+    None).  An ``HO_Sequence`` is discretised with the sampling keys of
+    ``sim_params`` (``"Δt"``, ``"Δt_rf"``, ``"sampling_rule"``), as
+    ``setup_simulation`` does (Simulate.jl:100)."""
+    if not isinstance(seq, HO_Sequence):
+        if not isinstance(seq, HO_DiscreteSequence):
+            raise ArgumentError("The sequence must be an HO_Sequence or an HO_DiscreteSequence.")
+        return seq, None, None
+    if sim_params is not None and not isinstance(sim_params, dict):
+        raise ArgumentError("sim_params must be a dictionary with string keys.")
+    seqd = discretize(seq, sampling_params=sim_params or {})
+    comp = get_adc_phase_compensation(seq)
+    if np.all(comp == 1):
+        comp = None
+    return seqd, comp, int(sum(a.N for a in seq.SEQ.ADC))
+
+
+def _setup(obj: HO_Phantom, seqd: HO_DiscreteSequence, sim_params, parts=None, excitation=None, native_adc=None):
     """Validation and block planning of ``setup_simulation`` (Simulate.jl:222-287)."""
     if sim_params is None:
         sim_params = {}
@@ -109,6 +131,8 @@ def _setup(obj: HO_Phantom, seqd: HO_DiscreteSequence, sim_params, parts=None, e
         excitation = [bool(e) for e in excitation]
     if not parts:
         raise ArgumentError("The sequence must contain a simulation interval.")
+    if native_adc is not None and sum(count_block_adc(seqd.adc, parts)) != native_adc:
+        raise DimensionMismatch("Sampled ADC count does not match the native sequence.")
     return params, parts, excitation
 
 
@@ -116,12 +140,14 @@ def _dtype(params):
     return _lib.HOMS_F64 if params["precision"] == "f64" else _lib.HOMS_F32
 
 
-def _finalize(params, sig, state_xy, state_z, parts, excitation, seqd, seconds):
-    """finalize_simulation! (Simulate.jl:195-214); the ADC phase compensation of
-    KomaMRIBase is the identity for zero-phase ADCs and is left to the caller."""
+def _finalize(params, sig, state_xy, state_z, parts, excitation, seqd, seconds, comp=None):
+    """finalize_simulation! (Simulate.jl:195-214).  ``comp`` is the ADC phase
+    compensation of an event-level sequence (None: all ones)."""
     rt = params["return_type"]
     if rt == "state":
         return Mag(state_xy, state_z)
+    if comp is not None and sig.shape[0]:
+        sig = sig * comp.astype(sig.dtype)[:, None]
     if rt == "mat":
         return sig[:, :, None]
     counts = count_block_adc(seqd.adc, parts)
@@ -235,7 +261,10 @@ def _resident_args(obj, sim_params):
 
 def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params=None, parts=None, excitation=None,
              state: Optional[Mag] = None, context: Optional[Context] = None, gpus=None, callbacks=(), verbose=False):
-    """Simulate ``obj`` under the sampled sequence ``seqd``.
+    """Simulate ``obj`` under ``seqd``: an ``HO_Sequence`` (discretised first,
+    with the ``"Δt"`` / ``"Δt_rf"`` sampling keys of ``sim_params``, and its
+    ADC phase compensation applied) or an already sampled
+    ``HO_DiscreteSequence``.
 
     ``sim_params`` keys follow the reference: ``"sim_method"``
     (BlochHighOrder), ``"precision"`` (f32/f64), ``"return_type"``
@@ -251,7 +280,8 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params
         raise ArgumentError("callbacks run between blocks on the reference's Julia side; use the block entry points "
                             "(homs_precession_block / homs_excitation_block) for per-block access.")
     obj, resident, sim_params = _resident_args(obj, sim_params)
-    params, parts, excitation = _setup(obj, seqd, sim_params, parts, excitation)
+    seqd, comp, native_adc = _sampled(seqd, sim_params)
+    params, parts, excitation = _setup(obj, seqd, sim_params, parts, excitation, native_adc)
     if gpus is not None:
         if not isinstance(gpus, (list, tuple)) or len(gpus) != 1 or not isinstance(gpus[0], (int, np.integer)) \
                 or isinstance(gpus[0], bool) or gpus[0] < 0:
@@ -281,7 +311,7 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params
                                               st_ref, sig.ctypes.data if nadc else None, _lib.HOMS_HOST),
                    ctx.handle)
     seconds = time.perf_counter() - t0
-    return _finalize(params, np.asarray(sig), xy, z, parts, excitation, seqd, seconds)
+    return _finalize(params, np.asarray(sig), xy, z, parts, excitation, seqd, seconds, comp)
 
 
 def run_blocks(obj: HO_Phantom, seqd: HO_DiscreteSequence, parts, excitation, method: BlochHighOrder,
@@ -320,10 +350,27 @@ def run_blocks(obj: HO_Phantom, seqd: HO_DiscreteSequence, parts, excitation, me
     return np.asarray(sig), xy, z
 
 
-def get_kspace(seqd: HO_DiscreteSequence, rf_start=None, rf_sign=None, skip_rf=None, adc_times=None,
-               gamma: float = GAMMA, context: Optional[Context] = None, precision: str = "f64"):
-    """``K_nominal, K_nominal_adc, K_dfc, K_dfc_adc`` of a sampled sequence on
-    the GPU (``get_kspace``, src/datatypes/HO_Sequence.jl:236-255).
+def _kspace_inputs(hoseq: HO_Sequence, dt, skip_rf, sampling_rule, gamma):
+    """Sampled sequence, RF breaks and ADC times of an event-level sequence
+    (HO_Sequence.jl:236-255): sampling at ``MaxStepSizeRule(dt, 5e-5)``, one
+    break per RF pulse at the first node at or after its centre."""
+    seqd = discretize(hoseq, sampling_rule=sampling_rule or MaxStepSizeRule(dt, 5e-5))
+    t = np.asarray(seqd.t[:-1], dtype=np.float64)
+    pulses = [(int(np.searchsorted(t, c - 1e-12 * max(1.0, abs(c)), side="left")), flip)
+              for c, flip in rf_pulses(hoseq, gamma)]
+    rf_start, rf_sign = rf_break_lists(pulses, skip_rf, t.shape[0])
+    return seqd, rf_start, rf_sign, get_adc_sampling_times(hoseq)
+
+
+def get_kspace(seqd, rf_start=None, rf_sign=None, skip_rf=None, adc_times=None,
+               gamma: float = GAMMA, context: Optional[Context] = None, precision: str = "f64", dt=1.0,
+               sampling_rule=None):
+    """``K_nominal, K_nominal_adc, K_dfc, K_dfc_adc`` of a sequence on the GPU
+    (``get_kspace``, src/datatypes/HO_Sequence.jl:236-255).
+
+    An ``HO_Sequence`` is sampled first (``dt``, ``sampling_rule``), its RF
+    pulses give the breaks and its ADC windows the ADC times.  For a sampled
+    ``HO_DiscreteSequence`` the arguments below apply.
 
     ``K_nominal`` (Nt-1 x 3) integrates the nominal gradients and ``K_dfc``
     (Nt-1 x 16) the sixteen field coefficients, with KomaMRICore's cumtrapz,
@@ -333,6 +380,10 @@ def get_kspace(seqd: HO_DiscreteSequence, rf_start=None, rf_sign=None, skip_rf=N
     refocusing, +1 kept) or, by default, ``rf_events(seqd, gamma, skip_rf)``.
     ``precision`` is the dtype the sequence arrays cross the ABI in; the
     integral is FP64 either way."""
+    if isinstance(seqd, HO_Sequence):
+        if rf_start is not None or rf_sign is not None or adc_times is not None:
+            raise ArgumentError("rf_start, rf_sign and adc_times come from the HO_Sequence itself.")
+        seqd, rf_start, rf_sign, adc_times = _kspace_inputs(seqd, dt, skip_rf, sampling_rule, gamma)
     seqd.validate()
     if rf_start is None:
         if rf_sign is not None:
@@ -368,7 +419,8 @@ class Plan:
 
     def __init__(self, obj, seqd, sys=None, sim_params=None, parts=None, excitation=None,
                  context: Optional[Context] = None):
-        params, parts, excitation = _setup(obj, seqd, dict(sim_params or {}), parts, excitation)
+        seqd, self.comp, native_adc = _sampled(seqd, sim_params)
+        params, parts, excitation = _setup(obj, seqd, dict(sim_params or {}), parts, excitation, native_adc)
         self.params = params
         self.parts, self.excitation = parts, excitation
         self.seqd = seqd
@@ -407,7 +459,7 @@ class Plan:
         params = dict(self.params)
         params["return_type"] = return_type
         return _finalize(params, np.asarray(sig), xy, z, self.parts, self.excitation, self.seqd,
-                         time.perf_counter() - t0)
+                         time.perf_counter() - t0, self.comp)
 
     def device_bytes(self) -> int:
         n = ctypes.c_size_t()
@@ -451,6 +503,7 @@ class _Request:
     excitation: Any
     seqd: Any
     structs: Tuple[Any, ...]
+    comp: Any = None
 
 
 class Server:
@@ -483,7 +536,8 @@ class Server:
         if self.handle is None:
             raise HomsError(6, "server is closed")
         obj, resident, sim_params = _resident_args(obj, sim_params)
-        params, parts, excitation = _setup(obj, seqd, sim_params, parts, excitation)
+        seqd, comp, native_adc = _sampled(seqd, sim_params)
+        params, parts, excitation = _setup(obj, seqd, sim_params, parts, excitation, native_adc)
         dt = _dtype(params)
         keep = _lib._Keep()
         ph = _lib.host_phantom(obj, keep, dt) if resident is None else None
@@ -507,7 +561,7 @@ class Server:
                                                              sig.ctypes.data if nadc else None, _lib.HOMS_HOST,
                                                              ctypes.byref(ticket)))
         self._requests[ticket.value] = _Request(keep, sig, xy, z, params, parts, excitation, seqd,
-                                                (ph, sq, st, opts, resident))
+                                                (ph, sq, st, opts, resident), comp)
         return ticket.value
 
     def done(self, ticket: int) -> bool:
@@ -528,7 +582,8 @@ class Server:
             msg = self._lib.homs_server_error(self.handle, int(ticket))
             raise HomsError(status, (msg or b"").decode() or _lib.load().homs_status_string(status).decode())
         t0, t1, t2 = self.times(ticket)
-        return _finalize(req.params, np.asarray(req.sig), req.xy, req.z, req.parts, req.excitation, req.seqd, t2 - t1)
+        return _finalize(req.params, np.asarray(req.sig), req.xy, req.z, req.parts, req.excitation, req.seqd, t2 - t1,
+                         req.comp)
 
     def release(self, ticket: int) -> None:
         """Forget a finished request (its buffers are released)."""

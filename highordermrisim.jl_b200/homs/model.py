@@ -310,6 +310,12 @@ def rf_events(seqd: HO_DiscreteSequence, gamma: float = GAMMA, skip_rf=None):
         start = next((n for n in range(i, j) if t[n] >= centre), j - 1)
         pulses.append((start, 360.0 * gamma * area))
         i = j
+    return rf_break_lists(pulses, skip_rf, m)
+
+
+def rf_break_lists(pulses, skip_rf, m: int):
+    """``(rf_start, rf_sign)`` from ``(break interval, flip angle)`` per RF
+    pulse over ``m`` intervals (``grad2kspace``, HO_Sequence.jl:262-279)."""
     if skip_rf is None:
         skip_rf = [False] * len(pulses)
     if len(skip_rf) != len(pulses):

@@ -21,6 +21,7 @@ from typing import List, Tuple
 import numpy as np
 
 from .model import GAMMA, BlochHighOrder, HO_DiscreteSequence, HO_Phantom, Mag, get_sim_ranges
+from .sequence import ADC, RF, Grad, HO_Sequence, Sequence
 
 
 @dataclass
@@ -134,6 +135,97 @@ def rf_acquisition_workload(nrf_first=3, nrf_last=2, npre=11, rf_on=True):
                      csm=np.array([[1, 1j, 0.5], [0.5 - 0.2j, -0.3 + 0.1j, 0.2j], [0.7, 0.2j, 0.4 - 0.3j]]))
     parts = [(0, n1 - 1), (n1 - 1, n2 - 1), (n2 - 1, t.shape[0] - 1)]
     return obj, seq, parts, [True, False, True]
+
+
+# ---------------------------------------------------------------------------
+# Event-level sequences (HO_Sequence built from Grad / RF / ADC events)
+# ---------------------------------------------------------------------------
+
+def compatibility_events():
+    """Event-level ``compatibility_sequence`` (test/support/compatibility_workload.jl:4-10):
+    a 90-degree hard pulse of 0.1 ms, then a 2 ms block with 5 ADC samples over 1 ms."""
+    rf_duration = 1e-4
+    gradients = [[Grad(0.0, 0.0), Grad(0.0, 0.0)] for _ in range(3)]
+    pulses = [RF(1 / (4 * GAMMA * rf_duration), rf_duration), RF(0.0, 0.0)]
+    adc = [ADC(0, 0.0), ADC(5, 1e-3)]
+    return Sequence(gradients, pulses, adc, [rf_duration, 2e-3])
+
+
+def compatibility_event_phantom():
+    """``compatibility_phantom`` (compatibility_workload.jl:12-18)."""
+    return HO_Phantom(x=[0.0, 0.01], rho=[1.0, 0.7], T1=[math.inf] * 2, T2=[math.inf] * 2,
+                      csm=np.array([[1, 1j], [0.5 - 0.2j, -0.3 + 0.1j]]))
+
+
+def rf_acquisition_events(nrf_first, nrf_last, npre, rf_on=True):
+    """Event-level ``rf_acquisition_sequence`` (compatibility_workload.jl:20-28): RF
+    pulses of 120 us that acquire during the pulse, around a 2 ms block."""
+    tau = 120e-6
+    gradients = [[Grad(0.0, 0.0)] * 3 for _ in range(3)]
+    a1 = 1 / (4 * GAMMA * tau) if rf_on else 0.0
+    a2 = 1 / (8 * GAMMA * tau) if rf_on else 0.0
+    pulses = [RF(a1, tau), RF(0.0, 0.0), RF(a2, tau)]
+
+    def rf_adc(n):
+        return ADC(0, 0.0) if n == 0 else ADC(n, tau / 2, tau / 4)
+
+    adcs = [rf_adc(nrf_first), ADC(0, 0.0) if npre == 0 else ADC(npre, 1e-3, 1e-4), rf_adc(nrf_last)]
+    return Sequence(gradients, pulses, adcs, [tau, 2e-3, tau])
+
+
+def gre_events(seed=7, ntr=3, nadc=64, dwell=4e-6, flip_deg=30.0, tr=12e-3, field_scale=1.0):
+    """Seeded gradient-echo TR loop as events: a windowed-sinc slab pulse on a
+    slice-select trapezoid (zero-rise edges included, so field jumps occur),
+    phase/readout prewinders, a readout trapezoid with its ADC, spoilers, and
+    measured high-order fields as sampled ``Grad`` waveforms (h0, the first
+    order rows, and a few second and third order rows) over every block.
+    Returns an ``HO_Sequence``."""
+    rng = np.random.default_rng(seed)
+    seq = None
+    gr_cols = []
+    for r in range(ntr):
+        # excitation: 1.6 ms sinc (time-bandwidth 4) on a flat slice gradient with
+        # a zero-rise start and a 0.2 ms ramp down
+        n = 33
+        x = np.linspace(-2, 2, n)
+        shape = np.sinc(x) * (0.54 + 0.46 * np.cos(np.pi * x / 2))
+        dur = 1.6e-3
+        area = np.sum((shape[1:] + shape[:-1]) / 2) * dur / (n - 1)
+        amp = np.deg2rad(flip_deg) / (2 * np.pi * GAMMA * area)
+        phase = np.exp(1j * np.pi * r * (r + 1) / 2 * 117 / 180)  # RF spoiling
+        rf = RF(amp * shape * phase, dur, df=float(rng.uniform(-50, 50)), delay=0.1e-3)
+        ss = Grad(8e-3, 1.8e-3, 0.0, 2e-4)
+        b_exc = Sequence([[Grad(0.0, 0.0)], [Grad(0.0, 0.0)], [ss]], [rf], [ADC(0, 0.0)])
+        # prewinders: readout, phase encoding, slice refocusing
+        ky = (r - ntr / 2) / max(ntr, 1)
+        pre = Sequence([[Grad(-6e-3, 0.4e-3, 1e-4)], [Grad(10e-3 * ky, 0.4e-3, 1e-4)], [Grad(-9e-3, 0.3e-3, 1e-4)]])
+        # readout with its ADC centred on the flat top
+        ro_T = nadc * dwell
+        ro = Sequence([[Grad(6e-3, ro_T, 1e-4)], [Grad(0.0, 0.0)], [Grad(0.0, 0.0)]], None,
+                      [ADC(nadc, ro_T - dwell, 1e-4 + dwell / 2)])
+        spoil = Sequence([[Grad(12e-3, 1e-3, 2e-4)], [Grad(-10e-3 * ky, 0.4e-3, 1e-4)], [Grad(15e-3, 1e-3, 2e-4)]])
+        block = b_exc + pre + ro + spoil
+        fill = tr - float(np.sum(block.DUR))
+        block = block + Sequence([[Grad(0.0, 0.0)]] * 3, None, None, [max(fill, 0.0)])
+        seq = block if seq is None else seq + block
+    # measured fields: a smooth random waveform per (channel, block), nominal-like in rows 1-3
+    rows = [0, 1, 2, 3, 4, 6, 8, 9, 12]
+    amps = {0: 2e-7, 1: 4e-5, 2: 4e-5, 3: 4e-5, 4: 2e-4, 6: 2e-4, 8: 2e-4, 9: 1e-3, 12: 1e-3}
+    nominal = {1: 0, 2: 1, 3: 2}
+    gr = np.empty((16, len(seq)), dtype=object)
+    for j in range(len(seq)):
+        D = float(seq.DUR[j])
+        for i in range(16):
+            if i in rows and D > 0:
+                ns = 9
+                a = field_scale * amps[i] * rng.standard_normal(ns).cumsum() / 3
+                if i in nominal:  # measured first order: the nominal waveform's area plus a perturbation
+                    g = seq.GR[nominal[i], j]
+                    a = a + (g.area() / D if D > 0 else 0.0)
+                gr[i, j] = Grad(a, D)
+            else:
+                gr[i, j] = Grad(0.0, 0.0)
+    return HO_Sequence(seq, gr)
 
 
 # ---------------------------------------------------------------------------
