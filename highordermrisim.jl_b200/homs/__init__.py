@@ -35,7 +35,7 @@ __all__ = [
     "initialize_spins_state", "GAMMA", "HIGH_ORDER_COIL_COMBINATIONS", "RawData", "run_blocks", "get_kspace",
     "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage", "grad2traj", "traj2grad", "InterpTrajTime",
     "Grad", "RF", "ADC", "Sequence", "HO_Sequence", "MaxStepSizeRule", "discretize", "get_adc_sampling_times",
-    "get_adc_phase_compensation", "get_block_start_times",
+    "get_adc_phase_compensation", "get_block_start_times", "read_seq", "demo2d_sequence", "demo3d_sequence",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -606,3 +606,5 @@ class Server:
 
 from .phantom import brain_phantom, csm_birdcage  # noqa: E402
 from .trajectory import InterpTrajTime, grad2traj, traj2grad  # noqa: E402
+from .pulseq import read_seq  # noqa: E402
+from .demo_inputs import demo2d_sequence, demo3d_sequence  # noqa: E402

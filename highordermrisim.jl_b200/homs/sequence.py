@@ -18,7 +18,8 @@ the reference does not vendor; their published definitions are restated here:
   (scalar ``A``) or a piecewise-linear shape (vector ``A`` over ``T``), zero
   outside ``[delay, delay + T]``, frequency offset ``df`` (Hz) on its
   support.  Its centre is ``delay + T/2`` for a hard pulse, else ``delay +
-  center`` or the first sample of largest magnitude.  Flip angle
+  center`` or the midpoint of the first and last samples within 1e-5 of the
+  largest magnitude (the peak plateau).  Flip angle
   ``360 gamma |integral B1 dt|`` degrees; up to 90.01 degrees it is an
   excitation, above a refocusing pulse.
 * ``ADC(N, T, delay=0, df=0, phi=0)``: samples at ``delay + T/2`` (N = 1) or
@@ -254,7 +255,9 @@ class RF:
         if self.center is not None:
             return self.delay + self.center
         t, a = self.knots()
-        return float(t[1 + int(np.argmax(np.abs(a[1:-1])))])
+        mag = np.abs(a[1:-1])
+        peak = np.flatnonzero(mag >= mag.max() * (1 - 1e-5))
+        return float((t[1 + peak[0]] + t[1 + peak[-1]]) / 2)
 
     def flip_angle(self, gamma: float = GAMMA) -> float:
         """360 gamma |integral B1 dt| in degrees."""
@@ -319,7 +322,9 @@ def _flatten(x):
 
 class Sequence:
     """KomaMRIBase ``Sequence``: ``GR`` (3 x N Grad), ``RF`` (1 x N),
-    ``ADC`` (N) and ``DUR`` (N block durations, s)."""
+    ``ADC`` (N) and ``DUR`` (N block durations, s), plus ``DEF`` (the
+    definitions of a sequence file) and ``EXT`` (one extension id per block,
+    not interpreted)."""
 
     def __init__(self, GR=None, RF_=None, ADC_=None, DUR=None):
         if GR is None:
@@ -363,11 +368,15 @@ class Sequence:
             if not np.all(np.isfinite(d)) or np.any(d < 0):
                 raise ArgumentError("Block durations must be finite and nonnegative.")
             self.DUR = d.copy()
+        self.DEF = {}
+        self.EXT = np.zeros(n, dtype=np.int64)
 
     @classmethod
-    def _raw(cls, GR, RF_, ADC_, DUR) -> "Sequence":
+    def _raw(cls, GR, RF_, ADC_, DUR, DEF=None, EXT=None) -> "Sequence":
         s = cls.__new__(cls)
         s.GR, s.RF, s.ADC, s.DUR = GR, RF_, ADC_, np.asarray(DUR, dtype=np.float64)
+        s.DEF = dict(DEF or {})
+        s.EXT = np.zeros(s.DUR.shape[0], dtype=np.int64) if EXT is None else np.asarray(EXT, dtype=np.int64)
         return s
 
     def __len__(self):
@@ -380,16 +389,17 @@ class Sequence:
     def __getitem__(self, idx):
         if isinstance(idx, (int, np.integer)):
             idx = [int(idx)]
-        return Sequence._raw(self.GR[:, idx], self.RF[:, idx], self.ADC[idx], self.DUR[idx])
+        return Sequence._raw(self.GR[:, idx], self.RF[:, idx], self.ADC[idx], self.DUR[idx], self.DEF, self.EXT[idx])
 
     def __add__(self, other: "Sequence") -> "Sequence":
         return Sequence._raw(np.concatenate([self.GR, other.GR], axis=1), np.concatenate([self.RF, other.RF], axis=1),
-                             np.concatenate([self.ADC, other.ADC]), np.concatenate([self.DUR, other.DUR]))
+                             np.concatenate([self.ADC, other.ADC]), np.concatenate([self.DUR, other.DUR]),
+                             {**other.DEF, **self.DEF}, np.concatenate([self.EXT, other.EXT]))
 
     def _map(self, grad=None, rf=None) -> "Sequence":
         g = self.GR if grad is None else np.vectorize(grad, otypes=[object])(self.GR)
         r = self.RF if rf is None else np.vectorize(rf, otypes=[object])(self.RF)
-        return Sequence._raw(g, r, self.ADC.copy(), self.DUR.copy())
+        return Sequence._raw(g, r, self.ADC.copy(), self.DUR.copy(), self.DEF, self.EXT.copy())
 
     def __neg__(self):
         return self._map(grad=lambda g: -g)
@@ -558,7 +568,7 @@ class HO_Sequence:  # noqa: N801
         ev = np.array([max([g.dur for g in seq.GR[:, j]] + [r.dur for r in seq.RF[:, j]] + [seq.ADC[j].dur])
                        for j in range(len(seq))], dtype=np.float64)
         dur = np.maximum.reduce([seq.DUR, self.DUR, _column_durations(self.GR_dfc), ev])
-        return Sequence._raw(seq.GR, seq.RF, seq.ADC, dur)
+        return Sequence._raw(seq.GR, seq.RF, seq.ADC, dur, seq.DEF, seq.EXT)
 
     def validate(self):
         validate_high_order_sequence(self)
