@@ -2,9 +2,10 @@
 
 ``brain_phantom`` is hophantom_brain (src/phantom/hophantom_brain.jl:2-58) for a
 volume of tissue classes that is already resampled to the target grid (what
-load_phantom_mat returns; reading and resampling the reference's .mat files is
-the caller's side).  ``csm_birdcage`` is csm_Birdcage
-(src/phantom/csm/Birdcage.jl:21-42).
+load_phantom_mat returns).  ``hophantom_brain`` adds the host resampling of the
+source volumes (class labels, receive map, off-resonance map) that the
+reference does with Interpolations.jl before building.  ``csm_birdcage`` is
+csm_Birdcage (src/phantom/csm/Birdcage.jl:21-42).
 """
 from __future__ import annotations
 
@@ -102,3 +103,133 @@ def csm_birdcage(nx: int, ny: int, ncoils: int, relative_radius: float = 1.5,
     _lib.check(_lib.load().homs_csm_birdcage(ctx.handle, int(nx), int(ny), int(ncoils), float(relative_radius),
                                              out.ctypes.data, _lib.HOMS_HOST), ctx.handle)
     return out
+
+
+# --------------------------------------------------------------------------- resampling (host)
+# The reference resamples its bundled volumes on the CPU with Interpolations.jl
+# before building the phantom; these are restatements of those steps.
+
+def _axis(n: int, res: float, location: float = 0.0) -> np.ndarray:
+    """Voxel centres ((0:n-1) - (n-1)/2) * res + location."""
+    return (np.arange(n) - (n - 1) / 2) * res + location
+
+
+def _check_grid(target_res, target_matrix, location):
+    if len(target_matrix) != 3 or not all(int(v) > 0 for v in target_matrix):
+        raise ArgumentError("Target matrix dimensions must be positive.")
+    if len(target_res) != 3 or not all(np.isfinite(v) and v > 0 for v in target_res):
+        raise ArgumentError("Target voxel sizes must be finite and positive.")
+    if len(location) != 3 or not all(np.isfinite(v) for v in location):
+        raise ArgumentError("The sampling location must be finite.")
+
+
+def _linear_axis(src: np.ndarray, coord: np.ndarray):
+    """Lower index and weight of linear interpolation on the centres ``src``."""
+    n = src.shape[0]
+    if n == 1:
+        return np.zeros(coord.shape[0], np.int64), np.zeros(coord.shape[0])
+    step = src[1] - src[0]
+    pos = (coord - src[0]) / step
+    i0 = np.clip(np.floor(pos).astype(np.int64), 0, n - 2)
+    return i0, pos - i0
+
+
+def _trilinear(data: np.ndarray, axes_idx):
+    """data[..., extra] sampled at the separable positions (i0, w) of each axis."""
+    out = data
+    for ax, (i0, w) in enumerate(axes_idx):
+        lo = np.take(out, i0, axis=ax)
+        hi = np.take(out, np.minimum(i0 + 1, out.shape[ax] - 1), axis=ax)
+        shape = [1] * out.ndim
+        shape[ax] = w.shape[0]
+        w = w.reshape(shape)
+        out = lo * (1 - w) + hi * w
+    return out
+
+
+def resample_labels(data, source_res, target_res, target_matrix, location=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Nearest-neighbour class volume on the target grid (load_phantom_mat,
+    src/phantom/load_phantom_mat.jl:1-37): targets within the source's outer
+    voxel faces take the nearest voxel (coordinates clamped to the outer
+    centres, ties to even), targets beyond the faces are 0."""
+    _check_grid(target_res, target_matrix, location)
+    if len(source_res) != 3 or not all(np.isfinite(v) and v > 0 for v in source_res):
+        raise ArgumentError("Source phantom voxel sizes must be finite and positive.")
+    data = np.asarray(data)
+    idx, valid = [], []
+    for ax in range(3):
+        n = data.shape[ax]
+        src = _axis(n, source_res[ax])
+        tgt = _axis(int(target_matrix[ax]), target_res[ax], location[ax])
+        valid.append(np.abs(tgt) <= n * source_res[ax] / 2)
+        c = np.clip(tgt, src[0], src[-1])
+        pos = (c - src[0]) / source_res[ax] if n > 1 else np.zeros_like(c)
+        idx.append(np.clip(np.rint(pos).astype(np.int64), 0, n - 1))
+    out = data[np.ix_(*idx)].astype(np.uint8)
+    mask = valid[0][:, None, None] & valid[1][None, :, None] & valid[2][None, None, :]
+    return np.where(mask, out, np.uint8(0))
+
+
+def resample_csm(data, source_res, target_res, target_matrix, location=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """(nx, ny, nz, nc) receive map on the target grid (_resample_csm,
+    src/phantom/csm/Real_32cha.jl:62-95): trilinear on the source centres,
+    coordinates clamped within the outer voxel faces, zero beyond them, and
+    each nonzero receive vector normalised to unit summed squared magnitude."""
+    _check_grid(target_res, target_matrix, location)
+    data = np.asarray(data, dtype=np.complex128)
+    if data.ndim != 4:
+        raise DimensionMismatch("The receive map must be (nx, ny, nz, ncoils).")
+    ai, valid = [], []
+    for ax in range(3):
+        n = data.shape[ax]
+        src = _axis(n, source_res[ax])
+        tgt = _axis(int(target_matrix[ax]), target_res[ax], location[ax])
+        valid.append(np.abs(tgt) <= n * source_res[ax] / 2)
+        ai.append(_linear_axis(src, np.clip(tgt, src[0], src[-1])))
+    out = _trilinear(data, ai)
+    mask = valid[0][:, None, None] & valid[1][None, :, None] & valid[2][None, None, :]
+    out = out * mask[..., None]
+    norm = np.sqrt(np.sum(np.abs(out) ** 2, axis=3, keepdims=True))
+    return out / np.where(norm == 0, 1.0, norm)
+
+
+def resample_b0(data, source_res, target_res, target_matrix, location=(0.0, 0.0, 0.0)) -> np.ndarray:
+    """Off-resonance map (Hz) on the target grid (b0_real,
+    src/phantom/b0map/b0_real.jl:26-51): trilinear between the source
+    centres, 0 outside them and where the source is NaN."""
+    _check_grid(target_res, target_matrix, location)
+    data = np.asarray(data, dtype=np.float64)
+    ai, inside = [], []
+    for ax in range(3):
+        n = data.shape[ax]
+        src = _axis(n, source_res[ax])
+        tgt = _axis(int(target_matrix[ax]), target_res[ax], location[ax])
+        inside.append((tgt >= src[0]) & (tgt <= src[-1]))
+        ai.append(_linear_axis(src, np.clip(tgt, src[0], src[-1])))
+    out = _trilinear(data, ai)
+    mask = inside[0][:, None, None] & inside[1][None, :, None] & inside[2][None, None, :]
+    out = np.where(mask, out, 0.0)
+    out[np.isnan(out)] = 0.0
+    return out
+
+
+def hophantom_brain(brain, brain_res, target_res, target_matrix, location=(0.0, 0.0, 0.0),
+                    offcenter=(0.0, 0.0, 0.0), *, fieldstrength: str = "1.5T", b0=None, b0_res=(4e-3,) * 3,
+                    csm=None, csm_res=(4e-3,) * 3, ncoils: int = 32,
+                    context: Optional[Context] = None) -> HO_Phantom:
+    """hophantom_brain (src/phantom/hophantom_brain.jl:2-58) from source
+    volumes: ``brain`` (class labels at ``brain_res``), ``b0`` (Hz at
+    ``b0_res``; None for the fat shift of b0_type = :fat) and ``csm``
+    (receive map at ``csm_res``, the first ``ncoils`` channels; None for one
+    unit coil).  The volumes are resampled on the host as the reference does;
+    the phantom is built on the device by ``brain_phantom``."""
+    labels = resample_labels(brain, brain_res, target_res, target_matrix, location)
+    fieldmap = None if b0 is None else resample_b0(b0, b0_res, target_res, target_matrix, location)
+    cmap = None
+    if csm is not None:
+        c = np.asarray(csm)
+        if not 1 <= ncoils <= c.shape[3]:
+            raise ArgumentError(f"The receive map supports 1 to {c.shape[3]} coils.")
+        cmap = resample_csm(c, csm_res, target_res, target_matrix, location)[..., :ncoils]
+    return brain_phantom(labels, target_res, offcenter, fieldstrength=fieldstrength, fieldmap=fieldmap, csm=cmap,
+                         context=context)

@@ -103,3 +103,26 @@ def test_built_phantom_simulates_like_its_host_copy(oracle, gpu_context):
     got = homs.simulate(obj, seq, sim_params=params, parts=[(0, 120)], excitation=[False], state=state,
                         context=gpu_context)
     assert np.linalg.norm(got[:, :, 0] - ref[0]) <= 1e-12 * np.linalg.norm(ref[0])
+
+
+@pytest.mark.parametrize("fat", [True, False])
+def test_hophantom_brain_from_source_volumes(gpu_context, fat):
+    """Source volumes (labels at 0.5 mm, receive and off-resonance maps at
+    4 mm) resampled on the host and built on the device, against the oracle
+    builder on the same resampled volumes."""
+    from homs.phantom import hophantom_brain, resample_b0, resample_csm, resample_labels
+    rng = np.random.default_rng(9)
+    brain = rng.choice(CLASSES, size=(90, 100, 40))
+    b0 = rng.normal(0, 40, (13, 14, 7))
+    csm = rng.standard_normal((13, 14, 7, 6)) + 1j * rng.standard_normal((13, 14, 7, 6))
+    tres, tmat, loc, off = (2e-3, 2e-3, 2.5e-3), (24, 26, 9), (0.001, -0.002, 0.003), (0.0, 0.0, 1e-3)
+    got = hophantom_brain(brain, (0.5e-3,) * 3, tres, tmat, loc, off, b0=None if fat else b0, csm=csm, ncoils=4,
+                          context=gpu_context)
+    lab = resample_labels(brain, (0.5e-3,) * 3, tres, tmat, loc)
+    fm = None if fat else resample_b0(b0, (4e-3,) * 3, tres, tmat, loc)
+    cm = resample_csm(csm, (4e-3,) * 3, tres, tmat, loc)[..., :4]
+    want = orc.brain_phantom_np(lab, tres, off, "1.5T", fm, cm)
+    assert len(got) == len(want["x"]) > 0
+    for k in FIELDS:
+        assert np.array_equal(getattr(got, k), want[k]), k
+    assert np.array_equal(got.csm, want["csm"])
