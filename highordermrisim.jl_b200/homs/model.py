@@ -131,7 +131,10 @@ class HO_Phantom:
             raise DimensionMismatch("The CSM must have one row per spin.")
 
     def __getitem__(self, idx):
-        sl = idx if isinstance(idx, slice) else slice(idx, idx + 1)
+        if isinstance(idx, slice) or (isinstance(idx, np.ndarray) and idx.ndim == 1) or isinstance(idx, list):
+            sl = idx
+        else:
+            sl = slice(int(idx), int(idx) + 1)
         out = HO_Phantom.__new__(HO_Phantom)
         out.name = self.name
         for k in ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw"):
