@@ -38,9 +38,12 @@ is a node at its exact time, one node per time point for every field, one
 ``dt`` and ``excitation`` value per interval, and the boundary merge of
 HO_DiscreteSequence.jl:98-131.  Per block, in block time:
 
-1. Breakpoints: 0, the block duration, every knot of the 3 nominal and 16
-   measured gradient waveforms and of the RF pulse, the RF centre and every
-   ADC sample time.  Times closer than 1e-12 s are one time.
+1. Breakpoints: 0, the block duration, every knot of the 16 measured field
+   waveforms, the RF pulse's start and end and every ADC sample time; by
+   default (``MaxStepSizeRule.preserve_samples``, as the reference's
+   ``(:gradients, :rf_center)``) also every knot of the 3 nominal gradients
+   and the RF centre, and on request every sample of a shaped pulse.  Times
+   closer than 1e-12 s are one time.
 2. Between consecutive breakpoints, uniform nodes at most ``min(dt, dt_rf)``
    apart inside the RF pulse and ``dt`` apart elsewhere (``MaxStepSizeRule``,
    defaults 1e-3 s and 5e-5 s as in HO_DiscreteSequence.jl:82-89).
@@ -588,17 +591,32 @@ def validate_high_order_sequence(hoseq: HO_Sequence) -> None:
         raise ArgumentError("High-order sampling supports a single transmit RF channel.")
 
 
-class MaxStepSizeRule:
-    """Largest node spacing outside (``dt``) and inside (``dt_rf``) RF pulses."""
+_PRESERVABLE = ("gradients", "rf_center", "rf")
 
-    def __init__(self, dt=1e-3, dt_rf=5e-5):
+
+class MaxStepSizeRule:
+    """Largest node spacing outside (``dt``) and inside (``dt_rf``) RF
+    pulses, and which event samples are kept as nodes: ``"gradients"`` (every
+    knot of the nominal gradients), ``"rf_center"`` (each pulse's centre) and
+    ``"rf"`` (every sample of a shaped pulse).  The default keeps gradients
+    and RF centres, as the reference's rule does (HO_DiscreteSequence.jl:82-89);
+    the measured field waveforms' knots, block boundaries, pulse ends and ADC
+    times are always nodes."""
+
+    def __init__(self, dt=1e-3, dt_rf=5e-5, preserve_samples=("gradients", "rf_center")):
         self.dt = _real(dt, "dt")
         self.dt_rf = _real(dt_rf, "dt_rf")
         if self.dt <= 0 or self.dt_rf <= 0:
             raise ArgumentError("Sampling steps must be positive.")
+        if isinstance(preserve_samples, str):
+            preserve_samples = (preserve_samples,)
+        ps = tuple(str(v).lstrip(":") for v in preserve_samples)
+        if not set(ps) <= set(_PRESERVABLE):
+            raise ArgumentError(f"preserve_samples entries must be among {_PRESERVABLE}.")
+        self.preserve_samples = ps
 
     def __repr__(self):
-        return f"MaxStepSizeRule(dt={self.dt}, dt_rf={self.dt_rf})"
+        return f"MaxStepSizeRule(dt={self.dt}, dt_rf={self.dt_rf}, preserve_samples={self.preserve_samples})"
 
 
 def get_block_start_times(seq: Sequence) -> np.ndarray:
@@ -653,6 +671,18 @@ def _snap(x: np.ndarray, reps: np.ndarray) -> np.ndarray:
     return reps[np.clip(np.searchsorted(reps, x, side="right") - 1, 0, reps.shape[0] - 1)]
 
 
+def _snap_near(x: np.ndarray, reps: np.ndarray) -> np.ndarray:
+    """Times within _TOL of a representative take its value; others stay."""
+    i = np.clip(np.searchsorted(reps, x, side="right") - 1, 0, reps.shape[0] - 1)
+    out = np.asarray(x, dtype=np.float64).copy()
+    lo = np.abs(x - reps[i]) <= _TOL
+    out[lo] = reps[i][lo]
+    j = np.minimum(i + 1, reps.shape[0] - 1)
+    hi = ~lo & (np.abs(reps[j] - x) <= _TOL)
+    out[hi] = reps[j][hi]
+    return out
+
+
 def _right(tk, ak, q):
     """Right limits of the piecewise-linear waveform (tk, ak) at q (0 outside)."""
     k = np.searchsorted(tk, q, side="right") - 1
@@ -688,14 +718,21 @@ def _sample_block(seq: Sequence, gr_dfc_col, j: int, rule: MaxStepSizeRule) -> _
     rf, adc = seq.RF[0, j], seq.ADC[j]
     rf_on = rf.is_on()
     knots = [w.knots() if w.is_on() else None for w in waves]
-    raw = [np.array([0.0, D]), adc.times()] + [k[0] for k in knots if k is not None]
+    keep = rule.preserve_samples
+    raw = [np.array([0.0, D]), adc.times()] + [k[0] for k in knots[3:] if k is not None]
+    if "gradients" in keep:
+        raw += [k[0] for k in knots[:3] if k is not None]
     if rf_on:
         rk = rf.knots()
-        raw += [rk[0], np.array([rf.center_time()])]
+        raw.append(rk[0][[0, -1]])
+        if "rf_center" in keep:
+            raw.append(np.array([rf.center_time()]))
+        if "rf" in keep:
+            raw.append(rk[0])
     reps = _clusters(np.concatenate(raw))
-    knots = [None if k is None else (_snap(k[0], reps), k[1]) for k in knots]
+    knots = [None if k is None else (_snap_near(k[0], reps), k[1]) for k in knots]
     if rf_on:
-        rk = (_snap(rk[0], reps), rk[1])
+        rk = (_snap_near(rk[0], reps), rk[1])
         rf_s, rf_e = rk[0][0], rk[0][-1]
 
     # uniform fill between breakpoints
@@ -825,7 +862,8 @@ def _rule(sampling_params, sampling_rule) -> MaxStepSizeRule:
     p = sampling_params or {}
     if "sampling_rule" in p:
         return _rule(None, p["sampling_rule"])
-    return MaxStepSizeRule(p.get("Δt", p.get("dt", 1e-3)), p.get("Δt_rf", p.get("dt_rf", 5e-5)))
+    return MaxStepSizeRule(p.get("Δt", p.get("dt", 1e-3)), p.get("Δt_rf", p.get("dt_rf", 5e-5)),
+                           p.get("preserve_samples", ("gradients", "rf_center")))
 
 
 def discretize(hoseq: HO_Sequence, sampling_params=None, sampling_rule: Optional[MaxStepSizeRule] = None,

@@ -250,3 +250,27 @@ def test_adc_phase_compensation():
     assert np.allclose(comp[:2], np.exp(-0.4j), rtol=1e-7) and np.all(comp[2:] == 1)
     seqd, c, native = homs._sampled(HO_Sequence(seq), {})
     assert native == 5 and c is not None
+
+
+def test_preserved_samples_follow_the_rule():
+    n = 201
+    shape = np.sinc(np.linspace(-3, 3, n)).astype(np.complex128) * 1e-6
+    wave = 1e-3 * np.sin(np.linspace(0, 6, 97))
+    seq = Sequence([[Grad(wave, 2e-3, 0.0, 0.0, 1.3e-3)], [Grad(0.0, 0.0)], [Grad(0.0, 0.0)]], [RF(shape, 1e-3, 0.0, 2e-4)],
+                   [ADC(0, 0.0)])
+    hoseq = HO_Sequence(seq)
+    default = discretize(hoseq, sampling_rule=MaxStepSizeRule(1e-3, 5e-5))
+    exc = int(default.excitation.sum())
+    assert exc == 20  # 1 ms at 50 us, the centre falling on the grid
+    assert math.isclose(default.t[np.flatnonzero(default.excitation)[0]], 2e-4, rel_tol=1e-12)
+    every = discretize(hoseq, sampling_rule=MaxStepSizeRule(1e-3, 5e-5, ("gradients", "rf_center", "rf")))
+    assert int(every.excitation.sum()) == n - 1
+    # the nominal waveform's knots are nodes by default, so its area is exact; without them it is sampled
+    area = seq.GR[0, 0].area()
+    assert abs(_trapz(default.dt, default.gx) - area) <= 1e-12 * abs(area)
+    coarse = discretize(hoseq, sampling_rule=MaxStepSizeRule(1e-3, 5e-5, ("rf_center",)))
+    assert coarse.nnodes < default.nnodes
+    knots = seq.GR[0, 0].knots()[0]
+    assert not np.all(np.isin(np.round(knots[2:-2], 12), np.round(coarse.t, 12)))
+    with pytest.raises(ArgumentError):
+        MaxStepSizeRule(1e-3, 5e-5, ("adc",))
