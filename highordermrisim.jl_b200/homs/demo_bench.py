@@ -1,0 +1,129 @@
+"""The reference's demo3D workload on one GPU.
+
+demo3D/1_load_seq.jl builds the sequence (a Pulseq 1.4 3D stack of spirals,
+40 TRs of 500 ms, 35 partitions x 3,800 ADC samples, with field-camera
+gradients in the readouts), demo3D/2_load_phantom.jl the phantom (the
+0.5 mm brain class volume resampled to the sequence's 100 x 100 x 35 grid
+at 2 mm around z = 20 mm, the real 32-channel receive map and the real
+off-resonance map, 1.5 T tissue), and demo3D/3_run_sim.jl runs
+BlochHighOrder("1111") with FP32 arrays.  Two steps:
+
+    python -m homs.demo_bench stage --demo-dir DEMO3D --phantom-dir PHANTOM --out DIR
+        (CPU) copies the three demo files and writes the phantom's class and
+        off-resonance volumes, resampled to the target grid, and the source
+        receive map to DIR (about 40 MB).
+    python -m homs.demo_bench run --staged DIR [--runs 4]
+        (GPU) builds the sequence and the phantom, prepares one plan per
+        mode (split and plain, FP32 and FP64 arrays), times repeated plan
+        runs (host wall time of ``Plan.run``, signal copied to host memory
+        included; the best of ``--runs``) and prints one JSON line with the
+        times, spin*sample*coil/s and each mode's NRMSE against plain FP64.
+
+DEMO3D holds Spiral_2p0x2p0x2p0_100x100x35_1x4_int1_9p5ms_tr500_te5p0{.seq,
+.mat,_skope.mat}; PHANTOM holds brain3D_0.5_0.5_0.5.mat, csm/csm_4p0.mat and
+b0map/b0_4p0.mat, as in the reference's source tree.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import sys
+import time
+
+import numpy as np
+
+NAME = "Spiral_2p0x2p0x2p0_100x100x35_1x4_int1_9p5ms_tr500_te5p0"
+TARGET_RES = (0.002, 0.002, 0.002)
+TARGET_MATRIX = (100, 100, 35)
+LOCATION = (0.0, 0.0, 0.02)
+
+
+def stage(demo_dir: str, phantom_dir: str, out: str) -> None:
+    import scipy.io as sio
+
+    from .phantom import resample_b0, resample_labels
+    os.makedirs(out, exist_ok=True)
+    for suffix in (".seq", ".mat", "_skope.mat"):
+        shutil.copyfile(os.path.join(demo_dir, NAME + suffix), os.path.join(out, NAME + suffix))
+    brain = sio.loadmat(os.path.join(phantom_dir, "brain3D_0.5_0.5_0.5.mat"))["data"]
+    labels = resample_labels(brain, (0.5e-3,) * 3, TARGET_RES, TARGET_MATRIX, LOCATION)
+    b0 = sio.loadmat(os.path.join(phantom_dir, "b0map", "b0_4p0.mat"))["b0"]
+    fieldmap = resample_b0(b0, (4e-3,) * 3, TARGET_RES, TARGET_MATRIX, LOCATION)
+    csm = sio.loadmat(os.path.join(phantom_dir, "csm", "csm_4p0.mat"))["csm"].astype(np.complex64)
+    np.savez(os.path.join(out, "phantom_volumes.npz"), labels=labels, fieldmap=fieldmap.astype(np.float32),
+             csm_source=csm)
+
+
+def _nrmse(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def run(staged: str, runs: int = 4) -> dict:
+    from . import Context, prepare_simulation
+    from .demo_inputs import demo3d_sequence
+    from .model import BlochHighOrder
+    from .phantom import brain_phantom, resample_csm
+    from .sequence import discretize
+
+    out = {"workload": "demo3D: Pulseq 3D stack of spirals with field-camera gradients, brain phantom with real "
+                       "32-channel receive and off-resonance maps"}
+    t0 = time.perf_counter()
+    hoseq = demo3d_sequence(*(os.path.join(staged, NAME + s) for s in (".seq", ".mat", "_skope.mat")))
+    out["sequence_build_s"] = time.perf_counter() - t0
+    vol = np.load(os.path.join(staged, "phantom_volumes.npz"))
+    csm = resample_csm(vol["csm_source"], (4e-3,) * 3, TARGET_RES, TARGET_MATRIX, LOCATION)
+    ctx = Context(0)
+    t0 = time.perf_counter()
+    obj = brain_phantom(vol["labels"], TARGET_RES, fieldstrength="1.5T",
+                        fieldmap=vol["fieldmap"].astype(np.float64), csm=csm, context=ctx)
+    out["phantom_build_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    seqd = discretize(hoseq)
+    out["discretize_s"] = time.perf_counter() - t0
+    out.update(spins=len(obj), coils=obj.ncoils, nodes=seqd.nnodes, adc=int(seqd.adc.sum()),
+               rf_intervals=int(seqd.excitation.sum()))
+    out["units"] = out["spins"] * out["adc"] * out["coils"]
+    method = BlochHighOrder("1111", True, True)
+    sig = {}
+    for name, prec, mode in (("split_f32", "f32", "split"), ("split_f64", "f64", "split"),
+                             ("plain_f64", "f64", "plain"), ("plain_f32", "f32", "plain")):
+        src = obj if prec == "f64" else obj.astype(np.float32)
+        params = {"sim_method": method, "precision": prec, "homs_precision": mode}
+        with prepare_simulation(src, hoseq, sim_params=params, context=ctx) as plan:
+            s = plan.run()
+            best = float("inf")
+            for _ in range(runs):
+                t0 = time.perf_counter()
+                s = plan.run()
+                best = min(best, time.perf_counter() - t0)
+        sig[name] = s[:, :, 0].astype(np.complex128)
+        out[name + "_ms"] = best * 1e3
+        out[name + "_units_per_s"] = out["units"] / best
+    for name in ("split_f32", "split_f64", "plain_f32"):
+        out[name + "_nrmse_vs_plain_f64"] = _nrmse(sig[name], sig["plain_f64"])
+    ctx.close()
+    return out
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    s = sub.add_parser("stage")
+    s.add_argument("--demo-dir", required=True)
+    s.add_argument("--phantom-dir", required=True)
+    s.add_argument("--out", required=True)
+    r = sub.add_parser("run")
+    r.add_argument("--staged", required=True)
+    r.add_argument("--runs", type=int, default=4)
+    a = ap.parse_args(argv)
+    if a.cmd == "stage":
+        stage(a.demo_dir, a.phantom_dir, a.out)
+    else:
+        print(json.dumps(run(a.staged, a.runs)))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -243,3 +243,18 @@ def test_demo2d_through_the_oracle(oracle):
     # the measured fields follow the nominal gradients: the signals start together and drift apart
     assert abs(sig[0, 0] - nominal[0, 0]) <= 1e-2 * abs(nominal[0, 0])
     assert np.linalg.norm(sig - nominal) > 1e-3 * np.linalg.norm(nominal)
+
+
+@needs_demo
+def test_demo_bench_stage(tmp_path):
+    from homs import demo_bench
+    phantom_dir = os.path.join(REF, "src", "phantom")
+    if not os.path.exists(os.path.join(phantom_dir, "brain3D_0.5_0.5_0.5.mat")):
+        pytest.skip("the reference's phantom volumes are not present")
+    demo_bench.stage(os.path.join(REF, "demo3D"), phantom_dir, str(tmp_path))
+    vol = np.load(tmp_path / "phantom_volumes.npz")
+    assert vol["labels"].shape == (100, 100, 35) and vol["labels"].dtype == np.uint8
+    assert vol["fieldmap"].shape == (100, 100, 35) and np.all(np.isfinite(vol["fieldmap"]))
+    assert vol["csm_source"].shape[3] == 32
+    assert (vol["labels"] != 0).sum() > 100000
+    assert signature_ok(str(tmp_path / (demo_bench.NAME + ".seq")))
