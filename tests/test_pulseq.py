@@ -252,9 +252,12 @@ def test_demo_bench_stage(tmp_path):
     if not os.path.exists(os.path.join(phantom_dir, "brain3D_0.5_0.5_0.5.mat")):
         pytest.skip("the reference's phantom volumes are not present")
     demo_bench.stage(os.path.join(REF, "demo3D"), phantom_dir, str(tmp_path))
-    vol = np.load(tmp_path / "phantom_volumes.npz")
+    vol = np.load(tmp_path / "demo3d_phantom_volumes.npz")
     assert vol["labels"].shape == (100, 100, 35) and vol["labels"].dtype == np.uint8
     assert vol["fieldmap"].shape == (100, 100, 35) and np.all(np.isfinite(vol["fieldmap"]))
     assert vol["csm_source"].shape[3] == 32
     assert (vol["labels"] != 0).sum() > 100000
     assert signature_ok(str(tmp_path / (demo_bench.NAME + ".seq")))
+    demo_bench.stage(os.path.join(REF, "demo2D"), phantom_dir, str(tmp_path), "demo2d")
+    vol2 = np.load(tmp_path / "demo2d_phantom_volumes.npz")
+    assert vol2["labels"].shape == (200, 200, 1) and (vol2["labels"] != 0).sum() > 10000
