@@ -85,12 +85,11 @@ def _akima_tangents(t: np.ndarray, y: np.ndarray) -> np.ndarray:
     ext[0] = 2 * ext[1] - m[0]
     ext[n + 1] = 2 * m[-1] - m[-2]
     ext[n + 2] = 2 * ext[n + 1] - m[-1]
-    tan = np.empty(n)
-    for i in range(n):
-        mm2, mm1, m0, mp1 = ext[i], ext[i + 1], ext[i + 2], ext[i + 3]
-        w1, w2 = abs(mp1 - m0), abs(mm1 - mm2)
-        tan[i] = 0.5 * (mm1 + m0) if w1 + w2 == 0 else (w1 * mm1 + w2 * m0) / (w1 + w2)
-    return tan
+    mm2, mm1, m0, mp1 = ext[0:n], ext[1:n + 1], ext[2:n + 2], ext[3:n + 3]
+    w1, w2 = np.abs(mp1 - m0), np.abs(mm1 - mm2)
+    den = w1 + w2
+    flat = den == 0
+    return np.where(flat, 0.5 * (mm1 + m0), (w1 * mm1 + w2 * m0) / np.where(flat, 1.0, den))
 
 
 def _interp_column(t: np.ndarray, y: np.ndarray, q: np.ndarray, mode: str) -> np.ndarray:
