@@ -259,8 +259,9 @@ def _resident_args(obj, sim_params):
     return obj.obj, obj, sim_params
 
 
-def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params=None, parts=None, excitation=None,
-             state: Optional[Mag] = None, context: Optional[Context] = None, gpus=None, callbacks=(), verbose=False):
+def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence = None, sys=None, *, sim_params=None, parts=None,
+             excitation=None, state: Optional[Mag] = None, context: Optional[Context] = None, gpus=None, callbacks=(),
+             verbose=False, return_type=None):
     """Simulate ``obj`` under ``seqd``: an ``HO_Sequence`` (discretised first,
     with the ``"Δt"`` / ``"Δt_rf"`` sampling keys of ``sim_params``, and its
     ADC phase compensation applied) or an already sampled
@@ -275,7 +276,21 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence, sys=None, *, sim_params
     ``sys`` (the KomaMRI Scanner) is accepted and unused, as in the reference
     path.  Returns (Nadc, Nc, 1) complex for "mat", ``Mag`` for "state".
     The caller's dictionary is never modified.
+
+    ``simulate(plan, return_type=...)`` runs a prepared ``Plan`` instead
+    (``simulate(plan::PreparedSimulation)``, PreparedSimulation.jl:218-258).
     """
+    if isinstance(obj, Plan):
+        if seqd is not None or sim_params is not None or parts is not None or state is not None:
+            raise ArgumentError("A prepared simulation takes only return_type (and callbacks, verbose).")
+        if callbacks:
+            raise ArgumentError("callbacks run between blocks on the reference's Julia side; use the block entry "
+                                "points (homs_precession_block / homs_excitation_block) for per-block access.")
+        return obj.run(return_type)
+    if return_type is not None:
+        raise ArgumentError("return_type is a sim_params key here; the keyword is for prepared simulations.")
+    if seqd is None:
+        raise ArgumentError("simulate needs a sequence (or a prepared simulation).")
     if callbacks:
         raise ArgumentError("callbacks run between blocks on the reference's Julia side; use the block entry points "
                             "(homs_precession_block / homs_excitation_block) for per-block access.")
@@ -487,8 +502,21 @@ class Plan:
         self.close()
 
 
-def prepare_simulation(obj, seqd, sys=None, *, sim_params=None, parts=None, excitation=None, context=None):
-    """Create a ``Plan`` (use as a context manager or call ``close()``)."""
+def prepare_simulation(obj, seqd, sys=None, *args, sim_params=None, parts=None, excitation=None, context=None):
+    """Create a ``Plan`` (use as a context manager or call ``close()``).
+
+    ``prepare_simulation(f, obj, seqd, ...)`` is the do-block form of
+    PreparedSimulation.jl:181-188: it returns ``f(plan)`` and closes the plan
+    whatever happens."""
+    if callable(obj) and not isinstance(obj, (HO_Phantom, ResidentPhantom)):
+        f, obj, seqd, sys = obj, seqd, sys, (args[0] if args else None)
+        plan = Plan(obj, seqd, sys, sim_params, parts, excitation, context)
+        try:
+            return f(plan)
+        finally:
+            plan.close()
+    if args:
+        raise ArgumentError("prepare_simulation takes (obj, seqd, sys) or (f, obj, seqd, sys).")
     return Plan(obj, seqd, sys, sim_params, parts, excitation, context)
 
 

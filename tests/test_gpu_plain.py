@@ -343,3 +343,10 @@ def test_prepared_plan_reuse(gpu_context, precision):
     plan.close()
     with pytest.raises(homs.ArgumentError):
         plan.run()
+    # simulate(plan) and the do-block form (PreparedSimulation.jl:181-258)
+    got = homs.prepare_simulation(lambda pl: (homs.simulate(pl), homs.simulate(pl, return_type="state"), pl), obj, seq,
+                                  sim_params=params)
+    assert np.array_equal(got[0], baseline)
+    assert np.array_equal(got[1].xy, expected_state.xy) and got[2].closed
+    with pytest.raises(homs.ArgumentError):
+        homs.simulate(got[2])
