@@ -557,6 +557,8 @@ def run_homs(args):
         out["serving"] = serving_benchmark()
         out["serving"]["plain_per_request_units_per_s"] = plain_per_request()
         out["serving_resident"] = serving_benchmark(resident=True)
+    if ws == 1 and not args.no_refgpu and args.config == CONFIG_INDEX and args.spin_stride == 1:
+        out["reference_gpu_equivalent"] = reference_gpu_leg(w, sig_dev, ms_max, units)
     if ws == 1 and not args.no_kspace:
         out["kspace"] = kspace_benchmark(ctx, hbm_peak, peak_kind)
         out["phantom"] = phantom_benchmark(ctx, hbm_peak, peak_kind)
@@ -565,6 +567,152 @@ def run_homs(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def reference_gpu_equivalent(w, dtype: str = "f32", block: int = 32, device: str = "cuda", time_it: bool = True):
+    """The reference's own GPU design, restated with torch and cuBLAS and run on
+    this GPU: the comparator for the fused kernels (not part of the product).
+
+    Excitation parts step an elementwise spinor over the spins per node
+    (kernels/HighOrderGPU.jl:181-233).  Precession runs in blocks of at most
+    ``block`` intervals, as the reference's workspace is sized
+    (kernels/HighOrderGPU.jl:6-58): per block, the field of every spin and node
+    is a (spins x 17) by (17 x nodes) GEMM of the unnormalised basis against the
+    masked coefficients (:63-93), the phase its trapezoid sum, and the states
+    M0 exp(i phi - t/T2) at the block's ADC nodes are materialised and reduced
+    into the coils by one complex GEMM, states^T csm (:95-178, the default
+    "gemm" coil combination).  The state carries across blocks and parts.
+
+    Returns (signal (Nadc x Nc) as numpy, ms on the device or None)."""
+    import torch
+
+    from homs.model import GAMMA, BlochHighOrder
+    rt = torch.float64 if dtype == "f64" else torch.float32
+    ct = torch.complex128 if dtype == "f64" else torch.complex64
+    dev = torch.device(device)
+    obj, seq = w.obj, w.seq
+    T = lambda a, d=rt: torch.as_tensor(np.ascontiguousarray(a), device=dev).to(d)  # noqa: E731
+    x, y, z, rho, T1, T2, dw = (T(getattr(obj, k)) for k in ("x", "y", "z", "rho", "T1", "T2", "dw"))
+    csm = T(np.asarray(obj.csm), ct)
+    m = BlochHighOrder(w.mask).flags
+    ho0, ho1, ho2, ho3, dw_exc, dw_prec = (bool(m & b) for b in (1, 2, 4, 8, 16, 32))
+    r2 = x * x + y * y + z * z
+    one = torch.ones_like(x)
+    basis = torch.stack([one, x, y, z, x * y, z * y, 3 * z * z - r2, x * z, x * x - y * y,
+                         3 * y * x * x - y ** 3, x * z * y, (5 * z * z - r2) * y, 5 * z ** 3 - 3 * z * r2,
+                         (5 * z * z - r2) * x, x * x * z - y * y * z, x ** 3 - 3 * x * y * y,
+                         dw / (2 * np.pi * GAMMA) if dw_prec else torch.zeros_like(x)], dim=1)
+    h = np.asarray(seq.h, dtype=np.float64).copy()
+    if not ho0:
+        h[0] = 0
+    if not ho1:
+        h[1], h[2], h[3] = seq.gx, seq.gy, seq.gz
+    if not ho2:
+        h[4:9] = 0
+    if not ho3:
+        h[9:16] = 0
+    coef = T(np.vstack([h, np.ones((1, h.shape[1]))]))
+    dt = T(seq.dt)
+    gx, gy, gz, df, psi = T(seq.gx), T(seq.gy), T(seq.gz), T(seq.df), T(seq.psi)
+    b1 = T(np.asarray(seq.b1), ct)
+    adc = np.asarray(seq.adc, dtype=bool)
+    nadc = sum(int(adc[f + 1:l + 1].sum()) for f, l in w.parts)
+    sig = torch.zeros((nadc, csm.shape[1]), dtype=ct, device=dev)
+    mxy = torch.zeros_like(x, dtype=ct)
+    mz = rho.clone()
+    c_neg = -2 * np.pi * GAMMA
+    eps = float(np.finfo(np.float64 if dtype == "f64" else np.float32).eps)
+    # block plan (ADC columns as slices, or index tensors built before the timed region)
+    blocks = {}
+    for (f, l), exc in zip(w.parts, w.excitation):
+        if exc:
+            continue
+        a = f
+        while a < l:
+            b = min(l, a + block)
+            cols = np.flatnonzero(adc[a + 1:b + 1])
+            if cols.size and np.array_equal(cols, np.arange(cols[0], cols[0] + cols.size)):
+                sel = slice(int(cols[0]), int(cols[0]) + cols.size)
+            else:
+                sel = torch.as_tensor(cols, device=dev) if cols.size else None
+            blocks[a] = (b, sel, int(cols.size))
+            a = b
+    start = torch.cuda.Event(enable_timing=True) if time_it else None
+    stop = torch.cuda.Event(enable_timing=True) if time_it else None
+    if time_it:
+        torch.cuda.synchronize()
+        start.record()
+    row = 0
+    for (f, l), exc in zip(w.parts, w.excitation):
+        if exc:
+            mxy = mxy * torch.polar(torch.ones_like(x), -psi[f].expand_as(x))
+            off = dw / (2 * np.pi * GAMMA) if dw_exc else torch.zeros_like(x)
+            for n in range(f, l):
+                bz = (gx[n] * x + gy[n] * y) + gz[n] * z + (off - df[n] / GAMMA)
+                bb = torch.sqrt(b1[n].abs() ** 2 + bz * bz)
+                bb = torch.where(bb == 0, torch.full_like(bb, eps), bb)
+                half = c_neg * (bb * dt[n]) / 2
+                sh, ch = torch.sin(half), torch.cos(half)
+                al = torch.complex(ch, -(bz / bb) * sh)
+                be = torch.complex((b1[n].imag / bb) * sh, -(b1[n].real / bb) * sh)
+                nxy = 2 * al.conj() * be * mz + al.conj() ** 2 * mxy - be ** 2 * mxy.conj()
+                nmz = (al.abs() ** 2 - be.abs() ** 2) * mz - 2 * (al * be * mxy.conj()).real
+                e1 = torch.exp(-dt[n] / T1)
+                mxy = nxy * torch.exp(-dt[n] / T2)
+                mz = nmz * e1 + rho * (1 - e1)
+                if adc[n + 1]:
+                    s_ = mxy * torch.polar(torch.ones_like(x), psi[n + 1].expand_as(x))
+                    sig[row] = s_ @ csm
+                    row += 1
+            mxy = mxy * torch.polar(torch.ones_like(x), psi[l].expand_as(x))
+            continue
+        a = f
+        while a < l:
+            b, sel, ncol = blocks[a]
+            bz = basis @ coef[:, a:b + 1]
+            d = dt[a:b]
+            phi = torch.cumsum((bz[:, :-1] + bz[:, 1:]) * (-np.pi * GAMMA * d), dim=1)
+            tr = torch.cumsum(d, dim=0)
+            mblk = mxy[:, None] * torch.exp(torch.complex(-tr[None, :] / T2[:, None], phi))
+            if ncol:
+                states = mblk[:, sel]
+                sig[row:row + ncol] = states.transpose(0, 1) @ csm
+                row += ncol
+            mxy = mblk[:, -1]
+            e1 = torch.exp(-tr[-1] / T1)
+            mz = mz * e1 + rho * (1 - e1)
+            a = b
+    ms = None
+    if time_it:
+        stop.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop)
+    return sig.cpu().numpy(), ms
+
+
+def reference_gpu_leg(w, fused_sig, fused_ms: float, units: float) -> dict:
+    """Time ``reference_gpu_equivalent`` once per precision on the full
+    workload (after a warm-up on a spin subsample) and compare its FP64 signal
+    with the fused kernel's."""
+    import torch
+    out = {"design": "the reference's GPU path restated with torch/cuBLAS: per block of <= 32 nodes a basis x "
+                     "coefficient GEMM for the field, trapezoid phase, materialised ADC states, and a complex "
+                     "cuBLAS GEMM states^T csm (kernels/HighOrderGPU.jl:6-178); host loop over blocks",
+           "block_nodes": 32}
+    try:
+        small = _workload(50)
+        for dt in ("f32", "f64"):
+            reference_gpu_equivalent(small, dt)
+            sig, ms = reference_gpu_equivalent(w, dt)
+            out[dt] = {"ms": ms, "units_per_s": units / (ms / 1e3), "fused_speedup": ms / fused_ms}
+            if dt == "f64":
+                fused = fused_sig.transpose(0, 1).cpu().numpy()
+                out[dt]["nrmse_fused_vs_this"] = float(np.linalg.norm(fused - sig) / np.linalg.norm(sig))
+            del sig
+            torch.cuda.empty_cache()
+    except Exception as e:  # the comparator must not take the bench line down
+        out["error"] = f"{type(e).__name__}: {e}"
+    return out
 
 
 def _pinned(torch, a: np.ndarray) -> np.ndarray:
@@ -592,6 +740,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-kspace", action="store_true", help="skip the encoding-export measurement")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="skip timing the restatement of the reference's GPU design (reference_gpu_equivalent)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
