@@ -569,7 +569,8 @@ def run_homs(args):
     return 0
 
 
-def reference_gpu_equivalent(w, dtype: str = "f32", block: int = 32, device: str = "cuda", time_it: bool = True):
+def reference_gpu_equivalent(w, dtype: str = "f32", block: int = 32, device: str = "cuda", time_it: bool = True,
+                             graph: bool = False, times: dict = None):
     """The reference's own GPU design, restated with torch and cuBLAS and run on
     this GPU: the comparator for the fused kernels (not part of the product).
 
@@ -582,6 +583,11 @@ def reference_gpu_equivalent(w, dtype: str = "f32", block: int = 32, device: str
     M0 exp(i phi - t/T2) at the block's ADC nodes are materialised and reduced
     into the coils by one complex GEMM, states^T csm (:95-178, the default
     "gemm" coil combination).  The state carries across blocks and parts.
+
+    With ``graph`` the whole run is captured once into a CUDA graph and the
+    timed run is its replay, so the host loop's launch overhead is excluded;
+    ``times`` (a dict) then receives ``eager_ms`` (the host loop) and
+    ``graph_ms`` (the replay).
 
     Returns (signal (Nadc x Nc) as numpy, ms on the device or None)."""
     import torch
@@ -618,8 +624,8 @@ def reference_gpu_equivalent(w, dtype: str = "f32", block: int = 32, device: str
     adc = np.asarray(seq.adc, dtype=bool)
     nadc = sum(int(adc[f + 1:l + 1].sum()) for f, l in w.parts)
     sig = torch.zeros((nadc, csm.shape[1]), dtype=ct, device=dev)
-    mxy = torch.zeros_like(x, dtype=ct)
-    mz = rho.clone()
+    mxy0 = torch.zeros_like(x, dtype=ct)
+    mz0 = rho.clone()
     c_neg = -2 * np.pi * GAMMA
     eps = float(np.finfo(np.float64 if dtype == "f64" else np.float32).eps)
     # block plan (ADC columns as slices, or index tensors built before the timed region)
@@ -637,56 +643,88 @@ def reference_gpu_equivalent(w, dtype: str = "f32", block: int = 32, device: str
                 sel = torch.as_tensor(cols, device=dev) if cols.size else None
             blocks[a] = (b, sel, int(cols.size))
             a = b
-    start = torch.cuda.Event(enable_timing=True) if time_it else None
-    stop = torch.cuda.Event(enable_timing=True) if time_it else None
-    if time_it:
-        torch.cuda.synchronize()
-        start.record()
-    row = 0
-    for (f, l), exc in zip(w.parts, w.excitation):
-        if exc:
-            mxy = mxy * torch.polar(torch.ones_like(x), -psi[f].expand_as(x))
-            off = dw / (2 * np.pi * GAMMA) if dw_exc else torch.zeros_like(x)
-            for n in range(f, l):
-                bz = (gx[n] * x + gy[n] * y) + gz[n] * z + (off - df[n] / GAMMA)
-                bb = torch.sqrt(b1[n].abs() ** 2 + bz * bz)
-                bb = torch.where(bb == 0, torch.full_like(bb, eps), bb)
-                half = c_neg * (bb * dt[n]) / 2
-                sh, ch = torch.sin(half), torch.cos(half)
-                al = torch.complex(ch, -(bz / bb) * sh)
-                be = torch.complex((b1[n].imag / bb) * sh, -(b1[n].real / bb) * sh)
-                nxy = 2 * al.conj() * be * mz + al.conj() ** 2 * mxy - be ** 2 * mxy.conj()
-                nmz = (al.abs() ** 2 - be.abs() ** 2) * mz - 2 * (al * be * mxy.conj()).real
-                e1 = torch.exp(-dt[n] / T1)
-                mxy = nxy * torch.exp(-dt[n] / T2)
-                mz = nmz * e1 + rho * (1 - e1)
-                if adc[n + 1]:
-                    s_ = mxy * torch.polar(torch.ones_like(x), psi[n + 1].expand_as(x))
-                    sig[row] = s_ @ csm
-                    row += 1
-            mxy = mxy * torch.polar(torch.ones_like(x), psi[l].expand_as(x))
-            continue
-        a = f
-        while a < l:
-            b, sel, ncol = blocks[a]
-            bz = basis @ coef[:, a:b + 1]
-            d = dt[a:b]
-            phi = torch.cumsum((bz[:, :-1] + bz[:, 1:]) * (-np.pi * GAMMA * d), dim=1)
-            tr = torch.cumsum(d, dim=0)
-            mblk = mxy[:, None] * torch.exp(torch.complex(-tr[None, :] / T2[:, None], phi))
-            if ncol:
-                states = mblk[:, sel]
-                sig[row:row + ncol] = states.transpose(0, 1) @ csm
-                row += ncol
-            mxy = mblk[:, -1]
-            e1 = torch.exp(-tr[-1] / T1)
-            mz = mz * e1 + rho * (1 - e1)
-            a = b
+    def body():
+        _run(mxy0, mz0)
+
+    def _run(mxy, mz):
+        row = 0
+        for (f, l), exc in zip(w.parts, w.excitation):
+            if exc:
+                mxy = mxy * torch.polar(torch.ones_like(x), -psi[f].expand_as(x))
+                off = dw / (2 * np.pi * GAMMA) if dw_exc else torch.zeros_like(x)
+                for n in range(f, l):
+                    bz = (gx[n] * x + gy[n] * y) + gz[n] * z + (off - df[n] / GAMMA)
+                    bb = torch.sqrt(b1[n].abs() ** 2 + bz * bz)
+                    bb = torch.where(bb == 0, torch.full_like(bb, eps), bb)
+                    half = c_neg * (bb * dt[n]) / 2
+                    sh, ch = torch.sin(half), torch.cos(half)
+                    al = torch.complex(ch, -(bz / bb) * sh)
+                    be = torch.complex((b1[n].imag / bb) * sh, -(b1[n].real / bb) * sh)
+                    nxy = 2 * al.conj() * be * mz + al.conj() ** 2 * mxy - be ** 2 * mxy.conj()
+                    nmz = (al.abs() ** 2 - be.abs() ** 2) * mz - 2 * (al * be * mxy.conj()).real
+                    e1 = torch.exp(-dt[n] / T1)
+                    mxy = nxy * torch.exp(-dt[n] / T2)
+                    mz = nmz * e1 + rho * (1 - e1)
+                    if adc[n + 1]:
+                        s_ = mxy * torch.polar(torch.ones_like(x), psi[n + 1].expand_as(x))
+                        sig[row] = s_ @ csm
+                        row += 1
+                mxy = mxy * torch.polar(torch.ones_like(x), psi[l].expand_as(x))
+                continue
+            a = f
+            while a < l:
+                b, sel, ncol = blocks[a]
+                bz = basis @ coef[:, a:b + 1]
+                d = dt[a:b]
+                phi = torch.cumsum((bz[:, :-1] + bz[:, 1:]) * (-np.pi * GAMMA * d), dim=1)
+                tr = torch.cumsum(d, dim=0)
+                mblk = mxy[:, None] * torch.exp(torch.complex(-tr[None, :] / T2[:, None], phi))
+                if ncol:
+                    states = mblk[:, sel]
+                    sig[row:row + ncol] = states.transpose(0, 1) @ csm
+                    row += ncol
+                mxy = mblk[:, -1]
+                e1 = torch.exp(-tr[-1] / T1)
+                mz = mz * e1 + rho * (1 - e1)
+                a = b
     ms = None
-    if time_it:
+    if graph:
+        torch.cuda.synchronize()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            e0, e1_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(side)
+            body()  # the eager run, also the warm-up before the capture (cuBLAS handles, workspaces)
+            e1_.record(side)
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        if times is not None:
+            times["eager_ms"] = e0.elapsed_time(e1_)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            body()
+        torch.cuda.synchronize()
+        sig.zero_()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        g.replay()
         stop.record()
         torch.cuda.synchronize()
         ms = start.elapsed_time(stop)
+        if times is not None:
+            times["graph_ms"] = ms
+        del g
+    elif time_it:
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        start.record()
+        body()
+        stop.record()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop)
+    else:
+        body()
     return sig.cpu().numpy(), ms
 
 
@@ -703,8 +741,10 @@ def reference_gpu_leg(w, fused_sig, fused_ms: float, units: float) -> dict:
         small = _workload(50)
         for dt in ("f32", "f64"):
             reference_gpu_equivalent(small, dt)
-            sig, ms = reference_gpu_equivalent(w, dt)
-            out[dt] = {"ms": ms, "units_per_s": units / (ms / 1e3), "fused_speedup": ms / fused_ms}
+            tm = {}
+            sig, ms = reference_gpu_equivalent(w, dt, graph=True, times=tm)
+            out[dt] = {"ms": ms, "units_per_s": units / (ms / 1e3), "fused_speedup": ms / fused_ms,
+                       "host_loop_ms": tm.get("eager_ms"), "timing": "CUDA-graph replay of the whole block loop"}
             if dt == "f64":
                 fused = fused_sig.transpose(0, 1).cpu().numpy()
                 out[dt]["nrmse_fused_vs_this"] = float(np.linalg.norm(fused - sig) / np.linalg.norm(sig))

@@ -34,3 +34,6 @@ def test_comparator_matches_the_oracle_on_gpu(oracle):
     assert ms > 0 and nrmse(got, ref) <= 1e-11
     got32, _ = bench.reference_gpu_equivalent(w, "f32", 32)
     assert nrmse(got32, ref) <= 1e-4
+    times = {}
+    got_g, ms_g = bench.reference_gpu_equivalent(w, "f64", 32, graph=True, times=times)
+    assert ms_g > 0 and times["eager_ms"] > 0 and nrmse(got_g, ref) <= 1e-11
