@@ -36,6 +36,9 @@ METRIC = "spin*sample*coil/s"
 UNIT = "spin*sample*coil/s"
 CONFIG_INDEX = 2
 FLOPS_PER_UNIT = 8.0  # one complex multiply-accumulate per spin*sample*coil
+F16_FLOPS_PER_UNIT = 32.0  # the split contraction as issued: hi and lo passes against B hi|lo columns
+FP64_FLOPS_PER_SPIN_SAMPLE = 32.0  # the phase tile on the FP64 DMMA pipe
+FP64_DMMA_PEAK = 37.0  # TFLOP/s, m8n8k4.f64 rate measured by a probe on this pool's B200s
 
 
 def _dist():
@@ -536,6 +539,17 @@ def run_homs(args):
             "fallback 1.59 PFLOP/s", "kernel": "split_precession_kernel" if args.mode == "split" else
             "segment_kernel", "kernel_ms_per_launch": avg_launch_ms,
             "units_per_launch": seg_units, "flops_per_unit": FLOPS_PER_UNIT}
+    if args.mode == "split" and achieved_tflops:
+        # What the kernel issues to the shared tensor pipe: the FP16 hi/lo contraction (8 MMAs of
+        # 128x128x16 per 32-spin chunk = 32 flops per unit) against the dense FP16/bf16 peak, and the
+        # FP64 DMMA phase (32 flops per spin*sample) against the DMMA rate a probe measured (37 TF/s).
+        secs = avg_launch_ms / 1e3
+        f16 = F16_FLOPS_PER_UNIT * seg_units / secs / 1e12
+        f64 = FP64_FLOPS_PER_SPIN_SAMPLE * (seg_units / nc) / secs / 1e12
+        roof["tensor_pipe"] = {"f16_mma_tflops": f16, "f16_flops_per_unit": F16_FLOPS_PER_UNIT,
+                               "fp64_dmma_tflops": f64, "fp64_flops_per_spin_sample": FP64_FLOPS_PER_SPIN_SAMPLE,
+                               "fp64_dmma_peak_tflops": FP64_DMMA_PEAK, "combined_share": f16 / bf16_peak +
+                               f64 / FP64_DMMA_PEAK}
     base = None
     if ws == 1 and not args.no_cpu_baseline and args.config == CONFIG_INDEX:
         base, _ = cpu_baseline()
