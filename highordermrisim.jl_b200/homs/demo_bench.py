@@ -79,7 +79,7 @@ def run(staged: str, runs: int = 4, modes=tuple(MODES), workload: str = "demo3d"
     from .demo_inputs import demo2d_sequence, demo3d_sequence
     from .model import BlochHighOrder
     from .phantom import brain_phantom, resample_csm
-    from .sequence import discretize
+    from .sequence import discretize, get_adc_phase_compensation
 
     w = WORKLOADS[workload]
     out = {"workload": {"demo3d": "demo3D: Pulseq 3D stack of spirals with field-camera gradients, brain phantom "
@@ -126,6 +126,14 @@ def run(staged: str, runs: int = 4, modes=tuple(MODES), workload: str = "demo3d"
     for name in sig:
         if name != "plain_f64" and "plain_f64" in sig:
             out[name + "_nrmse_vs_plain_f64"] = _nrmse(sig[name], sig["plain_f64"])
+    if "split_f32" in sig and "plain_f64" in sig:
+        # the FP32-array run against plain FP64 on the same FP32-rounded inputs: the split path's own error
+        seqd32 = seqd.astype(np.float32).astype(np.float64)
+        obj32 = obj.astype(np.float32).astype(np.float64)
+        params = {"sim_method": method, "precision": "f64", "homs_precision": "plain"}
+        with prepare_simulation(obj32, seqd32, sim_params=params, context=ctx) as plan:
+            ref32 = plan.run()[:, :, 0] * get_adc_phase_compensation(hoseq).astype(np.complex128)[:, None]
+        out["split_f32_nrmse_vs_plain_f64_same_inputs"] = _nrmse(sig["split_f32"], ref32)
     ctx.close()
     return out
 
