@@ -18,7 +18,7 @@ import ctypes
 import math
 import time
 from dataclasses import dataclass, field
-from typing import Any, Dict, List, Optional, Tuple
+from typing import Any, Dict, List, NamedTuple, Optional, Tuple
 
 import numpy as np
 
@@ -36,6 +36,7 @@ __all__ = [
     "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage", "grad2traj", "traj2grad", "InterpTrajTime",
     "Grad", "RF", "ADC", "Sequence", "HO_Sequence", "MaxStepSizeRule", "discretize", "get_adc_sampling_times",
     "get_adc_phase_compensation", "get_block_start_times", "read_seq", "demo2d_sequence", "demo3d_sequence",
+    "Progress", "SimulationBlocks", "BlockData",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -277,6 +278,11 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence = None, sys=None, *, sim
     path.  Returns (Nadc, Nc, 1) complex for "mat", ``Mag`` for "state".
     The caller's dictionary is never modified.
 
+    ``callbacks`` (callables) are called after every block with
+    ``(Progress, SimulationBlocks, BlockData, sim_params)``, as the
+    reference's block loop calls them (SimulatorCore.jl:144-149); the blocks
+    then run one at a time, each from the state the previous one left.
+
     ``simulate(plan, return_type=...)`` runs a prepared ``Plan`` instead
     (``simulate(plan::PreparedSimulation)``, PreparedSimulation.jl:218-258).
     """
@@ -291,9 +297,6 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence = None, sys=None, *, sim
         raise ArgumentError("return_type is a sim_params key here; the keyword is for prepared simulations.")
     if seqd is None:
         raise ArgumentError("simulate needs a sequence (or a prepared simulation).")
-    if callbacks:
-        raise ArgumentError("callbacks run between blocks on the reference's Julia side; use the block entry points "
-                            "(homs_precession_block / homs_excitation_block) for per-block access.")
     obj, resident, sim_params = _resident_args(obj, sim_params)
     seqd, comp, native_adc = _sampled(seqd, sim_params)
     params, parts, excitation = _setup(obj, seqd, sim_params, parts, excitation, native_adc)
@@ -305,6 +308,9 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence = None, sys=None, *, sim
     if resident is not None and gpus is None:
         params["gpu_device"] = resident.device
     ctx = context or _context(int(params["gpu_device"]))
+    if callbacks:
+        sig, cur, seconds = _run_with_callbacks(obj, seqd, params, parts, excitation, state, ctx, callbacks)
+        return _finalize(params, sig, cur.xy, cur.z, parts, excitation, seqd, seconds, comp)
     dt = _dtype(params)
     keep = _lib._Keep()
     ph = _lib.host_phantom(obj, keep, dt) if resident is None else None
@@ -327,6 +333,62 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence = None, sys=None, *, sim
                    ctx.handle)
     seconds = time.perf_counter() - t0
     return _finalize(params, np.asarray(sig), xy, z, parts, excitation, seqd, seconds, comp)
+
+
+class Progress(NamedTuple):
+    """``progress_info`` of the reference's block loop (SimulatorCore.jl:144):
+    the block just finished (1-based), the number of blocks, RF blocks so far,
+    and the 1-based index of the next ADC sample."""
+    block: int
+    Nblocks: int
+    rfs: int
+    samples: int
+
+
+class SimulationBlocks(NamedTuple):
+    """``simulation_blocks_info``: excitation flag and 0-based inclusive node range of every block."""
+    excitation_bool: List[bool]
+    parts: List[Tuple[int, int]]
+
+
+class BlockData(NamedTuple):
+    """``device_data`` after a block: phantom, sampled sequence, the signal so
+    far (rows of later blocks still zero) and the spin state ``Xt``."""
+    obj: Any
+    seqd: Any
+    sig: np.ndarray
+    Xt: Mag
+
+
+def _run_with_callbacks(obj, seqd, params, parts, excitation, state, ctx, callbacks):
+    """The block loop of run_sim_time_iter! (SimulatorCore.jl:96-152) with its
+    callbacks: each block runs on the device by itself, from the state the
+    previous block left, and every callback is called after it with
+    ``(Progress, SimulationBlocks, BlockData, sim_params)`` on completed data."""
+    for cb in callbacks:
+        if not callable(cb):
+            raise ArgumentError("callbacks must be callables.")
+    method, prec, mode = params["sim_method"], params["precision"], params["homs_precision"]
+    cdt = np.complex128 if prec == "f64" else np.complex64
+    fdt = np.float64 if prec == "f64" else np.float32
+    nadc = sum(count_block_adc(seqd.adc, parts))
+    sig = np.zeros((nadc, obj.ncoils), dtype=cdt, order="F")
+    cur = state if state is not None else Mag(np.zeros(len(obj), cdt), np.asarray(obj.rho, fdt).copy())
+    info = SimulationBlocks(list(excitation), list(parts))
+    samples, rfs = 1, 0
+    t0 = time.perf_counter()
+    for b, ((f, l), e) in enumerate(zip(parts, excitation), start=1):
+        blk, xy, z = run_blocks(obj, seqd.view(f, l), [(0, l - f)], [e], method, prec, mode, cur, ctx,
+                                params["gamma"])
+        sig[samples - 1:samples - 1 + blk.shape[0]] = blk
+        samples += blk.shape[0]
+        rfs += int(bool(e))
+        cur = Mag(xy, z)
+        progress = Progress(b, len(parts), rfs, samples)
+        data = BlockData(obj, seqd, sig, cur)
+        for cb in callbacks:
+            cb(progress, info, data, params)
+    return sig, cur, time.perf_counter() - t0
 
 
 def run_blocks(obj: HO_Phantom, seqd: HO_DiscreteSequence, parts, excitation, method: BlochHighOrder,

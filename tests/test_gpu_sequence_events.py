@@ -126,3 +126,37 @@ def test_encoding_export_of_event_sequences(oracle, gpu_context):
         assert np.linalg.norm(got[:, j] - k_ref[:, j]) <= 1e-12 * scale
         qs = max(np.linalg.norm(kq_ref[:, j]), 1e-300)
         assert np.linalg.norm(got_q[:, j] - kq_ref[:, j]) <= 1e-12 * qs
+
+
+def test_callbacks_observe_every_block(gpu_context):
+    """test_koma_compatibility.jl:73-81: a callback after every block sees the
+    ADC samples done so far, in order, ending at 5; with callbacks the signal
+    equals the run without them."""
+    hoseq = HO_Sequence(W.compatibility_events())
+    obj = W.compatibility_event_phantom()
+    params = {"precision": "f64", "Nthreads": 1, "sim_method": BlochHighOrder("0000"), "return_type": "mat",
+              "Nblocks": 1}
+    signal = homs.simulate(obj, hoseq, sim_params=params, context=gpu_context)
+    seen, blocks = [], []
+
+    def callback(progress, info, data, p):
+        seen.append(progress.samples - 1)
+        blocks.append((progress.block, progress.Nblocks, len(info.parts), data.sig.shape, type(data.Xt).__name__))
+
+    split = homs.simulate(obj, hoseq, sim_params=dict(params, Nblocks=1000, Nthreads=2), context=gpu_context,
+                          callbacks=(callback,))
+    assert np.allclose(split, signal, atol=1e-12, rtol=0)
+    assert seen == sorted(seen) and seen[-1] == 5
+    assert [b[0] for b in blocks] == list(range(1, len(blocks) + 1))
+    assert all(b[1] == len(blocks) == b[2] and b[3] == (5, 2) and b[4] == "Mag" for b in blocks)
+    fields = HO_Sequence(W.compatibility_events())
+    fields.GR_dfc[0, 1] = Grad(20 / GAMMA, 1e-3)
+    for mode, tol in (("plain", 1e-12), ("split", 2e-6)):
+        p = dict(params, sim_method=BlochHighOrder("1111"), homs_precision=mode, Nblocks=3)
+        plainrun = homs.simulate(obj, fields, sim_params=p, context=gpu_context)
+        withcb = homs.simulate(obj, fields, sim_params=p, context=gpu_context, callbacks=(lambda *a: None,))
+        assert np.allclose(withcb, plainrun, atol=tol, rtol=0)
+        st = homs.simulate(obj, fields, sim_params=dict(p, return_type="state"), context=gpu_context,
+                           callbacks=(lambda *a: None,))
+        st0 = homs.simulate(obj, fields, sim_params=dict(p, return_type="state"), context=gpu_context)
+        assert np.allclose(st.xy, st0.xy, atol=tol) and np.allclose(st.z, st0.z, atol=tol)
