@@ -24,8 +24,8 @@ import numpy as np
 
 from . import _lib
 from ._lib import Context, HomsError
-from .model import (GAMMA, ArgumentError, BlochHighOrder, DimensionMismatch, HO_DiscreteSequence, HO_Phantom, Mag,
-                    count_block_adc, get_sim_ranges, initialize_spins_state, rf_break_lists, rf_events)
+from .model import (GAMMA, ArgumentError, Bloch, BlochHighOrder, DimensionMismatch, HO_DiscreteSequence, HO_Phantom,
+                    Mag, count_block_adc, get_sim_ranges, initialize_spins_state, rf_break_lists, rf_events)
 from .sequence import (ADC, RF, Grad, HO_Sequence, MaxStepSizeRule, Sequence, discretize, get_adc_phase_compensation,
                        get_adc_sampling_times, get_block_start_times, rf_pulses)
 
@@ -36,7 +36,7 @@ __all__ = [
     "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage", "grad2traj", "traj2grad", "InterpTrajTime",
     "Grad", "RF", "ADC", "Sequence", "HO_Sequence", "MaxStepSizeRule", "discretize", "get_adc_sampling_times",
     "get_adc_phase_compensation", "get_block_start_times", "read_seq", "demo2d_sequence", "demo3d_sequence",
-    "Progress", "SimulationBlocks", "BlockData",
+    "Progress", "SimulationBlocks", "BlockData", "Bloch",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -95,8 +95,8 @@ def _setup(obj: HO_Phantom, seqd: HO_DiscreteSequence, sim_params, parts=None, e
     if params["coil_combination"] not in HIGH_ORDER_COIL_COMBINATIONS:
         raise ArgumentError(f"Unknown coil_combination: {params['coil_combination']}.")
     method = params["sim_method"]
-    if not isinstance(method, BlochHighOrder):
-        raise ArgumentError("HO_Phantom currently supports BlochHighOrder() on this engine.")
+    if not isinstance(method, (BlochHighOrder, Bloch)):
+        raise ArgumentError("HO_Phantom currently supports Bloch() and BlochHighOrder().")
     if params["return_type"] not in ("mat", "state", "raw"):
         raise ArgumentError("return_type must be mat, state, or raw.")
     if params["precision"] not in ("f32", "f64"):
@@ -419,7 +419,7 @@ def run_blocks(obj: HO_Phantom, seqd: HO_DiscreteSequence, parts, excitation, me
         z = np.ascontiguousarray(np.asarray(state.z, dtype=fdt)).copy()
     st = _lib.State(xy.ctypes.data, z.ctypes.data, _lib.HOMS_HOST)
     opts = _lib.RunOptions()
-    opts.method = method.flags if isinstance(method, BlochHighOrder) else int(method)
+    opts.method = method.flags if isinstance(method, (BlochHighOrder, Bloch)) else int(method)
     opts.mode = _lib.HOMS_SPLIT if mode == "split" else _lib.HOMS_PLAIN
     _lib.check(_lib.load().homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
                                          ctypes.byref(st), sig.ctypes.data if nadc else None, _lib.HOMS_HOST),

@@ -78,6 +78,24 @@ class BlochHighOrder:
         return isinstance(other, BlochHighOrder) and self.flags == other.flags
 
 
+class Bloch:
+    """KomaMRICore's ``Bloch()`` on an ``HO_Phantom`` (accepted beside
+    ``BlochHighOrder`` by setup_simulation, Simulate.jl:85-86): the nominal
+    gradients and the off-resonance in both excitation and precession, no
+    measured fields -- the same physics as ``BlochHighOrder("0000")``."""
+
+    flags = DW_EXCITATION | DW_PRECESSION
+
+    def __repr__(self):
+        return "Bloch()"
+
+    def __eq__(self, other):
+        return isinstance(other, Bloch)
+
+    def __hash__(self):
+        return hash("Bloch")
+
+
 def _vec(a, n, default, dtype):
     if a is None:
         return np.full(n, default, dtype=dtype)

@@ -97,3 +97,21 @@ def test_execution_selection_and_block_lengths(gpu_context):
         raw = homs.simulate(obj, hoseq, sim_params=dict(p, return_type="raw"), context=gpu_context)
         assert sum(pr.shape[0] for pr in raw.profiles) == 5
         assert all(pr.shape[1] == 2 for pr in raw.profiles)
+
+
+def test_nominal_bloch_method_agrees_with_the_legacy_path(oracle, gpu_context):
+    """test_koma_compatibility.jl:107-115: Bloch() on an HO_Phantom runs the
+    nominal gradients only and agrees with the native path; here with
+    BlochHighOrder("0000") and with the oracle."""
+    hoseq = _fields(HO_Sequence(W.compatibility_events()))
+    obj = W.compatibility_event_phantom()
+    obj.dw[:] = [5.0, 25.0]
+    params = {"precision": "f64", "Nthreads": 1, "return_type": "mat"}
+    nominal = homs.simulate(obj, hoseq, sim_params=dict(params, sim_method=homs.Bloch()), context=gpu_context)
+    legacy = homs.simulate(obj, hoseq, sim_params=dict(params, sim_method=BlochHighOrder("0000")),
+                           context=gpu_context)
+    assert np.allclose(nominal, legacy, atol=1e-12, rtol=0)
+    seqd = discretize(hoseq)
+    parts, exc = get_sim_ranges(seqd)
+    ref = oracle.simulate_c(obj, seqd, parts, exc, homs.Bloch().flags)[0]
+    assert np.allclose(nominal[:, :, 0], ref, atol=1e-12, rtol=0)

@@ -94,3 +94,15 @@ def test_config2_size():
     n2 = sum(count_block_adc(w2.seq.adc, w2.parts))
     assert n2 == 4 * 9500 and w2.obj.ncoils == 32
     assert len(W.grid(100, 100, 35, 2e-3, 2e-3, 2e-3)[0]) == 350000
+
+
+def test_bloch_method_is_accepted_as_nominal_only():
+    import homs
+    from homs import workloads as W
+    from homs.model import Bloch, BlochHighOrder
+    seq, parts, exc, _ = W.compatibility_sequence()
+    obj = W.compatibility_phantom()
+    params, _, _ = homs._setup(obj, seq, {"sim_method": Bloch()})
+    assert params["sim_method"] == Bloch() and Bloch().flags == BlochHighOrder("0000").flags
+    with pytest.raises(homs.ArgumentError, match="Bloch"):
+        homs._setup(obj, seq, {"sim_method": "Bloch"})
