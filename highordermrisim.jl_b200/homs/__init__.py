@@ -36,7 +36,7 @@ __all__ = [
     "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage", "grad2traj", "traj2grad", "InterpTrajTime",
     "Grad", "RF", "ADC", "Sequence", "HO_Sequence", "MaxStepSizeRule", "discretize", "get_adc_sampling_times",
     "get_adc_phase_compensation", "get_block_start_times", "read_seq", "demo2d_sequence", "demo3d_sequence",
-    "Progress", "SimulationBlocks", "BlockData", "Bloch",
+    "Progress", "SimulationBlocks", "BlockData", "Bloch", "basisfunc_spha",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -697,4 +697,5 @@ class Server:
 from .phantom import brain_phantom, csm_birdcage  # noqa: E402
 from .trajectory import InterpTrajTime, grad2traj, traj2grad  # noqa: E402
 from .pulseq import read_seq  # noqa: E402
+from .sphericalharmonics import basisfunc_spha  # noqa: E402
 from .demo_inputs import demo2d_sequence, demo3d_sequence  # noqa: E402

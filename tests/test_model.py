@@ -106,3 +106,27 @@ def test_bloch_method_is_accepted_as_nominal_only():
     assert params["sim_method"] == Bloch() and Bloch().flags == BlochHighOrder("0000").flags
     with pytest.raises(homs.ArgumentError, match="Bloch"):
         homs._setup(obj, seq, {"sim_method": "Bloch"})
+
+
+def test_basisfunc_spha_terms():
+    """basisfunc_spha (basisfunction.jl:24-120): terms 1-16 are the basis the
+    simulation uses (the oracle's), and the higher orders are the solid
+    harmonics at closed-form points."""
+    from homs.sphericalharmonics import basisfunc_spha
+    from oracle import oracle as orc
+    rng = np.random.default_rng(5)
+    x, y, z = rng.uniform(-0.12, 0.12, (3, 50))
+    b = basisfunc_spha(x, y, z, list(range(1, 17)))
+    assert b.shape == (50, 16)
+    assert np.allclose(b, orc.basis_np(x, y, z), rtol=1e-13, atol=1e-18)
+    one = np.array([1.0])
+    zero = np.array([0.0])
+    assert basisfunc_spha(zero, zero, one, 21)[0] == 8.0          # 35 - 30 + 3
+    assert basisfunc_spha(one, zero, zero, 36)[0] == 1.0          # x^5
+    assert basisfunc_spha(zero, zero, one, 31)[0] == 8.0          # 63 - 70 + 15
+    assert basisfunc_spha(one, one, zero, 17)[0] == 0.0           # xy (x^2 - y^2)
+    assert basisfunc_spha(x, y, z, [36]).shape == (50, 1)
+    from homs.model import ArgumentError
+    with pytest.raises(ArgumentError):
+        basisfunc_spha(x, y, z, [37])
+    assert basisfunc_spha(x.astype(np.float32), y.astype(np.float32), z.astype(np.float32), [2]).dtype == np.float32
