@@ -233,3 +233,22 @@ def hophantom_brain(brain, brain_res, target_res, target_matrix, location=(0.0, 
         cmap = resample_csm(c, csm_res, target_res, target_matrix, location)[..., :ncoils]
     return brain_phantom(labels, target_res, offcenter, fieldstrength=fieldstrength, fieldmap=fieldmap, csm=cmap,
                          context=context)
+
+
+def generate_grid(fov, matrix_size) -> np.ndarray:
+    """(nR, nP, nS, 3) voxel centres in metres (generate_grid,
+    src/grid/Grid.jl:64-108): ((0:n-1) - (n-1)/2) * fov/n along each axis."""
+    if len(fov) != 3 or len(matrix_size) != 3:
+        raise ArgumentError("Both fov and matrix_size must be 3-element vectors.")
+    if not all(np.isfinite(v) and float(v) == int(v) and v > 0 for v in matrix_size):
+        raise ArgumentError("Matrix dimensions must be positive integers.")
+    f = np.asarray(fov, dtype=np.float64)
+    if not np.all(np.isfinite(f)) or np.any(f <= 0):
+        raise ArgumentError("The field of view must be finite and positive.")
+    n = [int(v) for v in matrix_size]
+    grid = np.empty((n[0], n[1], n[2], 3))
+    for k in range(3):
+        shape = [1, 1, 1]
+        shape[k] = n[k]
+        grid[..., k] = _axis(n[k], f[k] / n[k]).reshape(shape)
+    return grid

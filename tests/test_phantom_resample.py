@@ -136,3 +136,17 @@ def test_real_receive_map_border():
     assert np.all(beyond == 0)
     full = resample_csm(src, res, res, (2, 3, 1), (0.0, 0.0, 0.0))
     assert full.shape == (2, 3, 1, 32) and np.all(np.isfinite(full))
+
+
+def test_generate_grid():
+    """generate_grid (src/grid/Grid.jl:64-108) against the oracle's grid, and its argument checks."""
+    from homs.phantom import generate_grid
+    from oracle import oracle as orc
+    for fov, n in (((0.2, 0.2, 0.07), (100, 100, 35)), ((0.1, 0.05, 0.004), (3, 4, 1))):
+        assert np.array_equal(generate_grid(fov, n), orc.generate_grid_np(fov, n))
+    with pytest.raises(ArgumentError):
+        generate_grid((0.2, 0.2), (4, 4, 4))
+    with pytest.raises(ArgumentError):
+        generate_grid((0.2, 0.2, 0.2), (4, 4.5, 4))
+    with pytest.raises(ArgumentError):
+        generate_grid((0.2, -0.2, 0.2), (4, 4, 4))
