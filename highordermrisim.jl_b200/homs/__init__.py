@@ -14,6 +14,7 @@ fallback: without the library or a B200 the calls raise ``HomsError``.
 """
 from __future__ import annotations
 
+import copy
 import ctypes
 import math
 import time
@@ -289,10 +290,7 @@ def simulate(obj: HO_Phantom, seqd: HO_DiscreteSequence = None, sys=None, *, sim
     if isinstance(obj, Plan):
         if seqd is not None or sim_params is not None or parts is not None or state is not None:
             raise ArgumentError("A prepared simulation takes only return_type (and callbacks, verbose).")
-        if callbacks:
-            raise ArgumentError("callbacks run between blocks on the reference's Julia side; use the block entry "
-                                "points (homs_precession_block / homs_excitation_block) for per-block access.")
-        return obj.run(return_type)
+        return obj.run(return_type, callbacks)
     if return_type is not None:
         raise ArgumentError("return_type is a sim_params key here; the keyword is for prepared simulations.")
     if seqd is None:
@@ -501,6 +499,7 @@ class Plan:
         self.params = params
         self.parts, self.excitation = parts, excitation
         self.seqd = seqd
+        self._host = copy.deepcopy(obj)  # snapshot for runs with callbacks (block by block)
         self.ctx = context or _context(int(params["gpu_device"]))
         self.dtype = _dtype(params)
         self.ns, self.nc = len(obj), obj.ncoils
@@ -515,13 +514,22 @@ class Plan:
         self.handle = h
         self.closed = False
 
-    def run(self, return_type=None):
+    def run(self, return_type=None, callbacks=()):
+        """One run from Mxy = 0, Mz = rho.  With ``callbacks`` the run goes block
+        by block from the plan's snapshot of the phantom, calling each callback
+        after every block as ``simulate`` does."""
         if return_type is None:
             return_type = self.params["return_type"]
         if return_type not in ("mat", "state", "raw"):
             raise ArgumentError("return_type must be mat, state, or raw.")
         if self.closed:
             raise ArgumentError("The prepared simulation is closed.")
+        if callbacks:
+            params = dict(self.params)
+            params["return_type"] = return_type
+            sig, cur, seconds = _run_with_callbacks(self._host, self.seqd, params, self.parts, self.excitation, None,
+                                                    self.ctx, callbacks)
+            return _finalize(params, sig, cur.xy, cur.z, self.parts, self.excitation, self.seqd, seconds, self.comp)
         cdt = np.complex128 if self.dtype == _lib.HOMS_F64 else np.complex64
         fdt = np.float64 if self.dtype == _lib.HOMS_F64 else np.float32
         sig = np.zeros((self.nadc, self.nc), dtype=cdt, order="F")

@@ -350,3 +350,11 @@ def test_prepared_plan_reuse(gpu_context, precision):
     assert np.array_equal(got[1].xy, expected_state.xy) and got[2].closed
     with pytest.raises(homs.ArgumentError):
         homs.simulate(got[2])
+    # callbacks on a prepared simulation: after every block, with the same result
+    seen = []
+    with homs.prepare_simulation(obj, seq, sim_params=params) as plan:
+        cb = homs.simulate(plan, callbacks=(lambda pr, info, data, p: seen.append(pr.block),))
+        assert np.allclose(cb, baseline, atol=1e-11 if precision == "f64" else 3e-5, rtol=0)
+        assert seen == list(range(1, len(plan.parts) + 1))
+        st = plan.run(return_type="state", callbacks=(lambda *a: None,))
+        assert np.allclose(st.xy, expected_state.xy, atol=1e-11 if precision == "f64" else 3e-5)
