@@ -102,15 +102,22 @@ def _vec(a, n, default, dtype):
     return np.asarray(a, dtype=dtype)
 
 
+_SPIN_FIELDS = ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw", "Dlambda1", "Dlambda2", "Dtheta")
+
+
 class HO_Phantom:
     """Spin phantom with receive sensitivities (``src/datatypes/HO_Phantom.jl:47-71``).
 
     Omitting ``csm`` gives one ideal receive coil with sensitivity ``1+0j`` at
-    every spin.  Positions in metres, T1/T2 in seconds, ``dw`` in rad/s.
+    every spin.  Positions in metres, T1/T2 in seconds, ``dw`` in rad/s.  The
+    diffusion parameters ``Dlambda1``, ``Dlambda2``, ``Dtheta`` (Julia's Dλ1,
+    Dλ2, Dθ) are carried along and not used by BlochHighOrder.  ``a + b``
+    concatenates spins, ``alpha * obj`` scales the proton density only
+    (HO_Phantom.jl:181-233).
     """
 
     def __init__(self, x, y=None, z=None, rho=None, T1=None, T2=None, T2s=None, dw=None, csm=None,
-                 name="spins", dtype=np.float64):
+                 name="spins", dtype=np.float64, Dlambda1=None, Dlambda2=None, Dtheta=None):
         x = np.asarray(x, dtype=dtype)
         n = x.shape[0] if x.ndim else 1
         self.name = name
@@ -122,6 +129,9 @@ class HO_Phantom:
         self.T2 = _vec(T2, n, 1_000_000.0, dtype)
         self.T2s = _vec(T2s, n, 1_000_000.0, dtype)
         self.dw = _vec(dw, n, 0.0, dtype)
+        self.Dlambda1 = _vec(Dlambda1, n, 0.0, dtype)
+        self.Dlambda2 = _vec(Dlambda2, n, 0.0, dtype)
+        self.Dtheta = _vec(Dtheta, n, 0.0, dtype)
         cdt = np.complex64 if np.dtype(dtype) == np.float32 else np.complex128
         # Column-major, as the reference's Julia arrays and the C ABI: the
         # array crosses to libhoms without a per-call transpose.
@@ -141,7 +151,7 @@ class HO_Phantom:
     def validate(self):
         """Storage checks of ``validate_phantom`` (HO_Phantom.jl:97-109)."""
         n = len(self)
-        for name in ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw"):
+        for name in _SPIN_FIELDS:
             v = getattr(self, name)
             if v.ndim != 1 or v.shape[0] != n:
                 raise DimensionMismatch(f"Phantom field {name} must contain one value per spin.")
@@ -155,7 +165,7 @@ class HO_Phantom:
             sl = slice(int(idx), int(idx) + 1)
         out = HO_Phantom.__new__(HO_Phantom)
         out.name = self.name
-        for k in ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw"):
+        for k in _SPIN_FIELDS:
             setattr(out, k, getattr(self, k)[sl])
         out.csm = self.csm[sl]
         return out
@@ -163,10 +173,56 @@ class HO_Phantom:
     def astype(self, dtype):
         out = HO_Phantom.__new__(HO_Phantom)
         out.name = self.name
-        for k in ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw"):
+        for k in _SPIN_FIELDS:
             setattr(out, k, np.asarray(getattr(self, k), dtype=dtype))
         out.csm = np.asfortranarray(self.csm, dtype=np.complex64 if np.dtype(dtype) == np.float32 else np.complex128)
         return out
+
+    def __repr__(self):
+        ns, nc = self.csm.shape
+        head = f"HO_Phantom[{self.name} | nCoil={nc} | nSpin={ns} | "
+        if self.x.shape[0] == 0:
+            return head + "empty ]"
+
+        def span(v):
+            lo, hi = (round(float(f) * 1e2, 2) for f in (np.min(v), np.max(v)))
+            return f"{lo}:{hi} cm"
+        return head + f"x={span(self.x)} | y={span(self.y)} | z={span(self.z)} ]"
+
+    def __iter__(self):
+        for i in range(len(self)):
+            yield self[i]
+
+    def __add__(self, other: "HO_Phantom") -> "HO_Phantom":
+        self.validate()
+        other.validate()
+        if self.ncoils != other.ncoils:
+            raise DimensionMismatch("Concatenated phantoms must have the same number of receive coils.")
+        out = HO_Phantom.__new__(HO_Phantom)
+        out.name = f"{self.name}+{other.name}"
+        for k in _SPIN_FIELDS:
+            setattr(out, k, np.concatenate([getattr(self, k), getattr(other, k)]))
+        out.csm = np.asfortranarray(np.concatenate([self.csm, other.csm], axis=0))
+        return out
+
+    def __mul__(self, alpha):
+        if isinstance(alpha, (complex, np.complexfloating)) or not np.isscalar(alpha):
+            return NotImplemented
+        out = HO_Phantom.__new__(HO_Phantom)
+        out.name = self.name
+        for k in _SPIN_FIELDS:
+            setattr(out, k, getattr(self, k))
+        out.rho = alpha * self.rho
+        out.csm = self.csm
+        return out
+
+    __rmul__ = __mul__
+
+    def allclose(self, other: "HO_Phantom", rtol=1e-5, atol=1e-8) -> bool:
+        """Field-wise closeness, as ``isapprox`` of two phantoms (HO_Phantom.jl:112-126)."""
+        return (len(self) == len(other) and self.csm.shape == other.csm.shape
+                and all(np.allclose(getattr(self, k), getattr(other, k), rtol=rtol, atol=atol) for k in _SPIN_FIELDS)
+                and np.allclose(self.csm, other.csm, rtol=rtol, atol=atol))
 
 
 class HO_DiscreteSequence:

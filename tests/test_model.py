@@ -130,3 +130,45 @@ def test_basisfunc_spha_terms():
     with pytest.raises(ArgumentError):
         basisfunc_spha(x, y, z, [37])
     assert basisfunc_spha(x.astype(np.float32), y.astype(np.float32), z.astype(np.float32), [2]).dtype == np.float32
+
+
+def test_phantom_display_defaults_and_container():
+    """test_phantom_construction.jl:7-76 and HO_Phantom.jl:74-233: the summary
+    string, the ideal default coil and defaults per spin, concatenation and
+    density scaling."""
+    from homs.model import DimensionMismatch, HO_Phantom
+    for dt in (np.float32, np.float64):
+        obj = HO_Phantom(x=np.zeros(0, dt), dtype=dt)
+        assert repr(obj) == "HO_Phantom[spins | nCoil=1 | nSpin=0 | empty ]" and obj.csm.shape == (0, 1)
+        for nc in (0, 2):
+            e = HO_Phantom(name="empty", x=np.zeros(0, dt), csm=np.zeros((0, nc)), dtype=dt)
+            assert repr(e) == f"HO_Phantom[empty | nCoil={nc} | nSpin=0 | empty ]"
+        obj = HO_Phantom(name="display", x=[-0.125, 0.25], y=[0.5, -0.75], z=[-1, 1.5], csm=np.ones((2, 2)),
+                         dtype=dt)
+        assert repr(obj) == ("HO_Phantom[display | nCoil=2 | nSpin=2 | x=-12.5:25.0 cm | y=-75.0:50.0 cm | "
+                             "z=-100.0:150.0 cm ]")
+        assert repr(obj[0:0]) == "HO_Phantom[display | nCoil=2 | nSpin=0 | empty ]"
+        for n in (0, 1, 3):
+            o = HO_Phantom(x=np.zeros(n, dt), dtype=dt)
+            assert o.csm.shape == (n, 1) and np.all(o.csm == 1)
+            for k in ("y", "z", "dw", "Dlambda1", "Dlambda2", "Dtheta"):
+                assert np.array_equal(getattr(o, k), np.zeros(n)) and getattr(o, k).dtype == dt
+            assert np.array_equal(o.rho, np.ones(n))
+            for k in ("T1", "T2", "T2s"):
+                assert np.array_equal(getattr(o, k), np.full(n, 1_000_000.0))
+            other = HO_Phantom(x=np.zeros(n, dt), dtype=dt)
+            if n:
+                o.csm[0, 0] = 0
+                assert np.all(other.csm == 1)
+    a = HO_Phantom(name="a", x=[0.0, 0.01], rho=[1.0, 0.5], csm=np.ones((2, 3)))
+    b = HO_Phantom(name="b", x=[0.02], rho=[0.25], csm=2 * np.ones((1, 3)), Dtheta=[0.3])
+    ab = a + b
+    assert ab.name == "a+b" and len(ab) == 3 and ab.csm.shape == (3, 3)
+    assert np.array_equal(ab.rho, [1.0, 0.5, 0.25]) and np.array_equal(ab.Dtheta, [0, 0, 0.3])
+    assert np.array_equal(ab.csm[2], [2, 2, 2])
+    with pytest.raises(DimensionMismatch):
+        a + HO_Phantom(x=[0.0], csm=np.ones((1, 2)))
+    s = 2.0 * a
+    assert np.array_equal(s.rho, [2.0, 1.0]) and s.x is a.x and s.allclose(a * 2.0)
+    assert not s.allclose(a) and a.allclose(a[0:2])
+    assert [len(p) for p in a] == [1, 1]
