@@ -112,6 +112,9 @@ def _setup(obj: HO_Phantom, seqd: HO_DiscreteSequence, sim_params, parts=None, e
     obj.validate()
     if len(obj) == 0:
         raise ArgumentError("The phantom must contain at least one spin.")
+    if not obj.has_static_coordinates():
+        raise ArgumentError("Moving phantoms (ux, uy, uz) need the reference's array path; the libhoms kernels, "
+                            "like the reference's CUDA kernels, simulate static coordinates.")
     if obj.ncoils < 1:
         raise ArgumentError("The CSM must contain at least one coil.")
     seqd.validate()

@@ -103,6 +103,12 @@ def _vec(a, n, default, dtype):
 
 
 _SPIN_FIELDS = ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw", "Dlambda1", "Dlambda2", "Dtheta")
+_MOTION = ("ux", "uy", "uz")
+
+
+def no_displacement(x, y, z, t):
+    """The static phantom's displacement (HO_Phantom.jl:1)."""
+    return 0
 
 
 class HO_Phantom:
@@ -111,13 +117,21 @@ class HO_Phantom:
     Omitting ``csm`` gives one ideal receive coil with sensitivity ``1+0j`` at
     every spin.  Positions in metres, T1/T2 in seconds, ``dw`` in rad/s.  The
     diffusion parameters ``Dlambda1``, ``Dlambda2``, ``Dtheta`` (Julia's Dλ1,
-    Dλ2, Dθ) are carried along and not used by BlochHighOrder.  ``a + b``
-    concatenates spins, ``alpha * obj`` scales the proton density only
+    Dλ2, Dθ) are carried along and not used by BlochHighOrder.  ``ux``, ``uy``,
+    ``uz`` are displacement functions f(x, y, z, t); the engine's kernels, like
+    the reference's, need static coordinates (``no_displacement``).  ``a + b``
+    concatenates spins (non-empty phantoms must share their displacement
+    functions), ``alpha * obj`` scales the proton density only
     (HO_Phantom.jl:181-233).
     """
 
     def __init__(self, x, y=None, z=None, rho=None, T1=None, T2=None, T2s=None, dw=None, csm=None,
-                 name="spins", dtype=np.float64, Dlambda1=None, Dlambda2=None, Dtheta=None):
+                 name="spins", dtype=np.float64, Dlambda1=None, Dlambda2=None, Dtheta=None,
+                 ux=no_displacement, uy=no_displacement, uz=no_displacement):
+        for f in (ux, uy, uz):
+            if not callable(f):
+                raise ArgumentError("ux, uy and uz must be functions of (x, y, z, t).")
+        self.ux, self.uy, self.uz = ux, uy, uz
         x = np.asarray(x, dtype=dtype)
         n = x.shape[0] if x.ndim else 1
         self.name = name
@@ -167,6 +181,8 @@ class HO_Phantom:
         out.name = self.name
         for k in _SPIN_FIELDS:
             setattr(out, k, getattr(self, k)[sl])
+        for k in _MOTION:
+            setattr(out, k, getattr(self, k))
         out.csm = self.csm[sl]
         return out
 
@@ -175,6 +191,8 @@ class HO_Phantom:
         out.name = self.name
         for k in _SPIN_FIELDS:
             setattr(out, k, np.asarray(getattr(self, k), dtype=dtype))
+        for k in _MOTION:
+            setattr(out, k, getattr(self, k))
         out.csm = np.asfortranarray(self.csm, dtype=np.complex64 if np.dtype(dtype) == np.float32 else np.complex128)
         return out
 
@@ -198,8 +216,13 @@ class HO_Phantom:
         other.validate()
         if self.ncoils != other.ncoils:
             raise DimensionMismatch("Concatenated phantoms must have the same number of receive coils.")
+        if len(self) and len(other) and not all(getattr(self, k) is getattr(other, k) for k in _MOTION):
+            raise ArgumentError("Cannot concatenate phantoms with different motion functions.")
+        motion = other if len(self) == 0 else self
         out = HO_Phantom.__new__(HO_Phantom)
         out.name = f"{self.name}+{other.name}"
+        for k in _MOTION:
+            setattr(out, k, getattr(motion, k))
         for k in _SPIN_FIELDS:
             setattr(out, k, np.concatenate([getattr(self, k), getattr(other, k)]))
         out.csm = np.asfortranarray(np.concatenate([self.csm, other.csm], axis=0))
@@ -213,8 +236,13 @@ class HO_Phantom:
         for k in _SPIN_FIELDS:
             setattr(out, k, getattr(self, k))
         out.rho = alpha * self.rho
+        for k in _MOTION:
+            setattr(out, k, getattr(self, k))
         out.csm = self.csm
         return out
+
+    def has_static_coordinates(self) -> bool:
+        return all(getattr(self, k) is no_displacement for k in _MOTION)
 
     __rmul__ = __mul__
 

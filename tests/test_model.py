@@ -172,3 +172,47 @@ def test_phantom_display_defaults_and_container():
     assert np.array_equal(s.rho, [2.0, 1.0]) and s.x is a.x and s.allclose(a * 2.0)
     assert not s.allclose(a) and a.allclose(a[0:2])
     assert [len(p) for p in a] == [1, 1]
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_phantom_interfaces_and_input_validation(dt):
+    """test_phantom_interfaces.jl:7-49: iteration; malformed fields fail with
+    DimensionMismatch before any device is touched (simulate and
+    prepare_simulation, Bloch() and BlochHighOrder); displacement functions
+    follow the concatenation rules and moving phantoms are refused by the
+    kernels."""
+    import copy as _copy
+
+    import homs
+    from homs import workloads as W
+    from homs.model import Bloch, BlochHighOrder, DimensionMismatch, HO_Phantom
+    from homs.sequence import HO_Sequence
+    empty = HO_Phantom(x=np.zeros(0, dt), dtype=dt)
+    assert list(empty) == []
+    obj = HO_Phantom(x=np.array([0, 0.01, -0.02], dt), dtype=dt)
+    assert [s.x[0] for s in obj] == list(obj.x)
+    params = {"precision": "f32" if dt == np.float32 else "f64", "Nthreads": 1, "return_type": "mat"}
+    hoseq = HO_Sequence(W.compatibility_events())
+    for name in ("x", "y", "z", "rho", "T1", "T2", "T2s", "dw", "Dlambda1", "Dlambda2", "Dtheta"):
+        bad = _copy.deepcopy(obj)
+        setattr(bad, name, np.zeros(2, dt))
+        for method in (Bloch(), BlochHighOrder("1111")):
+            with pytest.raises(DimensionMismatch):
+                homs.simulate(bad, hoseq, sim_params=dict(params, sim_method=method))
+        with pytest.raises(DimensionMismatch):
+            homs.prepare_simulation(bad, hoseq, sim_params=dict(params, sim_method=BlochHighOrder("1111")))
+    for axis in ("ux", "uy", "uz"):
+        moving = _copy.deepcopy(obj)
+
+        def displacement(x, y, z, t):
+            return t
+        setattr(moving, axis, displacement)
+        with pytest.raises(homs.ArgumentError):
+            obj + moving
+        with pytest.raises(homs.ArgumentError):
+            moving + obj
+        joined = moving + moving
+        assert getattr(joined, axis) is displacement and np.array_equal(joined.rho, np.concatenate([moving.rho] * 2))
+        assert getattr(empty + moving, axis) is displacement and getattr(moving + empty, axis) is displacement
+        with pytest.raises(homs.ArgumentError, match="static"):
+            homs.simulate(moving, hoseq, sim_params=dict(params, sim_method=BlochHighOrder("1111")))
