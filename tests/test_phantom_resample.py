@@ -150,3 +150,32 @@ def test_generate_grid():
         generate_grid((0.2, 0.2, 0.2), (4, 4.5, 4))
     with pytest.raises(ArgumentError):
         generate_grid((0.2, -0.2, 0.2), (4, 4, 4))
+
+
+BRAIN_MAT = os.path.join(REF, "src", "phantom", "brain3D_0.5_0.5_0.5.mat")
+B0_MAT = os.path.join(REF, "src", "phantom", "b0map", "b0_4p0.mat")
+
+
+@pytest.mark.skipif(not (os.path.exists(BRAIN_MAT) and os.path.exists(CSM_MAT) and os.path.exists(B0_MAT)),
+                    reason="the reference's phantom volumes are not present")
+def test_real_volumes_on_target_grids():
+    """test_HOPhantom.jl: the brain phantom's volumes at 2 mm on the reference's
+    2D and 3D target matrices and orientations (the device build itself is
+    covered by the GPU tests on synthetic volumes)."""
+    import scipy.io as sio
+    from homs.phantom import generate_grid
+    brain = sio.loadmat(BRAIN_MAT)["data"]
+    csm = sio.loadmat(CSM_MAT)["csm"]
+    b0 = sio.loadmat(B0_MAT)["b0"]
+    res = (2e-3,) * 3
+    for tm in ((100, 100, 10), (1, 100, 100), (100, 1, 100), (100, 100, 1), (10, 100, 100), (100, 10, 100)):
+        lab = resample_labels(brain, (0.5e-3,) * 3, res, tm, (0.0, 0.0, 0.0))
+        assert lab.shape == tm and lab.dtype == np.uint8 and (lab != 0).sum() > 0
+        assert generate_grid(np.array(tm) * 2e-3, tm).shape == tm + (3,)
+    tm = (100, 100, 10)
+    cm = resample_csm(csm, (4e-3,) * 3, res, tm, (0.0, 0.0, 0.0))
+    assert cm.shape == tm + (32,) and np.all(np.isfinite(cm))
+    nz = np.abs(cm).sum(axis=3) > 0
+    assert np.allclose(np.sum(np.abs(cm[nz]) ** 2, axis=1), 1, rtol=1e-12)
+    fm = resample_b0(b0, (4e-3,) * 3, res, tm, (0.0, 0.0, 0.0))
+    assert fm.shape == tm and np.all(np.isfinite(fm))
