@@ -37,7 +37,7 @@ __all__ = [
     "rf_events", "ResidentPhantom", "brain_phantom", "csm_birdcage", "grad2traj", "traj2grad", "InterpTrajTime",
     "Grad", "RF", "ADC", "Sequence", "HO_Sequence", "MaxStepSizeRule", "discretize", "get_adc_sampling_times",
     "get_adc_phase_compensation", "get_block_start_times", "read_seq", "demo2d_sequence", "demo3d_sequence",
-    "Progress", "SimulationBlocks", "BlockData", "Bloch", "basisfunc_spha", "generate_grid", "hophantom_brain",
+    "Progress", "SimulationBlocks", "BlockData", "Bloch", "basisfunc_spha", "generate_grid", "hophantom_brain", "Grid",
 ]
 
 # Accepted for source compatibility; every choice runs the fused libhoms kernel
@@ -705,7 +705,7 @@ class Server:
         self.close()
 
 
-from .phantom import brain_phantom, csm_birdcage, generate_grid, hophantom_brain  # noqa: E402
+from .phantom import Grid, brain_phantom, csm_birdcage, generate_grid, hophantom_brain  # noqa: E402
 from .trajectory import InterpTrajTime, grad2traj, traj2grad  # noqa: E402
 from .pulseq import read_seq  # noqa: E402
 from .sphericalharmonics import basisfunc_spha  # noqa: E402

@@ -240,7 +240,7 @@ def generate_grid(fov, matrix_size) -> np.ndarray:
     src/grid/Grid.jl:64-108): ((0:n-1) - (n-1)/2) * fov/n along each axis."""
     if len(fov) != 3 or len(matrix_size) != 3:
         raise ArgumentError("Both fov and matrix_size must be 3-element vectors.")
-    if not all(np.isfinite(v) and float(v) == int(v) and v > 0 for v in matrix_size):
+    if not all(np.isfinite(v) and v > 0 and float(v) == int(v) for v in matrix_size):
         raise ArgumentError("Matrix dimensions must be positive integers.")
     f = np.asarray(fov, dtype=np.float64)
     if not np.all(np.isfinite(f)) or np.any(f <= 0):
@@ -252,3 +252,42 @@ def generate_grid(fov, matrix_size) -> np.ndarray:
         shape[k] = n[k]
         grid[..., k] = _axis(n[k], f[k] / n[k]).reshape(shape)
     return grid
+
+
+class Grid:
+    """Voxel-centre grid of nX x nY x nZ voxels (Grid, src/grid/Grid.jl:1-58):
+    ``x``, ``y``, ``z`` are flattened with x fastest, centred, in the
+    spacing's float type; ``exchange_xy`` and ``reverse_x/y/z`` reorder them
+    as the reference does."""
+
+    def __init__(self, nX: int, nY: int, nZ: int, dx, dy, dz, exchange_xy=False, reverse_x=False, reverse_y=False,
+                 reverse_z=False):
+        if not all(int(n) == n and n > 0 for n in (nX, nY, nZ)):
+            raise ArgumentError("Grid dimensions must be positive.")
+        if not all(np.isfinite(v) and v > 0 for v in (dx, dy, dz)):
+            raise ArgumentError("Grid spacing must be finite and positive.")
+        dt = np.result_type(np.asarray(dx).dtype, np.asarray(dy).dtype, np.asarray(dz).dtype)
+        if not np.issubdtype(dt, np.floating):
+            dt = np.float64
+        nX, nY, nZ = int(nX), int(nY), int(nZ)
+        zz, yy, xx = np.meshgrid(np.arange(1, nZ + 1), np.arange(1, nY + 1), np.arange(1, nX + 1), indexing="ij")
+        x = (xx.ravel() - (nX + 1) / 2) * float(dx)
+        y = (yy.ravel() - (nY + 1) / 2) * float(dy)
+        z = (zz.ravel() - (nZ + 1) / 2) * float(dz)
+        if exchange_xy:
+            x, y = y, x
+        if reverse_x:
+            x = x[::-1]
+        if reverse_y:
+            y = y[::-1]
+        if reverse_z:
+            z = z[::-1]
+        self.nX, self.nY, self.nZ = nX, nY, nZ
+        self.dx, self.dy, self.dz = dx, dy, dz
+        self.x, self.y, self.z = (np.ascontiguousarray(v, dtype=dt) for v in (x, y, z))
+        self.matrixSize = (nX, nY, nZ)
+        self.resolution = (dx, dy, dz)
+
+    def __repr__(self):
+        r = [round(float(v) * 1e3, 2) for v in self.resolution]
+        return f"Grid [ MatrixSize: {self.nX} x {self.nY} x {self.nZ}, Resolution: {r[0]} x {r[1]} x {r[2]} mm³ ]"

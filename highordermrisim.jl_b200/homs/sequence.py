@@ -330,8 +330,16 @@ class Sequence:
     not interpreted)."""
 
     def __init__(self, GR=None, RF_=None, ADC_=None, DUR=None):
+        if GR is None and RF_ is None and ADC_ is None and DUR is None:
+            # Sequence(): no blocks, to be built up with ``seq += event``
+            z = np.empty((3, 0), dtype=object)
+            self.GR, self.RF, self.ADC, self.DUR = z, np.empty((1, 0), dtype=object), np.empty(0, dtype=object), \
+                np.zeros(0)
+            self.DEF, self.EXT = {}, np.zeros(0, dtype=np.int64)
+            return
         if GR is None:
-            GR = [[Grad(0.0, 0.0)] for _ in range(3)]
+            n = len(ADC_) if ADC_ is not None else (np.shape(RF_)[-1] if RF_ is not None else len(DUR))
+            GR = [[Grad(0.0, 0.0)] * n for _ in range(3)]
         gr = _objects(GR, Grad, "GR")
         if gr.ndim == 1:
             gr = gr.reshape(-1, 1)
@@ -394,7 +402,21 @@ class Sequence:
             idx = [int(idx)]
         return Sequence._raw(self.GR[:, idx], self.RF[:, idx], self.ADC[idx], self.DUR[idx], self.DEF, self.EXT[idx])
 
-    def __add__(self, other: "Sequence") -> "Sequence":
+    @staticmethod
+    def block(event) -> "Sequence":
+        """One block holding a single event: an RF pulse, an ADC window or an
+        x gradient (KomaMRIBase's ``seq + event``)."""
+        if isinstance(event, RF):
+            return Sequence([[Grad(0.0, 0.0)]] * 3, [event], [ADC(0, 0.0)])
+        if isinstance(event, ADC):
+            return Sequence([[Grad(0.0, 0.0)]] * 3, [RF(0.0, 0.0)], [event])
+        if isinstance(event, Grad):
+            return Sequence([[event], [Grad(0.0, 0.0)], [Grad(0.0, 0.0)]])
+        raise ArgumentError("A block holds a Sequence, an RF, an ADC or a Grad.")
+
+    def __add__(self, other) -> "Sequence":
+        if not isinstance(other, Sequence):
+            other = Sequence.block(other)
         return Sequence._raw(np.concatenate([self.GR, other.GR], axis=1), np.concatenate([self.RF, other.RF], axis=1),
                              np.concatenate([self.ADC, other.ADC]), np.concatenate([self.DUR, other.DUR]),
                              {**other.DEF, **self.DEF}, np.concatenate([self.EXT, other.EXT]))

@@ -179,3 +179,38 @@ def test_real_volumes_on_target_grids():
     assert np.allclose(np.sum(np.abs(cm[nz]) ** 2, axis=1), 1, rtol=1e-12)
     fm = resample_b0(b0, (4e-3,) * 3, res, tm, (0.0, 0.0, 0.0))
     assert fm.shape == tm and np.all(np.isfinite(fm))
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+def test_voxel_centre_grid_geometry(dt):
+    """test_grid.jl: generate_grid's centres and argument checks, and Grid's
+    flattened coordinates against them."""
+    from homs.phantom import Grid, generate_grid
+    fov = np.array([0.2, 0.3, 0.004], dt)
+    dims = [2, 3, 1]
+    xyz = generate_grid(fov, dims)
+    assert xyz.shape == (2, 3, 1, 3) and xyz.dtype == np.float64
+    assert np.allclose(xyz[:, 0, 0, 0], np.array([-1, 1]) * float(fov[0]) / 4)
+    assert np.allclose(xyz[0, :, 0, 1], np.array([-1, 0, 1]) * float(fov[1]) / 3)
+    assert np.all(xyz[..., 2] == 0)
+    spacing = (fov / np.array(dims)).astype(dt)
+    g = Grid(*dims, *spacing)
+    for axis, v in enumerate((g.x, g.y, g.z)):
+        assert v.dtype == dt
+        assert np.allclose(v, xyz[..., axis].ravel(order="F"), atol=np.finfo(dt).eps)
+    with pytest.raises(ArgumentError):
+        Grid(0, 3, 1, *spacing)
+    with pytest.raises(ArgumentError):
+        Grid(2, 3, 1, dt(0), spacing[1], spacing[2])
+    with pytest.raises(ArgumentError):
+        Grid(2, 3, 1, dt(np.inf), spacing[1], spacing[2])
+    for bad_fov in ([0.0, 0.2, 0.2], [-1.0, 0.2, 0.2], [np.inf, 0.2, 0.2], [np.nan, 0.2, 0.2]):
+        with pytest.raises(ArgumentError):
+            generate_grid(bad_fov, [2, 3, 1])
+    for bad_dims in ([0, 3, 1], [-1, 3, 1], [1.5, 3, 1], [np.inf, 3, 1], [np.nan, 3, 1]):
+        with pytest.raises(ArgumentError):
+            generate_grid([0.2, 0.3, 0.004], bad_dims)
+    with pytest.raises(ArgumentError):
+        generate_grid([0.2, 0.3], [2, 3, 1])
+    assert repr(Grid(100, 100, 35, 0.002, 0.002, 0.002)) == \
+        "Grid [ MatrixSize: 100 x 100 x 35, Resolution: 2.0 x 2.0 x 2.0 mm³ ]"
