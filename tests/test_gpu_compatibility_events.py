@@ -115,3 +115,37 @@ def test_nominal_bloch_method_agrees_with_the_legacy_path(oracle, gpu_context):
     parts, exc = get_sim_ranges(seqd)
     ref = oracle.simulate_c(obj, seqd, parts, exc, homs.Bloch().flags)[0]
     assert np.allclose(nominal[:, :, 0], ref, atol=1e-12, rtol=0)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("rf_limit", [1, np.inf])
+@pytest.mark.parametrize("scenario", [(0, 0, 11, True), (3, 2, 11, True), (5, 2, 0, True), (0, 0, 11, False),
+                                      (0, 0, 0, True)])
+def test_rf_acquisition_through_public_simulate(oracle, gpu_context, precision, rf_limit, scenario):
+    """test_gpu_rf_buffers.jl:57-111 on the event-level rf_acquisition_sequence:
+    ADC samples during the pulses, every coil-combination name, state and raw."""
+    n1, n2, npre, rf_on = scenario
+    hoseq = HO_Sequence(W.rf_acquisition_events(n1, n2, npre, rf_on))
+    obj = HO_Phantom(x=[-0.01, 0.0, 0.01], y=[0.02, -0.01, 0.0], rho=[1.0, 0.7, 0.2], T1=[0.9, 1.0, 1.1],
+                     T2=[0.07, 0.08, 0.09], dw=[-20.0, 5.0, 25.0],
+                     csm=np.array([[1, 1j, 0.5], [0.5 - 0.2j, -0.3 + 0.1j, 0.2j], [0.7, 0.2j, 0.4 - 0.3j]]))
+    params = {"precision": precision, "implementation": "kernel", "sim_method": BlochHighOrder("1111"),
+              "return_type": "mat", "max_block_length": 32, "max_rf_block_length": rf_limit}
+    tol = 3e-5 if precision == "f32" else 1e-11
+    cpu = _oracle(oracle, obj, hoseq, "1111", params)
+    src = obj if precision == "f64" else obj.astype(np.float32)
+    reference = homs.simulate(src, hoseq, sim_params=params, context=gpu_context)
+    assert reference.shape == (n1 + n2 + npre, 3, 1)
+    assert np.allclose(reference[:, :, 0], cpu, atol=tol, rtol=tol)
+    ref_state = homs.simulate(src, hoseq, sim_params=dict(params, return_type="state"), context=gpu_context)
+    for mode in ("fused_warp", "fused_tiled"):
+        p = dict(params, coil_combination=mode)
+        owned = dict(p)
+        signal = homs.simulate(src, hoseq, sim_params=p, context=gpu_context)
+        assert np.allclose(signal, reference, atol=tol, rtol=tol) and np.all(np.isfinite(signal)) and p == owned
+        state = homs.simulate(src, hoseq, sim_params=dict(p, return_type="state"), context=gpu_context)
+        assert np.array_equal(state.xy, ref_state.xy) and np.array_equal(state.z, ref_state.z)
+        if n1 + n2 + npre:
+            raw = homs.simulate(src, hoseq, sim_params=dict(p, return_type="raw"), context=gpu_context)
+            assert sum(pr.shape[0] for pr in raw.profiles) == n1 + n2 + npre
+            assert all(pr.shape[1] == 3 for pr in raw.profiles)
