@@ -365,10 +365,15 @@ def _run_with_callbacks(obj, seqd, params, parts, excitation, state, ctx, callba
     """The block loop of run_sim_time_iter! (SimulatorCore.jl:96-152) with its
     callbacks: each block runs on the device by itself, from the state the
     previous block left, and every callback is called after it with
-    ``(Progress, SimulationBlocks, BlockData, sim_params)`` on completed data."""
+    ``(Progress, SimulationBlocks, BlockData, sim_params)`` on completed data.
+    The phantom and sequence the callbacks see are this run's copies; an edit
+    to them or to the state reaches the following blocks of the run only."""
     for cb in callbacks:
         if not callable(cb):
             raise ArgumentError("callbacks must be callables.")
+    # The run's own copies: a callback may edit them, and later blocks of this
+    # run see the edits, as they see the reference's device copies.
+    obj, seqd = copy.deepcopy(obj), copy.deepcopy(seqd)
     method, prec, mode = params["sim_method"], params["precision"], params["homs_precision"]
     cdt = np.complex128 if prec == "f64" else np.complex64
     fdt = np.float64 if prec == "f64" else np.float32
@@ -503,6 +508,7 @@ class Plan:
         self.parts, self.excitation = parts, excitation
         self.seqd = seqd
         self._host = copy.deepcopy(obj)  # snapshot for runs with callbacks (block by block)
+        self._busy = False
         self.ctx = context or _context(int(params["gpu_device"]))
         self.dtype = _dtype(params)
         self.ns, self.nc = len(obj), obj.ncoils
@@ -525,13 +531,19 @@ class Plan:
             return_type = self.params["return_type"]
         if return_type not in ("mat", "state", "raw"):
             raise ArgumentError("return_type must be mat, state, or raw.")
+        if self._busy:
+            raise ArgumentError("A prepared simulation cannot be used recursively from its callback.")
         if self.closed:
             raise ArgumentError("The prepared simulation is closed.")
         if callbacks:
             params = dict(self.params)
             params["return_type"] = return_type
-            sig, cur, seconds = _run_with_callbacks(self._host, self.seqd, params, self.parts, self.excitation, None,
-                                                    self.ctx, callbacks)
+            self._busy = True
+            try:
+                sig, cur, seconds = _run_with_callbacks(self._host, self.seqd, params, self.parts, self.excitation,
+                                                        None, self.ctx, callbacks)
+            finally:
+                self._busy = False
             return _finalize(params, sig, cur.xy, cur.z, self.parts, self.excitation, self.seqd, seconds, self.comp)
         cdt = np.complex128 if self.dtype == _lib.HOMS_F64 else np.complex64
         fdt = np.float64 if self.dtype == _lib.HOMS_F64 else np.float32
@@ -563,6 +575,8 @@ class Plan:
         return int(st.value), (why.value or b"").decode()
 
     def close(self):
+        if self._busy:
+            raise ArgumentError("A prepared simulation cannot be closed from its callback.")
         if not self.closed:
             _lib.load().homs_plan_destroy(self.handle)
             self.handle = None

@@ -358,3 +358,41 @@ def test_prepared_plan_reuse(gpu_context, precision):
         assert seen == list(range(1, len(plan.parts) + 1))
         st = plan.run(return_type="state", callbacks=(lambda *a: None,))
         assert np.allclose(st.xy, expected_state.xy, atol=1e-11 if precision == "f64" else 3e-5)
+
+
+def test_prepared_callbacks_failure_edits_and_recursion(gpu_context):
+    """test_prepared_simulation.jl:40-61: a failing callback leaves the plan
+    and the caller's phantom intact; a callback's state edit reaches the next
+    block, as on the one-shot path; recursive use from a callback is refused
+    and the plan keeps working."""
+    obj, seq, parts, exc = W.rf_acquisition_workload(3, 2, 11)
+    density = obj.rho.copy()
+    params = {"sim_method": BlochHighOrder("1111"), "precision": "f64", "max_block_length": 4,
+              "max_rf_block_length": 5}
+    with homs.prepare_simulation(obj, seq, sim_params=params, context=gpu_context) as plan:
+        baseline = plan.run()
+
+        def fail(progress, info, data, p):
+            data.obj.rho[:] = 0
+            data.Xt.xy[:] = 0
+            raise RuntimeError("intentional prepared callback failure")
+
+        with pytest.raises(RuntimeError):
+            homs.simulate(plan, callbacks=(fail,))
+        assert np.array_equal(homs.simulate(plan), baseline) and np.array_equal(obj.rho, density)
+
+        def observe(progress, info, data, p):
+            assert np.all(np.isfinite(data.Xt.xy))
+            data.Xt.xy *= 1j
+
+        changed = homs.simulate(plan, callbacks=(observe,))
+        reference = homs.simulate(obj, seq, sim_params=dict(params, synchronization="block"), callbacks=(observe,),
+                                  context=gpu_context)
+        assert np.array_equal(changed, reference) and not np.allclose(changed, baseline)
+        with pytest.raises(homs.ArgumentError, match="recursively"):
+            homs.simulate(plan, callbacks=(lambda *a: homs.simulate(plan),))
+        assert np.array_equal(homs.simulate(plan), baseline)
+        with pytest.raises(homs.ArgumentError, match="closed from its callback"):
+            homs.simulate(plan, callbacks=(lambda *a: plan.close(),))
+        assert not plan.closed and np.array_equal(plan.run(), baseline)
+    assert plan.closed
