@@ -908,6 +908,16 @@ def discretize(hoseq: HO_Sequence, sampling_params=None, sampling_rule: Optional
     seq = hoseq.simulation_sequence()
     starts = get_block_start_times(seq)
     join = _Joiner()
+    # A block's samples depend only on its duration and events: blocks that
+    # share their event objects (a Pulseq file's repeated ids) are sampled once.
+    cache = {}
     for j in range(len(seq)):
-        join.append(_sample_block(seq, hoseq.GR_dfc[:, j], j, rule), float(starts[j]))
+        waves = list(seq.GR[:, j]) + list(hoseq.GR_dfc[:, j])
+        rf, adc = seq.RF[0, j], seq.ADC[j]
+        key = (float(seq.DUR[j]), tuple(id(w) if w.is_on() else None for w in waves),
+               id(rf) if rf.is_on() else None, id(adc) if adc.N else None)
+        blk = cache.get(key)
+        if blk is None:
+            blk = cache[key] = _sample_block(seq, hoseq.GR_dfc[:, j], j, rule)
+        join.append(blk, float(starts[j]))
     return join.finish()

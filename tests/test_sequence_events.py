@@ -274,3 +274,30 @@ def test_preserved_samples_follow_the_rule():
     assert not np.all(np.isin(np.round(knots[2:-2], 12), np.round(coarse.t, 12)))
     with pytest.raises(ArgumentError):
         MaxStepSizeRule(1e-3, 5e-5, ("adc",))
+
+
+def test_repeated_blocks_sample_once_and_identically():
+    """Blocks sharing their event objects are sampled once; the result equals
+    the same sequence built from distinct, equal events."""
+    import copy
+
+    def tr(fresh):
+        mk = (lambda e: copy.deepcopy(e)) if fresh else (lambda e: e)
+        return (Sequence([[mk(exc_g)], [mk(zero)], [mk(ss)]], [mk(rf)], [mk(no_adc)])
+                + Sequence([[mk(ro)], [mk(zero)], [mk(zero)]], None, [mk(adc)]))
+
+    zero, no_adc = Grad(0.0, 0.0), ADC(0, 0.0)
+    exc_g, ss = Grad(0.0, 0.0), Grad(5e-3, 1e-3, 1e-4)
+    rf = RF(np.sinc(np.linspace(-2, 2, 41)) * 2e-6, 1e-3, 0.0, 1e-4)
+    ro, adc = Grad(4e-3, 2e-3, 1e-4), ADC(64, 2e-3 - 3e-5, 1e-4)
+    shared = tr(False)
+    for _ in range(199):
+        shared = shared + tr(False)
+    distinct = tr(True)
+    for _ in range(199):
+        distinct = distinct + tr(True)
+    a = discretize(HO_Sequence(shared))
+    b = discretize(HO_Sequence(distinct))
+    for k in ("t", "dt", "gx", "gy", "gz", "b1", "df", "adc", "excitation", "h"):
+        assert np.array_equal(getattr(a, k), getattr(b, k)), k
+    assert int(a.adc.sum()) == 200 * 64
