@@ -73,7 +73,7 @@ from .model import GAMMA, ArgumentError, DimensionMismatch, HO_DiscreteSequence
 
 __all__ = [
     "Grad", "RF", "ADC", "Sequence", "HO_Sequence", "MaxStepSizeRule", "discretize", "get_block_start_times",
-    "get_adc_sampling_times", "get_adc_phase_compensation", "rf_pulses", "validate_high_order_sequence",
+    "get_adc_sampling_times", "get_adc_phase_compensation", "rf_pulses", "validate_high_order_sequence", "get_samples",
 ]
 
 _TOL = 1e-12  # seconds: sample times closer than this are one time
@@ -599,7 +599,44 @@ class HO_Sequence:  # noqa: N801
         validate_high_order_sequence(self)
 
     def __repr__(self):
-        return f"HO_Sequence({len(self)} blocks, {float(np.sum(self.DUR)) * 1e3:.3f} ms)"
+        s = self.SEQ
+        ngr = sum(int(g.is_on()) for g in s.GR.ravel())
+        nadc = sum(int(a.N > 0) for a in s.ADC)
+        nrf = sum(int(r.is_on()) for r in s.RF.ravel())
+        tau = round(float(np.sum(s.DUR)) * 1e3, 3)
+        return f"HO_Sequence[ τ = {tau} ms | blocks: {len(s)} | ADC: {nadc} | GR: {ngr} | RF: {nrf} | DEF: {len(s.DEF)} ]"
+
+
+def get_samples(hoseq: HO_Sequence, off_val=0.0) -> dict:
+    """Event samples of every channel in sequence time (``get_samples``,
+    HO_Sequence.jl:169-200): ``"h0"``..``"h15"``, ``"gx"``, ``"gy"``, ``"gz"``
+    and ``"rf"`` as (t, A) knot arrays, ``"adc"`` as (sample times, ones).
+    ``off_val`` replaces zero field amplitudes (to hide them in plots)."""
+    seq = hoseq.simulation_sequence()
+    starts = get_block_start_times(seq)
+    out = {}
+
+    def chain(events):
+        ts, vs = [], []
+        for j, e in enumerate(events):
+            t, a = e.knots()
+            ts.append(starts[j] + t)
+            vs.append(a)
+        if not ts:
+            return np.zeros(0), np.zeros(0)
+        return np.concatenate(ts), np.concatenate(vs)
+
+    for k in range(16):
+        t, a = chain(hoseq.GR_dfc[k])
+        if off_val != 0:
+            a = np.where(a == 0, off_val, a)
+        out[f"h{k}"] = (t, a)
+    for k, name in enumerate(("gx", "gy", "gz")):
+        out[name] = chain(seq.GR[k])
+    out["rf"] = chain(seq.RF[0])
+    t = get_adc_sampling_times(seq)
+    out["adc"] = (t, np.ones_like(t))
+    return out
 
 
 def validate_high_order_sequence(hoseq: HO_Sequence) -> None:

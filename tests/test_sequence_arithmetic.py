@@ -37,6 +37,14 @@ def _seq_close(a, b):
                     zip(a.RF.ravel(), b.RF.ravel())) and np.array_equal(a.DUR, b.DUR))
 
 
+def _event_samples_equal(a, b, rtol=10 * EPS):
+    from homs.sequence import get_samples
+    sa, sb = get_samples(a), get_samples(b)
+    for name in sb:
+        assert np.array_equal(sa[name][0], sb[name][0]), name
+        assert np.allclose(sa[name][1], sb[name][1], rtol=rtol, atol=0), name
+
+
 def _sampled_equal(a, b, rtol=10 * EPS):
     sa, sb = discretize(a), discretize(b)
     assert np.array_equal(sa.t, sb.t) and np.array_equal(sa.adc, sb.adc)
@@ -66,6 +74,7 @@ def test_subtraction_is_concatenation_with_negation():
     assert [r.A for r in actual.SEQ.RF.ravel()] == [r.A for r in np.concatenate([x.SEQ.RF, y.SEQ.RF], 1).ravel()]
     assert [a.N for a in actual.SEQ.ADC] == [a.N for a in np.concatenate([x.SEQ.ADC, y.SEQ.ADC])]
     _sampled_equal(actual, expected)
+    _event_samples_equal(actual, expected)
     assert _seq_close(x.SEQ, ox.SEQ) and _seq_close(y.SEQ, oy.SEQ)
     assert np.array_equal(x.DUR, ox.DUR) and np.array_equal(y.DUR, oy.DUR)
 
@@ -80,6 +89,7 @@ def test_division_scales_every_field_channel(alpha):
         assert _grads_close(g, e)
         assert np.allclose(np.asarray(g.A), np.asarray(o.A) / alpha, rtol=10 * EPS, atol=0)
     _sampled_equal(actual, expected)
+    _event_samples_equal(actual, expected)
 
 
 @pytest.mark.parametrize("orders", ["0000", "1111"])

@@ -301,3 +301,33 @@ def test_repeated_blocks_sample_once_and_identically():
     for k in ("t", "dt", "gx", "gy", "gz", "b1", "df", "adc", "excitation", "h"):
         assert np.array_equal(getattr(a, k), getattr(b, k)), k
     assert int(a.adc.sum()) == 200 * 64
+
+
+def test_sequence_display_and_event_samples():
+    """HO_Sequence's summary (HO_Sequence.jl:139-147) and get_samples (:169-200)."""
+    from homs.sequence import get_samples
+    h = HO_Sequence(W.compatibility_events())
+    assert repr(h) == "HO_Sequence[ τ = 2.1 ms | blocks: 2 | ADC: 1 | GR: 0 | RF: 1 | DEF: 0 ]"
+    g = get_samples(h)
+    assert set(g) == {f"h{k}" for k in range(16)} | {"gx", "gy", "gz", "rf", "adc"}
+    assert np.allclose(g["adc"][0], get_adc_sampling_times(h.SEQ)) and np.all(g["adc"][1] == 1)
+    t, a = g["rf"]
+    assert t[1] == 0 and np.isclose(a[1].real, 1 / (4 * GAMMA * 1e-4))
+    h.GR_dfc[0, 1] = Grad(2e-7, 1e-3)
+    t0, a0 = get_samples(h)["h0"]
+    assert np.isclose(t0.max(), 1.1e-3) and np.isclose(a0.max(), 2e-7)
+    assert np.all(get_samples(h, off_val=np.inf)["h3"][1] == np.inf)
+
+
+def test_rf_sampling_converges(oracle):
+    """Halving dt_rf roughly halves the change of the signal: a shaped pulse is
+    sampled at dt_rf with the engine's left-point excitation rule (first order)."""
+    hoseq = W.gre_events(seed=4, ntr=1, nadc=32)
+    obj, _, _ = W.high_order_workload(nspins=64, nsteps=4, ncoils=2)
+    sig = []
+    for dt_rf in (1e-4, 5e-5, 2.5e-5, 1.25e-5):
+        sd = discretize(hoseq, sampling_rule=MaxStepSizeRule(1e-4, dt_rf))
+        parts, exc = get_sim_ranges(sd)
+        sig.append(oracle.simulate_c(obj, sd, parts, exc, BlochHighOrder("1111").flags)[0])
+    d = [np.linalg.norm(sig[i + 1] - sig[i]) for i in range(3)]
+    assert d[1] < 0.7 * d[0] and d[2] < 0.7 * d[1]
