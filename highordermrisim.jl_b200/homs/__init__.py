@@ -6,8 +6,16 @@ Mirrors HighOrderMRISim.jl's simulation interface for the BlochHighOrder path:
   (``src/simulation/Simulate.jl:52-67`` / ``:204-219``);
 * ``prepare_simulation(...)`` / ``Plan.run()`` / ``Plan.close()`` -- resident
   inputs reused across runs (``src/simulation/PreparedSimulation.jl:144-258``);
-* the sampled-sequence and phantom containers, ``BlochHighOrder``, and
-  ``get_sim_ranges`` (see ``model``).
+* the sampled-sequence and phantom containers, ``BlochHighOrder``, ``Bloch``
+  and ``get_sim_ranges`` (see ``model``);
+* event-level sequences (``Grad``, ``RF``, ``ADC``, ``Sequence``,
+  ``HO_Sequence``) and ``discretize`` (see ``sequence``), Pulseq 1.4 files
+  (``read_seq``) and the reference's demo inputs (``demo_inputs``,
+  ``demo_bench``);
+* the encoding export ``get_kspace``, the phantom builders
+  (``brain_phantom``, ``hophantom_brain``, ``csm_birdcage``, ``generate_grid``,
+  ``Grid``), ``basisfunc_spha`` and the trajectory utilities;
+* ``Server``, the continuous-batching front end, and ``ResidentPhantom``.
 
 Every run executes in libhoms.so (sm_100a CUDA kernels).  There is no CPU
 fallback: without the library or a B200 the calls raise ``HomsError``.
