@@ -136,6 +136,13 @@ class Grad:
         self.first = _real(first, "first")
         self.last = _real(last, "last")
 
+    @classmethod
+    def zero(cls) -> "Grad":
+        """A fresh ``Grad(0.0, 0.0)`` (built without argument checks)."""
+        g = cls.__new__(cls)
+        g.A, g.T, g.rise, g.fall, g.delay, g.first, g.last = 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0
+        return g
+
     def _copy(self, scale: float) -> "Grad":
         g = Grad.__new__(Grad)
         g.A = self.A * scale if np.ndim(self.A) == 0 else np.asarray(self.A) * scale
@@ -460,9 +467,10 @@ def _padded(gr: np.ndarray) -> np.ndarray:
     if not 1 <= m <= 16:
         raise ArgumentError("Expected 1 to 16 high-order field channels.")
     out = np.empty((16, n), dtype=object)
-    for i in range(16):
+    out[:m] = gr
+    for i in range(m, 16):
         for j in range(n):
-            out[i, j] = gr[i, j] if i < m else Grad(0.0, 0.0)
+            out[i, j] = Grad.zero()
     return out
 
 
