@@ -37,7 +37,7 @@ from __future__ import annotations
 
 import hashlib
 import math
-from typing import Dict, List, Tuple
+from typing import Dict, List
 
 import numpy as np
 

@@ -612,7 +612,8 @@ class HO_Sequence:  # noqa: N801
         nadc = sum(int(a.N > 0) for a in s.ADC)
         nrf = sum(int(r.is_on()) for r in s.RF.ravel())
         tau = round(float(np.sum(s.DUR)) * 1e3, 3)
-        return f"HO_Sequence[ τ = {tau} ms | blocks: {len(s)} | ADC: {nadc} | GR: {ngr} | RF: {nrf} | DEF: {len(s.DEF)} ]"
+        return (f"HO_Sequence[ τ = {tau} ms | blocks: {len(s)} | ADC: {nadc} | GR: {ngr} | RF: {nrf} | "
+                f"DEF: {len(s.DEF)} ]")
 
 
 def get_samples(hoseq: HO_Sequence, off_val=0.0) -> dict:

@@ -3,7 +3,6 @@ import ctypes
 import os
 import re
 
-import numpy as np
 import pytest
 
 from homs import _lib

@@ -2,7 +2,6 @@
 completes runs out, the kernel records it in a device error word and
 returns, and the host reports HOMS_ETIMEDOUT.  The same context then runs a
 simulation correctly."""
-import numpy as np
 import pytest
 
 import homs

@@ -1,13 +1,11 @@
 """Host-side mirror of the reference interface: validation and block planning."""
-import math
-
 import numpy as np
 import pytest
 
 import homs
 from homs import workloads as W
-from homs.model import (ArgumentError, BlochHighOrder, DimensionMismatch, HO_DiscreteSequence, HO_Phantom,
-                        count_block_adc, get_sim_ranges)
+from homs.model import (ArgumentError, BlochHighOrder, DimensionMismatch, HO_Phantom, count_block_adc,
+                        get_sim_ranges)
 
 
 def test_bloch_high_order_mask_rules():

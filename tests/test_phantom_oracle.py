@@ -4,7 +4,6 @@ SpinProperty's tables (src/phantom/SpinProperty.jl), generate_grid
 (src/phantom/hophantom_brain.jl:27-31), csm_Birdcage (src/phantom/csm/Birdcage.jl)
 and the size invariants of test/unit/test_HOPhantom.jl:18-25."""
 import numpy as np
-import pytest
 
 from oracle import oracle as orc
 

@@ -1,7 +1,6 @@
 """The comparator that restates the reference's GPU design (materialised states
 per block of nodes, cuBLAS coil GEMM; bench.reference_gpu_equivalent) against
 the FP64 oracle: on torch's CPU device here, and on the GPU (marked gpu)."""
-import numpy as np
 import pytest
 
 import bench

@@ -256,7 +256,8 @@ def test_preserved_samples_follow_the_rule():
     n = 201
     shape = np.sinc(np.linspace(-3, 3, n)).astype(np.complex128) * 1e-6
     wave = 1e-3 * np.sin(np.linspace(0, 6, 97))
-    seq = Sequence([[Grad(wave, 2e-3, 0.0, 0.0, 1.3e-3)], [Grad(0.0, 0.0)], [Grad(0.0, 0.0)]], [RF(shape, 1e-3, 0.0, 2e-4)],
+    seq = Sequence([[Grad(wave, 2e-3, 0.0, 0.0, 1.3e-3)], [Grad(0.0, 0.0)], [Grad(0.0, 0.0)]],
+                   [RF(shape, 1e-3, 0.0, 2e-4)],
                    [ADC(0, 0.0)])
     hoseq = HO_Sequence(seq)
     default = discretize(hoseq, sampling_rule=MaxStepSizeRule(1e-3, 5e-5))
