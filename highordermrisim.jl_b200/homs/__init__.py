@@ -72,9 +72,11 @@ def _sampled(seq, sim_params):
     None).  An ``HO_Sequence`` is discretised with the sampling keys of
     ``sim_params`` (``"Δt"``, ``"Δt_rf"``, ``"sampling_rule"``), as
     ``setup_simulation`` does (Simulate.jl:100)."""
+    if isinstance(seq, Sequence):
+        seq = HO_Sequence(seq)  # a native sequence: no measured fields
     if not isinstance(seq, HO_Sequence):
         if not isinstance(seq, HO_DiscreteSequence):
-            raise ArgumentError("The sequence must be an HO_Sequence or an HO_DiscreteSequence.")
+            raise ArgumentError("The sequence must be a Sequence, an HO_Sequence or an HO_DiscreteSequence.")
         return seq, None, None
     if sim_params is not None and not isinstance(sim_params, dict):
         raise ArgumentError("sim_params must be a dictionary with string keys.")
@@ -471,6 +473,8 @@ def get_kspace(seqd, rf_start=None, rf_sign=None, skip_rf=None, adc_times=None,
     refocusing, +1 kept) or, by default, ``rf_events(seqd, gamma, skip_rf)``.
     ``precision`` is the dtype the sequence arrays cross the ABI in; the
     integral is FP64 either way."""
+    if isinstance(seqd, Sequence):
+        seqd = HO_Sequence(seqd)
     if isinstance(seqd, HO_Sequence):
         if rf_start is not None or rf_sign is not None or adc_times is not None:
             raise ArgumentError("rf_start, rf_sign and adc_times come from the HO_Sequence itself.")

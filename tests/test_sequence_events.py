@@ -332,3 +332,15 @@ def test_rf_sampling_converges(oracle):
         sig.append(oracle.simulate_c(obj, sd, parts, exc, BlochHighOrder("1111").flags)[0])
     d = [np.linalg.norm(sig[i + 1] - sig[i]) for i in range(3)]
     assert d[1] < 0.7 * d[0] and d[2] < 0.7 * d[1]
+
+
+def test_native_sequence_is_accepted_as_high_order_sequence():
+    import homs
+    seq = W.compatibility_events()
+    a, comp_a, na = homs._sampled(seq, {})
+    b, comp_b, nb = homs._sampled(HO_Sequence(seq), {})
+    assert na == nb == 5 and comp_a is None and comp_b is None
+    for k in ("t", "dt", "gx", "b1", "adc", "excitation", "h"):
+        assert np.array_equal(getattr(a, k), getattr(b, k))
+    with pytest.raises(ArgumentError, match="Sequence"):
+        homs._sampled("not a sequence", {})
