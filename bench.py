@@ -12,6 +12,14 @@ prepared plan, signal written to device memory); `e2e` is the same metric
 through the C ABI (homs_simulate) from pinned host buffers, with all
 host<->device copies inside the timed region.  With N > 1 every rank runs an
 independent replica (the engine does not shard spins across GPUs).
+
+Further keys on one GPU: ``roofline`` (with ``tensor_pipe``: the FP16
+contraction and FP64 DMMA phase work the split kernel issues, and their
+combined share of the tensor pipe), ``cpu_baseline``, ``clocks``,
+``serving`` / ``serving_resident`` (the mixed request stream),
+``reference_gpu_equivalent`` (the reference's GPU design restated with
+torch/cuBLAS and timed on the same workload), ``kspace`` (encoding export)
+and ``phantom`` (device phantom builder).
 """
 from __future__ import annotations
 
