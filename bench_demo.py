@@ -8,11 +8,11 @@ at 2 mm around z = 20 mm, the real 32-channel receive map and the real
 off-resonance map, 1.5 T tissue), and demo3D/3_run_sim.jl runs
 BlochHighOrder("1111") with FP32 arrays.  Two steps:
 
-    python -m homs.demo_bench stage --demo-dir DEMO3D --phantom-dir PHANTOM --out DIR
+    python bench_demo.py stage --demo-dir DEMO3D --phantom-dir PHANTOM --out DIR
         (CPU) copies the three demo files and writes the phantom's class and
         off-resonance volumes, resampled to the target grid, and the source
         receive map to DIR (about 40 MB).
-    python -m homs.demo_bench run --staged DIR [--runs 4] [--modes split_f32,...]
+    python bench_demo.py run --staged DIR [--runs 4] [--modes split_f32,...]
         (GPU) builds the sequence and the phantom, prepares one plan per
         mode (split and plain, FP32 and FP64 arrays), times repeated plan
         runs (host wall time of ``Plan.run``, signal copied to host memory
@@ -37,6 +37,10 @@ import time
 
 import numpy as np
 
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if os.path.join(ROOT, "highordermrisim.jl_b200") not in sys.path:
+    sys.path.insert(0, os.path.join(ROOT, "highordermrisim.jl_b200"))
+
 NAME = "Spiral_2p0x2p0x2p0_100x100x35_1x4_int1_9p5ms_tr500_te5p0"
 NAME_2D = "7T_1p0_200_r4"
 # target grid (resolution, matrix, location), files, and the demo's B0 / T2 switches
@@ -52,7 +56,7 @@ TARGET_RES, TARGET_MATRIX, LOCATION = (WORKLOADS["demo3d"][k] for k in ("res", "
 def stage(demo_dir: str, phantom_dir: str, out: str, workload: str = "demo3d") -> None:
     import scipy.io as sio
 
-    from .phantom import resample_b0, resample_labels
+    from homs.phantom import resample_b0, resample_labels
     w = WORKLOADS[workload]
     os.makedirs(out, exist_ok=True)
     for f in w["files"]:
@@ -75,11 +79,11 @@ MODES = {"split_f32": ("f32", "split"), "split_f64": ("f64", "split"), "plain_f6
 
 
 def run(staged: str, runs: int = 4, modes=tuple(MODES), workload: str = "demo3d") -> dict:
-    from . import Context, prepare_simulation
-    from .demo_inputs import demo2d_sequence, demo3d_sequence
-    from .model import BlochHighOrder
-    from .phantom import brain_phantom, resample_csm
-    from .sequence import discretize, get_adc_phase_compensation
+    from homs import Context, prepare_simulation
+    from homs.demo_inputs import demo2d_sequence, demo3d_sequence
+    from homs.model import BlochHighOrder
+    from homs.phantom import brain_phantom, resample_csm
+    from homs.sequence import discretize, get_adc_phase_compensation
 
     w = WORKLOADS[workload]
     out = {"workload": {"demo3d": "demo3D: Pulseq 3D stack of spirals with field-camera gradients, brain phantom "

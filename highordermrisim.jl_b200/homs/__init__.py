@@ -10,8 +10,8 @@ Mirrors HighOrderMRISim.jl's simulation interface for the BlochHighOrder path:
   and ``get_sim_ranges`` (see ``model``);
 * event-level sequences (``Grad``, ``RF``, ``ADC``, ``Sequence``,
   ``HO_Sequence``) and ``discretize`` (see ``sequence``), Pulseq 1.4 files
-  (``read_seq``) and the reference's demo inputs (``demo_inputs``,
-  ``demo_bench``);
+  (``read_seq``) and the reference's demo inputs (``demo_inputs``; the
+  timed demo workloads are ``bench_demo.py`` beside ``bench.py``);
 * the encoding export ``get_kspace``, the phantom builders
   (``brain_phantom``, ``hophantom_brain``, ``csm_birdcage``, ``generate_grid``,
   ``Grid``), ``basisfunc_spha`` and the trajectory utilities;

@@ -11,8 +11,10 @@ import pytest
 from homs.model import ArgumentError
 from homs.phantom import resample_b0, resample_csm, resample_labels
 
-REF = os.environ.get("HOMS_REFERENCE_ROOT", "/root/reference")
-CSM_MAT = os.path.join(REF, "src", "phantom", "csm", "csm_4p0.mat")
+# The reference's data files are read only when HOMS_REFERENCE_ROOT names its source tree.
+REF = os.environ.get("HOMS_REFERENCE_ROOT", "")
+_ref = (lambda *parts: os.path.join(REF, *parts)) if REF else (lambda *parts: "")
+CSM_MAT = _ref("src", "phantom", "csm", "csm_4p0.mat")
 
 SPACING = (0.004, 0.006, 0.008)
 DIMS = (3, 4, 2)
@@ -152,8 +154,8 @@ def test_generate_grid():
         generate_grid((0.2, -0.2, 0.2), (4, 4, 4))
 
 
-BRAIN_MAT = os.path.join(REF, "src", "phantom", "brain3D_0.5_0.5_0.5.mat")
-B0_MAT = os.path.join(REF, "src", "phantom", "b0map", "b0_4p0.mat")
+BRAIN_MAT = _ref("src", "phantom", "brain3D_0.5_0.5_0.5.mat")
+B0_MAT = _ref("src", "phantom", "b0map", "b0_4p0.mat")
 
 
 @pytest.mark.skipif(not (os.path.exists(BRAIN_MAT) and os.path.exists(CSM_MAT) and os.path.exists(B0_MAT)),
