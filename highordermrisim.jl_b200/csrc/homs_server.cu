@@ -28,6 +28,7 @@
 
 #include "../../include/homs.h"
 #include "homs_internal.cuh"
+#include "homs_split.cuh"
 
 namespace {
 
@@ -64,10 +65,10 @@ size_t estimate_bytes(int64_t nspins, int32_t ncoils, homs_dtype dtype, const ho
     b += nt * (26 * es + 2);                               // sampled sequence
     b += (double)nadc * nc * 2 * es;                       // signal
     if (o.mode == HOMS_SPLIT) {
-        const double groups = std::ceil(nc / 32.0);
-        if (!resident) b += ns * (128.0 + 512.0 * groups);  // basis, pre-split sensitivities
-        b += ns * 152.0;                                    // spin table
-        b += 4500.0 * 128 * 64 * 8 + (double)nadc * 192.0;  // split-K partials, phase prefix
+        if (!resident) b += ns * homs::split_bytes_per_spin(ncoils);  // basis, phase and coil digit operands
+        b += ns * 12.0;                                               // per-segment spin parameters
+        // split-K partials (at most ~8,000 items of 128 x 64 FP64), phase prefix, phase A tiles, sample rows
+        b += 8000.0 * 128 * 64 * 8 + (double)nadc * (192.0 + 96.0 + 8.0);
     } else {
         const double grid = std::ceil(ns / 256.0);
         b += std::min(768.0 * (1 << 20), grid * nc * 2 * es * (double)nadc);  // split-K partials

@@ -1,47 +1,60 @@
-// Split-precision fused precession + coil contraction on sm_100a tensor cores.
+// Split-precision fused precession + coil contraction on sm_100a tensor cores,
+// in exact integer arithmetic on the int8 tcgen05 pipe.
 //
 // Math (one precession segment = a run of consecutive precession blocks):
-//   phase in turns   theta(s,j) = theta0(s) + w(s) kappa_16(j) + sum_k b_k(s) kappa_k(j),  k = 0..15
-//     b_0..15  : the 16 solid-harmonic basis values of spin s (FP64, resident)
-//     w        : dw/(2 pi) (0 when dw is off),  kappa_16 = -t_j
-//     theta0   : arg(m0)/(2 pi)
-//     kappa_k  : -gamma * trapezoid integral of field column k from the segment
-//                start to ADC sample j (FP64 prefix table)
+//   phase in turns   theta(s,j) = theta0(s) + kappa_0(j) + sum_k b_k(s) kappa_k(j)
+//     k = 1..15 : the unnormalised solid-harmonic basis terms of spin s,
+//                 kappa_k = -gamma * trapezoid integral of field column k from
+//                 the segment start to ADC sample j
+//     k = 16    : b_16 = dw/(2 pi),  kappa_16 = -t_j (0 when dw is off)
+//     kappa_0   : the h0 term (basis value 1), theta0 = arg(m0)/(2 pi)
 //   M(s,j)   = |m0| 2^(t_j * r2(s)) * cis(2 pi theta)   (r2 = -log2(e)/T2)
 //   S(j,c)   = sum_s M(s,j) csm(s,c)                      (no conjugation)
 // This is the reference's phi = -2 pi gamma cumtrapz(dt, Bz) and
 // Mxy = M0 exp(i phi - t/T2) (src/simulation/Bloch/BlochHighOrderSimulatitonMethod.jl:76-92)
 // with the cumulative integral factored into per-spin x per-sample terms.
 //
-// Precision.  theta(s,j) is a small FP64 GEMM (samples x 16) * (16 x spins)
-// on FP64 tensor-core MMAs (mma.sync m8n8k4.f64), its accumulator initialised
-// with theta0 + w kappa_16.  One FP64 add of 1.5*2^20 leaves frac(theta) as a
-// 32-bit fixed-point turn count in the low mantissa word: the mod-2pi range
-// reduction, exact to 2^-32 turn.  cos/sin of 2 pi frac(theta) in [-pi, pi)
-// and the decay come from the SFU (sin/cos/ex2.approx).  M and the
-// sensitivities are split into FP16 hi + lo pairs after exact power-of-two
-// scaling (per coil, and per segment for the amplitude), and the coil
-// contraction runs as two kind::f16 tcgen05 MMAs per 16-deep K-step, each with
-// N = 2 x columns: A_lo x [B_hi | B_lo] first, then A_hi x [B_hi | B_lo], so
-// one accumulator generation (per 32-spin chunk) holds A.B_hi and A.B_lo side
-// by side.  The drain adds the two halves in FP32 into a TMEM row accumulator
-// and every WINDOW chunks promotes it into FP64 split-K partials; the final
-// sum undoes the scaling exactly.
+// Phase, exactly.  Per field term k the coefficient is the integer
+// B_k(s) = rint(b_k 2^38 / bmax_k) and the integral K_k(j) =
+// rint(kappa_k bmax_k 2^26), so that B K 2^-64 = b kappa to 2^-27 turn
+// (|K| <= 2^38 requires bmax_k * max|kappa_k| <= 2^12 turns, checked per
+// segment).  Both are split into five balanced int8 digits (base 256); the
+// digit products of equal weight 2^(8w) are summed exactly by int8 tcgen05
+// MMAs (int32 accumulators), and only the classes w = 2..7 reach the 32-bit
+// turn fraction: w >= 8 are whole turns (the mod-2pi reduction is the
+// integer wraparound) and w <= 1 lie below 2^-32 turn.  The turn fraction
+//   u = sum_w S_w 2^(8w-32) mod 2^32
+// is exact up to the rounding of B and K.
+//
+// Trigonometry.  u is reduced to the nearest quarter turn in integers
+// (|x| <= pi/4, which keeps the float scale of the angle from biasing the
+// phase at the wrap), then sin/cos.approx and a quadrant rotation; the decay
+// is ex2.approx of a small argument.  |M| <= 1 after a power-of-two scale per
+// segment.
+//
+// Coil contraction, exactly.  M and the per-coil scaled sensitivities become
+// 22-bit integers, three int8 digits each (M: two low bytes unsigned and the
+// top byte offset by 64; sensitivities balanced).  Six int8 MMAs per 32-spin
+// chunk accumulate the digit classes T4..T1 (weights 2^32..2^8; T0 lies below
+// 2^-36 of the signal) in int32 TMEM for a whole work item, with no rounding
+// at all; each item's classes become one FP64 split-K partial.  The offset of
+// the top digit is removed once per output column in the finalize.
 //
 // Kernel organisation (one CTA per SM, persistent, slab-major work items of
 // (time tile of 128 samples) x (range of 32-spin chunks)):
-//   warps 0-7   phase: warp w computes the turn fractions of the 16 tile rows
-//               32(w%4) + 16(w/4) .. +15 for each chunk (DMMA) and writes them
-//               to TMEM in the m8n8 fragment layout (tcgen05.st.16x256b).
-//   warps 8-15  magnetisation: the same 16 rows for warp w-8; read the turn
-//               fractions, form M, split it into FP16 hi/lo and write the A
-//               operand to TMEM; drain the accumulator.
-//   warp 16     MMA issuer: tcgen05.mma.kind::f16, A in TMEM, B (the
-//               sensitivities, pre-split) in shared memory; tcgen05.commit
-//               releases shared-memory stages, A buffers and accumulators.
-//   warp 17     loader: cp.async.bulk of each chunk's B operand and spin table.
-// TMEM (512 columns for N <= 64 output columns): accumulators 2 x 2N, A
-// operands 2 x 64, turn fractions 2 x 32, FP32 row accumulator N.
+//   warps 0-15  magnetisation: warp w owns tile rows 32(w%4) .. +31 (its
+//               TMEM lane quarter) and spins 8(w/4) .. +7 of every chunk:
+//               reads the phase classes, forms the turn, M and its digits,
+//               writes the coil MMA's A operand to TMEM; drains the coil
+//               classes into the item's FP64 partial.
+//   warp 16     MMA issuer: per chunk 3 phase MMAs (A: the tile's integral
+//               digits in shared memory, B: the chunk's coefficient digits)
+//               one chunk ahead, and 6 coil MMAs (A in TMEM, B: the chunk's
+//               sensitivity digits); tcgen05.commit releases shared-memory
+//               stages and TMEM buffers.
+//   warp 17     loader: cp.async.bulk of each item's phase A tile and each
+//               chunk's operands (non-multicast).
+// TMEM (512 columns): phase classes 192, coil A operand 48, coil classes 4N.
 // Every wait is bounded: on time-out the kernel records the place in a device
 // error word and returns without hanging the GPU.
 #include <algorithm>
@@ -49,8 +62,6 @@
 #include <cstring>
 #include <string>
 #include <vector>
-
-#include <cuda_fp16.h>
 
 #include "homs_common.cuh"
 #include "homs_split.cuh"
@@ -61,50 +72,46 @@ namespace split {
 
 constexpr int TM = 128;          // samples per tile (UMMA M)
 constexpr int KC = 32;           // spins per chunk
-constexpr int KSTEPS = 4;        // (2*KC real K values) / 16 per f16 MMA
-constexpr int MAX_STAGE = 6;     // shared-memory stages of B operand + spin table
-constexpr int NTERM = 16;        // phase GEMM depth (DMMA K): the 16 basis terms
+constexpr int NSLOT = 16;        // phase terms per spin: basis 1..15 and dw/(2 pi)
+constexpr int PHASE_DIGITS = 5;  // base-256 digits of the phase integers
 constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_16, t at PREFIX_T
 constexpr int PREFIX_T = 20;
 constexpr int GROUP_COILS = 32;  // coils per kernel pass (N <= 64 output columns)
-// Warp roles: 8 phase warps and 8 magnetisation warps (2 of each per TMEM
-// lane quarter, paired by the 16 rows they share), MMA issuer, loader.
-constexpr int NPHASE_WARPS = 8;
-constexpr int NMAG_WARPS = 8;
+constexpr int NMAG_WARPS = 16;
 constexpr int MMA_WARP = 16;
 constexpr int LOAD_WARP = 17;
 constexpr int THREADS = 576;
 constexpr uint32_t TMEM_COLS = 512;
+constexpr int MAX_STAGE = 6;
+constexpr int MAX_ITEM_CHUNKS = 256;  // int32 coil classes stay below 2^31 over an item
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
-// FLUSH chunks (8 MMAs each) form one FP32 TMEM accumulator generation: the
-// tensor core's accumulator add is not round-to-nearest, and its error is
-// systematic and grows with |D| and with the number of MMAs per generation
-// (two chunks per generation raised the signal NRMSE from 4.6e-7 to 5.2e-7 on
-// the 3D workload for a 1% gain, so each chunk keeps its own).
-// The drain adds generations (round to nearest, FP32) in a TMEM row
-// accumulator and promotes it to the FP64 partials every WINDOW chunks.
-constexpr int FLUSH = 1;
-constexpr int WINDOW = 32;  // a multiple of FLUSH
+constexpr double PHASE_RANGE_LIMIT = 4096.0;     // turns: bmax_k * max|kappa_k| per term and segment
 
-// TMEM column map for N output columns (N <= 64).
-__host__ __device__ constexpr uint32_t d_col(int n, int buf) { return (uint32_t)(buf * 2 * n); }
-__host__ __device__ constexpr uint32_t a_col(int n, int buf) { return (uint32_t)(4 * n + buf * 64); }
-__host__ __device__ constexpr uint32_t t_col(int n, int tb) { return (uint32_t)(4 * n + 128 + tb * 32); }
-__host__ __device__ constexpr uint32_t acc_col(int n) { return (uint32_t)(4 * n + 192); }
+// Phase MMAs: A' tiles [a4|a3], [a2|a1], [a0|0] (128 rows x 32 bytes each) and
+// B' blocks of 32 spin rows per digit class w (classes 7..2 at TMEM columns
+// (7 - w) * 32): MMA 1 covers w = 7..2 (N = 192; its class-2 block is zero
+// and only clears those columns), MMA 2 w = 6..2 (N = 160, columns 32..191),
+// MMA 3 w = 4..2 (N = 96, columns 96..191).
+constexpr int PH_N1 = 192, PH_N2 = 160, PH_N3 = 96;
+constexpr int PH_OFF2 = PH_N1 * 32, PH_OFF3 = (PH_N1 + PH_N2) * 32;
+constexpr int PHASE_B_BYTES = (PH_N1 + PH_N2 + PH_N3) * 32;  // per chunk
+constexpr int PHASE_A_BYTES = 3 * TM * 32;                   // per tile
+constexpr int PARAM_BYTES = 3 * KC * 4;                      // per chunk
+// Coil B operand per chunk: 2 K-steps of 16 spins x (re, im) = 32 int8, each
+// [c2 | c1 | c0] x N rows.
+__host__ __device__ constexpr int coil_b_bytes(int n) { return 2 * 3 * n * 32; }
 
-// B operand of one chunk: KSTEPS slabs of 2N rows ([B_hi | B_lo]) x 16 f16,
-// no-swizzle K-major (core matrices of 8 rows x 16 bytes).
-__host__ __device__ constexpr int b_bytes(int n) { return KSTEPS * 2 * n * 32; }
+// TMEM columns.
+constexpr uint32_t P_COL = 0;    // phase classes
+constexpr uint32_t A_COL = 192;  // coil A: per K-step [m2 | m1 | m0], 8 columns each
+constexpr uint32_t D_COL = 256;  // coil classes [T4 | T3 | T2 | T1], N columns each
 
-// Spin table of a chunk, in doubles: basis term k (0..15) of local spin s at
-// ((k/4)*KC + s)*4 + k%4, so that one DMMA B fragment (k = 4ks + tq, spin
-// base + gq) is 32 consecutive doubles; then theta0 = arg(m0)/(2 pi) and
-// dw/(2 pi) per spin, and one packed float2 (-log2(e)/T2, log2|m0|) per spin.
-__host__ __device__ inline int tab_index(int k, int s) { return (((k >> 2) * KC + s) << 2) + (k & 3); }
-constexpr int TAB_THETA0 = NTERM * KC;
-constexpr int TAB_DW = TAB_THETA0 + KC;
-constexpr int TAB_PACK = TAB_DW + KC;
-constexpr int SPIN_BYTES = (TAB_PACK + KC) * 8;
+// Canonical no-swizzle K-major layout of an operand with 32 bytes of K per
+// row: core matrices of 8 rows x 16 bytes, K-direction stride 128 B, 8-row
+// group stride 256 B.
+__host__ __device__ inline int kmaj(int row, int kbyte) {
+    return (row >> 3) * 256 + (kbyte >> 4) * 128 + (row & 7) * 16 + (kbyte & 15);
+}
 
 // Smallest e with 2^e >= x for a non-negative double given by its bits (0 for 0).
 __host__ __device__ inline int pow2_ceil_exp(unsigned long long bits) {
@@ -112,6 +119,17 @@ __host__ __device__ inline int pow2_ceil_exp(unsigned long long bits) {
     int e = (int)((bits >> 52) & 0x7FF) - 1023;
     if (bits & 0xFFFFFFFFFFFFFull) e += 1;
     return e;
+}
+
+// Balanced base-256 digit i of v (digits 0..n-2 in [-128, 127]; the top one
+// takes the rest).
+__host__ __device__ inline int balanced_digit(long long v, int i, int n) {
+    for (int k = 0; k < i; ++k) {
+        const long long d = ((v + 128) & 255) - 128;
+        v = (v - d) >> 8;
+    }
+    if (i == n - 1) return (int)v;
+    return (int)(((v + 128) & 255) - 128);
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -159,22 +177,24 @@ __device__ __forceinline__ void tc_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
-
-__device__ __forceinline__ void tc_mma_f16(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
+// int8 MMA, A and B from shared memory (descriptors).
+__device__ __forceinline__ void tc_mma_i8_ss(uint32_t d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                             uint32_t accum) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
-        "r"(a), "l"(bdesc), "r"(idesc), "r"(accum)
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
         : "memory");
 }
-// FP64 tensor-core MMA, 8x8x4: c += a * b in the m8n8k4 fragment layouts
-// (a: row groupID, col threadID_in_group; b: row threadID_in_group, col
-// groupID; c: row groupID, cols 2*threadID_in_group + {0,1}).
-__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-        : "+d"(c0), "+d"(c1)
-        : "d"(a), "d"(b));
+// int8 MMA, A in TMEM, B from shared memory.
+__device__ __forceinline__ void tc_mma_i8_ts(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+        "r"(a), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
 }
 __device__ __forceinline__ float ex2_approx(float x) {
     float r;
@@ -191,75 +211,44 @@ __device__ __forceinline__ float cos_approx(float x) {
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+}
 
-// 16 TMEM lanes x 8r columns (r = 2 or 4 repetitions): thread t writes lanes
-// t/4 (v[4i], v[4i+1]) and t/4+8 (v[4i+2], v[4i+3]), columns 8i + 2*(t%4) + {0,1}.
-__device__ __forceinline__ void tmem_st_16x256b_x2(uint32_t taddr, const uint32_t *v) {
-    asm volatile("tcgen05.st.sync.aligned.16x256b.x2.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_st_16x256b_x4(uint32_t taddr, const uint32_t *v) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.16x256b.x4.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-        "%14, %15, %16};" ::"r"(taddr),
-        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
-        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
-        : "memory");
-}
-__device__ __forceinline__ void tmem_ld_16x256b_x4(uint32_t taddr, uint32_t *v) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-        : "r"(taddr)
-        : "memory");
-}
-// 32 TMEM lanes (thread <-> lane) x 8 or 16 consecutive columns.
-__device__ __forceinline__ void tmem_ld_32x32b_x8(uint32_t taddr, float *v) {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+// 32 TMEM lanes (thread <-> lane) x 4 or 8 consecutive columns.
+__device__ __forceinline__ void tmem_ld_x4(uint32_t taddr, uint32_t *v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
                  : "r"(taddr)
                  : "memory");
-#pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
-__device__ __forceinline__ void tmem_ld_32x32b_x16(uint32_t taddr, float *v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr)
-        : "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_st_32x32b_x8(uint32_t taddr, const float *v) {
-    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
-                 "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+__device__ __forceinline__ void tmem_ld_x8(uint32_t taddr, uint32_t *v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr)
                  : "memory");
 }
-__device__ __forceinline__ void tmem_st_32x32b_x16(uint32_t taddr, const float *v) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-        "%14, %15, %16};" ::"r"(taddr),
-        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
-        "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15])
-        : "memory");
+__device__ __forceinline__ void tmem_st_x4(uint32_t taddr, const uint32_t *v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
+                 "r"(v[2]), "r"(v[3])
+                 : "memory");
 }
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// No-swizzle K-major shared-memory matrix descriptor: core matrices of
-// 8 rows x 16 bytes, K-direction core stride (LBO) 128 B, row-group stride
-// (SBO) 256 B, descriptor version 1.
-__device__ __forceinline__ uint64_t bdesc(uint32_t saddr) {
+// Shared-memory matrix descriptor of the canonical layout above (descriptor
+// version 1, no swizzle).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(256 >> 4) << 32) |
            (1ull << 46);
+}
+// Instruction descriptor of kind::i8, M = 128, K-major A and B, int32 D:
+// a_signed/b_signed select s8 (1) or u8 (0).
+__host__ __device__ constexpr uint32_t idesc_i8(int n, bool a_signed, bool b_signed) {
+    return (2u << 4) | ((a_signed ? 1u : 0u) << 7) | ((b_signed ? 1u : 0u) << 10) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(TM >> 4) << 24);
 }
 
 // Work items of one launch.  The (tile x chunk) grid is cut into `slabs`
@@ -268,70 +257,72 @@ __device__ __forceinline__ uint64_t bdesc(uint32_t saddr) {
 // read the chunks of two or three consecutive slabs, which stay in L2 for
 // every tile that needs them.  Item (tile, z) owns partial slot z.
 struct KernelArgs {
-    const double *prefix;      // [rows][PREFIX_STRIDE]
-    const uint8_t *b_operand;  // [nchunks][b_bytes]
-    const double *spin_table;  // [nchunks][SPIN_BYTES / 8]
+    const uint8_t *phase_a;    // [tiles][PHASE_A_BYTES]
+    const uint8_t *phase_b;    // [nchunks][PHASE_B_BYTES]
+    const uint8_t *coil_b;     // [nchunks][coil_b_bytes(N)] of this coil group
+    const uint8_t *params;     // [nchunks][PARAM_BYTES]
+    const uint32_t *rows;      // [tiles * TM][2]: base turn, elapsed time (float bits)
     const unsigned long long *amp_max;  // bits of max |m0| over the segment's spins
-    double *partial;           // [tiles][slabs][TM][N], FP64 split-K partials
+    double *partial;           // [tiles][slabs][TM][N]
     unsigned int *err;
-    int64_t nsamples;
     int n_chunks;
     int tiles;
     int slabs;
-    int nstage;  // shared-memory stages of B operand + spin table
+    int nstage;
 };
 
-struct Item {
-    int tile, z, c0, c1;
+struct Cursor {
+    int i, c, c0, c1, tile, z, local;
+    bool valid;
 };
-__device__ __forceinline__ Item item_of(const KernelArgs &a, int i) {
-    Item it;
-    it.z = i / a.tiles;
-    it.tile = i - it.z * a.tiles;
-    it.c0 = (int)((int64_t)a.n_chunks * it.z / a.slabs);
-    it.c1 = (int)((int64_t)a.n_chunks * (it.z + 1) / a.slabs);
-    return it;
+__device__ __forceinline__ void cursor_item(const KernelArgs &a, Cursor &cu) {
+    cu.valid = cu.i < a.tiles * a.slabs;
+    if (!cu.valid) return;
+    cu.z = cu.i / a.tiles;
+    cu.tile = cu.i - cu.z * a.tiles;
+    cu.c0 = (int)((int64_t)a.n_chunks * cu.z / a.slabs);
+    cu.c1 = (int)((int64_t)a.n_chunks * (cu.z + 1) / a.slabs);
+    cu.c = cu.c0;
+}
+__device__ __forceinline__ Cursor cursor_start(const KernelArgs &a) {
+    Cursor cu;
+    cu.i = blockIdx.x;
+    cu.local = 0;
+    cursor_item(a, cu);
+    return cu;
+}
+__device__ __forceinline__ void cursor_next(const KernelArgs &a, Cursor &cu) {
+    if (++cu.c < cu.c1) return;
+    cu.i += gridDim.x;
+    ++cu.local;
+    cursor_item(a, cu);
 }
 
-// The phase accumulator starts at TURN_BIAS + theta0 + w kappa_16: with
-// |theta| < 2^18, every partial sum stays in [2^20, 2^21), where the FP64
-// spacing is 2^-32, so the low mantissa word of the result is frac(theta)
-// * 2^32 (the mod-2pi range reduction) and each DMMA add rounds at 2^-33 turn.
-constexpr double TURN_BIAS = 1572864.0;  // 1.5 * 2^20
-__device__ __forceinline__ uint32_t turn_fraction(double biased_th) { return (uint32_t)__double2loint(biased_th); }
-
-// A operand words of one spin-sample: M = 2^(tj r2 + l2) cis(2 pi u / 2^32),
-// split into FP16 hi + lo, each packed as (re low half, im high half).
-__device__ __forceinline__ void magnetisation(uint32_t u, float tj, float r2, float l2, uint32_t &hi, uint32_t &lo) {
-    const float x = (float)(int32_t)u * 1.4629180792671596e-09f;  // 2 pi / 2^32, x in [-pi, pi)
-    const float a = ex2_approx(fmaf(tj, r2, l2));
-    const float mre = a * cos_approx(x), mim = a * sin_approx(x);
-    const __half2 h = __floats2half2_rn(mre, mim);
-    const float2 hf = __half22float2(h);
-    const __half2 l = __floats2half2_rn(mre - hf.x, mim - hf.y);
-    hi = *reinterpret_cast<const uint32_t *>(&h);
-    lo = *reinterpret_cast<const uint32_t *>(&l);
-}
+constexpr float TWO_PI_2M25 = 1.8725351414619534e-07f;  // 2 pi / 2^25: one unit of the 23-bit quarter-turn angle
+constexpr float MAGIC_1P5_2P23 = 12582912.0f;           // 1.5 * 2^23
 
 template <int N>
 __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
-    constexpr int BB = b_bytes(N);
-    constexpr int HALF = N / 2;  // accumulator columns drained per magnetisation thread
+    constexpr int CB = coil_b_bytes(N);
+    constexpr int STAGE_BYTES = CB + PHASE_B_BYTES + PARAM_BYTES;
+    constexpr int NQ = N / 4;  // coil columns drained per magnetisation warp
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     const int NSTAGE = args.nstage;
-    uint8_t *sB = smem;                                             // NSTAGE * BB
-    double *sSpin = reinterpret_cast<double *>(sB + NSTAGE * BB);  // NSTAGE * SPIN_BYTES
-    uint64_t *bars = reinterpret_cast<uint64_t *>(reinterpret_cast<uint8_t *>(sSpin) + NSTAGE * SPIN_BYTES);
-    uint64_t *full = bars;                    // [NSTAGE] loader -> consumers (tx)
-    uint64_t *empty = bars + MAX_STAGE;       // [NSTAGE] MMA commit -> loader
-    uint64_t *a_full = bars + 2 * MAX_STAGE;  // [2] magnetisation warps -> MMA
-    uint64_t *a_empty = a_full + 2;           // [2] MMA commit -> magnetisation warps
-    uint64_t *d_full = a_empty + 2;           // [2] MMA commit -> drain
-    uint64_t *d_empty = d_full + 2;           // [2] drain -> MMA
-    uint64_t *t_full = d_empty + 2;           // [8 row groups][2] phase warp -> magnetisation warp
-    uint64_t *t_empty = t_full + 16;          // [8 row groups][2] magnetisation warp -> phase warp
-    uint64_t *done = t_empty + 16;            // [1] final MMA commit
+    uint8_t *sA = smem;                                  // 2 x PHASE_A_BYTES
+    uint8_t *sStage = smem + 2 * PHASE_A_BYTES;          // NSTAGE x STAGE_BYTES
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sStage + (size_t)NSTAGE * STAGE_BYTES);
+    uint64_t *full = bars;                   // [NSTAGE] loader -> MMA, magnetisation (tx)
+    uint64_t *empty = bars + MAX_STAGE;      // [NSTAGE] coil MMA commit -> loader
+    uint64_t *a_full_ph = empty + MAX_STAGE; // [2] loader -> MMA (phase A tile, tx)
+    uint64_t *a_empty_ph = a_full_ph + 2;    // [2] last phase MMA of an item -> loader
+    uint64_t *p_full = a_empty_ph + 2;       // phase MMA commit -> magnetisation
+    uint64_t *p_empty = p_full + 1;          // magnetisation warps -> MMA
+    uint64_t *a_full = p_empty + 1;          // magnetisation warps -> MMA (coil A written)
+    uint64_t *a_empty = a_full + 1;          // coil MMA commit -> magnetisation
+    uint64_t *d_full = a_empty + 1;          // last coil MMA of an item -> drain
+    uint64_t *d_empty = d_full + 1;          // drain (coil classes cleared) -> MMA
+    uint64_t *done = d_empty + 1;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -341,15 +332,15 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             mbar_init(&empty[i], 1);
         }
         for (int i = 0; i < 2; ++i) {
-            mbar_init(&a_full[i], NMAG_WARPS);  // one elected arrive per magnetisation warp
-            mbar_init(&a_empty[i], 1);
-            mbar_init(&d_full[i], 1);
-            mbar_init(&d_empty[i], NMAG_WARPS);
+            mbar_init(&a_full_ph[i], 1);
+            mbar_init(&a_empty_ph[i], 1);
         }
-        for (int i = 0; i < 16; ++i) {
-            mbar_init(&t_full[i], 1);
-            mbar_init(&t_empty[i], 1);
-        }
+        mbar_init(p_full, 1);
+        mbar_init(p_empty, NMAG_WARPS);
+        mbar_init(a_full, NMAG_WARPS);
+        mbar_init(a_empty, 1);
+        mbar_init(d_full, 1);
+        mbar_init(d_empty, NMAG_WARPS);
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -363,269 +354,151 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
-
-    const int n_items = args.tiles * args.slabs;
-    const int G = (int)gridDim.x;
-    const int gq = lane >> 2, tq = lane & 3;
     bool dead = false;
 
     if (warp == LOAD_WARP) {
         if (lane == 0) {
-            int stage = 0;
-            uint32_t eph = 1;  // parity of empty[stage] that frees it (the first pass is free)
-            for (int i = blockIdx.x; i < n_items && !dead; i += G) {
-                const Item it = item_of(args, i);
-                for (int c = it.c0; c < it.c1; ++c) {
-                    if (!mbar_wait(&empty[stage], eph)) {
+            int g = 0;
+            int issued[MAX_STAGE] = {0, 0, 0, 0, 0, 0};
+            int issued_a[2] = {0, 0};
+            for (Cursor cu = cursor_start(args); cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
+                const int ib = cu.local & 1;
+                if (!mbar_wait(&a_empty_ph[ib], (uint32_t)(((cu.local >> 1) + 1) & 1))) {
+                    atomicOr(args.err, 1u);
+                    dead = true;
+                    break;
+                }
+                mbar_expect_tx(&a_full_ph[ib], (uint32_t)PHASE_A_BYTES);
+                bulk_g2s(sA + ib * PHASE_A_BYTES, args.phase_a + (size_t)cu.tile * PHASE_A_BYTES, PHASE_A_BYTES,
+                         &a_full_ph[ib]);
+                ++issued_a[ib];
+                for (int c = cu.c0; c < cu.c1; ++c, ++g) {
+                    const int stage = g % NSTAGE;
+                    if (!mbar_wait(&empty[stage], (uint32_t)(((g / NSTAGE) + 1) & 1))) {
                         atomicOr(args.err, 1u);
                         dead = true;
                         break;
                     }
-                    mbar_expect_tx(&full[stage], (uint32_t)(BB + SPIN_BYTES));
-                    bulk_g2s(sB + (size_t)stage * BB, args.b_operand + (size_t)c * BB, (uint32_t)BB, &full[stage]);
-                    bulk_g2s(reinterpret_cast<uint8_t *>(sSpin) + (size_t)stage * SPIN_BYTES,
-                             reinterpret_cast<const uint8_t *>(args.spin_table) + (size_t)c * SPIN_BYTES,
-                             (uint32_t)SPIN_BYTES, &full[stage]);
-                    if (++stage == NSTAGE) {
-                        stage = 0;
-                        eph ^= 1u;
-                    }
+                    uint8_t *st = sStage + (size_t)stage * STAGE_BYTES;
+                    mbar_expect_tx(&full[stage], (uint32_t)STAGE_BYTES);
+                    bulk_g2s(st, args.coil_b + (size_t)c * CB, CB, &full[stage]);
+                    bulk_g2s(st + CB, args.phase_b + (size_t)c * PHASE_B_BYTES, PHASE_B_BYTES, &full[stage]);
+                    bulk_g2s(st + CB + PHASE_B_BYTES, args.params + (size_t)c * PARAM_BYTES, PARAM_BYTES,
+                             &full[stage]);
+                    ++issued[stage];
                 }
             }
+            // Before the CTA leaves (also on the failure path), let every copy
+            // this warp issued land: no bulk copy may still be writing into
+            // shared memory when the CTA exits.
+            for (int s = 0; s < NSTAGE; ++s)
+                if (issued[s] > 0) (void)mbar_wait_budget(&full[s], (uint32_t)((issued[s] - 1) & 1), 100000000LL);
+            for (int b = 0; b < 2; ++b)
+                if (issued_a[b] > 0)
+                    (void)mbar_wait_budget(&a_full_ph[b], (uint32_t)((issued_a[b] - 1) & 1), 100000000LL);
         }
         __syncwarp();
     } else if (warp == MMA_WARP) {
         if (lane == 0) {
-            // kind::f16: D f32 (bit 4), A and B f16 (format 0), both K-major; N = 2N columns.
-            constexpr uint32_t idesc = (1u << 4) | ((uint32_t)((2 * N) >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-            int g = 0;    // chunks issued; chunk g uses A buffer g % 2
-            int gen = 0;  // accumulator generations issued; generation gen uses accumulator gen % 2
-            int stage = 0;
-            uint32_t fph = 0;  // parity of full[stage] for chunk g
-            for (int i = blockIdx.x; i < n_items && !dead; i += G) {
-                const Item it = item_of(args, i);
-                for (int c = it.c0; c < it.c1; ++c, ++g) {
-                    const int buf = g & 1, dbuf = gen & 1;
-                    const int ci = c - it.c0;
-                    const bool gen_first = (ci % FLUSH) == 0;
-                    const bool gen_last = (ci % FLUSH) == FLUSH - 1 || c + 1 == it.c1;
-                    if (gen_first && !mbar_wait(&d_empty[dbuf], (uint32_t)(((gen >> 1) + 1) & 1))) {
-                        atomicOr(args.err, 2u);
-                        dead = true;
-                        break;
-                    }
-                    if (!mbar_wait(&full[stage], fph) || !mbar_wait(&a_full[buf], (uint32_t)((g >> 1) & 1))) {
-                        atomicOr(args.err, 4u);
-                        dead = true;
-                        break;
-                    }
-                    tc_fence_after();
-                    const uint32_t dcol = tmem + d_col(N, dbuf);
-                    const uint32_t acol = tmem + a_col(N, buf);
-                    const uint32_t sbase = smem_u32(sB + (size_t)stage * BB);
-                    // The small lo pass goes first, while D is small, then the hi pass.
+            constexpr uint32_t id_ph1 = idesc_i8(PH_N1, true, true);
+            constexpr uint32_t id_ph2 = idesc_i8(PH_N2, true, true);
+            constexpr uint32_t id_ph3 = idesc_i8(PH_N3, true, true);
+            constexpr uint32_t id_c3 = idesc_i8(3 * N, false, true);
+            constexpr uint32_t id_c2 = idesc_i8(2 * N, false, true);
+            Cursor cp = cursor_start(args), cc = cp;
+            int gp = 0, gc = 0;
+            // Phase MMAs of chunk gp (cursor cp): classes into TMEM columns P_COL.
+            auto issue_phase = [&]() -> bool {
+                const int stage = gp % NSTAGE;
+                const int ib = cp.local & 1;
+                if (!mbar_wait(&full[stage], (uint32_t)((gp / NSTAGE) & 1))) return false;
+                if (cp.c == cp.c0 && !mbar_wait(&a_full_ph[ib], (uint32_t)((cp.local >> 1) & 1))) return false;
+                if (!mbar_wait(p_empty, (uint32_t)((gp + 1) & 1))) return false;
+                tc_fence_after();
+                const uint32_t a0 = smem_u32(sA + ib * PHASE_A_BYTES);
+                const uint32_t b0 = smem_u32(sStage + (size_t)stage * STAGE_BYTES + CB);
+                tc_mma_i8_ss(tmem + P_COL, sdesc(a0), sdesc(b0), id_ph1, 0u);
+                tc_mma_i8_ss(tmem + P_COL + 32u, sdesc(a0 + TM * 32), sdesc(b0 + PH_OFF2), id_ph2, 1u);
+                tc_mma_i8_ss(tmem + P_COL + 96u, sdesc(a0 + 2 * TM * 32), sdesc(b0 + PH_OFF3), id_ph3, 1u);
+                tc_commit(p_full);
+                if (cp.c + 1 == cp.c1) tc_commit(&a_empty_ph[ib]);
+                ++gp;
+                cursor_next(args, cp);
+                return true;
+            };
+            // Coil MMAs of chunk gc (cursor cc): digit classes into TMEM columns D_COL.
+            auto issue_coil = [&]() -> bool {
+                const int stage = gc % NSTAGE;
+                if (!mbar_wait(a_full, (uint32_t)(gc & 1))) return false;
+                if (cc.c == cc.c0 && !mbar_wait(d_empty, (uint32_t)(cc.local & 1))) return false;
+                tc_fence_after();
+                const uint32_t b0 = smem_u32(sStage + (size_t)stage * STAGE_BYTES);
 #pragma unroll
-                    for (int ks = 0; ks < KSTEPS; ++ks)
-                        tc_mma_f16(dcol, acol + 32u + (uint32_t)ks * 8u, bdesc(sbase + (uint32_t)(ks * 2 * N * 32)),
-                                   idesc, (gen_first && ks == 0) ? 0u : 1u);
-#pragma unroll
-                    for (int ks = 0; ks < KSTEPS; ++ks)
-                        tc_mma_f16(dcol, acol + (uint32_t)ks * 8u, bdesc(sbase + (uint32_t)(ks * 2 * N * 32)), idesc,
-                                   1u);
-                    tc_commit(&empty[stage]);
-                    tc_commit(&a_empty[buf]);
-                    if (gen_last) {
-                        tc_commit(&d_full[dbuf]);
-                        ++gen;
-                    }
-                    if (++stage == NSTAGE) {
-                        stage = 0;
-                        fph ^= 1u;
-                    }
+                for (int ks = 0; ks < 2; ++ks) {
+                    const uint64_t bd = sdesc(b0 + (uint32_t)(ks * 3 * N * 32));
+                    const uint32_t acol = tmem + A_COL + (uint32_t)(ks * 24);
+                    tc_mma_i8_ts(tmem + D_COL, acol, bd, id_c3, 1u);                       // m2 x [c2|c1|c0]
+                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)N, acol + 8u, bd, id_c3, 1u);   // m1 x [c2|c1|c0]
+                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)(2 * N), acol + 16u, bd, id_c2, 1u);  // m0 x [c2|c1]
+                }
+                tc_commit(&empty[stage]);
+                tc_commit(a_empty);
+                if (cc.c + 1 == cc.c1) tc_commit(d_full);
+                ++gc;
+                cursor_next(args, cc);
+                return true;
+            };
+            if (cp.valid && !issue_phase()) {
+                atomicOr(args.err, 2u);
+                dead = true;
+            }
+            while (cc.valid && !dead) {
+                if (cp.valid && !issue_phase()) {
+                    atomicOr(args.err, 2u);
+                    dead = true;
+                    break;
+                }
+                if (!issue_coil()) {
+                    atomicOr(args.err, 4u);
+                    dead = true;
+                    break;
                 }
             }
-            // Drain: wait for every issued MMA before TMEM is released.
+            // Wait for every issued MMA before TMEM is released.
             tc_commit(done);
             if (!mbar_wait(done, 0)) atomicOr(args.err, 8u);
         }
         __syncwarp();
-    } else if (warp < NPHASE_WARPS) {
-        // Phase warp w: turn fractions of tile rows 32q + 16p .. +15 (q = w % 4,
-        // p = w / 4): 2 x 4 DMMA 8x8 tiles per chunk, K = 16, accumulators
-        // initialised with TURN_BIAS + theta0 + w kappa_16; written to TMEM
-        // columns t_col(tb) + spin of those rows.
-        const int q = warp & 3, p = warp >> 2;
-        const int grp = q * 2 + p;  // row group shared with magnetisation warp 8 + warp
-        const uint32_t t_lane = (uint32_t)(q * 32 + p * 16) << 16;
-        int stage = 0, tb = 0;
-        uint32_t fph = 0, tk = 0;  // parities of full[stage] and of this use of turn buffer tb
-        for (int i = blockIdx.x; i < n_items && !dead; i += G) {
-            const Item it = item_of(args, i);
-            // A fragments: kappa[row 32q + 16p + 8mt + gq][k = 4ks + tq], and kappa_16 of the row.
-            double ka[2][4], k16[2];
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                int64_t j = (int64_t)it.tile * TM + q * 32 + p * 16 + mt * 8 + gq;
-                if (j >= args.nsamples) j = args.nsamples - 1;
-                const double *pr = args.prefix + (size_t)j * PREFIX_STRIDE;
-#pragma unroll
-                for (int ks = 0; ks < 4; ++ks) ka[mt][ks] = pr[4 * ks + tq];
-                k16[mt] = pr[16];
-            }
-            for (int c = it.c0; c < it.c1; ++c) {
-                bool ok = mbar_wait(&full[stage], fph);
-                ok = ok && mbar_wait(&t_empty[grp * 2 + tb], tk ^ 1u);
-                __syncwarp();
-                if (!__all_sync(0xffffffffu, ok)) {
-                    if (lane == 0) atomicOr(args.err, 128u);
-                    dead = true;
-                    break;
-                }
-                tc_fence_after();
-                const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                const uint32_t tcol = tmem + t_col(N, tb) + t_lane;
-                // Two spin groups at a time: 4 independent accumulator chains,
-                // k-step outermost.
-#pragma unroll
-                for (int np = 0; np < 2; ++np) {
-                    double bf[2][4], th[2][2][2];
-#pragma unroll
-                    for (int n2 = 0; n2 < 2; ++n2) {
-                        const int nt = 2 * np + n2;
-#pragma unroll
-                        for (int ks = 0; ks < 4; ++ks) bf[n2][ks] = tab[tab_index(4 * ks + tq, 8 * nt + gq)];
-                        const double2 t0 = *reinterpret_cast<const double2 *>(tab + TAB_THETA0 + 8 * nt + 2 * tq);
-                        const double2 dw = *reinterpret_cast<const double2 *>(tab + TAB_DW + 8 * nt + 2 * tq);
-                        const double b0 = t0.x + TURN_BIAS, b1 = t0.y + TURN_BIAS;
-#pragma unroll
-                        for (int mt = 0; mt < 2; ++mt) {
-                            th[n2][mt][0] = fma(dw.x, k16[mt], b0);
-                            th[n2][mt][1] = fma(dw.y, k16[mt], b1);
-                        }
-                    }
-#pragma unroll
-                    for (int ks = 0; ks < 4; ++ks)
-#pragma unroll
-                        for (int n2 = 0; n2 < 2; ++n2)
-#pragma unroll
-                            for (int mt = 0; mt < 2; ++mt)
-                                dmma_8x8x4(th[n2][mt][0], th[n2][mt][1], ka[mt][ks], bf[n2][ks]);
-                    // Spin groups 2np, 2np+1: 16x256b.x2 register order [4 n2 + 2 mt + i].
-                    uint32_t v[8];
-#pragma unroll
-                    for (int n2 = 0; n2 < 2; ++n2)
-#pragma unroll
-                        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                            for (int ii = 0; ii < 2; ++ii) v[4 * n2 + 2 * mt + ii] = turn_fraction(th[n2][mt][ii]);
-                    tmem_st_16x256b_x2(tcol + (uint32_t)(16 * np), v);
-                }
-                tmem_wait_st();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&t_full[grp * 2 + tb]);
-                if (++stage == NSTAGE) {
-                    stage = 0;
-                    fph ^= 1u;
-                }
-                if (++tb == 2) {
-                    tb = 0;
-                    tk ^= 1u;
-                }
-            }
-        }
     } else {
-        // Magnetisation warp w: TMEM lane quarter q = w % 4, half h: tile rows
-        // 32q + 16h .. +15 (the rows of phase warp w - 8) and all 32 spins of
-        // each chunk.  For the accumulator drain it takes thread <-> tile row
-        // 32q + lane and output columns [h N/2, (h+1) N/2).
-        const int q = warp & 3, h = (warp - NPHASE_WARPS) >> 2;
-        const int grp = q * 2 + h;
-        const uint32_t q_lane = (uint32_t)(q * 32) << 16;
-        const uint32_t m_lane = (uint32_t)(q * 32 + h * 16) << 16;
+        // Magnetisation warp: lane quarter q (tile rows 32q + lane), spins 8cq .. 8cq+7.
+        const int q = warp & 3, cq = warp >> 2;
+        const uint32_t lq = (uint32_t)(q * 32) << 16;
         const int row = q * 32 + lane;
-        // Amplitude scale of the segment: M is formed as M / 2^eA (|M| <= 1).
-        const float l2off = (float)pow2_ceil_exp(*args.amp_max);
-        int g = 0;    // chunks produced by this CTA
-        int gen = 0;  // accumulator generations completed
-        int stage = 0, tb = 0;
-        uint32_t tk = 0;
-        int pend = -1;  // accumulator generation waiting to be drained
-        double *pend_dst = nullptr;
-        bool pend_wfirst = false, pend_promote = false, pend_pfirst = false;
-        // Drain: add the generation's two halves (A.B_hi, A.B_lo) into the
-        // FP32 row accumulator in TMEM; every WINDOW chunks, and at the end of
-        // an item, add the accumulator into the FP64 split-K partial instead.
-        auto drain = [&]() -> bool {
-            const int buf = pend & 1;
-            const bool ok = mbar_wait(&d_full[buf], (uint32_t)((pend >> 1) & 1));
+        const int ks = cq >> 1;
+        // Amplitude scale of the segment: M is formed as M / 2^eA (the ex2
+        // argument stays small, so its float rounding stays near 2^-24
+        // relative), then times 2^22 by adding 22 to the exponent field.
+        const float l2off = (float)(-pow2_ceil_exp(*args.amp_max));
+        // Clear the coil classes (completion 0 of d_empty releases the first item).
+        {
+            const uint32_t z[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+#pragma unroll
+                for (int cb = 0; cb < NQ; cb += 4)
+                    tmem_st_x4(tmem + lq + D_COL + (uint32_t)(t * N + cq * NQ + cb), z);
+            tmem_wait_st();
+            tc_fence_before();
             __syncwarp();
-            if (!__all_sync(0xffffffffu, ok)) {
-                if (lane == 0) atomicOr(args.err, 32u);
-                return false;
-            }
-            tc_fence_after();
-            const uint32_t dsrc = tmem + q_lane + d_col(N, buf) + (uint32_t)(h * HALF);
-            const uint32_t asrc = tmem + q_lane + acc_col(N) + (uint32_t)(h * HALF);
-#pragma unroll
-            for (int cb = 0; cb < HALF; cb += 16) {
-                constexpr int W0 = HALF >= 16 ? 16 : 8;
-                const int w = (HALF - cb) >= 16 ? 16 : 8;
-                (void)W0;
-                float d1[16], d2[16], ac[16];
-                if (w == 16) {
-                    tmem_ld_32x32b_x16(dsrc + (uint32_t)cb, d1);
-                    tmem_ld_32x32b_x16(dsrc + (uint32_t)(N + cb), d2);
-                    if (!pend_wfirst) tmem_ld_32x32b_x16(asrc + (uint32_t)cb, ac);
-                } else {
-                    tmem_ld_32x32b_x8(dsrc + (uint32_t)cb, d1);
-                    tmem_ld_32x32b_x8(dsrc + (uint32_t)(N + cb), d2);
-                    if (!pend_wfirst) tmem_ld_32x32b_x8(asrc + (uint32_t)cb, ac);
-                }
-                tmem_wait_ld();
-                if (cb + 16 >= HALF) {
-                    tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(&d_empty[buf]);
-                }
-#pragma unroll
-                for (int e = 0; e < 16; ++e)
-                    if (e < w) d1[e] = pend_wfirst ? d1[e] + d2[e] : (d1[e] + d2[e]) + ac[e];
-                if (pend_promote) {
-                    double *d = pend_dst + cb;
-#pragma unroll
-                    for (int e = 0; e < 16; e += 2) {
-                        if (e < w) {
-                            double2 o = pend_pfirst ? make_double2(0.0, 0.0) : *reinterpret_cast<double2 *>(d + e);
-                            o.x += (double)d1[e];
-                            o.y += (double)d1[e + 1];
-                            *reinterpret_cast<double2 *>(d + e) = o;
-                        }
-                    }
-                } else if (w == 16) {
-                    tmem_st_32x32b_x16(asrc + (uint32_t)cb, d1);
-                } else {
-                    tmem_st_32x32b_x8(asrc + (uint32_t)cb, d1);
-                }
-            }
-            pend = -1;
-            return true;
-        };
-        for (int i = blockIdx.x; i < n_items && !dead; i += G) {
-            const Item it = item_of(args, i);
-            double *dst_piece =
-                args.partial + (((size_t)it.tile * args.slabs + it.z) * TM + row) * (size_t)N + h * HALF;
-            float tj[2];
-#pragma unroll
-            for (int mt = 0; mt < 2; ++mt) {
-                int64_t j = (int64_t)it.tile * TM + q * 32 + h * 16 + mt * 8 + gq;
-                if (j >= args.nsamples) j = args.nsamples - 1;
-                tj[mt] = (float)args.prefix[(size_t)j * PREFIX_STRIDE + PREFIX_T];
-            }
-            for (int c = it.c0; c < it.c1; ++c) {
-                const int buf = g & 1;
-                bool ok = mbar_wait(&t_full[grp * 2 + tb], tk);
-                ok = ok && mbar_wait(&a_empty[buf], (uint32_t)(((g >> 1) + 1) & 1));
+            if (lane == 0) mbar_arrive(d_empty);
+        }
+        int g = 0;
+        for (Cursor cu = cursor_start(args); cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
+            const uint32_t base = args.rows[2 * ((size_t)cu.tile * TM + row)];
+            const float tj = __uint_as_float(args.rows[2 * ((size_t)cu.tile * TM + row) + 1]);
+            for (int c = cu.c0; c < cu.c1; ++c, ++g) {
+                const int stage = g % NSTAGE;
+                bool ok = mbar_wait(p_full, (uint32_t)(g & 1));
                 __syncwarp();
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(args.err, 16u);
@@ -633,69 +506,113 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     break;
                 }
                 tc_fence_after();
-                // Turn fractions of rows 16h + 8mt + gq, spins 8nt + 2tq + i:
-                // 16x256b.x4 register order [4 nt + 2 mt + i].
-                uint32_t tu[16];
-                tmem_ld_16x256b_x4(tmem + t_col(N, tb) + m_lane, tu);
+                // Phase classes w = 7..2 (columns (7 - w) * 32) of this warp's 8 spins.
+                uint32_t pc[6][8];
+#pragma unroll
+                for (int t = 0; t < 6; ++t) tmem_ld_x8(tmem + lq + P_COL + (uint32_t)(t * 32 + cq * 8), pc[t]);
                 tmem_wait_ld();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&t_empty[grp * 2 + tb]);
-                const double *tab = sSpin + (size_t)stage * (SPIN_BYTES / 8);
-                const uint32_t acol = tmem + a_col(N, buf) + m_lane;
-#pragma unroll
-                for (int np = 0; np < 2; ++np) {
-                    // Spin groups 2np, 2np+1: 16x256b.x2 register order [4 n2 + 2 mt + i].
-                    uint32_t hi[8], lo[8];
-#pragma unroll
-                    for (int n2 = 0; n2 < 2; ++n2) {
-                        // This thread's spins of group nt: 8nt + 2tq + i.
-                        const int nt = 2 * np + n2;
-                        const float4 rl = *reinterpret_cast<const float4 *>(tab + TAB_PACK + 8 * nt + 2 * tq);
-                        const float r2v[2] = {rl.x, rl.z};
-                        const float l2v[2] = {rl.y - l2off, rl.w - l2off};
-#pragma unroll
-                        for (int mt = 0; mt < 2; ++mt)
-#pragma unroll
-                            for (int ii = 0; ii < 2; ++ii) {
-                                const int e = 4 * n2 + 2 * mt + ii;
-                                magnetisation(tu[4 * nt + 2 * mt + ii], tj[mt], r2v[ii], l2v[ii], hi[e], lo[e]);
-                            }
-                    }
-                    tmem_st_16x256b_x2(acol + (uint32_t)(16 * np), hi);
-                    tmem_st_16x256b_x2(acol + 32u + (uint32_t)(16 * np), lo);
-                }
-                tmem_wait_st();
-                tc_fence_before();
+                if (lane == 0) mbar_arrive(p_empty);
+                ok = mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1));
                 __syncwarp();
-                if (lane == 0) mbar_arrive(&a_full[buf]);
-                // The previous generation has had a whole chunk of time to
-                // finish: drain it now.
-                if (pend >= 0 && !drain()) {
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(args.err, 32u);
                     dead = true;
                     break;
                 }
-                const int ci = c - it.c0;
-                if ((ci % FLUSH) == FLUSH - 1 || c + 1 == it.c1) {
-                    const int gstart = ci - ci % FLUSH;  // first chunk of this generation
-                    pend = gen++;
-                    pend_dst = dst_piece;
-                    pend_wfirst = (gstart % WINDOW) == 0;
-                    pend_promote = (ci % WINDOW) == WINDOW - 1 || c + 1 == it.c1;
-                    pend_pfirst = gstart < WINDOW;
+                const uint32_t *par =
+                    reinterpret_cast<const uint32_t *>(sStage + (size_t)stage * STAGE_BYTES + CB + PHASE_B_BYTES);
+                uint32_t wd[3][4];  // digit planes m0, m1, m2+64 of spins (2p, 2p+1)
+#pragma unroll
+                for (int pp = 0; pp < 4; ++pp) {
+                    uint32_t vre[2], vim[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int i = 2 * pp + h;
+                        const int s = cq * 8 + i;
+                        const uint32_t u = base + par[s] + (uint32_t)((int32_t)pc[5][i] >> 16) +
+                                           (uint32_t)((int32_t)pc[4][i] >> 8) + pc[3][i] + (pc[2][i] << 8) +
+                                           (pc[1][i] << 16) + (pc[0][i] << 24);
+                        // Quarter-turn reduction: u = turn + 2^29 + 64, quadrant u >> 30,
+                        // remainder (u & (2^30 - 1)) - 2^29 rounded to 23 bits.
+                        const uint32_t fb = ((u >> 7) & 0x7FFFFFu) | 0x4B000000u;
+                        const float x = (__uint_as_float(fb) - MAGIC_1P5_2P23) * TWO_PI_2M25;
+                        const float sn = sin_approx(x), cs = cos_approx(x);
+                        const bool odd = (u & 0x40000000u) != 0u;
+                        const float re = odd ? sn : cs, im = odd ? cs : sn;
+                        const float r2 = __uint_as_float(par[KC + s]);
+                        const float l2 = __uint_as_float(par[2 * KC + s]);
+                        const uint32_t ab = __float_as_uint(ex2_approx(fmaf(tj, r2, l2 + l2off))) + (22u << 23);
+                        const float are = __uint_as_float(ab ^ ((u + 0x40000000u) & 0x80000000u));
+                        const float aim = __uint_as_float(ab ^ (u & 0x80000000u));
+                        // 1.5 * 2^23 + y rounds y to an integer: its bits are 0x4B400000 + y,
+                        // bytes 0, 1 the low digits and byte 2 the top digit + 64.
+                        vre[h] = __float_as_uint(fmaf(are, re, MAGIC_1P5_2P23));
+                        vim[h] = __float_as_uint(fmaf(aim, im, MAGIC_1P5_2P23));
+                    }
+                    // K order of a word: (re, im) of spin 2pp, then of spin 2pp+1.
+                    const uint32_t p0 = prmt(vre[0], vim[0], 0x5140u), p1 = prmt(vre[1], vim[1], 0x5140u);
+                    const uint32_t q0 = prmt(vre[0], vim[0], 0x6262u), q1 = prmt(vre[1], vim[1], 0x6262u);
+                    wd[0][pp] = prmt(p0, p1, 0x5410u);
+                    wd[1][pp] = prmt(p0, p1, 0x7632u);
+                    wd[2][pp] = prmt(q0, q1, 0x5410u);
                 }
-                ++g;
-                if (++stage == NSTAGE) stage = 0;
-                if (++tb == 2) {
-                    tb = 0;
-                    tk ^= 1u;
+                ok = mbar_wait(a_empty, (uint32_t)((g + 1) & 1));
+                __syncwarp();
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) atomicOr(args.err, 128u);
+                    dead = true;
+                    break;
                 }
+                tc_fence_after();
+                const uint32_t acol = tmem + lq + A_COL + (uint32_t)(ks * 24 + 4 * (cq & 1));
+                tmem_st_x4(acol, wd[2]);        // m2 + 64
+                tmem_st_x4(acol + 8u, wd[1]);   // m1
+                tmem_st_x4(acol + 16u, wd[0]);  // m0
+                tmem_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(a_full);
             }
             if (dead) break;
-            if (pend >= 0 && !drain()) {
+            // Item end: the coil classes of this warp's rows and columns into the
+            // item's FP64 partial, then clear them for the next item.
+            bool ok = mbar_wait(d_full, (uint32_t)(cu.local & 1));
+            __syncwarp();
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) atomicOr(args.err, 512u);
                 dead = true;
                 break;
             }
+            tc_fence_after();
+            double *dst = args.partial + (((size_t)cu.tile * args.slabs + cu.z) * TM + row) * (size_t)N + cq * NQ;
+            const uint32_t z[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int cb = 0; cb < NQ; cb += 4) {
+                uint32_t t4[4], t3[4], t2[4], t1[4];
+                const uint32_t col = tmem + lq + D_COL + (uint32_t)(cq * NQ + cb);
+                tmem_ld_x4(col, t4);
+                tmem_ld_x4(col + (uint32_t)N, t3);
+                tmem_ld_x4(col + (uint32_t)(2 * N), t2);
+                tmem_ld_x4(col + (uint32_t)(3 * N), t1);
+                tmem_wait_ld();
+                double v[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const long long s = ((long long)(int32_t)t4[e] << 32) + ((long long)(int32_t)t3[e] << 24) +
+                                        ((long long)(int32_t)t2[e] << 16) + ((long long)(int32_t)t1[e] << 8);
+                    v[e] = ldexp((double)s, -44);
+                }
+                *reinterpret_cast<double2 *>(dst + cb) = make_double2(v[0], v[1]);
+                *reinterpret_cast<double2 *>(dst + cb + 2) = make_double2(v[2], v[3]);
+#pragma unroll
+                for (int t = 0; t < 4; ++t) tmem_st_x4(col + (uint32_t)(t * N), z);
+            }
+            tmem_wait_st();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(d_empty);
         }
     }
     tc_fence_before();
@@ -707,11 +624,14 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 }
 
 // Sum the split-K partials of each (sample, column) in slab order (FP64),
-// undo the power-of-two scaling of the operands and write complex samples:
-// column n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
+// remove the offset of the top magnetisation digit (64 * 2^16 times the
+// column's sensitivity integers, 2^-22 colsum after the 2^-44 scale), undo the
+// power-of-two scaling of the operands and write complex samples: column
+// n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
 template <typename T>
 __global__ void __launch_bounds__(256) split_finalize_kernel(const double *partial, int64_t nsamples, int32_t ncg,
-                                                             int n_cols, int slabs, const int *coil_exp,
+                                                             int n_cols, int slabs, const long long *colsum,
+                                                             const int *coil_exp,
                                                              const unsigned long long *amp_max, cplx<T> *sig,
                                                              int64_t ldsig) {
     // A block sums FIN_ROWS rows x n_cols columns of one time tile over the
@@ -740,7 +660,7 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
             const int e = threadIdx.x + k * 256;
-            if (e < elems) sacc[e] = acc[k];
+            if (e < elems) sacc[e] = acc[k] - ldexp((double)colsum[e % n_cols], -22);
         }
         __syncthreads();
         for (int q = threadIdx.x; q < FIN_ROWS * ncg; q += blockDim.x) {
@@ -783,10 +703,88 @@ __global__ void basis_kernel(const double *x, const double *y, const double *z, 
     }
 }
 
+// Coefficient of phase term `slot` of spin s: basis term slot + 1, or dw/(2 pi).
+__device__ __forceinline__ double term_coef(const double *basis, const double *dw, int64_t s, int slot) {
+    return slot < NSLOT - 1 ? basis[s * 16 + slot + 1] : dw[s] * (1.0 / (2.0 * 3.141592653589793));
+}
 
-// Largest |Re| or |Im| of each coil's sensitivity (bits of a non-negative
-// double, combined with an unsigned max).
-// Per coil: the largest |Re| or |Im| of its sensitivities, as the bits of a
+// Largest |coefficient| of every phase term over the spins (bits of
+// non-negative doubles, combined with an unsigned max).
+__global__ void term_max_kernel(const double *basis, const double *dw, int64_t ns, unsigned long long *mx) {
+    __shared__ unsigned long long smax[NSLOT];
+    if (threadIdx.x < NSLOT) smax[threadIdx.x] = 0ull;
+    __syncthreads();
+    unsigned long long local[NSLOT];
+#pragma unroll
+    for (int k = 0; k < NSLOT; ++k) local[k] = 0ull;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns; s += (int64_t)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NSLOT; ++k)
+            local[k] = max(local[k], (unsigned long long)__double_as_longlong(fabs(term_coef(basis, dw, s, k))));
+#pragma unroll
+    for (int k = 0; k < NSLOT; ++k) atomicMax(&smax[k], local[k]);
+    __syncthreads();
+    if (threadIdx.x < NSLOT && smax[threadIdx.x]) atomicMax(&mx[threadIdx.x], smax[threadIdx.x]);
+}
+
+// Phase B operand of every chunk: per spin the five balanced digits of
+// B_k = rint(b_k 2^38 / bmax_k) for the 16 terms (16 bytes per digit), placed
+// as the B' rows of the three phase MMAs (class block w, spin s):
+//   MMA 1: row (7 - w) 32 + s, K halves digits (w - 4, w - 3), w = 7..2
+//   MMA 2: row (6 - w) 32 + s, K halves digits (w - 2, w - 1), w = 6..2
+//   MMA 3: row (4 - w) 32 + s, K halves digits (w, none),      w = 4..2
+// with zeros where the digit index is outside 0..4 and for padding spins.
+__global__ void phase_b_kernel(const double *basis, const double *dw, int64_t ns, int64_t nchunks,
+                               const unsigned long long *term_max, uint8_t *out) {
+    const int64_t total = nchunks * KC;
+    for (int64_t gs = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gs < total;
+         gs += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t chunk = gs / KC;
+        const int s = (int)(gs % KC);
+        uint32_t dig[PHASE_DIGITS][4];  // digit d of the 16 terms, 4 bytes per word
+#pragma unroll
+        for (int d = 0; d < PHASE_DIGITS; ++d)
+#pragma unroll
+            for (int w = 0; w < 4; ++w) dig[d][w] = 0u;
+        if (gs < ns) {
+            for (int k = 0; k < NSLOT; ++k) {
+                const double bmax = __longlong_as_double((long long)term_max[k]);
+                long long v = 0;
+                if (bmax > 0.0) v = llrint(ldexp(term_coef(basis, dw, gs, k) / bmax, 38));
+                for (int d = 0; d < PHASE_DIGITS; ++d) {
+                    long long dd;
+                    if (d < PHASE_DIGITS - 1) {
+                        dd = ((v + 128) & 255) - 128;
+                        v = (v - dd) >> 8;
+                    } else {
+                        dd = v;
+                    }
+                    dig[d][k >> 2] |= ((uint32_t)dd & 0xFFu) << (8 * (k & 3));
+                }
+            }
+        }
+        uint8_t *base = out + (size_t)chunk * PHASE_B_BYTES;
+        auto put = [&](int off, int row, int kc, int d) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (d >= 0 && d < PHASE_DIGITS) v = make_uint4(dig[d][0], dig[d][1], dig[d][2], dig[d][3]);
+            *reinterpret_cast<uint4 *>(base + off + kmaj(row, kc * 16)) = v;
+        };
+        for (int w = 7; w >= 2; --w) {
+            put(0, (7 - w) * 32 + s, 0, w - 4);
+            put(0, (7 - w) * 32 + s, 1, w - 3);
+        }
+        for (int w = 6; w >= 2; --w) {
+            put(PH_OFF2, (6 - w) * 32 + s, 0, w - 2);
+            put(PH_OFF2, (6 - w) * 32 + s, 1, w - 1);
+        }
+        for (int w = 4; w >= 2; --w) {
+            put(PH_OFF3, (4 - w) * 32 + s, 0, w);
+            put(PH_OFF3, (4 - w) * 32 + s, 1, -1);
+        }
+    }
+}
+
+// Largest |Re| or |Im| of each coil's sensitivities, as the bits of a
 // non-negative double (which order like the values).  Each block reduces a
 // range of whole spin rows in shared memory first (blockDim a multiple of nc
 // when nc <= 256, so a thread always sees the same coil), then merges one
@@ -820,91 +818,101 @@ __global__ void coil_exp_kernel(const unsigned long long *mx, int32_t nc, int *c
         coil_exp[c] = pow2_ceil_exp(mx[c]);
 }
 
-// Sensitivities -> FP16 hi/lo B operand, per coil group of GROUP_COILS coils,
-// scaled by 2^-e(coil) so that every entry is at most 1 in magnitude.  Real
-// K index k = 2 s + comp of local spin s:
-//   B[n][k] = (n < ncg ? Re c(s,n) : Im c(s,n-ncg))   for comp = 0 (re of M),
-//   B[n][k] = (n < ncg ? -Im c(s,n) : Re c(s,n-ncg))  for comp = 1 (im of M);
-// rows 0..N-1 of each K-step slab hold the hi parts, rows N..2N-1 the lo parts.
-__global__ void b_operand_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_cols, int64_t nchunks,
-                                 int ngroups, const int *coil_exp, __half *out) {
-    // One thread per 16-byte core-matrix row: operand row nn (hi rows
-    // 0..n_cols-1, lo rows n_cols..2 n_cols-1) of K-step ks, K-half kb (8
-    // consecutive K = 4 spins x (re, im)).
-    const int64_t total = (int64_t)ngroups * nchunks * KSTEPS * (2 * n_cols) * 2;
+// Sensitivity integer of output column n (coil group coil0, ncg coils) for
+// component comp of M (0: Re M, 1: Im M) of spin sp: Re S = sum Re M Re c -
+// Im M Im c (column n < ncg), Im S = sum Re M Im c + Im M Re c (column ncg + n),
+// each sensitivity scaled by 2^(22 - e_coil), so |value| <= 2^22.
+__device__ __forceinline__ long long coil_int(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int coil0,
+                                              int ncg, const int *coil_exp, int n, int comp, int64_t sp) {
+    if (sp >= ns || n >= 2 * ncg) return 0;
+    const int coil = coil0 + (n < ncg ? n : n - ncg);
+    const cplx<double> cv = csm_rows[sp * nc + coil];
+    const double v = n < ncg ? (comp == 0 ? cv.re : -cv.im) : (comp == 0 ? cv.im : cv.re);
+    return llrint(ldexp(v, 22 - coil_exp[coil]));
+}
+
+// Coil B operand per coil group and chunk: K-step ks (spins 16 ks .. +15,
+// K byte 2 s + comp), rows [c2 | c1 | c0] x n_cols of the balanced digits of
+// the sensitivity integers.  One thread builds one 16-byte piece (one operand
+// row, one half of the K-step: 8 spins x (re, im)).
+__global__ void coil_b_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_cols, int64_t nchunks,
+                              int ngroups, const int *coil_exp, uint8_t *out) {
+    const int rows = 3 * n_cols;
+    const int64_t total = (int64_t)ngroups * nchunks * 2 * rows * 2;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
         int64_t r = i;
-        const int kb = (int)(r & 1);
+        const int kc = (int)(r & 1);
         r >>= 1;
-        const int nn = (int)(r % (2 * n_cols));
-        r /= 2 * n_cols;
-        const int ks = (int)(r % KSTEPS);
-        const int64_t gc = r / KSTEPS;  // group * nchunks + chunk
+        const int row = (int)(r % rows);
+        r /= rows;
+        const int ks = (int)(r & 1);
+        const int64_t gc = r >> 1;  // group * nchunks + chunk
         const int grp = (int)(gc / nchunks);
         const int64_t chunk = gc % nchunks;
-        const bool lopart = nn >= n_cols;
-        const int n = lopart ? nn - n_cols : nn;
+        const int digit = 2 - row / n_cols;  // rows c2, c1, c0
+        const int n = row % n_cols;
         const int coil0 = grp * GROUP_COILS;
         const int ncg = min(GROUP_COILS, nc - coil0);
-        const bool live = n < 2 * ncg;
-        const int coil = coil0 + (n < ncg ? n : n - ncg);
-        const int e = live ? coil_exp[coil] : 0;
-        __align__(16) __half row[8];
+        uint32_t w[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-        for (int j = 0; j < 8; j += 2) {
-            const int k = 16 * ks + 8 * kb + j;  // even: this spin's (re, im) pair is K = k, k + 1
-            const int64_t sp = chunk * KC + (k >> 1);
-            double v0 = 0.0, v1 = 0.0;
-            if (live && sp < ns) {
-                const cplx<double> cv = csm_rows[sp * nc + coil];
-                // Column n < ncg holds Re S: (re, -im); column ncg + n holds Im S: (im, re).
-                v0 = ldexp(n < ncg ? cv.re : cv.im, -e);
-                v1 = ldexp(n < ncg ? -cv.im : cv.re, -e);
-            }
-            const __half h0 = __double2half(v0), h1 = __double2half(v1);
-            row[j] = lopart ? __double2half(v0 - (double)__half2float(h0)) : h0;
-            row[j + 1] = lopart ? __double2half(v1 - (double)__half2float(h1)) : h1;
+        for (int b = 0; b < 16; ++b) {
+            const int kbyte = kc * 16 + b;
+            const int64_t sp = chunk * KC + ks * 16 + (kbyte >> 1);
+            const long long v = coil_int(csm_rows, ns, nc, coil0, ncg, coil_exp, n, kbyte & 1, sp);
+            const int d = balanced_digit(v, digit, 3);
+            w[b >> 2] |= ((uint32_t)d & 0xFFu) << (8 * (b & 3));
         }
-        uint8_t *base = reinterpret_cast<uint8_t *>(out) + (size_t)gc * b_bytes(n_cols) + (size_t)ks * 2 * n_cols * 32;
-        const size_t off = (size_t)(nn / 8) * 256 + (size_t)kb * 128 + (size_t)(nn % 8) * 16;
-        *reinterpret_cast<uint4 *>(base + off) = *reinterpret_cast<const uint4 *>(row);
+        uint8_t *base = out + (size_t)gc * coil_b_bytes(n_cols) + (size_t)ks * rows * 32;
+        *reinterpret_cast<uint4 *>(base + kmaj(row, kc * 16)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
-// Spin table of a segment, from the state at its start (layout of
-// tab_index per chunk): the 16 basis terms, theta0 = arg(m0)/(2 pi), dw/(2 pi)
-// (0 if dw is off in precession) and the packed float2 (-log2(e)/T2,
-// log2|m0|).  Also records the largest |m0| (amplitude scale of the FP16
-// operand) and checks the phase range: |theta| must stay below 2^18 turns for
-// the fixed-point reduction (error bit 64 otherwise).
-__global__ void spin_table_kernel(const double *basis, const double *dw, const double *T2, const cplx<double> *xy,
-                                  int64_t ns, int64_t nchunks, uint32_t method, const double *colmax,
-                                  unsigned int *err, unsigned long long *amp_max, double *table) {
+// Per coil group and output column: the sum over all spins and both
+// components of the sensitivity integers (exact, int64), one block per
+// column.
+__global__ void colsum_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_cols, const int *coil_exp,
+                              long long *colsum) {
+    __shared__ long long part[256];
+    const int grp = blockIdx.x / n_cols, n = blockIdx.x % n_cols;
+    const int coil0 = grp * GROUP_COILS;
+    const int ncg = min(GROUP_COILS, nc - coil0);
+    long long acc = 0;
+    for (int64_t sp = threadIdx.x; sp < ns; sp += blockDim.x)
+        acc += coil_int(csm_rows, ns, nc, coil0, ncg, coil_exp, n, 0, sp) +
+               coil_int(csm_rows, ns, nc, coil0, ncg, coil_exp, n, 1, sp);
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) colsum[blockIdx.x] = part[0];
+}
+
+// Per-segment spin parameters of every chunk, [turn of arg(m0) x 32 | r2 x 32
+// | l2 x 32]: the initial phase as a 32-bit turn fraction, -log2(e)/T2 and
+// log2|m0| (float); also the largest |m0| (amplitude scale of the segment).
+__global__ void spin_params_kernel(const double *T2, const cplx<double> *xy, int64_t ns, int64_t nchunks,
+                                   unsigned long long *amp_max, uint32_t *params) {
     const int64_t total = nchunks * KC;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total;
          s += (int64_t)gridDim.x * blockDim.x) {
-        double *t = table + (s / KC) * (SPIN_BYTES / 8);
+        uint32_t *p = params + (s / KC) * (PARAM_BYTES / 4);
         const int sl = (int)(s % KC);
-        double row[17];
-        for (int k = 0; k < 17; ++k) row[k] = 0.0;
-        double theta0 = 0.0;
-        float2 rl = make_float2(0.0f, -INFINITY);
+        uint32_t th = 0u;
+        float r2 = 0.0f, l2 = -INFINITY;
         unsigned long long amp = 0ull;
         if (s < ns) {
-            for (int k = 0; k < 16; ++k) row[k] = basis[s * 16 + k];
-            row[16] = (method & HOMS_DW_PRECESSION) ? dw[s] / (2.0 * 3.141592653589793) : 0.0;
             const cplx<double> m0 = xy[s];
             const double mag = hypot(m0.re, m0.im);
-            theta0 = atan2(m0.im, m0.re) / (2.0 * 3.141592653589793);
-            double bound = fabs(theta0);
-            for (int k = 0; k < 17; ++k) bound += fabs(row[k]) * colmax[k];
-            if (!(bound < 262144.0)) atomicOr(err, 64u);
-            rl.x = (float)(-1.4426950408889634 / T2[s]);
-            rl.y = mag > 0.0 ? (float)log2(mag) : -INFINITY;
+            const double t0 = atan2(m0.im, m0.re) * (1.0 / (2.0 * 3.141592653589793));
+            th = (uint32_t)(unsigned long long)llrint(ldexp(t0 - floor(t0), 32));
+            r2 = (float)(-1.4426950408889634 / T2[s]);
+            l2 = mag > 0.0 ? (float)log2(mag) : -INFINITY;
             amp = (unsigned long long)__double_as_longlong(mag);
         }
-        // One atomic per warp for the amplitude maximum (bits of non-negative doubles order like the values).
+        // One atomic per warp for the amplitude maximum.
         const unsigned active = __activemask();
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -912,10 +920,9 @@ __global__ void spin_table_kernel(const double *basis, const double *dw, const d
             if ((active >> ((threadIdx.x & 31) ^ o)) & 1u) amp = max(amp, other);
         }
         if ((threadIdx.x & 31) == __ffs(active) - 1 && amp) atomicMax(amp_max, amp);
-        for (int k = 0; k < NTERM; ++k) t[tab_index(k, sl)] = row[k];
-        t[TAB_THETA0 + sl] = theta0;
-        t[TAB_DW + sl] = row[16];
-        *reinterpret_cast<float2 *>(&t[TAB_PACK + sl]) = rl;
+        p[sl] = th;
+        p[KC + sl] = __float_as_uint(r2);
+        p[2 * KC + sl] = __float_as_uint(l2);
     }
 }
 
@@ -1000,17 +1007,81 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
     }
 }
 
+// Phase A operand of every tile of a segment and the per-sample rows: for
+// sample j the integers K_k(j) = rint(kappa_k(j) bmax_k 2^26) of the 16 terms
+// as five balanced digits, placed as the A' tiles [a4|a3], [a2|a1], [a0|0]
+// (row j % 128 of tile j / 128), the base turn rint(frac(kappa_0) 2^32) +
+// 2^29 + 64 (quarter-turn offset and the rounding of the 23-bit angle) and
+// the elapsed time.  Rows past nsamples are zero.  Sets error bit 64 when a
+// term's range bmax_k max|kappa_k| exceeds PHASE_RANGE_LIMIT turns.
+__global__ void phase_a_kernel(const double *prefix, int64_t nsamples, int64_t nrows,
+                               const unsigned long long *term_max, unsigned int *err, uint8_t *phase_a,
+                               uint32_t *rows) {
+    const double *kmax = prefix + (size_t)(nsamples + 1) * PREFIX_STRIDE;
+    if (blockIdx.x == 0 && threadIdx.x < NSLOT) {
+        const double bmax = __longlong_as_double((long long)term_max[threadIdx.x]);
+        if (!(bmax * kmax[threadIdx.x + 1] <= PHASE_RANGE_LIMIT)) atomicOr(err, 64u);
+    }
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nrows;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t dig[PHASE_DIGITS][4];
+#pragma unroll
+        for (int d = 0; d < PHASE_DIGITS; ++d)
+#pragma unroll
+            for (int w = 0; w < 4; ++w) dig[d][w] = 0u;
+        uint32_t base = 0x20000040u;
+        float tj = 0.0f;
+        if (j < nsamples) {
+            const double *pr = prefix + (size_t)j * PREFIX_STRIDE;
+            for (int k = 0; k < NSLOT; ++k) {
+                const double bmax = __longlong_as_double((long long)term_max[k]);
+                // |K| <= 2^38 is checked above; clamp so a failed check cannot overflow
+                const double kv = fmin(fmax(ldexp(pr[k + 1] * bmax, 26), -2.7e11), 2.7e11);
+                long long v = llrint(kv);
+                for (int d = 0; d < PHASE_DIGITS; ++d) {
+                    long long dd;
+                    if (d < PHASE_DIGITS - 1) {
+                        dd = ((v + 128) & 255) - 128;
+                        v = (v - dd) >> 8;
+                    } else {
+                        dd = v;
+                    }
+                    dig[d][k >> 2] |= ((uint32_t)dd & 0xFFu) << (8 * (k & 3));
+                }
+            }
+            const double k0 = pr[0];
+            base += (uint32_t)(unsigned long long)llrint(ldexp(k0 - floor(k0), 32));
+            tj = (float)pr[PREFIX_T];
+        }
+        const int64_t tile = j / TM;
+        const int r = (int)(j % TM);
+        uint8_t *t = phase_a + (size_t)tile * PHASE_A_BYTES;
+        auto put = [&](int m, int kc, int d) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (d >= 0) v = make_uint4(dig[d][0], dig[d][1], dig[d][2], dig[d][3]);
+            *reinterpret_cast<uint4 *>(t + m * TM * 32 + kmaj(r, kc * 16)) = v;
+        };
+        put(0, 0, 4);
+        put(0, 1, 3);
+        put(1, 0, 2);
+        put(1, 1, 1);
+        put(2, 0, 0);
+        put(2, 1, -1);
+        rows[2 * j] = base;
+        rows[2 * j + 1] = __float_as_uint(tj);
+    }
+}
+
 // Final state of a segment in FP64: Mxy = |m0| e^{-T/T2} cis(2 pi theta_end),
 // Mz = Mz e^{-T/T1} + rho (1 - e^{-T/T1}).
-__global__ void state_update_kernel(const double *table, const double *endrow, const double *T1, const double *T2,
-                                    const double *rho, int64_t ns, cplx<double> *xy, double *mz) {
+__global__ void state_update_kernel(const double *basis, const double *dw, const double *endrow, const double *T1,
+                                    const double *T2, const double *rho, int64_t ns, cplx<double> *xy, double *mz) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns; s += (int64_t)gridDim.x * blockDim.x) {
-        const double *t = table + (s / KC) * (SPIN_BYTES / 8);
-        const int sl = (int)(s % KC);
-        double th = fma(t[TAB_DW + sl], endrow[16], t[TAB_THETA0 + sl]);
-        for (int k = 0; k < NTERM; ++k) th = fma(t[tab_index(k, sl)], endrow[k], th);
-        const double T = endrow[PREFIX_T];
         const cplx<double> m0 = xy[s];
+        double th = fma(dw[s] * (1.0 / (2.0 * 3.141592653589793)), endrow[16],
+                        atan2(m0.im, m0.re) * (1.0 / (2.0 * 3.141592653589793)));
+        for (int k = 0; k < 16; ++k) th = fma(basis[s * 16 + k], endrow[k], th);
+        const double T = endrow[PREFIX_T];
         const double mag = hypot(m0.re, m0.im);
         const double f = th - rint(th);
         double sn, cs;
@@ -1023,7 +1094,6 @@ __global__ void state_update_kernel(const double *table, const double *endrow, c
 }
 
 inline int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32)); }
-
 
 // Self-test of the bounded-wait path: one thread waits, with `budget`
 // cycles, on an mbarrier that nothing arrives at; when the wait runs out it
@@ -1049,19 +1119,26 @@ cudaError_t wait_selftest(unsigned int *err, long long budget_cycles, cudaStream
     return cudaGetLastError();
 }
 
+double split_bytes_per_spin(int32_t ncoils) {
+    const int ngroups = (ncoils + GROUP_COILS - 1) / GROUP_COILS;
+    const int ncg_max = std::min<int32_t>(ncoils, GROUP_COILS);
+    const int n_cols = std::max(16, ((2 * ncg_max + 15) / 16) * 16);
+    return 128.0 + (double)PHASE_B_BYTES / KC + (double)ngroups * coil_b_bytes(n_cols) / KC + PARAM_BYTES / KC;
+}
+
 SplitResident::~SplitResident() {
-    for (void *p : {spin_table, prefix, tvec, partial, amp, err})
+    for (void *p : {params, prefix, phase_a, rows, partial, amp, err})
         if (p) cudaFree(p);
     if (!phantom_view)
-        for (void *p : {basis, b_operand, coil_exp})
+        for (void *p : {basis, phase_b, coil_b, colsum, term_max, coil_exp})
             if (p) cudaFree(p);
 }
 
 // Forget shared phantom operands (owned elsewhere) so that they are rebuilt.
 static void split_detach(SplitResident &r) {
     if (!r.phantom_view) return;
-    r.basis = r.b_operand = r.coil_exp = nullptr;
-    r.basis_bytes = r.b_bytes = r.coil_exp_bytes = 0;
+    r.basis = r.phase_b = r.coil_b = r.colsum = r.term_max = r.coil_exp = nullptr;
+    r.basis_bytes = r.phase_b_bytes = r.coil_b_bytes = r.colsum_bytes = r.term_max_bytes = r.coil_exp_bytes = 0;
     r.phantom_view = false;
 }
 
@@ -1077,7 +1154,6 @@ static cudaError_t grow(void *&p, size_t &have, size_t need) {
 
 cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *x, const void *y, const void *z,
                           const void *dw, const void *csm_rows, bool is_f64, cudaStream_t stream, std::string *err) {
-    (void)dw;
     if (!is_f64) {
         *err =
             "split mode takes FP64 phantom and sequence arrays: FP32 positions alone carry phase errors above the "
@@ -1096,22 +1172,27 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
     r.ns_pad = nchunks * KC;
     cudaError_t e;
     if ((e = grow(r.basis, r.basis_bytes, sizeof(double) * 16 * (size_t)ns)) != cudaSuccess) return e;
-    if ((e = grow(r.b_operand, r.b_bytes, (size_t)b_bytes(n_cols) * (size_t)nchunks * ngroups)) != cudaSuccess)
+    if ((e = grow(r.phase_b, r.phase_b_bytes, (size_t)PHASE_B_BYTES * (size_t)nchunks)) != cudaSuccess) return e;
+    if ((e = grow(r.coil_b, r.coil_b_bytes, (size_t)coil_b_bytes(n_cols) * (size_t)nchunks * ngroups)) != cudaSuccess)
         return e;
+    if ((e = grow(r.colsum, r.colsum_bytes, sizeof(long long) * (size_t)n_cols * ngroups)) != cudaSuccess) return e;
+    if ((e = grow(r.term_max, r.term_max_bytes, sizeof(unsigned long long) * NSLOT)) != cudaSuccess) return e;
     // Per-coil scale exponents, preceded by the per-coil maxima they come from.
     if ((e = grow(r.coil_exp, r.coil_exp_bytes, (sizeof(unsigned long long) + sizeof(int)) * (size_t)nc)) !=
         cudaSuccess)
         return e;
-    if (!r.amp) {
-        if ((e = cudaMalloc(&r.amp, sizeof(unsigned long long))) != cudaSuccess) return e;
-    }
-    if (!r.err) {
-        if ((e = cudaMalloc(&r.err, sizeof(unsigned int))) != cudaSuccess) return e;
-    }
+    if (!r.amp && (e = cudaMalloc(&r.amp, sizeof(unsigned long long))) != cudaSuccess) return e;
+    if (!r.err && (e = cudaMalloc(&r.err, sizeof(unsigned int))) != cudaSuccess) return e;
     unsigned long long *cmax = reinterpret_cast<unsigned long long *>(r.coil_exp);
     int *cexp = reinterpret_cast<int *>(cmax + nc);
     basis_kernel<<<grid_for(ns), 256, 0, stream>>>((const double *)x, (const double *)y, (const double *)z, ns,
                                                    (double *)r.basis);
+    if ((e = cudaMemsetAsync(r.term_max, 0, sizeof(unsigned long long) * NSLOT, stream)) != cudaSuccess) return e;
+    term_max_kernel<<<(int)std::max<int64_t>(1, std::min<int64_t>((ns + 255) / 256, 148 * 4)), 256, 0, stream>>>(
+        (const double *)r.basis, (const double *)dw, ns, (unsigned long long *)r.term_max);
+    phase_b_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>((const double *)r.basis, (const double *)dw, ns, nchunks,
+                                                           (const unsigned long long *)r.term_max,
+                                                           (uint8_t *)r.phase_b);
     if ((e = cudaMemsetAsync(cmax, 0, sizeof(unsigned long long) * (size_t)nc, stream)) != cudaSuccess) return e;
     {
         const int threads = nc <= 256 ? nc * (256 / nc) : 256;
@@ -1124,33 +1205,35 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
         coil_max_kernel<<<blocks, threads, smem, stream>>>((const cplx<double> *)csm_rows, ns, nc, cmax);
     }
     coil_exp_kernel<<<1, 128, 0, stream>>>(cmax, nc, cexp);
-    const int64_t total = (int64_t)ngroups * nchunks * KSTEPS * 2 * n_cols * 2;
-    b_operand_kernel<<<grid_for(total), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_cols, nchunks,
-                                                          ngroups, cexp, (__half *)r.b_operand);
+    const int64_t pieces = (int64_t)ngroups * nchunks * 2 * 3 * n_cols * 2;
+    coil_b_kernel<<<grid_for(pieces), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_cols, nchunks,
+                                                        ngroups, cexp, (uint8_t *)r.coil_b);
+    colsum_kernel<<<ngroups * n_cols, 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_cols, cexp,
+                                                        (long long *)r.colsum);
     return cudaGetLastError();
 }
 
-// Shared memory: 1 KB alignment slack, NSTAGE x (B operand + spin table), the barriers.
+// Shared memory: 1 KB alignment slack, two phase A tiles, NSTAGE stages, the barriers.
 constexpr size_t SMEM_LIMIT = 227 * 1024;
-constexpr size_t SMEM_FIXED = 1024 + 512;
+constexpr size_t SMEM_FIXED = 1024 + 2 * PHASE_A_BYTES + 256;
+
+static size_t stage_bytes(int n_cols) { return (size_t)coil_b_bytes(n_cols) + PHASE_B_BYTES + PARAM_BYTES; }
 
 static int kernel_stages(int n_cols) {
-    const size_t per = (size_t)b_bytes(n_cols) + SPIN_BYTES;
-    return (int)std::min<size_t>(MAX_STAGE, (SMEM_LIMIT - SMEM_FIXED) / per);
+    return (int)std::min<size_t>(MAX_STAGE, (SMEM_LIMIT - SMEM_FIXED) / stage_bytes(n_cols));
 }
 
-static size_t kernel_smem(int n_cols) {
-    return SMEM_FIXED + (size_t)kernel_stages(n_cols) * (b_bytes(n_cols) + SPIN_BYTES);
-}
+static size_t kernel_smem(int n_cols) { return SMEM_FIXED + (size_t)kernel_stages(n_cols) * stage_bytes(n_cols); }
 
 // Number of chunk slabs per tile: the smallest that keeps the busiest CTA's
 // work (items x (chunks per item + an allowance for the per-item start-up))
-// within reach of the best split.
+// within reach of the best split, with at most MAX_ITEM_CHUNKS chunks per item.
 static int choose_slabs(int64_t tiles, int64_t nchunks, int64_t G) {
-    int best = 1;
+    const int64_t zmin = std::max<int64_t>(1, (nchunks + MAX_ITEM_CHUNKS - 1) / MAX_ITEM_CHUNKS);
+    int best = (int)zmin;
     double best_cost = 1e300;
-    const int64_t zmax = std::min<int64_t>(nchunks, 4096);
-    for (int64_t z = 1; z <= zmax; ++z) {
+    const int64_t zmax = std::max<int64_t>(zmin, std::min<int64_t>(nchunks, 4096));
+    for (int64_t z = zmin; z <= zmax; ++z) {
         const int64_t per_cta = (tiles * z + G - 1) / G;
         const double cost = (double)per_cta * (double)((nchunks + z - 1) / z + 2);
         if (cost < best_cost * 0.995) {
@@ -1190,27 +1273,33 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         *err = "internal: split segment without its ADC rank and column tables";
         return cudaSuccess;
     }
-    const uint32_t m = a.method;
     const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2);
     if ((e = grow(r.prefix, r.prefix_bytes, prefix_rows * PREFIX_STRIDE * sizeof(double))) != cudaSuccess) return e;
-    if ((e = grow(r.spin_table, r.spin_bytes, (size_t)nchunks * SPIN_BYTES)) != cudaSuccess) return e;
+    if ((e = grow(r.params, r.params_bytes, (size_t)nchunks * PARAM_BYTES)) != cudaSuccess) return e;
     // The segment's samples are the global ADC indices sample0 .. sample0 + nsamples - 1.
     prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(a.src_dev),
                                           (const uint8_t *)a.adc, a.grank, sample0, n_lo, n_hi, nsamples, a.gamma,
                                           (double *)r.prefix);
     if ((e = cudaMemsetAsync(r.amp, 0, sizeof(unsigned long long), stream)) != cudaSuccess) return e;
-    spin_table_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>(
-        (const double *)r.basis, (const double *)a.dw, (const double *)a.T2, (const cplx<double> *)a.xy, r.ns, nchunks,
-        m, (const double *)r.prefix + (size_t)(nsamples + 1) * PREFIX_STRIDE, (unsigned int *)r.err,
-        (unsigned long long *)r.amp, (double *)r.spin_table);
+    spin_params_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>((const double *)a.T2, (const cplx<double> *)a.xy,
+                                                               r.ns, nchunks, (unsigned long long *)r.amp,
+                                                               (uint32_t *)r.params);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (a.launches) *a.launches += 2;
     if (nsamples > 0) {
+        if ((e = grow(r.phase_a, r.phase_a_bytes, (size_t)tiles * PHASE_A_BYTES)) != cudaSuccess) return e;
+        if ((e = grow(r.rows, r.rows_bytes, (size_t)tiles * TM * 2 * sizeof(uint32_t))) != cudaSuccess) return e;
+        phase_a_kernel<<<grid_for(tiles * TM), 256, 0, stream>>>(
+            (const double *)r.prefix, nsamples, tiles * TM, (const unsigned long long *)r.term_max,
+            (unsigned int *)r.err, (uint8_t *)r.phase_a, (uint32_t *)r.rows);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (a.launches) *a.launches += 1;
         int dev = 0, nsm = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
         const int slabs = choose_slabs(tiles, nchunks, nsm);
         const int64_t n_items = tiles * slabs;
-        if (tiles > INT32_MAX / slabs || nchunks > INT32_MAX) {
+        if (tiles > INT32_MAX / slabs || nchunks > INT32_MAX || slabs > nchunks) {
             *err = "split mode: segment too large for one launch";
             return cudaSuccess;
         }
@@ -1220,12 +1309,13 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         const size_t smem = kernel_smem(r.n_mma);
         const int *cexp = reinterpret_cast<const int *>(reinterpret_cast<const unsigned long long *>(r.coil_exp) + r.nc);
         KernelArgs ka;
-        ka.prefix = (const double *)r.prefix;
-        ka.spin_table = (const double *)r.spin_table;
+        ka.phase_a = (const uint8_t *)r.phase_a;
+        ka.phase_b = (const uint8_t *)r.phase_b;
+        ka.params = (const uint8_t *)r.params;
+        ka.rows = (const uint32_t *)r.rows;
         ka.amp_max = (const unsigned long long *)r.amp;
         ka.partial = (double *)r.partial;
         ka.err = (unsigned int *)r.err;
-        ka.nsamples = nsamples;
         ka.n_chunks = (int)nchunks;
         ka.tiles = (int)tiles;
         ka.slabs = slabs;
@@ -1236,7 +1326,7 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         for (int grp = 0; grp < r.ngroups; ++grp) {
             const int coil0 = grp * GROUP_COILS;
             const int ncg = std::min<int>(GROUP_COILS, r.nc - coil0);
-            ka.b_operand = (const uint8_t *)r.b_operand + (size_t)grp * nchunks * b_bytes(r.n_mma);
+            ka.coil_b = (const uint8_t *)r.coil_b + (size_t)grp * nchunks * coil_b_bytes(r.n_mma);
             e = launch_precession(r.n_mma, ka, (unsigned)G, smem, stream);
             if (a.ev_stop && grp + 1 == r.ngroups) cudaEventRecordWithFlags(a.ev_stop, stream, ev_flags);
             if (a.launches) *a.launches += 2;
@@ -1244,32 +1334,40 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
             const int fin_blocks = (int)std::min<int64_t>(tiles * (TM / 32), 148 * 8);
             if (a.sizeof_T == 8)
                 split_finalize_kernel<double><<<fin_blocks, 256, 0, stream>>>(
-                    (const double *)r.partial, nsamples, ncg, r.n_mma, slabs, cexp + coil0,
+                    (const double *)r.partial, nsamples, ncg, r.n_mma, slabs,
+                    (const long long *)r.colsum + (size_t)grp * r.n_mma, cexp + coil0,
                     (const unsigned long long *)r.amp, (cplx<double> *)a.sig + sample0 + (int64_t)coil0 * a.nadc,
                     a.nadc);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
     }
-    if (a.launches) *a.launches += 3;
+    if (a.launches) *a.launches += 1;
     state_update_kernel<<<grid_for(r.ns), 256, 0, stream>>>(
-        (const double *)r.spin_table, (const double *)r.prefix + (size_t)nsamples * PREFIX_STRIDE, (const double *)a.T1,
-        (const double *)a.T2, (const double *)a.rho, r.ns, (cplx<double> *)a.xy, (double *)a.mz);
+        (const double *)r.basis, (const double *)a.dw, (const double *)r.prefix + (size_t)nsamples * PREFIX_STRIDE,
+        (const double *)a.T1, (const double *)a.T2, (const double *)a.rho, r.ns, (cplx<double> *)a.xy,
+        (double *)a.mz);
     return cudaGetLastError();
 }
 
 cudaError_t split_attach(SplitResident &r, const SplitResident &src) {
     if (&r == &src) return cudaSuccess;
     if (!r.phantom_view) {
-        for (void **p : {&r.basis, &r.b_operand, &r.coil_exp}) {
+        for (void **p : {&r.basis, &r.phase_b, &r.coil_b, &r.colsum, &r.term_max, &r.coil_exp}) {
             if (*p) cudaFree(*p);
             *p = nullptr;
         }
     }
     r.basis = src.basis;
-    r.b_operand = src.b_operand;
+    r.phase_b = src.phase_b;
+    r.coil_b = src.coil_b;
+    r.colsum = src.colsum;
+    r.term_max = src.term_max;
     r.coil_exp = src.coil_exp;
     r.basis_bytes = src.basis_bytes;
-    r.b_bytes = src.b_bytes;
+    r.phase_b_bytes = src.phase_b_bytes;
+    r.coil_b_bytes = src.coil_b_bytes;
+    r.colsum_bytes = src.colsum_bytes;
+    r.term_max_bytes = src.term_max_bytes;
     r.coil_exp_bytes = src.coil_exp_bytes;
     r.ns = src.ns;
     r.ns_pad = src.ns_pad;
@@ -1307,7 +1405,8 @@ cudaError_t split_check(SplitResident &r, cudaStream_t stream, std::string *err)
     if (e != cudaSuccess) return e;
     if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return e;
     if (h & 64u)
-        *err = "split mode: the accumulated phase of a precession segment exceeds 2^18 turns";
+        *err = "split mode: a field term's phase range within one precession segment exceeds 4096 turns "
+               "(max |basis value| x max |field integral|); run it in plain mode";
     else if (h != 0)
         *err = "split kernel: a bounded device wait timed out (code " + std::to_string(h) + ")";
     return cudaSuccess;

@@ -9,34 +9,54 @@
 
 namespace homs {
 
-// Device operands that depend only on the phantom (built once per plan):
-// per-spin FP64 basis rows and the receive sensitivities, scaled per coil by a
-// power of two and split into FP16 hi/lo pairs, laid out in the canonical
-// no-swizzle K-major UMMA layout, one operand per group of 32 coils.
+// Device operands of the split path.  The phantom-dependent ones are built
+// once (split_prepare) and may be shared read-only by many runs
+// (split_attach); the per-segment ones belong to each SplitResident.
+//
+// Phantom operands (all exact integer digits of fixed-point values):
+//   basis     per-spin FP64 basis rows (state update, phase operand)
+//   phase_b   per 32-spin chunk: the phase MMAs' B operand, five balanced
+//             int8 digits of every spin's 16 field-term coefficients
+//             (basis terms 1..15 and dw/(2 pi)), laid out for the three
+//             phase MMAs
+//   coil_b    per coil group and chunk: three balanced int8 digits of the
+//             scaled sensitivities (real embedding of the complex product)
+//   colsum    per coil group and output column: sum of the sensitivity
+//             integers (undoes the offset of the top magnetisation digit)
+//   term_max  per field term: the largest |coefficient| over the spins (FP64)
+//   coil_exp  per coil: max |Re|,|Im| (u64 bits), then the scale exponent
 struct SplitResident {
-    void *basis = nullptr;     // [ns_pad][16] double
-    void *b_operand = nullptr; // [groups][nchunks][4 ksteps][2N rows (hi, lo)][16 f16]
-    void *spin_table = nullptr;  // per-segment spin parameters, [nchunks][608] double
-    void *prefix = nullptr;    // per-segment phase table, [nadc_seg_pad][24] double
-    void *tvec = nullptr;      // unused (the ADC ranks and column pointers come with SplitRunArgs)
-    void *partial = nullptr;   // FP64 split-K partials, [tiles][slabs][128][N]
-    void *coil_exp = nullptr;  // per coil: max |Re|,|Im| (u64 bits), then the scale exponent (int)
-    void *amp = nullptr;       // per segment: bits of the largest |m0| (u64)
-    void *err = nullptr;       // device error word
-    size_t basis_bytes = 0, b_bytes = 0, spin_bytes = 0, prefix_bytes = 0, tvec_bytes = 0, partial_bytes = 0,
-           coil_exp_bytes = 0;
+    void *basis = nullptr;
+    void *phase_b = nullptr;
+    void *coil_b = nullptr;
+    void *colsum = nullptr;
+    void *term_max = nullptr;
+    void *coil_exp = nullptr;
+    // per-segment work
+    void *params = nullptr;   // per chunk: turn of arg(m0), -log2(e)/T2, log2|m0|
+    void *prefix = nullptr;   // FP64 trapezoid prefix table, [rows][24]
+    void *phase_a = nullptr;  // per 128-sample tile: the phase MMAs' A operand
+    void *rows = nullptr;     // per sample: base turn (h0 term + offsets), elapsed time
+    void *partial = nullptr;  // FP64 split-K partials, [tiles][slabs][128][N]
+    void *amp = nullptr;      // bits of the largest |m0| of the segment (u64)
+    void *err = nullptr;      // device error word
+    size_t basis_bytes = 0, phase_b_bytes = 0, coil_b_bytes = 0, colsum_bytes = 0, term_max_bytes = 0,
+           coil_exp_bytes = 0, params_bytes = 0, prefix_bytes = 0, phase_a_bytes = 0, rows_bytes = 0,
+           partial_bytes = 0;
     int64_t ns = 0, ns_pad = 0;
     int32_t nc = 0, n_mma = 0, ngroups = 1;
-    // basis, b_operand and coil_exp belong to another SplitResident (a
-    // device-resident phantom shared by many runs); the rest is this one's.
+    // The phantom operands belong to another SplitResident (a device-resident
+    // phantom shared by many runs); the rest is this one's.
     bool phantom_view = false;
     SplitResident() = default;
     SplitResident(const SplitResident &) = delete;
     SplitResident &operator=(const SplitResident &) = delete;
     ~SplitResident();
     size_t device_bytes() const {
-        return (phantom_view ? 0 : basis_bytes + b_bytes + coil_exp_bytes) + spin_bytes + prefix_bytes + tvec_bytes +
-               partial_bytes;
+        return (phantom_view ? 0
+                             : basis_bytes + phase_b_bytes + coil_b_bytes + colsum_bytes + term_max_bytes +
+                                   coil_exp_bytes) +
+               params_bytes + prefix_bytes + phase_a_bytes + rows_bytes + partial_bytes;
     }
 };
 
@@ -99,7 +119,11 @@ cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n
 cudaError_t wait_selftest(unsigned int *err, long long budget_cycles, cudaStream_t stream);
 
 // Read the device error word (synchronises the stream).  Sets *err if a
-// bounded wait timed out or the phase range check failed.
+// bounded wait timed out or a segment's phase range is out of bounds.
 cudaError_t split_check(SplitResident &r, cudaStream_t stream, std::string *err);
+
+// Device bytes of the split path's operands per spin (phantom operands of one
+// simulation with `ncoils` coils), for admission estimates.
+double split_bytes_per_spin(int32_t ncoils);
 
 }  // namespace homs
