@@ -149,11 +149,12 @@ def test_split_fp32_plan_matches_simulate(gpu_context):
 
 
 def test_split_phase_range_is_reported(gpu_context):
-    # A spin 1 km from the isocentre accumulates more than 2^18 turns in a
-    # segment: the split path refuses it with HOMS_EUNSUPPORTED and a message.
+    # A spin 1 km from the isocentre makes a field term's phase range (largest
+    # basis value x largest field integral) exceed 4096 turns in a segment:
+    # the split path's fixed-point phase refuses it with HOMS_EUNSUPPORTED.
     obj, seq, st = W.high_order_workload(nspins=33, nsteps=8, ncoils=2)
     obj.x[5] = 1000.0
     with pytest.raises(homs.HomsError) as e:
         homs.run_blocks(obj, seq, [(0, 8)], [False], BlochHighOrder("1111"), "f64", "split", st)
     assert e.value.status == 3
-    assert "2^18" in str(e.value)
+    assert "4096 turns" in str(e.value)
