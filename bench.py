@@ -13,9 +13,15 @@ through the C ABI (homs_simulate) from pinned host buffers, with all
 host<->device copies inside the timed region.  With N > 1 every rank runs an
 independent replica (the engine does not shard spins across GPUs).
 
-Further keys on one GPU: ``roofline`` (with ``tensor_pipe``: the FP16
-contraction and FP64 DMMA phase work the split kernel issues, and their
-combined share of the tensor pipe), ``cpu_baseline``, ``clocks``,
+Further keys on one GPU: ``roofline`` (the algorithmic 8 flops per unit
+against dense bf16), ``pipes`` (what the split kernel issues: int8 tensor
+operations against the int8 rate, SFU operations against 16 per SM and clock
+at the sampled clock), ``plain_f64`` (the plain FP64 kernel on the same
+workload, device-timed, and the split/plain ratio), ``accuracy`` (signal
+NRMSE of split and plain against the CPU FP64 oracle on a spin subsample, and
+of split against plain FP64 at full size), ``configs`` (the 2D 1-coil, 2D
+8-coil and 3D TR-loop workloads: split and plain throughput and NRMSE),
+``cpu_baseline``, ``clocks``,
 ``serving`` / ``serving_resident`` (the mixed request stream),
 ``reference_gpu_equivalent`` (the reference's GPU design restated with
 torch/cuBLAS and timed on the same workload), ``kspace`` (encoding export)
@@ -44,9 +50,12 @@ METRIC = "spin*sample*coil/s"
 UNIT = "spin*sample*coil/s"
 CONFIG_INDEX = 2
 FLOPS_PER_UNIT = 8.0  # one complex multiply-accumulate per spin*sample*coil
-F16_FLOPS_PER_UNIT = 32.0  # the split contraction as issued: hi and lo passes against B hi|lo columns
-FP64_FLOPS_PER_SPIN_SAMPLE = 32.0  # the phase tile on the FP64 DMMA pipe
-FP64_DMMA_PEAK = 37.0  # TFLOP/s, m8n8k4.f64 rate measured by a probe on this pool's B200s
+# What the split kernel issues per 32-spin x 128-sample chunk tile (N = 64 output columns):
+# 3 phase MMAs of 128 x (192, 160, 96) x 32 int8 and 6 coil MMAs of 128 x (192, 192, 128) x 32 int8.
+I8_MACS_PER_SPIN_SAMPLE = (192 + 160 + 96 + 2 * (192 + 192 + 128)) * 32 / 32.0  # MACs per spin*sample
+SFU_OPS_PER_SPIN_SAMPLE = 3.0  # sin, cos, ex2 on the MUFU (XU) pipe
+SFU_PER_SM_CLK = 16.0  # MUFU results per SM and clock
+N_SM = 148
 
 
 def _dist():
@@ -67,7 +76,8 @@ def _peaks():
 
 
 def _traffic_per_launch():
-    """DRAM bytes per launch of the split kernel from the committed ncu summary."""
+    """DRAM bytes per launch of the split kernel, quoted from the committed ncu
+    summary (not measured by this run: bench.py runs without a profiler)."""
     path = os.path.join(ROOT, "profiles", "split_precession_kernel_cfg2.md")
     try:
         for line in open(path):
@@ -172,29 +182,121 @@ def _units(w):
     return len(w.obj) * sum(count_block_adc(w.seq.adc, w.parts)) * w.obj.ncoils
 
 
-def cpu_baseline(seconds_target=20.0, threads=None):
+def cpu_baseline(seconds_target=20.0, threads=None, k=CONFIG_INDEX, stride=None):
     """Time the CPU oracle (a port of the reference's CPU Float64 path) on a
-    deterministic spin subsample of the workload, on all host threads."""
+    deterministic spin subsample of workload ``k``, on all host threads.
+
+    The subsample is grown until one run takes about half of
+    ``seconds_target`` (or taken as given by ``stride``).  Returns the
+    baseline record, the stride, the subsampled workload and the oracle's
+    signal: the same run is the checker of the GPU results on that subsample
+    (``accuracy_on``)."""
     from homs.model import BlochHighOrder
     from oracle import oracle as orc
     orc.build()
     if threads is None:
         threads = max(1, len(os.sched_getaffinity(0)))
-    # The oracle's cost is linear in the spin count; grow the subsample until
-    # one run takes at least half of the target time.
-    stride = 400
+    fixed = stride is not None
+    stride = stride or 400
     while True:
-        w = _workload(stride=stride)
+        w = _workload(stride=stride, k=k)
         flags = BlochHighOrder(w.mask).flags
         t0 = time.perf_counter()
-        orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)
+        sig = orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)[0]
         dt = time.perf_counter() - t0
-        if dt >= seconds_target / 2 or stride == 1:
+        if fixed or dt >= seconds_target / 2 or stride == 1:
             break
         stride = max(1, int(stride * dt / seconds_target))
-    return {"value": _units(w) / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"every {stride}th spin ({len(w.obj)} spins) x 38000 samples x 32 coils, full sequence, "
-                      f"{dt:.1f} s"}, stride
+    from homs.model import count_block_adc
+    nadc = sum(count_block_adc(w.seq.adc, w.parts))
+    return ({"value": _units(w) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+             "sample": f"every {stride}th spin ({len(w.obj)} spins) x {nadc} samples x {w.obj.ncoils} coils, full "
+                       f"sequence, {dt:.2f} s"}, stride, w, sig)
+
+
+def accuracy_on(w, ref_sig, ctx, modes=("split", "plain")):
+    """Signal NRMSE of the engine's modes against the oracle signal of the
+    same (subsampled) workload, both from FP64 arrays."""
+    import homs
+    from homs.model import BlochHighOrder
+    method = BlochHighOrder(w.mask)
+    den = float(np.linalg.norm(ref_sig))
+    out = {}
+    for mode in modes:
+        got = homs.run_blocks(w.obj, w.seq, w.parts, w.excitation, method, "f64", mode, context=ctx)[0]
+        out[mode] = float(np.linalg.norm(got - ref_sig) / den)
+    return out
+
+
+def time_plan(ctx, w, mode, precision="f64", steps=3, warmup=1):
+    """Device time of prepared-plan runs of workload ``w`` (inputs resident,
+    signal to device memory; CUDA events on the context's stream).  Returns
+    the timing record and the last run's signal (device tensor, Nc x Nadc)."""
+    import torch
+
+    import homs
+    from homs import _lib
+    from homs.model import BlochHighOrder
+    lib = _lib.load()
+    params = {"sim_method": BlochHighOrder(w.mask), "precision": precision, "homs_precision": mode}
+    plan = homs.prepare_simulation(w.obj, w.seq, sim_params=params, parts=w.parts, excitation=w.excitation,
+                                   context=ctx)
+    sig = torch.empty((plan.nc, plan.nadc), dtype=torch.complex128 if precision == "f64" else torch.complex64,
+                      device="cuda")
+
+    def step():
+        _lib.check(lib.homs_plan_run(plan.handle, ctypes.c_void_p(sig.data_ptr()), _lib.HOMS_DEVICE, None),
+                   ctx.handle)
+
+    for _ in range(warmup):
+        step()
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    fused_ms, fused_n = 0.0, 0
+    a.record(stream)
+    for _ in range(steps):
+        step()
+        t = _lib.Timing()
+        _lib.check(lib.homs_plan_timing(plan.handle, ctypes.byref(t)))
+        fused_ms += t.fused_kernel_ms
+        fused_n += t.fused_launches
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    plan.close()
+    units = _units(w)
+    return {"ms_per_step": ms, "units_per_s": units / (ms / 1e3), "steps": steps, "warmup": warmup,
+            "fused_kernel_ms_per_launch": fused_ms / max(fused_n, 1)}, sig
+
+
+def config_legs(ctx):
+    """The other named workloads: split and plain FP64 throughput (device
+    time of plan runs) and each mode's signal NRMSE against the CPU oracle
+    on a spin subsample (the oracle run is that config's CPU baseline).  The
+    3D TR loop runs split at full size and plain FP64 on every 20th spin
+    (its time is linear in the spin count; 32 s per full step)."""
+    import torch
+    out = {}
+    for k, split_stride, plain_stride, oracle_stride, steps in ((0, 1, 1, 1, 5), (1, 1, 1, 1, 3),
+                                                                (3, 1, 20, 2003, 1)):
+        from homs import workloads as W
+        rec = {"workload": _workload_name(k, 1)}
+        w = _workload(split_stride, k)
+        sp, _ = time_plan(ctx, w, "split", steps=steps, warmup=1)
+        rec["split"] = dict(sp, spins=len(w.obj))
+        wp = w if plain_stride == split_stride else _workload(plain_stride, k)
+        pl, _ = time_plan(ctx, wp, "plain", steps=1 if k == 3 else steps, warmup=1)
+        rec["plain_f64"] = dict(pl, spins=len(wp.obj), sample=(f"every {plain_stride}th spin" if plain_stride > 1
+                                                                  else "full workload"))
+        rec["split_over_plain_f64"] = sp["units_per_s"] / pl["units_per_s"]
+        del w, wp
+        torch.cuda.empty_cache()
+        base, stride, ws, ref = cpu_baseline(k=k, stride=oracle_stride)
+        rec["cpu_baseline"] = base
+        rec["nrmse_vs_oracle"] = dict(accuracy_on(ws, ref, ctx), sample=base["sample"])
+        out[W.CONFIG_NAMES[k]] = rec
+    return out
 
 
 def serving_benchmark(n_pool=16, passes=10, load=0.9, slots=4, resident=False):
@@ -394,26 +496,36 @@ def run_reference(args):
     from homs.model import BlochHighOrder
     from oracle import oracle as orc
     # Calibrate a spin subsample of a few seconds per step, then time each
-    # step on that same subsample.
-    base, stride = cpu_baseline(seconds_target=max(3.0, 30.0 / max(args.steps + args.warmup, 1)))
-    w = _workload(stride=stride)
+    # step on that same subsample and report what was timed; the projection
+    # to the full workload (the oracle's time is linear in the spin count)
+    # is a separate, labelled field.
+    base, stride, w, _ = cpu_baseline(seconds_target=max(3.0, 30.0 / max(args.steps + args.warmup, 1)))
     flags = BlochHighOrder(w.mask).flags
     threads = base["cores"]
-    vals = []
+    times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         orc.simulate_c(w.obj, w.seq, w.parts, w.excitation, flags, nthreads=threads)
         if i >= args.warmup:
-            vals.append(_units(w) / (time.perf_counter() - t0))
-    v = statistics.median(vals)
+            times.append(time.perf_counter() - t0)
+    step_s = statistics.median(times)
+    units = _units(w)
+    v = units / step_s
+    full = _workload(1)
+    full_units = _units(full)
+    nadc = units // (len(w.obj) * w.obj.ncoils)
     base["value"] = v
-    base["sample"] = f"every {stride}th spin ({len(w.obj)} spins) x 38000 samples x 32 coils per step, median of " \
-                     f"{args.steps} steps"
+    base["sample"] = (f"every {stride}th spin ({len(w.obj)} spins) x {nadc} samples x {w.obj.ncoils} coils per "
+                      f"step, median of {args.steps} steps")
+    base["projection"] = {"workload": _workload_name(CONFIG_INDEX, 1), "spins": len(full.obj),
+                          "ms_per_step": full_units / v * 1e3, "extrapolated": True,
+                          "basis": "the oracle's cost is linear in the spin count"}
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": _units(_workload(1)) / v * 1e3 if v else None, "higher_is_better": True,
+           "ms_per_step": step_s * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "3d_stack_of_spirals_100x100x35_350000spins_32coils_4x9500adc",
-                      "spins": 350000, "samples": 38000, "coils": 32, "mask": "1111"},
+           "config": {"workload": _workload_name(CONFIG_INDEX, stride), "spins": len(w.obj),
+                      "spins_timed": len(w.obj), "stride": stride, "samples": int(nadc), "coils": w.obj.ncoils,
+                      "mask": w.mask, "extrapolated": False},
            "impl": "reference", "cpu_baseline": base,
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
@@ -516,18 +628,19 @@ def run_homs(args):
             _lib.check(lib.homs_simulate(ctx.handle, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
                                          ctypes.byref(st), sig_h.ctypes.data, _lib.HOMS_HOST), ctx.handle)
 
-        for _ in range(max(1, args.warmup // 2)):
+        for _ in range(args.warmup):
             e2e_step()
         barrier()
         t0 = time.perf_counter()
-        n_e2e = max(1, min(args.steps, 3))
+        n_e2e = args.steps
         for _ in range(n_e2e):
             e2e_step()
         barrier()
         e_ms = (time.perf_counter() - t0) * 1e3 / n_e2e
         e_value, e_max = replica_throughput(e_ms, units, ws)
         e2e = {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "ms_per_step": e_max}
+               "ms_per_step": e_max, "steps": n_e2e, "warmup": args.warmup,
+               "timing": "host wall time of homs_simulate calls (pinned host buffers, copies inside)"}
 
     if rank != 0:
         if ws > 1:
@@ -547,34 +660,63 @@ def run_homs(args):
             "fallback 1.59 PFLOP/s", "kernel": "split_precession_kernel" if args.mode == "split" else
             "segment_kernel", "kernel_ms_per_launch": avg_launch_ms,
             "units_per_launch": seg_units, "flops_per_unit": FLOPS_PER_UNIT}
-    if args.mode == "split" and achieved_tflops:
-        # What the kernel issues to the shared tensor pipe: the FP16 hi/lo contraction (8 MMAs of
-        # 128x128x16 per 32-spin chunk = 32 flops per unit) against the dense FP16/bf16 peak, and the
-        # FP64 DMMA phase (32 flops per spin*sample) against the DMMA rate a probe measured (37 TF/s).
+    if traffic is not None:
+        roof["traffic_source"] = "quoted from profiles/split_precession_kernel_cfg2.md (one ncu capture)"
+    clk = clocks.summary()
+    pipes = None
+    if args.mode == "split" and avg_launch_ms > 0:
+        # What the split kernel issues, from the same launch times: int8 tensor MACs (exact digit
+        # products) against the int8 rate (twice the dense bf16 rate per MMA shape on sm_100: the
+        # measured bf16 peak x 2; 4.5 POPS nominal) and MUFU ops (sin, cos, ex2) against 16 per SM and
+        # clock at the median sampled SM clock.
         secs = avg_launch_ms / 1e3
-        f16 = F16_FLOPS_PER_UNIT * seg_units / secs / 1e12
-        f64 = FP64_FLOPS_PER_SPIN_SAMPLE * (seg_units / nc) / secs / 1e12
-        roof["tensor_pipe"] = {"f16_mma_tflops": f16, "f16_flops_per_unit": F16_FLOPS_PER_UNIT,
-                               "fp64_dmma_tflops": f64, "fp64_flops_per_spin_sample": FP64_FLOPS_PER_SPIN_SAMPLE,
-                               "fp64_dmma_peak_tflops": FP64_DMMA_PEAK, "combined_share": f16 / bf16_peak +
-                               f64 / FP64_DMMA_PEAK}
-    base = None
-    if ws == 1 and not args.no_cpu_baseline and args.config == CONFIG_INDEX:
-        base, _ = cpu_baseline()
+        spin_samples = seg_units / nc
+        i8_tops = 2.0 * I8_MACS_PER_SPIN_SAMPLE * spin_samples / secs / 1e12
+        mhz = clk.get("sm_mhz") or 1965.0
+        sfu_peak = SFU_PER_SM_CLK * N_SM * mhz * 1e6
+        pipes = {"int8_tensor_tops": i8_tops, "int8_macs_per_spin_sample": I8_MACS_PER_SPIN_SAMPLE,
+                 "int8_peak_tops": 2.0 * bf16_peak, "int8_frac": i8_tops / (2.0 * bf16_peak),
+                 "int8_peak_source": f"2 x {peak_kind} dense bf16",
+                 "sfu_ops_per_s": SFU_OPS_PER_SPIN_SAMPLE * spin_samples / secs,
+                 "sfu_ops_per_spin_sample": SFU_OPS_PER_SPIN_SAMPLE, "sfu_peak_ops_per_s": sfu_peak,
+                 "sfu_frac": SFU_OPS_PER_SPIN_SAMPLE * spin_samples / secs / sfu_peak,
+                 "sfu_peak_source": f"{SFU_PER_SM_CLK:.0f} per SM and clock x {N_SM} SMs x {mhz:.0f} MHz (sampled)",
+                 "spin_samples_per_launch": spin_samples, "kernel_ms_per_launch": avg_launch_ms}
+    base = accuracy = None
+    if ws == 1 and not args.no_cpu_baseline:
+        base, _, w_sub, ref_sub = cpu_baseline(k=args.config)
+        accuracy = {"sample": base["sample"], "nrmse_vs_oracle": accuracy_on(w_sub, ref_sub, ctx)}
+        del w_sub, ref_sub
+    plain = None
+    if ws == 1 and args.mode == "split" and not args.no_plain:
+        pl, sig_plain = time_plan(ctx, w, "plain", precision=args.precision, steps=3, warmup=1)
+        plain = dict(pl, split_over_plain_f64=value / pl["units_per_s"],
+                     note="the plain kernel (the reference's per-spin sequential trapezoid, FP64) on the same "
+                          "workload, device-timed plan runs")
+        d = float(torch.linalg.vector_norm(sig_plain).item())
+        nr = float(torch.linalg.vector_norm(sig_dev - sig_plain).item()) / d
+        if accuracy is None:
+            accuracy = {}
+        accuracy["nrmse_split_vs_plain_f64_full"] = nr
+        del sig_plain
+        torch.cuda.empty_cache()
     nchunks = -(-len(w.obj) // 32)
-    op_mb = nchunks * 16384 * -(-nc // 32) / 1e6 if args.mode == "split" else 0.0
+    op_mb = nchunks * (12288 + 14336) * -(-nc // 32) / 1e6 if args.mode == "split" else 0.0
     csm_mb = len(w.obj) * nc * 16 / 1e6
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-           "dtype": "f64 phase / f32 sfu trig / f16x3 tensor" if args.mode == "split" else args.precision,
+           "dtype": ("int8 tensor: fixed-point phase (5 digits) and coil contraction (3 digits), exact int32 sums;"
+                     " f32 sfu trig; f64 tables") if args.mode == "split" else args.precision,
            "data": "synthetic",
            "config": {"workload": _workload_name(args.config, args.spin_stride), "spins": len(w.obj),
                       "samples": nadc, "coils": nc, "mask": w.mask, "mode": args.mode,
                       "l2": (f"inputs larger than L2 (csm {csm_mb:.0f} MB" +
                              (f", split operand {op_mb:.0f} MB)" if op_mb else ")")) if csm_mb > 126 else
                       f"inputs smaller than L2 (csm {csm_mb:.0f} MB)", "parallelism": f"replicas{ws}"},
-           "roofline": roof, "cpu_baseline": base, "e2e": e2e, "gpu_launches": launches,
-           "clocks": clocks.summary()}
+           "roofline": roof, "pipes": pipes, "plain_f64": plain, "accuracy": accuracy, "cpu_baseline": base,
+           "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+    if ws == 1 and not args.no_configs and args.config == CONFIG_INDEX and args.spin_stride == 1:
+        out["configs"] = config_legs(ctx)
     if ws == 1 and not args.no_serve:
         out["serving"] = serving_benchmark()
         out["serving"]["plain_per_request_units_per_s"] = plain_per_request()
@@ -801,6 +943,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparator on the same workload")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other workloads (2D 1-coil, 2D 8-coil, TR loop)")
     ap.add_argument("--no-kspace", action="store_true", help="skip the encoding-export measurement")
     ap.add_argument("--no-refgpu", action="store_true",
                     help="skip timing the restatement of the reference's GPU design (reference_gpu_equivalent)")
