@@ -32,13 +32,17 @@
 // is ex2.approx of a small argument.  |M| <= 1 after a power-of-two scale per
 // segment.
 //
-// Coil contraction, exactly.  M and the per-coil scaled sensitivities become
-// 22-bit integers, three int8 digits each (M: two low bytes unsigned and the
-// top byte offset by 64; sensitivities balanced).  Six int8 MMAs per 32-spin
-// chunk accumulate the digit classes T4..T1 (weights 2^32..2^8; T0 lies below
-// 2^-36 of the signal) in int32 TMEM for a whole work item, with no rounding
-// at all; each item's classes become one FP64 split-K partial.  The offset of
-// the top digit is removed once per output column in the finalize.
+// Coil contraction, exactly.  M becomes a 30-bit integer (|M| <= 2^30), four
+// int8 digits: the rounding of M 2^22 gives three unsigned bytes (the top one
+// offset by 64) and the float residual of that rounding, times 256, a signed
+// low byte; 30 bits keep spins of small amplitude (outside an excited slice,
+// for instance) precise against a signal that cancels.  The per-coil scaled
+// sensitivities become 22-bit integers, three balanced digits.  Eight int8
+// MMAs per 32-spin chunk accumulate the digit classes T5..T2 (weights
+// 2^40..2^16 of the 2^52 full scale; lower classes lie below 2^-28 of it) in
+// int32 TMEM for a whole work item, with no rounding at all; each item's
+// classes become one FP64 split-K partial.  The offset of the top digit is
+// removed once per output column in the finalize.
 //
 // Kernel organisation (one CTA per SM, persistent, slab-major work items of
 // (time tile of 128 samples) x (range of 32-spin chunks)):
@@ -49,12 +53,12 @@
 //               classes into the item's FP64 partial.
 //   warp 16     MMA issuer: per chunk 3 phase MMAs (A: the tile's integral
 //               digits in shared memory, B: the chunk's coefficient digits)
-//               one chunk ahead, and 6 coil MMAs (A in TMEM, B: the chunk's
+//               one chunk ahead, and 8 coil MMAs (A in TMEM, B: the chunk's
 //               sensitivity digits); tcgen05.commit releases shared-memory
 //               stages and TMEM buffers.
 //   warp 17     loader: cp.async.bulk of each item's phase A tile and each
 //               chunk's operands (non-multicast).
-// TMEM (512 columns): phase classes 192, coil A operand 48, coil classes 4N.
+// TMEM (512 columns): phase classes 192, coil A operand 64, coil classes 4N.
 // Every wait is bounded: on time-out the kernel records the place in a device
 // error word and returns without hanging the GPU.
 #include <algorithm>
@@ -103,8 +107,8 @@ __host__ __device__ constexpr int coil_b_bytes(int n) { return 2 * 3 * n * 32; }
 
 // TMEM columns.
 constexpr uint32_t P_COL = 0;    // phase classes
-constexpr uint32_t A_COL = 192;  // coil A: per K-step [m2 | m1 | m0], 8 columns each
-constexpr uint32_t D_COL = 256;  // coil classes [T4 | T3 | T2 | T1], N columns each
+constexpr uint32_t A_COL = 192;  // coil A: per K-step [d3 | d2 | d1 | d0], 8 columns each
+constexpr uint32_t D_COL = 256;  // coil classes [T5 | T4 | T3 | T2], N columns each
 
 // Canonical no-swizzle K-major layout of an operand with 32 bytes of K per
 // row: core matrices of 8 rows x 16 bytes, K-direction stride 128 B, 8-row
@@ -405,6 +409,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             constexpr uint32_t id_ph3 = idesc_i8(PH_N3, true, true);
             constexpr uint32_t id_c3 = idesc_i8(3 * N, false, true);
             constexpr uint32_t id_c2 = idesc_i8(2 * N, false, true);
+            constexpr uint32_t id_c1 = idesc_i8(N, true, true);  // signed low digit of M
             Cursor cp = cursor_start(args), cc = cp;
             int gp = 0, gc = 0;
             // Phase MMAs of chunk gp (cursor cp): classes into TMEM columns P_COL.
@@ -436,10 +441,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 #pragma unroll
                 for (int ks = 0; ks < 2; ++ks) {
                     const uint64_t bd = sdesc(b0 + (uint32_t)(ks * 3 * N * 32));
-                    const uint32_t acol = tmem + A_COL + (uint32_t)(ks * 24);
-                    tc_mma_i8_ts(tmem + D_COL, acol, bd, id_c3, 1u);                       // m2 x [c2|c1|c0]
-                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)N, acol + 8u, bd, id_c3, 1u);   // m1 x [c2|c1|c0]
-                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)(2 * N), acol + 16u, bd, id_c2, 1u);  // m0 x [c2|c1]
+                    const uint32_t acol = tmem + A_COL + (uint32_t)(ks * 32);
+                    tc_mma_i8_ts(tmem + D_COL, acol, bd, id_c3, 1u);                       // d3 x [c2|c1|c0]
+                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)N, acol + 8u, bd, id_c3, 1u);   // d2 x [c2|c1|c0]
+                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)(2 * N), acol + 16u, bd, id_c2, 1u);  // d1 x [c2|c1]
+                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)(3 * N), acol + 24u, bd, id_c1, 1u);  // d0 x [c2]
                 }
                 tc_commit(&empty[stage]);
                 tc_commit(a_empty);
@@ -477,7 +483,8 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         const int ks = cq >> 1;
         // Amplitude scale of the segment: M is formed as M / 2^eA (the ex2
         // argument stays small, so its float rounding stays near 2^-24
-        // relative), then times 2^22 by adding 22 to the exponent field.
+        // relative), then times 2^22 by adding 22 to the exponent field; the
+        // low digit carries the next 8 bits.
         const float l2off = (float)(-pow2_ceil_exp(*args.amp_max));
         // Clear the coil classes (completion 0 of d_empty releases the first item).
         {
@@ -523,10 +530,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 }
                 const uint32_t *par =
                     reinterpret_cast<const uint32_t *>(sStage + (size_t)stage * STAGE_BYTES + CB + PHASE_B_BYTES);
-                uint32_t wd[3][4];  // digit planes m0, m1, m2+64 of spins (2p, 2p+1)
+                uint32_t wd[4][4];  // digit planes d1, d2, d3 (+64), d0 of spins (2p, 2p+1)
 #pragma unroll
                 for (int pp = 0; pp < 4; ++pp) {
-                    uint32_t vre[2], vim[2];
+                    uint32_t vre[2], vim[2], lre[2], lim[2];
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         const int i = 2 * pp + h;
@@ -547,16 +554,26 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                         const float are = __uint_as_float(ab ^ ((u + 0x40000000u) & 0x80000000u));
                         const float aim = __uint_as_float(ab ^ (u & 0x80000000u));
                         // 1.5 * 2^23 + y rounds y to an integer: its bits are 0x4B400000 + y,
-                        // bytes 0, 1 the low digits and byte 2 the top digit + 64.
-                        vre[h] = __float_as_uint(fmaf(are, re, MAGIC_1P5_2P23));
-                        vim[h] = __float_as_uint(fmaf(aim, im, MAGIC_1P5_2P23));
+                        // bytes 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64.
+                        const float hre = fmaf(are, re, MAGIC_1P5_2P23), him = fmaf(aim, im, MAGIC_1P5_2P23);
+                        vre[h] = __float_as_uint(hre);
+                        vim[h] = __float_as_uint(him);
+                        // The residual y - rint(y) is exact before its one rounding and lies in
+                        // [-0.5, 0.5]; rint(256 residual) (at most 127 after the clamp) is the
+                        // signed low digit d0, byte 0 of the same construction.
+                        const float rre = fminf(fmaf(are, re, -(hre - MAGIC_1P5_2P23)), 0.498f);
+                        const float rim = fminf(fmaf(aim, im, -(him - MAGIC_1P5_2P23)), 0.498f);
+                        lre[h] = __float_as_uint(fmaf(rre, 256.0f, MAGIC_1P5_2P23));
+                        lim[h] = __float_as_uint(fmaf(rim, 256.0f, MAGIC_1P5_2P23));
                     }
                     // K order of a word: (re, im) of spin 2pp, then of spin 2pp+1.
                     const uint32_t p0 = prmt(vre[0], vim[0], 0x5140u), p1 = prmt(vre[1], vim[1], 0x5140u);
                     const uint32_t q0 = prmt(vre[0], vim[0], 0x6262u), q1 = prmt(vre[1], vim[1], 0x6262u);
+                    const uint32_t r0 = prmt(lre[0], lim[0], 0x5140u), r1 = prmt(lre[1], lim[1], 0x5140u);
                     wd[0][pp] = prmt(p0, p1, 0x5410u);
                     wd[1][pp] = prmt(p0, p1, 0x7632u);
                     wd[2][pp] = prmt(q0, q1, 0x5410u);
+                    wd[3][pp] = prmt(r0, r1, 0x5410u);
                 }
                 ok = mbar_wait(a_empty, (uint32_t)((g + 1) & 1));
                 __syncwarp();
@@ -566,10 +583,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     break;
                 }
                 tc_fence_after();
-                const uint32_t acol = tmem + lq + A_COL + (uint32_t)(ks * 24 + 4 * (cq & 1));
-                tmem_st_x4(acol, wd[2]);        // m2 + 64
-                tmem_st_x4(acol + 8u, wd[1]);   // m1
-                tmem_st_x4(acol + 16u, wd[0]);  // m0
+                const uint32_t acol = tmem + lq + A_COL + (uint32_t)(ks * 32 + 4 * (cq & 1));
+                tmem_st_x4(acol, wd[2]);        // d3 + 64
+                tmem_st_x4(acol + 8u, wd[1]);   // d2
+                tmem_st_x4(acol + 16u, wd[0]);  // d1
+                tmem_st_x4(acol + 24u, wd[3]);  // d0 (signed)
                 tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
@@ -590,19 +608,20 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             const uint32_t z[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
             for (int cb = 0; cb < NQ; cb += 4) {
-                uint32_t t4[4], t3[4], t2[4], t1[4];
+                uint32_t t5[4], t4[4], t3[4], t2[4];
                 const uint32_t col = tmem + lq + D_COL + (uint32_t)(cq * NQ + cb);
-                tmem_ld_x4(col, t4);
-                tmem_ld_x4(col + (uint32_t)N, t3);
-                tmem_ld_x4(col + (uint32_t)(2 * N), t2);
-                tmem_ld_x4(col + (uint32_t)(3 * N), t1);
+                tmem_ld_x4(col, t5);
+                tmem_ld_x4(col + (uint32_t)N, t4);
+                tmem_ld_x4(col + (uint32_t)(2 * N), t3);
+                tmem_ld_x4(col + (uint32_t)(3 * N), t2);
                 tmem_wait_ld();
                 double v[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    const long long s = ((long long)(int32_t)t4[e] << 32) + ((long long)(int32_t)t3[e] << 24) +
-                                        ((long long)(int32_t)t2[e] << 16) + ((long long)(int32_t)t1[e] << 8);
-                    v[e] = ldexp((double)s, -44);
+                    // classes in units of 2^16 of the 2^52 full scale (|sum| < 2^55: exact in int64)
+                    const long long s = ((long long)(int32_t)t5[e] << 24) + ((long long)(int32_t)t4[e] << 16) +
+                                        ((long long)(int32_t)t3[e] << 8) + (long long)(int32_t)t2[e];
+                    v[e] = ldexp((double)s, -36);
                 }
                 *reinterpret_cast<double2 *>(dst + cb) = make_double2(v[0], v[1]);
                 *reinterpret_cast<double2 *>(dst + cb + 2) = make_double2(v[2], v[3]);
@@ -624,8 +643,8 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 }
 
 // Sum the split-K partials of each (sample, column) in slab order (FP64),
-// remove the offset of the top magnetisation digit (64 * 2^16 times the
-// column's sensitivity integers, 2^-22 colsum after the 2^-44 scale), undo the
+// remove the offset of the top magnetisation digit (64 * 2^24 times the
+// column's sensitivity integers, 2^-22 colsum after the 2^-52 scale), undo the
 // power-of-two scaling of the operands and write complex samples: column
 // n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
 template <typename T>
