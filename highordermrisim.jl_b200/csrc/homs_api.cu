@@ -1279,6 +1279,8 @@ homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins
             HOMS_CUDA(cudaMemset2DAsync(sig, es * (size_t)ldsig, 0, es * (size_t)nadc, (size_t)ncoils, ctx->stream));
             return HOMS_OK;
         }
+        HOMS_REQUIRE((nadc + PLAIN_STAGE - 1) / PLAIN_STAGE <= 65535,
+                     "nadc above 524280 samples per call (the reduction's grid)");
         const int64_t tiles = (nspins + PLAIN_THREADS - 1) / PLAIN_THREADS;
         HOMS_CUDA(ctx->scratch_partial.ensure(es * (size_t)tiles * (size_t)nadc * (size_t)ncoils));
         if (dtype == HOMS_F64) {

@@ -24,7 +24,12 @@ void *g_scratch_ptr[kMaxDevices];  // device address of g_reduce_scratch, per de
 
 // Device address of the scratch array on the current device.  Host code only
 // sees a host-side stand-in for the array's name, so the address is resolved
-// with cudaGetSymbolAddress once per device, with that device current.
+// with cudaGetSymbolAddress once per device, with that device current.  That
+// first resolution may make the CUDA driver load this library's device code
+// and back the array (an allocation of the driver's own, which can
+// synchronise the device); later calls only read the cached address.  The
+// cache is per device ordinal: after a cudaDeviceReset the address would be
+// stale, so a device reset is not supported while the library is in use.
 homs_status scratch_for_current_device(void **out) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HOMS_ECUDA;
@@ -52,6 +57,11 @@ extern "C" homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, 
     if (nadc > 0 && (!sig || ldsig < nadc)) return HOMS_EINVAL;
     if (nspins > 0 && nadc > 0 && (!states || ldstates < nspins)) return HOMS_EINVAL;
     if (nspins > 0 && (!csm || ldcsm < nspins)) return HOMS_EINVAL;
+    // Set-up first, even for an empty request, so that a call with nadc = 0
+    // at initialisation resolves (and lets the driver back) the array.
+    void *scratch = nullptr;
+    homs_status s = scratch_for_current_device(&scratch);
+    if (s != HOMS_OK) return s;
     if (nadc == 0) return HOMS_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t es = dtype == HOMS_F64 ? 16 : 8;
@@ -66,9 +76,6 @@ extern "C" homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, 
     const double need = (double)es * (double)tiles * (double)nadc * (double)ncoils;
     if (need > (double)kScratchBytes) return HOMS_EINVAL;
     if ((nadc + homs::PLAIN_STAGE - 1) / homs::PLAIN_STAGE > 65535) return HOMS_EINVAL;  // grid.y of the reduce step
-    void *scratch = nullptr;
-    homs_status s = scratch_for_current_device(&scratch);
-    if (s != HOMS_OK) return s;
     cudaError_t e;
     if (dtype == HOMS_F64) {
         e = homs::launch_coil_reduce<double>(nspins, nadc, ncoils, (const cplx<double> *)states, ldstates,

@@ -175,7 +175,11 @@ homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins
  * the call only enqueues work.  Calls on the same device share that array, so
  * two calls whose work can overlap on the GPU (other streams, other host
  * threads) race: order them on one stream.  The first call on each device
- * resolves the array's address; make it before any stream capture. */
+ * (any call, also one with nadc = 0) resolves the array's address, which may
+ * make the CUDA driver load this library's device code and back the array:
+ * make that call at initialisation, before any stream capture; later calls
+ * allocate nothing.  A device reset (cudaDeviceReset) is not supported while
+ * the library is in use: the resolved address would be stale. */
 homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, int64_t nspins, int64_t nadc, int32_t ncoils,
                                      const void *states, int64_t ldstates, const void *csm, int64_t ldcsm, void *sig,
                                      int64_t ldsig);

@@ -3,7 +3,10 @@
 The allocation-free entry point keeps its split-K partials in a fixed device
 array inside libhoms instead of context scratch.  It runs the same reduction
 kernels, so its output must equal homs_coil_reduce's bit for bit, on two calls
-in a row (the second must not see anything the first left in the array).
+in a row (the second must not see anything the first left in the array),
+and after the first call on a device it allocates nothing: neither the
+device's free memory nor the caller's own pooled allocator (torch here, as
+CUDA.jl's would be for a Julia host) changes across further calls.
 """
 import ctypes
 import math
@@ -104,3 +107,31 @@ def test_noalloc_edges_and_limits(gpu_context):
     g = got.cpu().numpy()[:, :nadc_max].T
     ref = states.T @ csm
     assert np.linalg.norm(g - ref) / np.linalg.norm(ref) < 5e-13
+
+
+def test_noalloc_allocates_nothing_after_set_up(gpu_context):
+    import torch
+    lib = _lib.load()
+    cdt = torch.complex128
+    stream = torch.cuda.Stream()
+    st = ctypes.c_void_p(stream.cuda_stream)
+    ns, nadc, nc = 4000, 24, 8
+    states, csm = _problem(9, ns, nadc, nc, "f64")
+    s_t, c_t = _device(states, cdt), _device(csm, cdt)
+    out = [_signal_buffer(nadc, nc, cdt) for _ in range(3)]
+    dummy = torch.zeros(1, dtype=cdt, device="cuda:0")
+    # set-up: an empty request resolves the array on this device
+    assert lib.homs_coil_reduce_noalloc(st, *_args(_lib.HOMS_F64, dummy, dummy, out[0], 0, 0, nc)) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    torch_alloc0 = torch.cuda.memory_allocated()
+    torch_reserved0 = torch.cuda.memory_reserved()
+    for k in range(3):
+        assert lib.homs_coil_reduce_noalloc(st, *_args(_lib.HOMS_F64, s_t, c_t, out[k], ns, nadc, nc)) == 0
+    stream.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert torch.cuda.memory_allocated() == torch_alloc0
+    assert torch.cuda.memory_reserved() == torch_reserved0
+    first = out[0].cpu().numpy()
+    for k in (1, 2):
+        assert np.array_equal(out[k].cpu().numpy(), first)
