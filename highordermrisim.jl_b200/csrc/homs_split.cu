@@ -33,10 +33,10 @@
 // segment.
 //
 // Coil contraction, exactly.  M becomes a 30-bit integer (|M| <= 2^30), four
-// int8 digits: the rounding of M 2^22 gives three unsigned bytes (the top one
-// offset by 64) and the float residual of that rounding, times 256, a signed
-// low byte; 30 bits keep spins of small amplitude (outside an excited slice,
-// for instance) precise against a signal that cancels.  The per-coil scaled
+// unsigned int8 digits: floor(M 2^22) gives three bytes (the top one offset
+// by 64) and the float residual of that floor, times 256 and floored, the low
+// byte; 30 bits keep spins of small amplitude (outside an excited slice, for
+// instance) precise against a signal that cancels.  The per-coil scaled
 // sensitivities become 22-bit integers, three balanced digits.  Eight int8
 // MMAs per 32-spin chunk accumulate the digit classes T5..T2 (weights
 // 2^40..2^16 of the 2^52 full scale; lower classes lie below 2^-28 of it) in
@@ -215,6 +215,24 @@ __device__ __forceinline__ float cos_approx(float x) {
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
+// Integer multiply-adds with the multiplier in a register (a kernel argument,
+// so that the power-of-two shifts they implement issue on the FMA pipe
+// rather than the busier integer ALU pipe): lo = a b + c, hi = hi32(a b) + c.
+__device__ __forceinline__ uint32_t mad_lo(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+    return r;
+}
+__device__ __forceinline__ uint32_t mad_hi_s(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm("mad.hi.s32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+    return r;
+}
+__device__ __forceinline__ uint32_t mul_hi_u(uint32_t a, uint32_t b) {
+    uint32_t r;
+    asm("mul.hi.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+    return r;
+}
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
     uint32_t r;
     asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
@@ -273,6 +291,7 @@ struct KernelArgs {
     int tiles;
     int slabs;
     int nstage;
+    uint32_t mul8, mul16, mul24, mul25;  // 2^8, 2^16, 2^24, 2^25 (multipliers of mad_lo / mad_hi)
 };
 
 struct Cursor {
@@ -409,7 +428,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             constexpr uint32_t id_ph3 = idesc_i8(PH_N3, true, true);
             constexpr uint32_t id_c3 = idesc_i8(3 * N, false, true);
             constexpr uint32_t id_c2 = idesc_i8(2 * N, false, true);
-            constexpr uint32_t id_c1 = idesc_i8(N, true, true);  // signed low digit of M
+            constexpr uint32_t id_c1 = idesc_i8(N, false, true);  // low digit of M
             Cursor cp = cursor_start(args), cc = cp;
             int gp = 0, gc = 0;
             // Phase MMAs of chunk gp (cursor cp): classes into TMEM columns P_COL.
@@ -481,11 +500,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         const uint32_t lq = (uint32_t)(q * 32) << 16;
         const int row = q * 32 + lane;
         const int ks = cq >> 1;
-        // Amplitude scale of the segment: M is formed as M / 2^eA (the ex2
-        // argument stays small, so its float rounding stays near 2^-24
-        // relative), then times 2^22 by adding 22 to the exponent field; the
+        // Amplitude scale of the segment: M is formed as M / 2^eA (log2|m0| - eA
+        // comes with the spin parameters, so the ex2 argument stays small and
+        // its float rounding near 2^-24 relative), then times 2^22 (exact); the
         // low digit carries the next 8 bits.
-        const float l2off = (float)(-pow2_ceil_exp(*args.amp_max));
         // Clear the coil classes (completion 0 of d_empty releases the first item).
         {
             const uint32_t z[4] = {0u, 0u, 0u, 0u};
@@ -499,37 +517,58 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             __syncwarp();
             if (lane == 0) mbar_arrive(d_empty);
         }
+        const uint32_t m8 = args.mul8, m16 = args.mul16, m24 = args.mul24, m25 = args.mul25;
+        const int n_items = args.tiles * args.slabs;
         int g = 0;
-        for (Cursor cu = cursor_start(args); cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
-            const uint32_t base = args.rows[2 * ((size_t)cu.tile * TM + row)];
-            const float tj = __uint_as_float(args.rows[2 * ((size_t)cu.tile * TM + row) + 1]);
-            for (int c = cu.c0; c < cu.c1; ++c, ++g) {
-                const int stage = g % NSTAGE;
-                bool ok = mbar_wait(p_full, (uint32_t)(g & 1));
-                __syncwarp();
-                if (!__all_sync(0xffffffffu, ok)) {
-                    if (lane == 0) atomicOr(args.err, 16u);
-                    dead = true;
-                    break;
-                }
-                tc_fence_after();
-                // Phase classes w = 7..2 (columns (7 - w) * 32) of this warp's 8 spins.
-                uint32_t pc[6][8];
+        // Phase classes w = 7..2 (columns (7 - w) * 32) of this warp's 8 spins: loaded for
+        // chunk g + 1 while chunk g's A operand is handed over (the load's latency overlaps).
+        uint32_t pc[6][8];
+        auto load_phase = [&](int gg) -> bool {
+            const bool ok = mbar_wait(p_full, (uint32_t)(gg & 1));
+            __syncwarp();
+            if (!__all_sync(0xffffffffu, ok)) return false;
+            tc_fence_after();
 #pragma unroll
-                for (int t = 0; t < 6; ++t) tmem_ld_x8(tmem + lq + P_COL + (uint32_t)(t * 32 + cq * 8), pc[t]);
+            for (int t = 0; t < 6; ++t) tmem_ld_x8(tmem + lq + P_COL + (uint32_t)(t * 32 + cq * 8), pc[t]);
+            return true;
+        };
+        Cursor cu = cursor_start(args);
+        if (cu.valid) {
+            if (!load_phase(0)) {
+                if (lane == 0) atomicOr(args.err, 16u);
+                dead = true;
+            } else {
                 tmem_wait_ld();
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) mbar_arrive(p_empty);
-                ok = mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1));
+            }
+        }
+        for (; cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
+            const uint32_t base = args.rows[2 * ((size_t)cu.tile * TM + row)];
+            const float tj = __uint_as_float(args.rows[2 * ((size_t)cu.tile * TM + row) + 1]);
+            for (int c = cu.c0; c < cu.c1; ++c, ++g) {
+                const int stage = g % NSTAGE;
+                bool ok = mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1));
                 __syncwarp();
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(args.err, 32u);
                     dead = true;
                     break;
                 }
+                // Spin parameters of this warp's 8 spins: turn of arg(m0), r2, log2|m0| - eA.
                 const uint32_t *par =
                     reinterpret_cast<const uint32_t *>(sStage + (size_t)stage * STAGE_BYTES + CB + PHASE_B_BYTES);
+                uint32_t th[8], r2b[8], l2b[8];
+#pragma unroll
+                for (int v = 0; v < 2; ++v) {
+                    const uint4 a4 = *reinterpret_cast<const uint4 *>(par + cq * 8 + 4 * v);
+                    const uint4 b4 = *reinterpret_cast<const uint4 *>(par + KC + cq * 8 + 4 * v);
+                    const uint4 c4 = *reinterpret_cast<const uint4 *>(par + 2 * KC + cq * 8 + 4 * v);
+                    th[4 * v] = a4.x, th[4 * v + 1] = a4.y, th[4 * v + 2] = a4.z, th[4 * v + 3] = a4.w;
+                    r2b[4 * v] = b4.x, r2b[4 * v + 1] = b4.y, r2b[4 * v + 2] = b4.z, r2b[4 * v + 3] = b4.w;
+                    l2b[4 * v] = c4.x, l2b[4 * v + 1] = c4.y, l2b[4 * v + 2] = c4.z, l2b[4 * v + 3] = c4.w;
+                }
                 uint32_t wd[4][4];  // digit planes d1, d2, d3 (+64), d0 of spins (2p, 2p+1)
 #pragma unroll
                 for (int pp = 0; pp < 4; ++pp) {
@@ -537,34 +576,37 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         const int i = 2 * pp + h;
-                        const int s = cq * 8 + i;
-                        const uint32_t u = base + par[s] + (uint32_t)((int32_t)pc[5][i] >> 16) +
-                                           (uint32_t)((int32_t)pc[4][i] >> 8) + pc[3][i] + (pc[2][i] << 8) +
-                                           (pc[1][i] << 16) + (pc[0][i] << 24);
-                        // Quarter-turn reduction: u = turn + 2^29 + 64, quadrant u >> 30,
-                        // remainder (u & (2^30 - 1)) - 2^29 rounded to 23 bits.
-                        const uint32_t fb = ((u >> 7) & 0x7FFFFFu) | 0x4B000000u;
+                        // u = turn + 2^29 + 64: classes 7, 6, 5 shifted left by 24, 16, 8 bits,
+                        // class 4 as is, classes 3, 2 shifted right (arithmetic) by 8, 16.
+                        uint32_t u = base + th[i] + pc[3][i];
+                        u = mad_lo(pc[2][i], m8, u);
+                        u = mad_lo(pc[1][i], m16, u);
+                        u = mad_lo(pc[0][i], m24, u);
+                        u = mad_hi_s(pc[4][i], m24, u);
+                        u = mad_hi_s(pc[5][i], m16, u);
+                        // Quarter-turn reduction: quadrant u >> 30, remainder (u & (2^30 - 1)) - 2^29
+                        // to 23 bits (the +64 of u rounds it).
+                        const uint32_t fb = (mul_hi_u(u, m25) & 0x7FFFFFu) | 0x4B000000u;
                         const float x = (__uint_as_float(fb) - MAGIC_1P5_2P23) * TWO_PI_2M25;
                         const float sn = sin_approx(x), cs = cos_approx(x);
                         const bool odd = (u & 0x40000000u) != 0u;
                         const float re = odd ? sn : cs, im = odd ? cs : sn;
-                        const float r2 = __uint_as_float(par[KC + s]);
-                        const float l2 = __uint_as_float(par[2 * KC + s]);
-                        const uint32_t ab = __float_as_uint(ex2_approx(fmaf(tj, r2, l2 + l2off))) + (22u << 23);
+                        const uint32_t ab = __float_as_uint(
+                            ex2_approx(fmaf(tj, __uint_as_float(r2b[i]), __uint_as_float(l2b[i]))) * 4194304.0f);
                         const float are = __uint_as_float(ab ^ ((u + 0x40000000u) & 0x80000000u));
                         const float aim = __uint_as_float(ab ^ (u & 0x80000000u));
-                        // 1.5 * 2^23 + y rounds y to an integer: its bits are 0x4B400000 + y,
-                        // bytes 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64.
-                        const float hre = fmaf(are, re, MAGIC_1P5_2P23), him = fmaf(aim, im, MAGIC_1P5_2P23);
+                        // floor(y) + 1.5 * 2^23 for y = M 2^22: bits 0x4B400000 + floor(y), bytes
+                        // 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64; the residual
+                        // y - floor(y) in [0, 1) (exact before its one downward rounding) gives
+                        // the low digit d0 = floor(256 residual), byte 0 of the same construction.
+                        const float hre = __fmaf_rd(are, re, MAGIC_1P5_2P23);
+                        const float him = __fmaf_rd(aim, im, MAGIC_1P5_2P23);
                         vre[h] = __float_as_uint(hre);
                         vim[h] = __float_as_uint(him);
-                        // The residual y - rint(y) is exact before its one rounding and lies in
-                        // [-0.5, 0.5]; rint(256 residual) (at most 127 after the clamp) is the
-                        // signed low digit d0, byte 0 of the same construction.
-                        const float rre = fminf(fmaf(are, re, -(hre - MAGIC_1P5_2P23)), 0.498f);
-                        const float rim = fminf(fmaf(aim, im, -(him - MAGIC_1P5_2P23)), 0.498f);
-                        lre[h] = __float_as_uint(fmaf(rre, 256.0f, MAGIC_1P5_2P23));
-                        lim[h] = __float_as_uint(fmaf(rim, 256.0f, MAGIC_1P5_2P23));
+                        const float rre = __fmaf_rd(are, re, -(hre - MAGIC_1P5_2P23));
+                        const float rim = __fmaf_rd(aim, im, -(him - MAGIC_1P5_2P23));
+                        lre[h] = __float_as_uint(__fmaf_rd(rre, 256.0f, MAGIC_1P5_2P23));
+                        lim[h] = __float_as_uint(__fmaf_rd(rim, 256.0f, MAGIC_1P5_2P23));
                     }
                     // K order of a word: (re, im) of spin 2pp, then of spin 2pp+1.
                     const uint32_t p0 = prmt(vre[0], vim[0], 0x5140u), p1 = prmt(vre[1], vim[1], 0x5140u);
@@ -575,10 +617,17 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     wd[2][pp] = prmt(q0, q1, 0x5410u);
                     wd[3][pp] = prmt(r0, r1, 0x5410u);
                 }
+                const bool more = c + 1 < cu.c1 || cu.i + (int)gridDim.x < n_items;
+                if (more && !load_phase(g + 1)) {
+                    if (lane == 0) atomicOr(args.err, 16u);
+                    dead = true;
+                    break;
+                }
                 ok = mbar_wait(a_empty, (uint32_t)((g + 1) & 1));
                 __syncwarp();
                 if (!__all_sync(0xffffffffu, ok)) {
                     if (lane == 0) atomicOr(args.err, 128u);
+                    tmem_wait_ld();
                     dead = true;
                     break;
                 }
@@ -587,11 +636,15 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 tmem_st_x4(acol, wd[2]);        // d3 + 64
                 tmem_st_x4(acol + 8u, wd[1]);   // d2
                 tmem_st_x4(acol + 16u, wd[0]);  // d1
-                tmem_st_x4(acol + 24u, wd[3]);  // d0 (signed)
+                tmem_st_x4(acol + 24u, wd[3]);  // d0
                 tmem_wait_st();
+                if (more) tmem_wait_ld();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(a_full);
+                if (lane == 0) {
+                    mbar_arrive(a_full);
+                    if (more) mbar_arrive(p_empty);
+                }
             }
             if (dead) break;
             // Item end: the coil classes of this warp's rows and columns into the
@@ -644,7 +697,9 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 
 // Sum the split-K partials of each (sample, column) in slab order (FP64),
 // remove the offset of the top magnetisation digit (64 * 2^24 times the
-// column's sensitivity integers, 2^-22 colsum after the 2^-52 scale), undo the
+// column's sensitivity integers, 2^-22 colsum after the 2^-52 scale) and the
+// mean of the floor that forms the magnetisation integers (-1/2 unit per
+// component: +2^-53 colsum), undo the
 // power-of-two scaling of the operands and write complex samples: column
 // n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
 template <typename T>
@@ -679,7 +734,10 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
             const int e = threadIdx.x + k * 256;
-            if (e < elems) sacc[e] = acc[k] - ldexp((double)colsum[e % n_cols], -22);
+            if (e < elems) {
+                const double cs = (double)colsum[e % n_cols];
+                sacc[e] = acc[k] - (ldexp(cs, -22) - ldexp(cs, -53));
+            }
         }
         __syncthreads();
         for (int q = threadIdx.x; q < FIN_ROWS * ncg; q += blockDim.x) {
@@ -911,7 +969,8 @@ __global__ void colsum_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t 
 
 // Per-segment spin parameters of every chunk, [turn of arg(m0) x 32 | r2 x 32
 // | l2 x 32]: the initial phase as a 32-bit turn fraction, -log2(e)/T2 and
-// log2|m0| (float); also the largest |m0| (amplitude scale of the segment).
+// log2|m0| (float; l2_shift_kernel then subtracts the segment's amplitude
+// exponent); also the largest |m0| (amplitude scale of the segment).
 __global__ void spin_params_kernel(const double *T2, const cplx<double> *xy, int64_t ns, int64_t nchunks,
                                    unsigned long long *amp_max, uint32_t *params) {
     const int64_t total = nchunks * KC;
@@ -942,6 +1001,19 @@ __global__ void spin_params_kernel(const double *T2, const cplx<double> *xy, int
         p[sl] = th;
         p[KC + sl] = __float_as_uint(r2);
         p[2 * KC + sl] = __float_as_uint(l2);
+    }
+}
+
+// log2|m0| - eA of every spin of the segment (eA: smallest power of two at or
+// above the largest |m0|), so that the magnetisation warps' ex2 argument
+// t r2 + l2 stays small.
+__global__ void l2_shift_kernel(uint32_t *params, int64_t nchunks, const unsigned long long *amp_max) {
+    const float ea = (float)pow2_ceil_exp(*amp_max);
+    const int64_t total = nchunks * KC;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t *p = params + (s / KC) * (PARAM_BYTES / 4) + 2 * KC + (s % KC);
+        *p = __float_as_uint(__uint_as_float(*p) - ea);
     }
 }
 
@@ -1303,8 +1375,10 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
     spin_params_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>((const double *)a.T2, (const cplx<double> *)a.xy,
                                                                r.ns, nchunks, (unsigned long long *)r.amp,
                                                                (uint32_t *)r.params);
+    l2_shift_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>((uint32_t *)r.params, nchunks,
+                                                            (const unsigned long long *)r.amp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (a.launches) *a.launches += 2;
+    if (a.launches) *a.launches += 3;
     if (nsamples > 0) {
         if ((e = grow(r.phase_a, r.phase_a_bytes, (size_t)tiles * PHASE_A_BYTES)) != cudaSuccess) return e;
         if ((e = grow(r.rows, r.rows_bytes, (size_t)tiles * TM * 2 * sizeof(uint32_t))) != cudaSuccess) return e;
@@ -1339,6 +1413,10 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         ka.tiles = (int)tiles;
         ka.slabs = slabs;
         ka.nstage = kernel_stages(r.n_mma);
+        ka.mul8 = 1u << 8;
+        ka.mul16 = 1u << 16;
+        ka.mul24 = 1u << 24;
+        ka.mul25 = 1u << 25;
         const unsigned ev_flags = a.capture ? cudaEventRecordExternal : cudaEventRecordDefault;
         if (a.ev_start) cudaEventRecordWithFlags(a.ev_start, stream, ev_flags);
         // One pass per group of GROUP_COILS coils.
