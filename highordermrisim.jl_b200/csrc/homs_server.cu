@@ -269,6 +269,15 @@ homs_status homs_server_times(homs_server *srv, int64_t ticket, homs_request_tim
     return it->second->done ? HOMS_OK : HOMS_EBUSY;
 }
 
+homs_status homs_server_estimate(homs_server *srv, int64_t ticket, int64_t *bytes) {
+    if (!srv || !bytes) return HOMS_EINVAL;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->requests.find(ticket);
+    if (it == srv->requests.end()) return HOMS_EINVAL;
+    *bytes = (int64_t)it->second->bytes;
+    return HOMS_OK;
+}
+
 const char *homs_server_error(homs_server *srv, int64_t ticket) {
     if (!srv) return "no server";
     std::lock_guard<std::mutex> lk(srv->mu);

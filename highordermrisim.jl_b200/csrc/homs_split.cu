@@ -32,11 +32,12 @@
 // is ex2.approx of a small argument.  |M| <= 1 after a power-of-two scale per
 // segment.
 //
-// Coil contraction, exactly.  M becomes a 30-bit integer (|M| <= 2^30), four
-// unsigned int8 digits: floor(M 2^22) gives three bytes (the top one offset
-// by 64) and the float residual of that floor, times 256 and floored, the low
-// byte; 30 bits keep spins of small amplitude (outside an excited slice, for
-// instance) precise against a signal that cancels.  The per-coil scaled
+// Coil contraction, exactly.  M becomes a 30-bit integer (|M| < 2^30), four
+// int8 digits: F = rint(M 2^22) gives three unsigned bytes (the top one offset
+// by 64) and the rounding residual, scaled to [-127, 127] and rounded, the
+// signed low byte; 30 bits keep spins of small amplitude (outside an excited
+// slice, for instance) precise against a signal that cancels, and a spin of
+// zero amplitude contributes exactly nothing.  The per-coil scaled
 // sensitivities become 22-bit integers, three balanced digits.  Eight int8
 // MMAs per 32-spin chunk accumulate the digit classes T5..T2 (weights
 // 2^40..2^16 of the 2^52 full scale; lower classes lie below 2^-28 of it) in
@@ -323,6 +324,26 @@ __device__ __forceinline__ void cursor_next(const KernelArgs &a, Cursor &cu) {
 
 constexpr float TWO_PI_2M25 = 1.8725351414619534e-07f;  // 2 pi / 2^25: one unit of the 23-bit quarter-turn angle
 constexpr float MAGIC_1P5_2P23 = 12582912.0f;           // 1.5 * 2^23
+// The angle is one FFMA, fb * TWO_PI_2M25 + ANGLE_OFFSET with fb = 2^23 + the
+// 23-bit remainder; ANGLE_OFFSET is -1.5 * 2^23 * TWO_PI_2M25 rounded to float,
+// so every angle carries the same offset angle_offset_error() (a few 1e-8
+// rad), which the finalize removes exactly by a rotation of the signal.
+constexpr float ANGLE_OFFSET = -MAGIC_1P5_2P23 * TWO_PI_2M25;
+inline __host__ __device__ double angle_offset_error() {
+    return (double)ANGLE_OFFSET + (double)MAGIC_1P5_2P23 * (double)TWO_PI_2M25;
+}
+// Low magnetisation digit: rint(r * 2^30 (1 - 2^-7)) for the rounding residual
+// |r| <= 2^-23 of the top three digits, so |digit| <= 127 without a clamp.
+constexpr float LOW_DIGIT_SCALE = 1065353216.0f;  // 2^30 - 2^23
+
+// Amplitude exponent of a segment: the smallest e with 2^e >= max|m0| (1 + 2^-19),
+// so that |M| / 2^e stays below 1 - 2^-20 and the sin/cos/ex2 approximations
+// (errors below 2^-20 relative) cannot carry |M 2^-e| to 1 or above.
+__device__ __forceinline__ int amp_exp(unsigned long long bits) {
+    if (bits == 0) return 0;
+    const double v = __longlong_as_double((long long)bits) * (1.0 + 0x1p-19);
+    return pow2_ceil_exp((unsigned long long)__double_as_longlong(v));
+}
 
 template <int N>
 __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
@@ -428,7 +449,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             constexpr uint32_t id_ph3 = idesc_i8(PH_N3, true, true);
             constexpr uint32_t id_c3 = idesc_i8(3 * N, false, true);
             constexpr uint32_t id_c2 = idesc_i8(2 * N, false, true);
-            constexpr uint32_t id_c1 = idesc_i8(N, false, true);  // low digit of M
+            constexpr uint32_t id_c1 = idesc_i8(N, true, true);   // signed low digit of M
             Cursor cp = cursor_start(args), cc = cp;
             int gp = 0, gc = 0;
             // Phase MMAs of chunk gp (cursor cp): classes into TMEM columns P_COL.
@@ -502,8 +523,8 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         const int ks = cq >> 1;
         // Amplitude scale of the segment: M is formed as M / 2^eA (log2|m0| - eA
         // comes with the spin parameters, so the ex2 argument stays small and
-        // its float rounding near 2^-24 relative), then times 2^22 (exact); the
-        // low digit carries the next 8 bits.
+        // its float rounding near 2^-24 relative); the top digits carry M to
+        // 2^-22 and the low digit the next 8 bits.
         // Clear the coil classes (completion 0 of d_empty releases the first item).
         {
             const uint32_t z[4] = {0u, 0u, 0u, 0u};
@@ -587,26 +608,28 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                         // Quarter-turn reduction: quadrant u >> 30, remainder (u & (2^30 - 1)) - 2^29
                         // to 23 bits (the +64 of u rounds it).
                         const uint32_t fb = (mul_hi_u(u, m25) & 0x7FFFFFu) | 0x4B000000u;
-                        const float x = (__uint_as_float(fb) - MAGIC_1P5_2P23) * TWO_PI_2M25;
+                        const float x = __fmaf_rn(__uint_as_float(fb), TWO_PI_2M25, ANGLE_OFFSET);
                         const float sn = sin_approx(x), cs = cos_approx(x);
                         const bool odd = (u & 0x40000000u) != 0u;
                         const float re = odd ? sn : cs, im = odd ? cs : sn;
-                        const uint32_t ab = __float_as_uint(
-                            ex2_approx(fmaf(tj, __uint_as_float(r2b[i]), __uint_as_float(l2b[i]))) * 4194304.0f);
+                        const uint32_t ab =
+                            __float_as_uint(ex2_approx(fmaf(tj, __uint_as_float(r2b[i]), __uint_as_float(l2b[i]))));
                         const float are = __uint_as_float(ab ^ ((u + 0x40000000u) & 0x80000000u));
                         const float aim = __uint_as_float(ab ^ (u & 0x80000000u));
-                        // floor(y) + 1.5 * 2^23 for y = M 2^22: bits 0x4B400000 + floor(y), bytes
-                        // 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64; the residual
-                        // y - floor(y) in [0, 1) (exact before its one downward rounding) gives
-                        // the low digit d0 = floor(256 residual), byte 0 of the same construction.
-                        const float hre = __fmaf_rd(are, re, MAGIC_1P5_2P23);
-                        const float him = __fmaf_rd(aim, im, MAGIC_1P5_2P23);
+                        // 3 + rint(M 2^22) 2^-22 (|M| < 1, so the sum stays in [2, 4) where the
+                        // float grid is 2^-22): bits 0x40400000 + F for F = rint(M 2^22), bytes
+                        // 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64.  The residual
+                        // M - F 2^-22 (|.| <= 2^-23, exact before its one rounding) gives the
+                        // signed low digit, byte 0 of MAGIC + rint(residual LOW_DIGIT_SCALE).
+                        // A spin of zero amplitude gives zero digits (no offset but the top one's).
+                        const float hre = __fmaf_rn(are, re, 3.0f);
+                        const float him = __fmaf_rn(aim, im, 3.0f);
                         vre[h] = __float_as_uint(hre);
                         vim[h] = __float_as_uint(him);
-                        const float rre = __fmaf_rd(are, re, -(hre - MAGIC_1P5_2P23));
-                        const float rim = __fmaf_rd(aim, im, -(him - MAGIC_1P5_2P23));
-                        lre[h] = __float_as_uint(__fmaf_rd(rre, 256.0f, MAGIC_1P5_2P23));
-                        lim[h] = __float_as_uint(__fmaf_rd(rim, 256.0f, MAGIC_1P5_2P23));
+                        const float rre = __fmaf_rn(are, re, __fsub_rn(3.0f, hre));
+                        const float rim = __fmaf_rn(aim, im, __fsub_rn(3.0f, him));
+                        lre[h] = __float_as_uint(__fmaf_rn(rre, LOW_DIGIT_SCALE, MAGIC_1P5_2P23));
+                        lim[h] = __float_as_uint(__fmaf_rn(rim, LOW_DIGIT_SCALE, MAGIC_1P5_2P23));
                     }
                     // K order of a word: (re, im) of spin 2pp, then of spin 2pp+1.
                     const uint32_t p0 = prmt(vre[0], vim[0], 0x5140u), p1 = prmt(vre[1], vim[1], 0x5140u);
@@ -697,10 +720,9 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 
 // Sum the split-K partials of each (sample, column) in slab order (FP64),
 // remove the offset of the top magnetisation digit (64 * 2^24 times the
-// column's sensitivity integers, 2^-22 colsum after the 2^-52 scale) and the
-// mean of the floor that forms the magnetisation integers (-1/2 unit per
-// component: +2^-53 colsum), undo the
-// power-of-two scaling of the operands and write complex samples: column
+// column's sensitivity integers, 2^-22 colsum after the 2^-52 scale), rotate
+// by -angle_offset_error() (the constant offset of the kernel's angles), undo
+// the power-of-two scaling of the operands and write complex samples: column
 // n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
 template <typename T>
 __global__ void __launch_bounds__(256) split_finalize_kernel(const double *partial, int64_t nsamples, int32_t ncg,
@@ -713,7 +735,9 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
     // then writes every coil's samples of those rows from shared memory.
     constexpr int FIN_ROWS = 32, PER = FIN_ROWS * 64 / 256;
     __shared__ double sacc[FIN_ROWS * 64];
-    const int ea = pow2_ceil_exp(*amp_max);
+    const int ea = amp_exp(*amp_max);
+    double rs, rc;
+    sincos(-angle_offset_error(), &rs, &rc);
     const int64_t tiles = (nsamples + TM - 1) / TM;
     const int64_t units = tiles * (TM / FIN_ROWS);
     const int elems = FIN_ROWS * n_cols;  // n_cols <= 64
@@ -736,7 +760,7 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
             const int e = threadIdx.x + k * 256;
             if (e < elems) {
                 const double cs = (double)colsum[e % n_cols];
-                sacc[e] = acc[k] - (ldexp(cs, -22) - ldexp(cs, -53));
+                sacc[e] = acc[k] - ldexp(cs, -22);
             }
         }
         __syncthreads();
@@ -745,8 +769,8 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
             const int64_t j = tile * TM + r0 + row;
             if (j < nsamples) {
                 const int e = coil_exp[c] + ea;
-                sig[j + (int64_t)c * ldsig] =
-                    cplx<T>{T(ldexp(sacc[row * n_cols + c], e)), T(ldexp(sacc[row * n_cols + ncg + c], e))};
+                const double re = sacc[row * n_cols + c], im = sacc[row * n_cols + ncg + c];
+                sig[j + (int64_t)c * ldsig] = cplx<T>{T(ldexp(re * rc - im * rs, e)), T(ldexp(re * rs + im * rc, e))};
             }
         }
         __syncthreads();
@@ -1004,11 +1028,10 @@ __global__ void spin_params_kernel(const double *T2, const cplx<double> *xy, int
     }
 }
 
-// log2|m0| - eA of every spin of the segment (eA: smallest power of two at or
-// above the largest |m0|), so that the magnetisation warps' ex2 argument
-// t r2 + l2 stays small.
+// log2|m0| - eA of every spin of the segment (eA = amp_exp of the largest
+// |m0|), so that the magnetisation warps' ex2 argument t r2 + l2 stays small.
 __global__ void l2_shift_kernel(uint32_t *params, int64_t nchunks, const unsigned long long *amp_max) {
-    const float ea = (float)pow2_ceil_exp(*amp_max);
+    const float ea = (float)amp_exp(*amp_max);
     const int64_t total = nchunks * KC;
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < total;
          s += (int64_t)gridDim.x * blockDim.x) {

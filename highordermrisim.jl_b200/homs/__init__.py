@@ -701,6 +701,12 @@ class Server:
         self._lib.homs_server_times(self.handle, int(ticket), ctypes.byref(t))
         return t.submitted, t.started, t.finished
 
+    def estimate(self, ticket: int) -> int:
+        """The request's admission estimate of its device footprint in bytes."""
+        b = ctypes.c_int64(0)
+        _lib.check(self._lib.homs_server_estimate(self.handle, int(ticket), ctypes.byref(b)))
+        return int(b.value)
+
     def result(self, ticket: int, timeout: float = 600.0):
         """Wait for a request and return what ``simulate`` returns for it."""
         req = self._requests[int(ticket)]

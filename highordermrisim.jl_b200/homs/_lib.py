@@ -26,7 +26,8 @@ EXPORTED = [
     "homs_synchronize", "homs_precession_block", "homs_excitation_block", "homs_coil_reduce", "homs_simulate",
     "homs_count_adc", "homs_plan_create", "homs_plan_run", "homs_plan_device_bytes", "homs_plan_timing",
     "homs_plan_destroy", "homs_coil_reduce_noalloc", "homs_server_create", "homs_server_submit", "homs_server_poll",
-    "homs_server_wait", "homs_server_times", "homs_server_error", "homs_server_release", "homs_server_destroy",
+    "homs_server_wait", "homs_server_times", "homs_server_estimate", "homs_server_error", "homs_server_release",
+    "homs_server_destroy",
     "homs_kspace", "homs_kspace_timing", "homs_resident_create", "homs_resident_device_bytes",
     "homs_resident_destroy", "homs_simulate_resident", "homs_server_submit_resident", "homs_plan_graph",
     "homs_brain_phantom_count", "homs_brain_phantom_fill", "homs_csm_birdcage", "homs_selftest_wait_timeout",
@@ -141,6 +142,7 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "homs_server_poll": (ctypes.c_int, [vp, i64]),
         "homs_server_wait": (ctypes.c_int, [vp, i64, ctypes.c_double]),
         "homs_server_times": (ctypes.c_int, [vp, i64, ctypes.POINTER(RequestTimes)]),
+        "homs_server_estimate": (ctypes.c_int, [vp, i64, ctypes.POINTER(i64)]),
         "homs_server_error": (ctypes.c_char_p, [vp, i64]),
         "homs_server_release": (ctypes.c_int, [vp, i64]),
         "homs_server_destroy": (ctypes.c_int, [vp]),

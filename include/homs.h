@@ -370,6 +370,9 @@ homs_status homs_server_poll(homs_server *srv, int64_t ticket);
 /* Block until the request finishes or `timeout_seconds` pass (HOMS_ETIMEDOUT). */
 homs_status homs_server_wait(homs_server *srv, int64_t ticket, double timeout_seconds);
 homs_status homs_server_times(homs_server *srv, int64_t ticket, homs_request_times *out);
+/* The request's admission estimate of its device footprint, in bytes (the
+ * amount it holds of max_device_bytes while it is in flight). */
+homs_status homs_server_estimate(homs_server *srv, int64_t ticket, int64_t *bytes);
 const char *homs_server_error(homs_server *srv, int64_t ticket);
 /* Forget a finished request. */
 homs_status homs_server_release(homs_server *srv, int64_t ticket);

@@ -72,12 +72,20 @@ def test_mixed_results_match_the_oracle(oracle, gpu_context):
 
 
 def test_budget_serialises_requests(gpu_context):
-    # Split-mode requests, each estimated at ~365-385 MB of device memory.
     reqs = [r for r in _requests() if r[4].get("homs_precision") == "split"]
     alone = [homs.simulate(o, s, sim_params=_params(p, m), parts=pa, excitation=ex, context=gpu_context)
              for o, s, pa, ex, p, m in reqs]
-    # A budget below any two requests together: one request in flight at a time.
-    with homs.Server(slots=4, max_device_bytes=500 << 20) as srv:
+    # The server's own admission estimates of the split-mode requests.
+    with homs.Server(slots=1) as probe:
+        tickets = [probe.submit(o, s, sim_params=_params(p, m), parts=pa, excitation=ex) for o, s, pa, ex, p, m in reqs]
+        est = sorted(probe.estimate(t) for t in tickets)
+        for t in tickets:
+            probe.result(t)
+    assert est[-1] < est[0] + est[1]
+    # A budget that admits each request alone but no two together: one request
+    # in flight at a time.
+    budget = (est[-1] + est[0] + est[1]) // 2
+    with homs.Server(slots=4, max_device_bytes=budget) as srv:
         tickets = [srv.submit(o, s, sim_params=_params(p, m), parts=pa, excitation=ex) for o, s, pa, ex, p, m in reqs]
         got = [srv.result(t) for t in tickets]
         spans = sorted(srv.times(t)[1:] for t in tickets)
