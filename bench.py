@@ -51,8 +51,9 @@ UNIT = "spin*sample*coil/s"
 CONFIG_INDEX = 2
 FLOPS_PER_UNIT = 8.0  # one complex multiply-accumulate per spin*sample*coil
 # What the split kernel issues per 32-spin x 128-sample chunk tile (N = 64 output columns):
-# 3 phase MMAs of 128 x (192, 160, 96) x 32 int8 and 6 coil MMAs of 128 x (192, 192, 128) x 32 int8.
-I8_MACS_PER_SPIN_SAMPLE = (192 + 160 + 96 + 2 * (192 + 192 + 128)) * 32 / 32.0  # MACs per spin*sample
+# 3 phase MMAs of 128 x (160, 128, 64) x 32 int8 and 8 coil MMAs of 128 x (192, 192, 128, 64) x 32 int8
+# (two K-steps of 16 spins).
+I8_MACS_PER_SPIN_SAMPLE = (160 + 128 + 64 + 2 * (192 + 192 + 128 + 64)) * 32 / 32.0  # MACs per spin*sample
 SFU_OPS_PER_SPIN_SAMPLE = 3.0  # sin, cos, ex2 on the MUFU (XU) pipe
 SFU_PER_SM_CLK = 16.0  # MUFU results per SM and clock
 N_SM = 148

@@ -20,11 +20,13 @@
 // (|K| <= 2^38 requires bmax_k * max|kappa_k| <= 2^12 turns, checked per
 // segment).  Both are split into five balanced int8 digits (base 256); the
 // digit products of equal weight 2^(8w) are summed exactly by int8 tcgen05
-// MMAs (int32 accumulators), and only the classes w = 2..7 reach the 32-bit
-// turn fraction: w >= 8 are whole turns (the mod-2pi reduction is the
-// integer wraparound) and w <= 1 lie below 2^-32 turn.  The turn fraction
-//   u = sum_w S_w 2^(8w-32) mod 2^32
-// is exact up to the rounding of B and K.
+// MMAs (int32 accumulators), and the classes w = 3..7 form the 32-bit turn
+// fraction: w >= 8 are whole turns (the mod-2pi reduction is the integer
+// wraparound), w <= 1 lie below 2^-32 turn and w = 2 adds at most 12 units
+// of 2^-32 turn (|S_2| <= 3 digit pairs x 16 terms x 2^14), so it is left
+// out.  The turn fraction
+//   u = sum_{w>=3} S_w 2^(8w-32) mod 2^32
+// is exact up to the rounding of B and K and that 12 * 2^-32 turn.
 //
 // Trigonometry.  u is reduced to the nearest quarter turn in integers
 // (|x| <= pi/4, which keeps the float scale of the angle from biasing the
@@ -52,14 +54,19 @@
 //               reads the phase classes, forms the turn, M and its digits,
 //               writes the coil MMA's A operand to TMEM; drains the coil
 //               classes into the item's FP64 partial.
-//   warp 16     MMA issuer: per chunk 3 phase MMAs (A: the tile's integral
-//               digits in shared memory, B: the chunk's coefficient digits)
-//               one chunk ahead, and 8 coil MMAs (A in TMEM, B: the chunk's
-//               sensitivity digits); tcgen05.commit releases shared-memory
-//               stages and TMEM buffers.
+//   warp 16     coil MMA issuer: per chunk 8 coil MMAs (A in TMEM, B: the
+//               chunk's sensitivity digits); one commit releases both the
+//               shared-memory stage and the A buffer.
 //   warp 17     loader: cp.async.bulk of each item's phase A tile and each
 //               chunk's operands (non-multicast).
-// TMEM (512 columns): phase classes 192, coil A operand 64, coil classes 4N.
+//   warp 18     phase MMA issuer: per chunk 3 phase MMAs (A: the tile's
+//               integral digits in shared memory, B: the chunk's coefficient
+//               digits), one chunk ahead of the magnetisation warps.
+// The two issuers keep either chain of waits and MMAs off the other's
+// critical path.  Issuing MMAs, commits and bulk copies costs issue slots of
+// the issuing warp's scheduler (warp w runs on scheduler w % 4): each helper
+// sits on its own scheduler, and scheduler 3 carries none.
+// TMEM (512 columns): phase classes 160, coil A operand 64, coil classes 4N.
 // Every wait is bounded: on time-out the kernel records the place in a device
 // error word and returns without hanging the GPU.
 #include <algorithm>
@@ -83,9 +90,10 @@ constexpr int PREFIX_STRIDE = 24;  // doubles per prefix row: kappa_0..kappa_16,
 constexpr int PREFIX_T = 20;
 constexpr int GROUP_COILS = 32;  // coils per kernel pass (N <= 64 output columns)
 constexpr int NMAG_WARPS = 16;
-constexpr int MMA_WARP = 16;
+constexpr int MMA_WARP = 16;    // coil MMA issuer (allocates TMEM)
 constexpr int LOAD_WARP = 17;
-constexpr int THREADS = 576;
+constexpr int PHASE_WARP = 18;  // phase MMA issuer
+constexpr int THREADS = 608;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int MAX_STAGE = 6;
 constexpr int MAX_ITEM_CHUNKS = 256;  // int32 coil classes stay below 2^31 over an item
@@ -93,11 +101,11 @@ constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
 constexpr double PHASE_RANGE_LIMIT = 4096.0;     // turns: bmax_k * max|kappa_k| per term and segment
 
 // Phase MMAs: A' tiles [a4|a3], [a2|a1], [a0|0] (128 rows x 32 bytes each) and
-// B' blocks of 32 spin rows per digit class w (classes 7..2 at TMEM columns
-// (7 - w) * 32): MMA 1 covers w = 7..2 (N = 192; its class-2 block is zero
-// and only clears those columns), MMA 2 w = 6..2 (N = 160, columns 32..191),
-// MMA 3 w = 4..2 (N = 96, columns 96..191).
-constexpr int PH_N1 = 192, PH_N2 = 160, PH_N3 = 96;
+// B' blocks of 32 spin rows per digit class w (classes 7..3 at TMEM columns
+// (7 - w) * 32): MMA 1 covers w = 7..3 (N = 160), MMA 2 w = 6..3 (N = 128,
+// columns 32..159), MMA 3 w = 4..3 (N = 64, columns 96..159).
+constexpr int PH_N1 = 160, PH_N2 = 128, PH_N3 = 64;
+constexpr int PH_CLASSES = 5;
 constexpr int PH_OFF2 = PH_N1 * 32, PH_OFF3 = (PH_N1 + PH_N2) * 32;
 constexpr int PHASE_B_BYTES = (PH_N1 + PH_N2 + PH_N3) * 32;  // per chunk
 constexpr int PHASE_A_BYTES = 3 * TM * 32;                   // per tile
@@ -107,7 +115,7 @@ constexpr int PARAM_BYTES = 3 * KC * 4;                      // per chunk
 __host__ __device__ constexpr int coil_b_bytes(int n) { return 2 * 3 * n * 32; }
 
 // TMEM columns.
-constexpr uint32_t P_COL = 0;    // phase classes
+constexpr uint32_t P_COL = 0;    // phase classes (160 columns)
 constexpr uint32_t A_COL = 192;  // coil A: per K-step [d3 | d2 | d1 | d0], 8 columns each
 constexpr uint32_t D_COL = 256;  // coil classes [T5 | T4 | T3 | T2], N columns each
 
@@ -163,6 +171,29 @@ __device__ __forceinline__ bool mbar_wait_budget(uint64_t *bar, uint32_t parity,
 }
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
     return mbar_wait_budget(bar, parity, WAIT_BUDGET);
+}
+// The single-thread helpers' wait: try_wait with a suspend-time hint (fewer
+// probes while waiting; a barrier probe takes issue slots from the other
+// warps of the prober's scheduler); bounded like mbar_wait.
+constexpr uint32_t SUSPEND_HINT_NS = 1000000u;
+__device__ __forceinline__ bool mbar_try_hint(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(SUSPEND_HINT_NS)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_helper(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_hint(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_hint(bar, parity)) {
+        if (clock64() - t0 > WAIT_BUDGET) return false;
+    }
+    return true;
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -356,18 +387,19 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     uint8_t *sA = smem;                                  // 2 x PHASE_A_BYTES
     uint8_t *sStage = smem + 2 * PHASE_A_BYTES;          // NSTAGE x STAGE_BYTES
     uint64_t *bars = reinterpret_cast<uint64_t *>(sStage + (size_t)NSTAGE * STAGE_BYTES);
-    uint64_t *full = bars;                   // [NSTAGE] loader -> MMA, magnetisation (tx)
-    uint64_t *empty = bars + MAX_STAGE;      // [NSTAGE] coil MMA commit -> loader
-    uint64_t *a_full_ph = empty + MAX_STAGE; // [2] loader -> MMA (phase A tile, tx)
+    // empty[s]: the coil MMAs of the stage's chunk are complete, so both the
+    // stage (-> loader) and the coil A buffer (-> magnetisation warps) are free.
+    uint64_t *full = bars;                   // [NSTAGE] loader -> MMA issuers, magnetisation (tx)
+    uint64_t *empty = bars + MAX_STAGE;      // [NSTAGE] coil MMA commit -> loader, magnetisation
+    uint64_t *a_full_ph = empty + MAX_STAGE; // [2] loader -> phase issuer (phase A tile, tx)
     uint64_t *a_empty_ph = a_full_ph + 2;    // [2] last phase MMA of an item -> loader
     uint64_t *p_full = a_empty_ph + 2;       // phase MMA commit -> magnetisation
-    uint64_t *p_empty = p_full + 1;          // magnetisation warps -> MMA
-    uint64_t *a_full = p_empty + 1;          // magnetisation warps -> MMA (coil A written)
-    uint64_t *a_empty = a_full + 1;          // coil MMA commit -> magnetisation
-    uint64_t *d_full = a_empty + 1;          // last coil MMA of an item -> drain
-    uint64_t *d_empty = d_full + 1;          // drain (coil classes cleared) -> MMA
-    uint64_t *done = d_empty + 1;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    uint64_t *p_empty = p_full + 1;          // magnetisation warps -> phase issuer
+    uint64_t *a_full = p_empty + 1;          // magnetisation warps -> coil issuer (coil A written)
+    uint64_t *d_full = a_full + 1;           // last coil MMA of an item -> drain
+    uint64_t *d_empty = d_full + 1;          // drain (coil classes cleared) -> coil issuer
+    uint64_t *done = d_empty + 1;            // [2] every MMA of the coil / phase issuer complete
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -379,13 +411,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             mbar_init(&a_full_ph[i], 1);
             mbar_init(&a_empty_ph[i], 1);
         }
+        for (int i = 0; i < 2; ++i) mbar_init(&done[i], 1);
         mbar_init(p_full, 1);
         mbar_init(p_empty, NMAG_WARPS);
         mbar_init(a_full, NMAG_WARPS);
-        mbar_init(a_empty, 1);
-        mbar_init(d_full, 1);
         mbar_init(d_empty, NMAG_WARPS);
-        mbar_init(done, 1);
+        mbar_init(d_full, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == MMA_WARP) {
@@ -402,12 +433,13 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
 
     if (warp == LOAD_WARP) {
         if (lane == 0) {
-            int g = 0;
+            int stage = 0;
+            uint32_t sph = 0;  // parity of the stage ring's current pass
             int issued[MAX_STAGE] = {0, 0, 0, 0, 0, 0};
             int issued_a[2] = {0, 0};
             for (Cursor cu = cursor_start(args); cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
                 const int ib = cu.local & 1;
-                if (!mbar_wait(&a_empty_ph[ib], (uint32_t)(((cu.local >> 1) + 1) & 1))) {
+                if (!mbar_wait_helper(&a_empty_ph[ib], (uint32_t)(((cu.local >> 1) + 1) & 1))) {
                     atomicOr(args.err, 1u);
                     dead = true;
                     break;
@@ -416,9 +448,8 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 bulk_g2s(sA + ib * PHASE_A_BYTES, args.phase_a + (size_t)cu.tile * PHASE_A_BYTES, PHASE_A_BYTES,
                          &a_full_ph[ib]);
                 ++issued_a[ib];
-                for (int c = cu.c0; c < cu.c1; ++c, ++g) {
-                    const int stage = g % NSTAGE;
-                    if (!mbar_wait(&empty[stage], (uint32_t)(((g / NSTAGE) + 1) & 1))) {
+                for (int c = cu.c0; c < cu.c1; ++c) {
+                    if (!mbar_wait_helper(&empty[stage], sph ^ 1u)) {
                         atomicOr(args.err, 1u);
                         dead = true;
                         break;
@@ -430,6 +461,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     bulk_g2s(st + CB + PHASE_B_BYTES, args.params + (size_t)c * PARAM_BYTES, PARAM_BYTES,
                              &full[stage]);
                     ++issued[stage];
+                    if (++stage == NSTAGE) {
+                        stage = 0;
+                        sph ^= 1u;
+                    }
                 }
             }
             // Before the CTA leaves (also on the failure path), let every copy
@@ -442,23 +477,23 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     (void)mbar_wait_budget(&a_full_ph[b], (uint32_t)((issued_a[b] - 1) & 1), 100000000LL);
         }
         __syncwarp();
-    } else if (warp == MMA_WARP) {
+    } else if (warp == PHASE_WARP) {
+        // Phase MMAs of every chunk: classes into TMEM columns P_COL, one chunk
+        // ahead of the magnetisation warps.
         if (lane == 0) {
             constexpr uint32_t id_ph1 = idesc_i8(PH_N1, true, true);
             constexpr uint32_t id_ph2 = idesc_i8(PH_N2, true, true);
             constexpr uint32_t id_ph3 = idesc_i8(PH_N3, true, true);
-            constexpr uint32_t id_c3 = idesc_i8(3 * N, false, true);
-            constexpr uint32_t id_c2 = idesc_i8(2 * N, false, true);
-            constexpr uint32_t id_c1 = idesc_i8(N, true, true);   // signed low digit of M
-            Cursor cp = cursor_start(args), cc = cp;
-            int gp = 0, gc = 0;
-            // Phase MMAs of chunk gp (cursor cp): classes into TMEM columns P_COL.
-            auto issue_phase = [&]() -> bool {
-                const int stage = gp % NSTAGE;
+            int stage = 0, gp = 0;
+            uint32_t sph = 0;
+            for (Cursor cp = cursor_start(args); cp.valid; ++gp) {
                 const int ib = cp.local & 1;
-                if (!mbar_wait(&full[stage], (uint32_t)((gp / NSTAGE) & 1))) return false;
-                if (cp.c == cp.c0 && !mbar_wait(&a_full_ph[ib], (uint32_t)((cp.local >> 1) & 1))) return false;
-                if (!mbar_wait(p_empty, (uint32_t)((gp + 1) & 1))) return false;
+                if (!mbar_wait_helper(&full[stage], sph) ||
+                    (cp.c == cp.c0 && !mbar_wait_helper(&a_full_ph[ib], (uint32_t)((cp.local >> 1) & 1))) ||
+                    !mbar_wait_helper(p_empty, (uint32_t)((gp + 1) & 1))) {
+                    atomicOr(args.err, 2u);
+                    break;
+                }
                 tc_fence_after();
                 const uint32_t a0 = smem_u32(sA + ib * PHASE_A_BYTES);
                 const uint32_t b0 = smem_u32(sStage + (size_t)stage * STAGE_BYTES + CB);
@@ -467,52 +502,53 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 tc_mma_i8_ss(tmem + P_COL + 96u, sdesc(a0 + 2 * TM * 32), sdesc(b0 + PH_OFF3), id_ph3, 1u);
                 tc_commit(p_full);
                 if (cp.c + 1 == cp.c1) tc_commit(&a_empty_ph[ib]);
-                ++gp;
+                if (++stage == NSTAGE) {
+                    stage = 0;
+                    sph ^= 1u;
+                }
                 cursor_next(args, cp);
-                return true;
-            };
-            // Coil MMAs of chunk gc (cursor cc): digit classes into TMEM columns D_COL.
-            auto issue_coil = [&]() -> bool {
-                const int stage = gc % NSTAGE;
-                if (!mbar_wait(a_full, (uint32_t)(gc & 1))) return false;
-                if (cc.c == cc.c0 && !mbar_wait(d_empty, (uint32_t)(cc.local & 1))) return false;
+            }
+            // Every issued MMA completes before TMEM is released.
+            tc_commit(&done[1]);
+            if (!mbar_wait(&done[1], 0)) atomicOr(args.err, 8u);
+        }
+        __syncwarp();
+    } else if (warp == MMA_WARP) {
+        // Coil MMAs of every chunk: digit classes into TMEM columns D_COL.
+        if (lane == 0) {
+            constexpr uint32_t id_c3 = idesc_i8(3 * N, false, true);
+            constexpr uint32_t id_c2 = idesc_i8(2 * N, false, true);
+            constexpr uint32_t id_c1 = idesc_i8(N, true, true);  // signed low digit of M
+            int stage = 0, gc = 0;
+            uint32_t sph = 0;
+            for (Cursor cc = cursor_start(args); cc.valid; ++gc) {
+                if (!mbar_wait_helper(&full[stage], sph) || !mbar_wait_helper(a_full, (uint32_t)(gc & 1)) ||
+                    (cc.c == cc.c0 && !mbar_wait_helper(d_empty, (uint32_t)(cc.local & 1)))) {
+                    atomicOr(args.err, 4u);
+                    break;
+                }
                 tc_fence_after();
                 const uint32_t b0 = smem_u32(sStage + (size_t)stage * STAGE_BYTES);
 #pragma unroll
                 for (int ks = 0; ks < 2; ++ks) {
                     const uint64_t bd = sdesc(b0 + (uint32_t)(ks * 3 * N * 32));
                     const uint32_t acol = tmem + A_COL + (uint32_t)(ks * 32);
-                    tc_mma_i8_ts(tmem + D_COL, acol, bd, id_c3, 1u);                       // d3 x [c2|c1|c0]
-                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)N, acol + 8u, bd, id_c3, 1u);   // d2 x [c2|c1|c0]
+                    tc_mma_i8_ts(tmem + D_COL, acol, bd, id_c3, 1u);                            // d3 x [c2|c1|c0]
+                    tc_mma_i8_ts(tmem + D_COL + (uint32_t)N, acol + 8u, bd, id_c3, 1u);        // d2 x [c2|c1|c0]
                     tc_mma_i8_ts(tmem + D_COL + (uint32_t)(2 * N), acol + 16u, bd, id_c2, 1u);  // d1 x [c2|c1]
                     tc_mma_i8_ts(tmem + D_COL + (uint32_t)(3 * N), acol + 24u, bd, id_c1, 1u);  // d0 x [c2]
                 }
                 tc_commit(&empty[stage]);
-                tc_commit(a_empty);
                 if (cc.c + 1 == cc.c1) tc_commit(d_full);
-                ++gc;
+                if (++stage == NSTAGE) {
+                    stage = 0;
+                    sph ^= 1u;
+                }
                 cursor_next(args, cc);
-                return true;
-            };
-            if (cp.valid && !issue_phase()) {
-                atomicOr(args.err, 2u);
-                dead = true;
             }
-            while (cc.valid && !dead) {
-                if (cp.valid && !issue_phase()) {
-                    atomicOr(args.err, 2u);
-                    dead = true;
-                    break;
-                }
-                if (!issue_coil()) {
-                    atomicOr(args.err, 4u);
-                    dead = true;
-                    break;
-                }
-            }
-            // Wait for every issued MMA before TMEM is released.
-            tc_commit(done);
-            if (!mbar_wait(done, 0)) atomicOr(args.err, 8u);
+            // Every issued MMA completes before TMEM is released.
+            tc_commit(&done[0]);
+            if (!mbar_wait(&done[0], 0)) atomicOr(args.err, 8u);
         }
         __syncwarp();
     } else {
@@ -540,39 +576,37 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
         }
         const uint32_t m8 = args.mul8, m16 = args.mul16, m24 = args.mul24, m25 = args.mul25;
         const int n_items = args.tiles * args.slabs;
-        int g = 0;
-        // Phase classes w = 7..2 (columns (7 - w) * 32) of this warp's 8 spins: loaded for
-        // chunk g + 1 while chunk g's A operand is handed over (the load's latency overlaps).
-        uint32_t pc[6][8];
-        auto load_phase = [&](int gg) -> bool {
-            const bool ok = mbar_wait(p_full, (uint32_t)(gg & 1));
+        int g = 0, stage = 0, prev_stage = 0;
+        uint32_t sph = 0, prev_sph = 0;
+        // Phase classes w = 7..3 (columns (7 - w) * 32) of this warp's 8 spins,
+        // loaded for chunk g + 1 once chunk g's A operand is handed over.
+        uint32_t pc[PH_CLASSES][8];
+        auto wait_all = [&](uint64_t *bar, uint32_t parity) -> bool {
+            const bool ok = mbar_wait(bar, parity);
             __syncwarp();
-            if (!__all_sync(0xffffffffu, ok)) return false;
+            return __all_sync(0xffffffffu, ok);
+        };
+        auto load_phase = [&](int gg) -> bool {
+            if (!wait_all(p_full, (uint32_t)(gg & 1))) return false;
             tc_fence_after();
 #pragma unroll
-            for (int t = 0; t < 6; ++t) tmem_ld_x8(tmem + lq + P_COL + (uint32_t)(t * 32 + cq * 8), pc[t]);
+            for (int t = 0; t < PH_CLASSES; ++t) tmem_ld_x8(tmem + lq + P_COL + (uint32_t)(t * 32 + cq * 8), pc[t]);
+            tmem_wait_ld();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(p_empty);
             return true;
         };
         Cursor cu = cursor_start(args);
-        if (cu.valid) {
-            if (!load_phase(0)) {
-                if (lane == 0) atomicOr(args.err, 16u);
-                dead = true;
-            } else {
-                tmem_wait_ld();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(p_empty);
-            }
+        if (cu.valid && !load_phase(0)) {
+            if (lane == 0) atomicOr(args.err, 16u);
+            dead = true;
         }
         for (; cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
             const uint32_t base = args.rows[2 * ((size_t)cu.tile * TM + row)];
             const float tj = __uint_as_float(args.rows[2 * ((size_t)cu.tile * TM + row) + 1]);
             for (int c = cu.c0; c < cu.c1; ++c, ++g) {
-                const int stage = g % NSTAGE;
-                bool ok = mbar_wait(&full[stage], (uint32_t)((g / NSTAGE) & 1));
-                __syncwarp();
-                if (!__all_sync(0xffffffffu, ok)) {
+                if (!wait_all(&full[stage], sph)) {
                     if (lane == 0) atomicOr(args.err, 32u);
                     dead = true;
                     break;
@@ -590,6 +624,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     r2b[4 * v] = b4.x, r2b[4 * v + 1] = b4.y, r2b[4 * v + 2] = b4.z, r2b[4 * v + 3] = b4.w;
                     l2b[4 * v] = c4.x, l2b[4 * v + 1] = c4.y, l2b[4 * v + 2] = c4.z, l2b[4 * v + 3] = c4.w;
                 }
+                const int cur_stage = stage;
+                const uint32_t cur_sph = sph;
+                if (++stage == NSTAGE) {
+                    stage = 0;
+                    sph ^= 1u;
+                }
                 uint32_t wd[4][4];  // digit planes d1, d2, d3 (+64), d0 of spins (2p, 2p+1)
 #pragma unroll
                 for (int pp = 0; pp < 4; ++pp) {
@@ -598,13 +638,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     for (int h = 0; h < 2; ++h) {
                         const int i = 2 * pp + h;
                         // u = turn + 2^29 + 64: classes 7, 6, 5 shifted left by 24, 16, 8 bits,
-                        // class 4 as is, classes 3, 2 shifted right (arithmetic) by 8, 16.
+                        // class 4 as is, class 3 shifted right (arithmetic) by 8.
                         uint32_t u = base + th[i] + pc[3][i];
                         u = mad_lo(pc[2][i], m8, u);
                         u = mad_lo(pc[1][i], m16, u);
                         u = mad_lo(pc[0][i], m24, u);
                         u = mad_hi_s(pc[4][i], m24, u);
-                        u = mad_hi_s(pc[5][i], m16, u);
                         // Quarter-turn reduction: quadrant u >> 30, remainder (u & (2^30 - 1)) - 2^29
                         // to 23 bits (the +64 of u rounds it).
                         const uint32_t fb = (mul_hi_u(u, m25) & 0x7FFFFFu) | 0x4B000000u;
@@ -640,20 +679,16 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     wd[2][pp] = prmt(q0, q1, 0x5410u);
                     wd[3][pp] = prmt(r0, r1, 0x5410u);
                 }
-                const bool more = c + 1 < cu.c1 || cu.i + (int)gridDim.x < n_items;
-                if (more && !load_phase(g + 1)) {
-                    if (lane == 0) atomicOr(args.err, 16u);
-                    dead = true;
-                    break;
-                }
-                ok = mbar_wait(a_empty, (uint32_t)((g + 1) & 1));
-                __syncwarp();
-                if (!__all_sync(0xffffffffu, ok)) {
+                // Hand the A operand to the coil issuer (once the previous chunk's coil
+                // MMAs, which read the buffer, are complete), then take the next
+                // chunk's phase classes.
+                if (g > 0 && !wait_all(&empty[prev_stage], prev_sph)) {
                     if (lane == 0) atomicOr(args.err, 128u);
-                    tmem_wait_ld();
                     dead = true;
                     break;
                 }
+                prev_stage = cur_stage;
+                prev_sph = cur_sph;
                 tc_fence_after();
                 const uint32_t acol = tmem + lq + A_COL + (uint32_t)(ks * 32 + 4 * (cq & 1));
                 tmem_st_x4(acol, wd[2]);        // d3 + 64
@@ -661,20 +696,20 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 tmem_st_x4(acol + 16u, wd[0]);  // d1
                 tmem_st_x4(acol + 24u, wd[3]);  // d0
                 tmem_wait_st();
-                if (more) tmem_wait_ld();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) {
-                    mbar_arrive(a_full);
-                    if (more) mbar_arrive(p_empty);
+                if (lane == 0) mbar_arrive(a_full);
+                const bool more = c + 1 < cu.c1 || cu.i + (int)gridDim.x < n_items;
+                if (more && !load_phase(g + 1)) {
+                    if (lane == 0) atomicOr(args.err, 16u);
+                    dead = true;
+                    break;
                 }
             }
             if (dead) break;
             // Item end: the coil classes of this warp's rows and columns into the
             // item's FP64 partial, then clear them for the next item.
-            bool ok = mbar_wait(d_full, (uint32_t)(cu.local & 1));
-            __syncwarp();
-            if (!__all_sync(0xffffffffu, ok)) {
+            if (!wait_all(d_full, (uint32_t)(cu.local & 1))) {
                 if (lane == 0) atomicOr(args.err, 512u);
                 dead = true;
                 break;
@@ -831,9 +866,9 @@ __global__ void term_max_kernel(const double *basis, const double *dw, int64_t n
 // Phase B operand of every chunk: per spin the five balanced digits of
 // B_k = rint(b_k 2^38 / bmax_k) for the 16 terms (16 bytes per digit), placed
 // as the B' rows of the three phase MMAs (class block w, spin s):
-//   MMA 1: row (7 - w) 32 + s, K halves digits (w - 4, w - 3), w = 7..2
-//   MMA 2: row (6 - w) 32 + s, K halves digits (w - 2, w - 1), w = 6..2
-//   MMA 3: row (4 - w) 32 + s, K halves digits (w, none),      w = 4..2
+//   MMA 1: row (7 - w) 32 + s, K halves digits (w - 4, w - 3), w = 7..3
+//   MMA 2: row (6 - w) 32 + s, K halves digits (w - 2, w - 1), w = 6..3
+//   MMA 3: row (4 - w) 32 + s, K halves digits (w, none),      w = 4..3
 // with zeros where the digit index is outside 0..4 and for padding spins.
 __global__ void phase_b_kernel(const double *basis, const double *dw, int64_t ns, int64_t nchunks,
                                const unsigned long long *term_max, uint8_t *out) {
@@ -870,15 +905,15 @@ __global__ void phase_b_kernel(const double *basis, const double *dw, int64_t ns
             if (d >= 0 && d < PHASE_DIGITS) v = make_uint4(dig[d][0], dig[d][1], dig[d][2], dig[d][3]);
             *reinterpret_cast<uint4 *>(base + off + kmaj(row, kc * 16)) = v;
         };
-        for (int w = 7; w >= 2; --w) {
+        for (int w = 7; w >= 3; --w) {
             put(0, (7 - w) * 32 + s, 0, w - 4);
             put(0, (7 - w) * 32 + s, 1, w - 3);
         }
-        for (int w = 6; w >= 2; --w) {
+        for (int w = 6; w >= 3; --w) {
             put(PH_OFF2, (6 - w) * 32 + s, 0, w - 2);
             put(PH_OFF2, (6 - w) * 32 + s, 1, w - 1);
         }
-        for (int w = 4; w >= 2; --w) {
+        for (int w = 4; w >= 3; --w) {
             put(PH_OFF3, (4 - w) * 32 + s, 0, w);
             put(PH_OFF3, (4 - w) * 32 + s, 1, -1);
         }
