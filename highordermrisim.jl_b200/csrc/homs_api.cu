@@ -1281,19 +1281,19 @@ homs_status homs_coil_reduce(homs_context *ctx, homs_dtype dtype, int64_t nspins
         }
         HOMS_REQUIRE((nadc + PLAIN_STAGE - 1) / PLAIN_STAGE <= 65535,
                      "nadc above 524280 samples per call (the reduction's grid)");
-        const int64_t tiles = (nspins + PLAIN_THREADS - 1) / PLAIN_THREADS;
-        HOMS_CUDA(ctx->scratch_partial.ensure(es * (size_t)tiles * (size_t)nadc * (size_t)ncoils));
+        const int64_t parts = coil_reduce_parts(nspins, nadc, ncoils);
+        HOMS_CUDA(ctx->scratch_partial.ensure(es * (size_t)parts * (size_t)nadc * (size_t)ncoils));
         if (dtype == HOMS_F64) {
             HOMS_CUDA(launch_coil_reduce<double>(nspins, nadc, ncoils, (const cplx<double> *)states, ldstates,
                                                  (const cplx<double> *)csm, ldcsm, reinterpret_cast<cplx<double> *>(ctx->scratch_partial.p),
                                                  ctx->stream));
-            HOMS_CUDA(launch_partial_finalize<double>(reinterpret_cast<cplx<double> *>(ctx->scratch_partial.p), tiles, nadc, ncoils,
+            HOMS_CUDA(launch_partial_finalize<double>(reinterpret_cast<cplx<double> *>(ctx->scratch_partial.p), parts, nadc, ncoils,
                                                       (cplx<double> *)sig, ldsig, ctx->stream));
         } else {
             HOMS_CUDA(launch_coil_reduce<float>(nspins, nadc, ncoils, (const cplx<float> *)states, ldstates,
                                                 (const cplx<float> *)csm, ldcsm, reinterpret_cast<cplx<float> *>(ctx->scratch_partial.p),
                                                 ctx->stream));
-            HOMS_CUDA(launch_partial_finalize<float>(reinterpret_cast<cplx<float> *>(ctx->scratch_partial.p), tiles, nadc, ncoils,
+            HOMS_CUDA(launch_partial_finalize<float>(reinterpret_cast<cplx<float> *>(ctx->scratch_partial.p), parts, nadc, ncoils,
                                                      (cplx<float> *)sig, ldsig, ctx->stream));
         }
         return HOMS_OK;

@@ -78,6 +78,11 @@ template <typename T>
 cudaError_t launch_partial_finalize(const cplx<T> *partial, int64_t nparts, int64_t nsamples, int32_t nc,
                                     cplx<T> *sig, int64_t ldsig, cudaStream_t stream);
 
+// Standalone coil reduction, split-K over spin ranges: coil_reduce_parts()
+// partial (nadc x nc) blocks, at most ceil(ns / PLAIN_THREADS) of them, which
+// launch_partial_finalize sums in part order.
+int64_t coil_reduce_parts(int64_t ns, int64_t nadc, int32_t nc);
+
 template <typename T>
 cudaError_t launch_coil_reduce(int64_t ns, int64_t nadc, int32_t nc, const cplx<T> *states, int64_t ldstates,
                                const cplx<T> *csm, int64_t ldcsm, cplx<T> *partial, cudaStream_t stream);

@@ -76,18 +76,20 @@ extern "C" homs_status homs_coil_reduce_noalloc(void *stream, homs_dtype dtype, 
     const double need = (double)es * (double)tiles * (double)nadc * (double)ncoils;
     if (need > (double)kScratchBytes) return HOMS_EINVAL;
     if ((nadc + homs::PLAIN_STAGE - 1) / homs::PLAIN_STAGE > 65535) return HOMS_EINVAL;  // grid.y of the reduce step
+    // The reduce step writes coil_reduce_parts() <= tiles partial blocks, so they fit.
+    const int64_t parts = homs::coil_reduce_parts(nspins, nadc, ncoils);
     cudaError_t e;
     if (dtype == HOMS_F64) {
         e = homs::launch_coil_reduce<double>(nspins, nadc, ncoils, (const cplx<double> *)states, ldstates,
                                              (const cplx<double> *)csm, ldcsm, (cplx<double> *)scratch, st);
         if (e == cudaSuccess)
-            e = homs::launch_partial_finalize<double>((const cplx<double> *)scratch, tiles, nadc, ncoils,
+            e = homs::launch_partial_finalize<double>((const cplx<double> *)scratch, parts, nadc, ncoils,
                                                       (cplx<double> *)sig, ldsig, st);
     } else {
         e = homs::launch_coil_reduce<float>(nspins, nadc, ncoils, (const cplx<float> *)states, ldstates,
                                             (const cplx<float> *)csm, ldcsm, (cplx<float> *)scratch, st);
         if (e == cudaSuccess)
-            e = homs::launch_partial_finalize<float>((const cplx<float> *)scratch, tiles, nadc, ncoils,
+            e = homs::launch_partial_finalize<float>((const cplx<float> *)scratch, parts, nadc, ncoils,
                                                      (cplx<float> *)sig, ldsig, st);
     }
     return e == cudaSuccess ? HOMS_OK : HOMS_ECUDA;

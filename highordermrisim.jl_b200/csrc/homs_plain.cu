@@ -382,73 +382,116 @@ __global__ void __launch_bounds__(PLAIN_THREADS)
     }
 }
 
-// sig[(j) + c*ldsig] = sum over parts of partial[(part*nsamples + j)*nc + c], in part order.
+// sig[(j) + c*ldsig] = sum over parts k of partial[(k*nsamples + j)*nc + c].
+// A block takes 32 consecutive outputs; warp q of its 8 sums the parts
+// k = q, q + 8, ... in increasing order (coalesced: 32 outputs of one part per
+// load), then warp 0 adds the 8 sums in warp order.  The order depends only on
+// nparts, so repeated runs are bit-identical.
+constexpr int FIN_OUT = 32, FIN_SLICES = 8;
 template <typename T>
-__global__ void partial_finalize_kernel(const cplx<T> *partial, int64_t nparts, int64_t nsamples, int32_t nc,
-                                        cplx<T> *sig, int64_t ldsig) {
+__global__ void __launch_bounds__(FIN_OUT *FIN_SLICES)
+    partial_finalize_kernel(const cplx<T> *partial, int64_t nparts, int64_t nsamples, int32_t nc, cplx<T> *sig,
+                            int64_t ldsig) {
+    __shared__ cplx<T> red[FIN_SLICES][FIN_OUT];
     const int64_t total = nsamples * nc;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t j = i / nc;
-        const int32_t c = (int32_t)(i % nc);
+    const int ol = threadIdx.x % FIN_OUT, q = threadIdx.x / FIN_OUT;
+    for (int64_t o0 = (int64_t)blockIdx.x * FIN_OUT; o0 < total; o0 += (int64_t)gridDim.x * FIN_OUT) {
+        const int64_t o = o0 + ol;
         cplx<T> acc{T(0), T(0)};
-        for (int64_t k = 0; k < nparts; ++k) {
-            cplx<T> v = partial[(k * nsamples + j) * nc + c];
-            acc.re = acc.re + v.re;
-            acc.im = acc.im + v.im;
-        }
-        sig[j + (int64_t)c * ldsig] = acc;
-    }
-}
-
-// Standalone reduction: one CTA per (spin tile, sample chunk); partial rows
-// per spin tile, summed afterwards by partial_finalize_kernel.
-template <typename T>
-__global__ void __launch_bounds__(PLAIN_THREADS)
-    coil_reduce_kernel(int64_t ns, int64_t nadc, int32_t nc, const cplx<T> *states, int64_t ldstates,
-                       const cplx<T> *csm, int64_t ldcsm, cplx<T> *partial) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<T> *X = reinterpret_cast<cplx<T> *>(smem_raw);
-    cplx<T> *P = X + PLAIN_STAGE * PLAIN_THREADS;
-    cplx<T> *csm_s = P + PLAIN_STAGE * PLAIN_THREADS;
-    const int64_t spin0 = (int64_t)blockIdx.x * PLAIN_THREADS;
-    const int nvalid = (int)imin64(PLAIN_THREADS, ns - spin0);
-    const int64_t j0 = (int64_t)blockIdx.y * PLAIN_STAGE;
-    const int na = (int)imin64(PLAIN_STAGE, nadc - j0);
-    const bool csm_in_smem = sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS <= 96 * 1024;
-    // Transposed sensitivities (rows s, coil-fastest) in shared memory, or a
-    // column-major global fallback via a row pointer with stride ldcsm.
-    const int s_local = threadIdx.x;
-    for (int a = 0; a < na; ++a) {
-        cplx<T> v{T(0), T(0)};
-        if (s_local < nvalid) v = states[(spin0 + s_local) + (j0 + a) * ldstates];
-        X[a * PLAIN_THREADS + s_local] = v;
-    }
-    if (csm_in_smem) {
-        for (int64_t i = threadIdx.x; i < (int64_t)nvalid * nc; i += PLAIN_THREADS) {
-            const int64_t sl = i / nc;
-            const int32_t c = (int32_t)(i % nc);
-            csm_s[i] = csm[(spin0 + sl) + c * ldcsm];
-        }
-    }
-    __syncthreads();
-    cplx<T> *out = partial + ((int64_t)blockIdx.x * nadc + j0) * nc;
-    if (csm_in_smem) {
-        reduce_stage(X, P, na, csm_s, nc, nvalid, nc, out);
-    } else {
-        // Large coil counts: contract straight from the column-major array.
-        const int t = threadIdx.x;
-        for (int64_t o = t; o < (int64_t)na * nc; o += PLAIN_THREADS) {
-            const int a = (int)(o / nc);
-            const int32_t c = (int32_t)(o % nc);
-            cplx<T> acc{T(0), T(0)};
-            for (int sl = 0; sl < nvalid; ++sl) {
-                cplx<T> v = cmul(X[a * PLAIN_THREADS + sl], csm[(spin0 + sl) + c * ldcsm]);
+        if (o < total)
+            for (int64_t k = q; k < nparts; k += FIN_SLICES) {
+                const cplx<T> v = partial[k * total + o];
                 acc.re = acc.re + v.re;
                 acc.im = acc.im + v.im;
             }
-            out[(int64_t)a * nc + c] = acc;
+        red[q][ol] = acc;
+        __syncthreads();
+        if (q == 0 && o < total) {
+            cplx<T> s = red[0][ol];
+            for (int qq = 1; qq < FIN_SLICES; ++qq) {
+                s.re = s.re + red[qq][ol].re;
+                s.im = s.im + red[qq][ol].im;
+            }
+            const int64_t jj = o / nc;
+            const int32_t c = (int32_t)(o % nc);
+            sig[jj + (int64_t)c * ldsig] = s;
         }
+        __syncthreads();
+    }
+}
+
+// Standalone coil reduction (states^T csm, no conjugation), split-K over spin
+// ranges.  CTA (p, jt, ct) sums spins [ns p / P, ns (p + 1) / P) for samples
+// 64 jt .. +63 and coils 32 ct .. +31 into its partial block: chunks of 16
+// spins of both operands are staged in shared memory with coalesced loads
+// along the spins (both arrays are column-major), then thread t accumulates
+// sample t % 64 against coils 8 (t / 64) .. +7 in registers (a warp reads 32
+// consecutive samples of one spin; the 8 sensitivities are broadcasts).
+constexpr int CR_JB = 64, CR_CB = 32, CR_SK = 16, CR_THREADS = 256, CR_CTAS_PER_SM = 2;
+constexpr int CR_XL = CR_SK * CR_JB / CR_THREADS, CR_CL = CR_SK * CR_CB / CR_THREADS;  // loads per thread and chunk
+template <typename T>
+__global__ void __launch_bounds__(CR_THREADS, CR_CTAS_PER_SM)
+    coil_reduce_kernel(int64_t ns, int64_t nadc, int32_t nc, const cplx<T> *states, int64_t ldstates,
+                       const cplx<T> *csm, int64_t ldcsm, int64_t parts, cplx<T> *partial) {
+    __shared__ cplx<T> Xs[CR_SK][CR_JB + 1];
+    __shared__ cplx<T> Cs[CR_SK][CR_CB + 1];
+    const int64_t p = blockIdx.x;
+    const int64_t j0 = (int64_t)blockIdx.y * CR_JB;
+    const int c0 = (int)blockIdx.z * CR_CB;
+    const int jn = (int)imin64(CR_JB, nadc - j0), cn = (int)imin64(CR_CB, nc - c0);
+    const int64_t s_begin = ns * p / parts, s_end = ns * (p + 1) / parts;
+    const int t = threadIdx.x;
+    const int jl = t % CR_JB, cb = (t / CR_JB) * 8;
+    // The next chunk's operands are fetched into registers while the current
+    // chunk is contracted from shared memory.
+    cplx<T> xr[CR_XL], cr[CR_CL];
+    auto fetch = [&](int64_t s0) {
+        const int sn = (int)imin64(CR_SK, s_end - s0);
+#pragma unroll
+        for (int r = 0; r < CR_XL; ++r) {
+            const int i = t + r * CR_THREADS, sl = i % CR_SK, jj = i / CR_SK;
+            xr[r] = (sl < sn && jj < jn) ? states[(s0 + sl) + (j0 + jj) * ldstates] : cplx<T>{T(0), T(0)};
+        }
+#pragma unroll
+        for (int r = 0; r < CR_CL; ++r) {
+            const int i = t + r * CR_THREADS, sl = i % CR_SK, c = i / CR_SK;
+            cr[r] = (sl < sn && c < cn) ? csm[(s0 + sl) + (int64_t)(c0 + c) * ldcsm] : cplx<T>{T(0), T(0)};
+        }
+    };
+    cplx<T> acc[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc[m] = cplx<T>{T(0), T(0)};
+    if (s_begin < s_end) fetch(s_begin);
+    for (int64_t s0 = s_begin; s0 < s_end; s0 += CR_SK) {
+        const int sn = (int)imin64(CR_SK, s_end - s0);
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < CR_XL; ++r) {
+            const int i = t + r * CR_THREADS;
+            Xs[i % CR_SK][i / CR_SK] = xr[r];
+        }
+#pragma unroll
+        for (int r = 0; r < CR_CL; ++r) {
+            const int i = t + r * CR_THREADS;
+            Cs[i % CR_SK][i / CR_SK] = cr[r];
+        }
+        __syncthreads();
+        if (s0 + CR_SK < s_end) fetch(s0 + CR_SK);
+        for (int sl = 0; sl < sn; ++sl) {
+            const cplx<T> x = Xs[sl][jl];
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const cplx<T> w = Cs[sl][cb + m];
+                acc[m].re = fma(x.re, w.re, fma(-x.im, w.im, acc[m].re));
+                acc[m].im = fma(x.re, w.im, fma(x.im, w.re, acc[m].im));
+            }
+        }
+    }
+    if (jl < jn) {
+        cplx<T> *out = partial + (p * nadc + j0 + jl) * nc + c0;
+#pragma unroll
+        for (int m = 0; m < 8; ++m)
+            if (cb + m < cn) out[cb + m] = acc[m];
     }
 }
 
@@ -474,24 +517,31 @@ cudaError_t launch_partial_finalize(const cplx<T> *partial, int64_t nparts, int6
                                     cplx<T> *sig, int64_t ldsig, cudaStream_t stream) {
     const int64_t total = nsamples * nc;
     if (total == 0) return cudaSuccess;
-    const int threads = 256;
-    const int64_t blocks = std::min<int64_t>((total + threads - 1) / threads, 148 * 16);
-    partial_finalize_kernel<T><<<(int)blocks, threads, 0, stream>>>(partial, nparts, nsamples, nc, sig, ldsig);
+    const int64_t blocks = std::min<int64_t>((total + FIN_OUT - 1) / FIN_OUT, 148 * 16);
+    partial_finalize_kernel<T><<<(int)blocks, FIN_OUT * FIN_SLICES, 0, stream>>>(partial, nparts, nsamples, nc, sig,
+                                                                                  ldsig);
     return cudaGetLastError();
+}
+
+// Parts of the split-K: one wave of CR_CTAS_PER_SM CTAs per SM over all
+// (sample, coil) tiles, at least 256 spins per part (so at most
+// ceil(ns / PLAIN_THREADS) parts).
+int64_t coil_reduce_parts(int64_t ns, int64_t nadc, int32_t nc) {
+    const int64_t tiles = ((nadc + CR_JB - 1) / CR_JB) * ((nc + CR_CB - 1) / CR_CB);
+    const int64_t want = std::max<int64_t>(1, (148 * CR_CTAS_PER_SM) / tiles);
+    return std::max<int64_t>(1, std::min<int64_t>(want, (ns + PLAIN_THREADS - 1) / PLAIN_THREADS));
 }
 
 template <typename T>
 cudaError_t launch_coil_reduce(int64_t ns, int64_t nadc, int32_t nc, const cplx<T> *states, int64_t ldstates,
                                const cplx<T> *csm, int64_t ldcsm, cplx<T> *partial, cudaStream_t stream) {
-    const int64_t tiles = (ns + PLAIN_THREADS - 1) / PLAIN_THREADS;
-    const int64_t chunks = (nadc + PLAIN_STAGE - 1) / PLAIN_STAGE;
-    if (tiles == 0 || chunks == 0) return cudaSuccess;
-    size_t smem = 2 * sizeof(cplx<T>) * PLAIN_STAGE * PLAIN_THREADS;
-    if (sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS <= 96 * 1024) smem += sizeof(cplx<T>) * (size_t)nc * PLAIN_THREADS;
-    cudaError_t e = allow_max_dynamic_smem((const void *)coil_reduce_kernel<T>);
-    if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)tiles, (unsigned)chunks);
-    coil_reduce_kernel<T><<<grid, PLAIN_THREADS, smem, stream>>>(ns, nadc, nc, states, ldstates, csm, ldcsm, partial);
+    if (ns == 0 || nadc == 0 || nc == 0) return cudaSuccess;
+    const int64_t parts = coil_reduce_parts(ns, nadc, nc);
+    const int64_t jt = (nadc + CR_JB - 1) / CR_JB, ct = (nc + CR_CB - 1) / CR_CB;
+    if (jt > 65535 || ct > 65535) return cudaErrorInvalidValue;
+    dim3 grid((unsigned)parts, (unsigned)jt, (unsigned)ct);
+    coil_reduce_kernel<T><<<grid, CR_THREADS, 0, stream>>>(ns, nadc, nc, states, ldstates, csm, ldcsm, parts,
+                                                          partial);
     return cudaGetLastError();
 }
 

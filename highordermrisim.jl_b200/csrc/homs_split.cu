@@ -1005,25 +1005,32 @@ __global__ void coil_b_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t 
 }
 
 // Per coil group and output column: the sum over all spins and both
-// components of the sensitivity integers (exact, int64), one block per
-// column.
+// components of the sensitivity integers (exact int64; colsum zeroed first).
+// A grid-stride pass over the spin-major rows (coalesced); each block sums
+// into shared int64 counters, then adds them to colsum.  Integer sums do not
+// depend on the order, so the result is exact and reproducible.
 __global__ void colsum_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int n_cols, const int *coil_exp,
-                              long long *colsum) {
-    __shared__ long long part[256];
-    const int grp = blockIdx.x / n_cols, n = blockIdx.x % n_cols;
-    const int coil0 = grp * GROUP_COILS;
-    const int ncg = min(GROUP_COILS, nc - coil0);
-    long long acc = 0;
-    for (int64_t sp = threadIdx.x; sp < ns; sp += blockDim.x)
-        acc += coil_int(csm_rows, ns, nc, coil0, ncg, coil_exp, n, 0, sp) +
-               coil_int(csm_rows, ns, nc, coil0, ncg, coil_exp, n, 1, sp);
-    part[threadIdx.x] = acc;
+                              unsigned long long *colsum) {
+    extern __shared__ unsigned long long csum[];  // ngroups * n_cols
+    const int ngroups = (nc + GROUP_COILS - 1) / GROUP_COILS;
+    for (int i = threadIdx.x; i < ngroups * n_cols; i += blockDim.x) csum[i] = 0ull;
     __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
-        __syncthreads();
+    const int64_t total = ns * nc;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int coil = (int)(i % nc);
+        const int grp = coil / GROUP_COILS, c = coil - grp * GROUP_COILS;
+        const int ncg = min(GROUP_COILS, nc - grp * GROUP_COILS);
+        const cplx<double> cv = csm_rows[i];
+        const int e = 22 - coil_exp[coil];
+        // the terms of coil_int: column c is Re c (Re M) + (-Im c) (Im M), column ncg + c is Im c + Re c
+        const long long re = llrint(ldexp(cv.re, e)), im = llrint(ldexp(cv.im, e)), mim = llrint(ldexp(-cv.im, e));
+        atomicAdd(&csum[grp * n_cols + c], (unsigned long long)(re + mim));
+        atomicAdd(&csum[grp * n_cols + ncg + c], (unsigned long long)(im + re));
     }
-    if (threadIdx.x == 0) colsum[blockIdx.x] = part[0];
+    __syncthreads();
+    for (int i = threadIdx.x; i < ngroups * n_cols; i += blockDim.x)
+        if (csum[i]) atomicAdd(&colsum[i], csum[i]);
 }
 
 // Per-segment spin parameters of every chunk, [turn of arg(m0) x 32 | r2 x 32
@@ -1357,8 +1364,11 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
     const int64_t pieces = (int64_t)ngroups * nchunks * 2 * 3 * n_cols * 2;
     coil_b_kernel<<<grid_for(pieces), 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_cols, nchunks,
                                                         ngroups, cexp, (uint8_t *)r.coil_b);
-    colsum_kernel<<<ngroups * n_cols, 256, 0, stream>>>((const cplx<double> *)csm_rows, ns, nc, n_cols, cexp,
-                                                        (long long *)r.colsum);
+    if ((e = cudaMemsetAsync(r.colsum, 0, sizeof(long long) * (size_t)n_cols * ngroups, stream)) != cudaSuccess)
+        return e;
+    if ((e = allow_max_dynamic_smem((const void *)colsum_kernel)) != cudaSuccess) return e;
+    colsum_kernel<<<grid_for(ns * nc), 256, sizeof(unsigned long long) * (size_t)n_cols * ngroups, stream>>>(
+        (const cplx<double> *)csm_rows, ns, nc, n_cols, cexp, (unsigned long long *)r.colsum);
     return cudaGetLastError();
 }
 
