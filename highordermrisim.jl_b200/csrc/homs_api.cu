@@ -640,6 +640,160 @@ void ensure_split_tables(homs_context *ctx, Resident<T> &r, uint32_t method) {
     }
 }
 
+// One split-mode run of the block plan, issued in steps so that several
+// runs can share the fused launches (the server's rounds):
+//   next()  issues everything up to the run's next fused job -- the RF
+//           launches before it and, at a segment's first coil group, the
+//           segment's prologue -- and returns the job;
+//   after() issues the job's finalize and, after the segment's last coil
+//           group, the state update.
+// A run on its own launches each job alone in between (run_resident).
+template <typename T>
+struct SplitRunner {
+    homs_context *ctx = nullptr;
+    Resident<T> *r = nullptr;
+    SplitRunArgs sa{};
+    std::vector<std::pair<Launch, T>> plan;
+    size_t i = 0;  // next plan entry
+    int grid = 0;
+    size_t row_bytes = 0;
+    // the segment in progress
+    bool in_segment = false;
+    size_t seg_next = 0;  // plan entry after the segment
+    int64_t seg_sample0 = 0;
+    int grp = 0;
+    SplitSegment seg;
+
+    void init(homs_context *c, Resident<T> &res, uint32_t method, bool capture) {
+        ctx = c;
+        r = &res;
+        sa.sizeof_T = sizeof(T);
+        sa.ns = res.ns;
+        sa.nc = res.nc;
+        sa.nt = res.nt;
+        sa.nadc = res.nadc;
+        sa.method = method;
+        sa.gamma = res.gamma;
+        sa.first = res.first.data();
+        sa.last = res.last.data();
+        sa.exc = res.exc.data();
+        sa.nblocks = (int32_t)res.first.size();
+        sa.adc_host = res.adc_host.data();
+        sa.grank = reinterpret_cast<const int32_t *>(res.grank.p);
+        sa.src_dev = reinterpret_cast<const void *const *>(res.src_table.p);
+        sa.capture = capture;
+        sa.t = res.t.p;
+        sa.dt = res.dt.p;
+        sa.gx = res.gx.p;
+        sa.gy = res.gy.p;
+        sa.gz = res.gz.p;
+        sa.b1 = res.b1.p;
+        sa.df = res.df.p;
+        sa.psi = res.psi.p;
+        sa.adc = res.adc.p;
+        sa.bnd = res.bnd.p;
+        for (int k = 0; k < 16; ++k) sa.h[k] = res.h[k].p;
+        sa.x = res.x.p;
+        sa.y = res.y.p;
+        sa.z = res.z.p;
+        sa.rho = res.rho.p;
+        sa.T1 = res.T1.p;
+        sa.T2 = res.T2.p;
+        sa.dw = res.dw.p;
+        sa.csm_rows = res.csm_rows.p;
+        sa.xy = res.xy.p;
+        sa.mz = res.mz.p;
+        sa.acc = res.acc.p;
+        sa.sig = res.sig.p;
+        sa.launches = &res.launches;
+        // RF runs use the plain FP64 excitation kernel; precession runs are
+        // whole segments on the split kernel.
+        grid = (int)((res.ns + PLAIN_THREADS - 1) / PLAIN_THREADS);
+        row_bytes = sizeof(cplx<T>) * (size_t)res.nc * (size_t)grid;
+        const int64_t max_samples = std::max<int64_t>(PLAIN_STAGE, (int64_t)((size_t(512) << 20) / row_bytes));
+        plan = plan_plain<T>(res, max_samples);
+        i = 0;
+        in_segment = false;
+    }
+
+    void rf_launch(const Launch &L, T tp0, cudaStream_t stream) {
+        HOMS_CUDA(r->partial.ensure(row_bytes * (size_t)std::max<int64_t>(L.nsamples, 1)));
+        SegmentArgs<T> a;
+        a.n_lo = L.n_lo;
+        a.n_hi = L.n_hi;
+        a.block_start = L.block_start;
+        a.tp0 = tp0;
+        a.nsamples = L.nsamples;
+        a.method = sa.method;
+        a.gamma = T(r->gamma);
+        a.gamma_d = r->gamma;
+        a.partial = reinterpret_cast<cplx<T> *>(r->partial.p);
+        PhantomDev<T> p = r->phantom();
+        SeqDev<T> q = r->seq();
+        StateDev<T> st{reinterpret_cast<cplx<T> *>(r->xy.p), reinterpret_cast<T *>(r->mz.p),
+                       reinterpret_cast<T *>(r->acc.p)};
+        HOMS_CUDA(launch_segment<T>(true, p, q, st, a, grid, stream));
+        r->launches += 1;
+        if (L.nsamples > 0) {
+            HOMS_CUDA(launch_partial_finalize<T>(a.partial, grid, L.nsamples, r->nc,
+                                                 reinterpret_cast<cplx<T> *>(r->sig.p) + L.sample0, r->nadc, stream));
+            r->launches += 1;
+        }
+    }
+
+    bool next(cudaStream_t stream, SplitJobDesc *job) {
+        if (in_segment) {
+            *job = split_segment_job(r->split, seg, grp);
+            return true;
+        }
+        while (i < plan.size()) {
+            const Launch &L = plan[i].first;
+            if (L.rf) {
+                rf_launch(L, plan[i].second, stream);
+                ++i;
+                continue;
+            }
+            // merge consecutive precession launches of one run into a segment
+            size_t j = i;
+            int64_t ns_total = 0;
+            while (j < plan.size() && !plan[j].first.rf && plan[j].first.run == L.run) {
+                ns_total += plan[j].first.nsamples;
+                ++j;
+            }
+            std::string err;
+            const cudaError_t e =
+                split_segment_begin(r->split, sa, L.n_lo, plan[j - 1].first.n_hi, L.sample0, ns_total, stream, &err,
+                                    &seg);
+            if (e != cudaSuccess) throw Failure{e == cudaErrorMemoryAllocation ? HOMS_ENOMEM : HOMS_ECUDA,
+                                                std::string("split segment: ") + cudaGetErrorString(e)};
+            if (!err.empty()) throw Failure{HOMS_EUNSUPPORTED, err};
+            if (ns_total == 0) {
+                HOMS_CUDA(split_segment_end(r->split, sa, seg, stream));
+                i = j;
+                continue;
+            }
+            in_segment = true;
+            seg_next = j;
+            seg_sample0 = L.sample0;
+            grp = 0;
+            *job = split_segment_job(r->split, seg, grp);
+            return true;
+        }
+        return false;
+    }
+
+    void after(cudaStream_t stream) {
+        HOMS_CUDA(split_segment_finalize(r->split, sa, seg, grp, seg_sample0, stream));
+        if (++grp < r->split.ngroups) return;
+        HOMS_CUDA(split_segment_end(r->split, sa, seg, stream));
+        in_segment = false;
+        i = seg_next;
+    }
+
+    bool first_group() const { return grp == 0; }
+    bool last_group() const { return grp + 1 == r->split.ngroups; }
+};
+
 // Issue one run of the block plan on ctx's stream.  With `capture` the
 // stream is being captured into a CUDA graph: every host-side table and
 // buffer must already be in place (an earlier run of the same plan built
@@ -666,102 +820,22 @@ void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opt
             ensure_split_tables<T>(ctx, r, method);
         }
         HOMS_CUDA(split_reset_error(r.split, ctx->stream));
-        SplitRunArgs sa;
-        sa.sizeof_T = sizeof(T);
-        sa.ns = r.ns;
-        sa.nc = r.nc;
-        sa.nt = r.nt;
-        sa.nadc = r.nadc;
-        sa.method = method;
-        sa.gamma = r.gamma;
-        sa.first = r.first.data();
-        sa.last = r.last.data();
-        sa.exc = r.exc.data();
-        sa.nblocks = (int32_t)r.first.size();
-        sa.adc_host = r.adc_host.data();
-        sa.grank = reinterpret_cast<const int32_t *>(r.grank.p);
-        sa.src_dev = reinterpret_cast<const void *const *>(r.src_table.p);
-        sa.capture = capture;
-        sa.t = r.t.p;
-        sa.dt = r.dt.p;
-        sa.gx = r.gx.p;
-        sa.gy = r.gy.p;
-        sa.gz = r.gz.p;
-        sa.b1 = r.b1.p;
-        sa.df = r.df.p;
-        sa.psi = r.psi.p;
-        sa.adc = r.adc.p;
-        sa.bnd = r.bnd.p;
-        for (int k = 0; k < 16; ++k) sa.h[k] = r.h[k].p;
-        sa.x = r.x.p;
-        sa.y = r.y.p;
-        sa.z = r.z.p;
-        sa.rho = r.rho.p;
-        sa.T1 = r.T1.p;
-        sa.T2 = r.T2.p;
-        sa.dw = r.dw.p;
-        sa.csm_rows = r.csm_rows.p;
-        sa.xy = r.xy.p;
-        sa.mz = r.mz.p;
-        sa.acc = r.acc.p;
-        sa.sig = r.sig.p;
-        // RF runs use the plain FP64 excitation kernel; precession runs are
-        // whole segments on the split kernel.
-        const int grid = (int)((r.ns + PLAIN_THREADS - 1) / PLAIN_THREADS);
-        const size_t row_bytes = sizeof(cplx<T>) * (size_t)r.nc * (size_t)grid;
-        const int64_t max_samples =
-            std::max<int64_t>(PLAIN_STAGE, (int64_t)((size_t(512) << 20) / row_bytes));
-        auto plan = plan_plain<T>(r, max_samples);
-        size_t i = 0;
-        PhantomDev<T> p = r.phantom();
-        SeqDev<T> q = r.seq();
-        StateDev<T> st{reinterpret_cast<cplx<T> *>(r.xy.p), reinterpret_cast<T *>(r.mz.p), reinterpret_cast<T *>(r.acc.p)};
-        while (i < plan.size()) {
-            const Launch &L = plan[i].first;
-            if (L.rf) {
-                HOMS_CUDA(r.partial.ensure(row_bytes * (size_t)std::max<int64_t>(L.nsamples, 1)));
-                SegmentArgs<T> a;
-                a.n_lo = L.n_lo;
-                a.n_hi = L.n_hi;
-                a.block_start = L.block_start;
-                a.tp0 = plan[i].second;
-                a.nsamples = L.nsamples;
-                a.method = method;
-                a.gamma = T(r.gamma);
-                a.gamma_d = r.gamma;
-                a.partial = reinterpret_cast<cplx<T> *>(r.partial.p);
-                HOMS_CUDA(launch_segment<T>(true, p, q, st, a, grid, ctx->stream));
-                r.launches += 1;
-                if (L.nsamples > 0) {
-                    HOMS_CUDA(launch_partial_finalize<T>(a.partial, grid, L.nsamples, r.nc,
-                                                         reinterpret_cast<cplx<T> *>(r.sig.p) + L.sample0, r.nadc, ctx->stream));
-                    r.launches += 1;
-                }
-                ++i;
-                continue;
+        SplitRunner<T> run;
+        run.init(ctx, r, method, capture);
+        const unsigned ev_flags = capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+        std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+        SplitJobDesc job;
+        while (run.next(ctx->stream, &job)) {
+            // CUDA events around each segment's fused launches (all its coil groups)
+            if (run.first_group()) {
+                ev = r.next_events();
+                cudaEventRecordWithFlags(ev.first, ctx->stream, ev_flags);
             }
-            // merge consecutive precession launches of one run
-            size_t j = i;
-            int64_t ns_total = 0;
-            while (j < plan.size() && !plan[j].first.rf && plan[j].first.run == L.run) {
-                ns_total += plan[j].first.nsamples;
-                ++j;
-            }
-            std::string err;
-            auto ev = r.next_events();
-            sa.ev_start = ev.first;
-            sa.ev_stop = ev.second;
-            sa.launches = &r.launches;
-            cudaError_t e = split_run_segment(r.split, sa, L.n_lo, plan[j - 1].first.n_hi, L.sample0, ns_total,
-                                              ctx->stream, &err);
-            if (ns_total == 0) {
-                // no fused launch happened: keep the pair unused
-                --r.events_used;
-            }
-            if (e != cudaSuccess) throw Failure{e == cudaErrorMemoryAllocation ? HOMS_ENOMEM : HOMS_ECUDA,
-                                                std::string("split segment: ") + cudaGetErrorString(e)};
-            if (!err.empty()) throw Failure{HOMS_EUNSUPPORTED, err};
-            i = j;
+            const cudaError_t e = split_launch(&job, 1, ctx->stream);
+            if (run.last_group()) cudaEventRecordWithFlags(ev.second, ctx->stream, ev_flags);
+            r.launches += 2;
+            if (e != cudaSuccess) throw Failure{HOMS_ECUDA, std::string("split segment: ") + cudaGetErrorString(e)};
+            run.after(ctx->stream);
         }
         if (check) check_split<T>(ctx, r);
     } else {
@@ -1692,3 +1766,152 @@ homs_status homs_kspace_timing(homs_context *ctx, double *ms) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Split-mode runs driven by the server's rounds (homs_server.cu)
+// ---------------------------------------------------------------------------
+
+namespace homs {
+
+struct ServerRun {
+    homs_context *ctx = nullptr;
+    std::unique_lock<std::mutex> lock;  // the context is the run's until server_run_free
+    Resident<double> *r = nullptr;
+    SplitRunner<double> runner;
+    homs_dtype out_dt = HOMS_F64;
+    cudaEvent_t ready = nullptr, done = nullptr;
+    bool waited = false, failed = false, done_recorded = false;
+};
+
+bool server_run_eligible(const homs_phantom *p, const homs_run_options *opts) {
+    (void)p;
+    return opts && opts->mode == HOMS_SPLIT;
+}
+
+homs_status server_run_prepare(homs_context *ctx, const homs_phantom *phantom, const homs_resident *resident,
+                               const homs_sequence *seq, const homs_run_options *opts, const homs_state *state,
+                               ServerRun **out) {
+    if (!ctx || !out || !opts) return HOMS_EINVAL;
+    *out = nullptr;
+    auto run = std::make_unique<ServerRun>();
+    run->ctx = ctx;
+    run->lock = std::unique_lock<std::mutex>(ctx->mu);
+    DeviceGuard g(ctx->device);
+    try {
+        validate_sequence(seq);
+        HOMS_REQUIRE(opts->mode == HOMS_SPLIT, "internal: server rounds run split mode");
+        HOMS_REQUIRE((opts->method & ~0x3Fu) == 0, "unknown method flag bits");
+        Resident<double> *r = nullptr;
+        if (resident) {
+            HOMS_REQUIRE(resident->res && resident->device == ctx->device,
+                         "the resident phantom lives on another device than the context");
+            HOMS_REQUIRE(resident->mode == HOMS_SPLIT,
+                         "the run mode must be the one the resident phantom was prepared for");
+            HOMS_REQUIRE(resident->res->dtype == HOMS_F64, "internal: split-mode residents are FP64");
+            const auto &src = static_cast<const Resident<double> &>(*resident->res);
+            r = cache_slot<double>(ctx);
+            attach_phantom<double>(r, src);
+            fill_sequence<double>(ctx, r, seq);
+            run->out_dt = resident->in_dtype;
+        } else {
+            validate_phantom(phantom);
+            r = cached_resident<double>(ctx, phantom, seq);
+            run->out_dt = phantom->dtype;
+        }
+        init_state<double>(ctx, *r, state, run->out_dt);
+        ensure_split<double>(ctx, *r);
+        ensure_split_tables<double>(ctx, *r, opts->method);
+        HOMS_CUDA(split_reset_error(r->split, ctx->stream));
+        r->events_used = 0;
+        r->launches = 0;
+        run->r = r;
+        run->runner.init(ctx, *r, opts->method, false);
+        HOMS_CUDA(cudaEventCreateWithFlags(&run->ready, cudaEventDisableTiming));
+        HOMS_CUDA(cudaEventCreateWithFlags(&run->done, cudaEventDisableTiming));
+        HOMS_CUDA(cudaEventRecord(run->ready, ctx->stream));
+    } catch (const Failure &f) {
+        cudaStreamSynchronize(ctx->stream);
+        ctx->cache[0].reset();
+        ctx->cache[1].reset();
+        const homs_status s = fail(ctx, f);
+        server_run_free(run.release());
+        return s;
+    } catch (const std::bad_alloc &) {
+        cudaStreamSynchronize(ctx->stream);
+        ctx->cache[0].reset();
+        ctx->cache[1].reset();
+        const homs_status s = fail(ctx, Failure{HOMS_ENOMEM, "host allocation failed"});
+        server_run_free(run.release());
+        return s;
+    }
+    *out = run.release();
+    return HOMS_OK;
+}
+
+homs_status server_run_next(ServerRun *run, cudaStream_t stream, SplitJobDesc *job, bool *has_job) {
+    *has_job = false;
+    DeviceGuard g(run->ctx->device);
+    try {
+        if (!run->waited) {
+            HOMS_CUDA(cudaStreamWaitEvent(stream, run->ready, 0));
+            run->waited = true;
+        }
+        *has_job = run->runner.next(stream, job);
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        run->failed = true;
+        return fail(run->ctx, f);
+    }
+}
+
+homs_status server_run_after(ServerRun *run, cudaStream_t stream) {
+    DeviceGuard g(run->ctx->device);
+    try {
+        run->runner.after(stream);
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        run->failed = true;
+        return fail(run->ctx, f);
+    }
+}
+
+void server_run_done(ServerRun *run, cudaStream_t stream) {
+    DeviceGuard g(run->ctx->device);
+    if (run->done && cudaEventRecord(run->done, stream) == cudaSuccess) run->done_recorded = true;
+}
+
+homs_status server_run_finish(ServerRun *run, void *sig, homs_memory sig_memory, homs_state *state) {
+    homs_context *ctx = run->ctx;
+    DeviceGuard g(ctx->device);
+    try {
+        HOMS_REQUIRE(run->done_recorded, "internal: the run's work was not issued");
+        HOMS_CUDA(cudaStreamWaitEvent(ctx->stream, run->done, 0));
+        HOMS_REQUIRE(sig_memory == HOMS_HOST || sig_memory == HOMS_DEVICE, "invalid signal memory kind");
+        check_split<double>(ctx, *run->r);
+        copy_out<double>(ctx, *run->r, sig, sig_memory, state, run->out_dt);
+        return HOMS_OK;
+    } catch (const Failure &f) {
+        run->failed = true;
+        return fail(ctx, f);
+    }
+}
+
+void server_run_free(ServerRun *run) {
+    if (!run) return;
+    homs_context *ctx = run->ctx;
+    {
+        DeviceGuard g(ctx->device);
+        // No work of the run may still use the context's buffers.
+        if (run->done_recorded) cudaEventSynchronize(run->done);
+        cudaStreamSynchronize(ctx->stream);
+        if (run->failed) {
+            ctx->cache[0].reset();
+            ctx->cache[1].reset();
+        }
+        if (run->ready) cudaEventDestroy(run->ready);
+        if (run->done) cudaEventDestroy(run->done);
+    }
+    delete run;  // releases the context
+}
+
+}  // namespace homs

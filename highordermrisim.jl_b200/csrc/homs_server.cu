@@ -3,14 +3,25 @@
 // The reference keeps one persistent worker per device and runs prepared
 // simulations one after another (src/simulation/PreparedSimulation.jl:144-258).
 // Here a server owns `slots` contexts -- each with its own CUDA stream and its
-// own cached device workspace -- and one worker thread per slot.  Requests
-// wait in submission order; the request at the head of the queue is admitted
-// as soon as a worker is free and its estimated device footprint fits in the
-// byte budget beside the requests already in flight.  Admitted requests run
-// homs_simulate on their worker's context, so requests that arrive while
-// others are on the GPU start as slots and memory free up, and their kernels
-// overlap on the device.  A request computes exactly what homs_simulate
-// computes for it: its result does not depend on what runs beside it.
+// own cached device workspace -- one worker thread per slot, and a dispatcher
+// thread with a stream of its own.  Requests wait in submission order; the
+// request at the head of the queue is admitted as soon as a worker is free and
+// its estimated device footprint fits in the byte budget beside the requests
+// already in flight.
+//
+// A split-mode request is prepared by its worker (phantom and sequence on the
+// device, initial state, split tables) and then joins the dispatcher's
+// rounds.  A round issues, for every request in it, the work up to its next
+// fused job (RF blocks, the next segment's prologue), then ONE persistent
+// launch of the split kernel over all those jobs per output width (the jobs'
+// (tile x chunk) work items in one device-side item space), then every
+// request's finalize.  Requests that arrive join at the next round, so small
+// requests share the GPU's SMs instead of each launching a partly empty grid.
+// When a request's last job is done its worker copies the results out.
+// Plain-mode requests run homs_simulate on their worker's context.  Either way
+// a request computes exactly what homs_simulate computes for it: each job's
+// work items, partial slots and finalize order are its own, so its result
+// does not depend on what runs beside it.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -94,6 +105,17 @@ struct homs_server {
     bool stopping = false;
     std::vector<homs_context *> contexts;
     std::vector<std::thread> workers;
+    // Split-mode runs handed to the dispatcher, and those in its rounds.
+    struct Active {
+        homs::ServerRun *run = nullptr;
+        bool finished = false;
+        homs_status status = HOMS_OK;
+    };
+    std::deque<Active *> pending;
+    std::condition_variable cv_dispatch, cv_run;
+    bool stop_dispatch = false;
+    std::thread dispatcher;
+    int64_t rounds = 0;  // rounds issued (diagnostics)
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
@@ -115,9 +137,12 @@ struct homs_server {
                 r->t_start = now();
             }
             homs_state *st = r->has_state ? &r->state : nullptr;
-            const homs_status s =
-                r->resident ? homs_simulate_resident(ctx, r->resident, &r->seq, &r->opts, st, r->sig, r->sig_memory)
-                            : homs_simulate(ctx, &r->phantom, &r->seq, &r->opts, st, r->sig, r->sig_memory);
+            homs_status s;
+            if (homs::server_run_eligible(r->resident ? nullptr : &r->phantom, &r->opts))
+                s = run_in_rounds(ctx, r, st);
+            else
+                s = r->resident ? homs_simulate_resident(ctx, r->resident, &r->seq, &r->opts, st, r->sig, r->sig_memory)
+                                : homs_simulate(ctx, &r->phantom, &r->seq, &r->opts, st, r->sig, r->sig_memory);
             {
                 std::lock_guard<std::mutex> lk(mu);
                 r->status = s;
@@ -129,6 +154,99 @@ struct homs_server {
             cv_done.notify_all();
             cv_work.notify_all();
         }
+    }
+
+    // A split-mode request: prepared here, its fused work done by the
+    // dispatcher's rounds, its results copied out here.
+    homs_status run_in_rounds(homs_context *ctx, Request *r, homs_state *st) {
+        homs::ServerRun *run = nullptr;
+        homs_status s = homs::server_run_prepare(ctx, r->resident ? nullptr : &r->phantom, r->resident, &r->seq,
+                                                 &r->opts, st, &run);
+        if (s != HOMS_OK) return s;
+        Active a;
+        a.run = run;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            pending.push_back(&a);
+            cv_dispatch.notify_all();
+            cv_run.wait(lk, [&] { return a.finished; });
+        }
+        s = a.status;
+        if (s == HOMS_OK) s = homs::server_run_finish(run, r->sig, r->sig_memory, st);
+        homs::server_run_free(run);
+        return s;
+    }
+
+    void dispatch() {
+        cudaSetDevice(device);
+        cudaStream_t ds = nullptr;
+        cudaStreamCreateWithFlags(&ds, cudaStreamNonBlocking);
+        // At most two rounds ahead of the device.
+        cudaEvent_t round_ev[2] = {nullptr, nullptr};
+        cudaEventCreateWithFlags(&round_ev[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&round_ev[1], cudaEventDisableTiming);
+        std::vector<Active *> act;
+        int64_t k = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_dispatch.wait(lk, [&] { return !pending.empty() || !act.empty() || stop_dispatch; });
+                if (act.empty() && pending.empty()) break;  // stopping
+                for (Active *a : pending) act.push_back(a);
+                pending.clear();
+            }
+            cudaEventSynchronize(round_ev[k & 1]);
+            // The round: every run's work up to its next job, the jobs (by
+            // output width, at most SPLIT_MAX_JOBS per launch), the finalizes.
+            std::vector<std::pair<Active *, homs::SplitJobDesc>> jobs;
+            std::vector<Active *> fin;
+            for (Active *a : act) {
+                homs::SplitJobDesc d;
+                bool has = false;
+                const homs_status s = homs::server_run_next(a->run, ds, &d, &has);
+                if (s != HOMS_OK) {
+                    a->status = s;
+                    fin.push_back(a);
+                } else if (has) {
+                    jobs.emplace_back(a, d);
+                } else {
+                    fin.push_back(a);
+                }
+            }
+            std::stable_sort(jobs.begin(), jobs.end(),
+                             [](const auto &x, const auto &y) { return x.second.n_mma < y.second.n_mma; });
+            for (size_t b = 0; b < jobs.size();) {
+                size_t e = b;
+                std::vector<homs::SplitJobDesc> batch;
+                while (e < jobs.size() && jobs[e].second.n_mma == jobs[b].second.n_mma &&
+                       batch.size() < (size_t)homs::SPLIT_MAX_JOBS)
+                    batch.push_back(jobs[e++].second);
+                if (homs::split_launch(batch.data(), (int)batch.size(), ds) != cudaSuccess)
+                    for (size_t q = b; q < e; ++q) jobs[q].first->status = HOMS_ECUDA;
+                b = e;
+            }
+            for (auto &ja : jobs) {
+                Active *a = ja.first;
+                if (a->status == HOMS_OK) a->status = homs::server_run_after(a->run, ds);
+                if (a->status != HOMS_OK) fin.push_back(a);
+            }
+            for (Active *a : fin) homs::server_run_done(a->run, ds);
+            cudaEventRecord(round_ev[k & 1], ds);
+            ++k;
+            if (!fin.empty()) {
+                std::lock_guard<std::mutex> lk(mu);
+                for (Active *a : fin) {
+                    a->finished = true;
+                    act.erase(std::find(act.begin(), act.end(), a));
+                }
+                rounds = k;
+                cv_run.notify_all();
+            }
+        }
+        cudaStreamSynchronize(ds);
+        cudaEventDestroy(round_ev[0]);
+        cudaEventDestroy(round_ev[1]);
+        cudaStreamDestroy(ds);
     }
 };
 
@@ -195,6 +313,7 @@ homs_status homs_server_create(const homs_server_options *opts, homs_server **ou
         srv->contexts.push_back(ctx);
     }
     homs_server *raw = srv.get();
+    srv->dispatcher = std::thread([raw] { raw->dispatch(); });
     for (homs_context *ctx : srv->contexts) srv->workers.emplace_back([raw, ctx] { raw->work(ctx); });
     *out = srv.release();
     return HOMS_OK;
@@ -304,6 +423,12 @@ homs_status homs_server_destroy(homs_server *srv) {
     }
     srv->cv_work.notify_all();
     for (std::thread &t : srv->workers) t.join();
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stop_dispatch = true;
+    }
+    srv->cv_dispatch.notify_all();
+    srv->dispatcher.join();
     for (homs_context *c : srv->contexts) homs_context_destroy(c);
     delete srv;
     return HOMS_OK;

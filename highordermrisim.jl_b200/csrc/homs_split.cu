@@ -305,52 +305,71 @@ __host__ __device__ constexpr uint32_t idesc_i8(int n, bool a_signed, bool b_sig
            ((uint32_t)(TM >> 4) << 24);
 }
 
-// Work items of one launch.  The (tile x chunk) grid is cut into `slabs`
-// ranges of chunks; item i is slab z = i / tiles of tile i % tiles, and CTA b
-// takes items b, b + G, b + 2G, ...  The CTAs running at any one time thus
-// read the chunks of two or three consecutive slabs, which stay in L2 for
-// every tile that needs them.  Item (tile, z) owns partial slot z.
-struct KernelArgs {
+// Work items.  A launch runs one or more jobs (a job: one precession
+// segment and coil group of one simulation; several simulations' jobs share
+// a launch in the server's rounds).  A job's (tile x chunk) grid is cut into
+// `slabs` ranges of chunks; its item k is slab z = k / tiles of tile
+// k % tiles, and the launch's items are the jobs' items one job after the
+// other.  CTA b takes items b, b + G, b + 2G, ...  The CTAs running at any
+// one time thus read the chunks of two or three consecutive slabs, which stay
+// in L2 for every tile that needs them.  Item (tile, z) owns partial slot z of
+// its job.
+constexpr int MAX_JOBS = SPLIT_MAX_JOBS;
+struct KernelJob {
     const uint8_t *phase_a;    // [tiles][PHASE_A_BYTES]
     const uint8_t *phase_b;    // [nchunks][PHASE_B_BYTES]
     const uint8_t *coil_b;     // [nchunks][coil_b_bytes(N)] of this coil group
     const uint8_t *params;     // [nchunks][PARAM_BYTES]
     const uint32_t *rows;      // [tiles * TM][2]: base turn, elapsed time (float bits)
-    const unsigned long long *amp_max;  // bits of max |m0| over the segment's spins
     double *partial;           // [tiles][slabs][TM][N]
-    unsigned int *err;
-    int n_chunks;
-    int tiles;
-    int slabs;
-    int nstage;
+    unsigned int *err;         // the job's device error word
+    int n_chunks, tiles, slabs;
+    int item0;                 // launch index of the job's first item
+};
+struct KernelArgs {
+    KernelJob job[MAX_JOBS];
+    int n_jobs, n_items, nstage;
     uint32_t mul8, mul16, mul24, mul25;  // 2^8, 2^16, 2^24, 2^25 (multipliers of mad_lo / mad_hi)
 };
 
+// The launch's job table (in shared memory) and item count.
+struct Work {
+    const KernelJob *jobs;
+    int n_jobs, n_items;
+};
 struct Cursor {
-    int i, c, c0, c1, tile, z, local;
+    int i, c, c0, c1, tile, z, local, job;
     bool valid;
 };
-__device__ __forceinline__ void cursor_item(const KernelArgs &a, Cursor &cu) {
-    cu.valid = cu.i < a.tiles * a.slabs;
+__device__ __forceinline__ void cursor_item(const Work &w, Cursor &cu) {
+    cu.valid = cu.i < w.n_items;
     if (!cu.valid) return;
-    cu.z = cu.i / a.tiles;
-    cu.tile = cu.i - cu.z * a.tiles;
-    cu.c0 = (int)((int64_t)a.n_chunks * cu.z / a.slabs);
-    cu.c1 = (int)((int64_t)a.n_chunks * (cu.z + 1) / a.slabs);
+    while (cu.i >= w.jobs[cu.job].item0 + w.jobs[cu.job].tiles * w.jobs[cu.job].slabs) ++cu.job;
+    const KernelJob &J = w.jobs[cu.job];
+    const int k = cu.i - J.item0;
+    cu.z = k / J.tiles;
+    cu.tile = k - cu.z * J.tiles;
+    cu.c0 = (int)((int64_t)J.n_chunks * cu.z / J.slabs);
+    cu.c1 = (int)((int64_t)J.n_chunks * (cu.z + 1) / J.slabs);
     cu.c = cu.c0;
 }
-__device__ __forceinline__ Cursor cursor_start(const KernelArgs &a) {
+__device__ __forceinline__ Cursor cursor_start(const Work &w) {
     Cursor cu;
     cu.i = blockIdx.x;
     cu.local = 0;
-    cursor_item(a, cu);
+    cu.job = 0;
+    cursor_item(w, cu);
     return cu;
 }
-__device__ __forceinline__ void cursor_next(const KernelArgs &a, Cursor &cu) {
+__device__ __forceinline__ void cursor_next(const Work &w, Cursor &cu) {
     if (++cu.c < cu.c1) return;
     cu.i += gridDim.x;
     ++cu.local;
-    cursor_item(a, cu);
+    cursor_item(w, cu);
+}
+// A failed wait is reported in the error word of every job of the launch.
+__device__ __forceinline__ void report(const Work &w, unsigned int code) {
+    for (int j = 0; j < w.n_jobs; ++j) atomicOr(w.jobs[j].err, code);
 }
 
 constexpr float TWO_PI_2M25 = 1.8725351414619534e-07f;  // 2 pi / 2^25: one unit of the 23-bit quarter-turn angle
@@ -377,7 +396,7 @@ __device__ __forceinline__ int amp_exp(unsigned long long bits) {
 }
 
 template <int N>
-__global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs args) {
+__global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(const __grid_constant__ KernelArgs args) {
     constexpr int CB = coil_b_bytes(N);
     constexpr int STAGE_BYTES = CB + PHASE_B_BYTES + PARAM_BYTES;
     constexpr int NQ = N / 4;  // coil columns drained per magnetisation warp
@@ -400,8 +419,16 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
     uint64_t *d_empty = d_full + 1;          // drain (coil classes cleared) -> coil issuer
     uint64_t *done = d_empty + 1;            // [2] every MMA of the coil / phase issuer complete
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 2);
+    KernelJob *sjobs = reinterpret_cast<KernelJob *>(done + 4);  // the launch's job table
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    {
+        constexpr int WORDS = (int)(sizeof(KernelJob) / sizeof(unsigned long long));
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(args.job);
+        for (int k = threadIdx.x; k < args.n_jobs * WORDS; k += blockDim.x)
+            reinterpret_cast<unsigned long long *>(sjobs)[k] = src[k];
+    }
+    const Work W{sjobs, args.n_jobs, args.n_items};
     if (threadIdx.x == 0) {
         for (int i = 0; i < NSTAGE; ++i) {
             mbar_init(&full[i], 1);
@@ -437,29 +464,29 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             uint32_t sph = 0;  // parity of the stage ring's current pass
             int issued[MAX_STAGE] = {0, 0, 0, 0, 0, 0};
             int issued_a[2] = {0, 0};
-            for (Cursor cu = cursor_start(args); cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
+            for (Cursor cu = cursor_start(W); cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(W, cu)) {
                 const int ib = cu.local & 1;
                 if (!mbar_wait_helper(&a_empty_ph[ib], (uint32_t)(((cu.local >> 1) + 1) & 1))) {
-                    atomicOr(args.err, 1u);
+                    report(W, 1u);
                     dead = true;
                     break;
                 }
                 mbar_expect_tx(&a_full_ph[ib], (uint32_t)PHASE_A_BYTES);
-                bulk_g2s(sA + ib * PHASE_A_BYTES, args.phase_a + (size_t)cu.tile * PHASE_A_BYTES, PHASE_A_BYTES,
+                const KernelJob &J = sjobs[cu.job];
+                bulk_g2s(sA + ib * PHASE_A_BYTES, J.phase_a + (size_t)cu.tile * PHASE_A_BYTES, PHASE_A_BYTES,
                          &a_full_ph[ib]);
                 ++issued_a[ib];
                 for (int c = cu.c0; c < cu.c1; ++c) {
                     if (!mbar_wait_helper(&empty[stage], sph ^ 1u)) {
-                        atomicOr(args.err, 1u);
+                        report(W, 1u);
                         dead = true;
                         break;
                     }
                     uint8_t *st = sStage + (size_t)stage * STAGE_BYTES;
                     mbar_expect_tx(&full[stage], (uint32_t)STAGE_BYTES);
-                    bulk_g2s(st, args.coil_b + (size_t)c * CB, CB, &full[stage]);
-                    bulk_g2s(st + CB, args.phase_b + (size_t)c * PHASE_B_BYTES, PHASE_B_BYTES, &full[stage]);
-                    bulk_g2s(st + CB + PHASE_B_BYTES, args.params + (size_t)c * PARAM_BYTES, PARAM_BYTES,
-                             &full[stage]);
+                    bulk_g2s(st, J.coil_b + (size_t)c * CB, CB, &full[stage]);
+                    bulk_g2s(st + CB, J.phase_b + (size_t)c * PHASE_B_BYTES, PHASE_B_BYTES, &full[stage]);
+                    bulk_g2s(st + CB + PHASE_B_BYTES, J.params + (size_t)c * PARAM_BYTES, PARAM_BYTES, &full[stage]);
                     ++issued[stage];
                     if (++stage == NSTAGE) {
                         stage = 0;
@@ -486,12 +513,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             constexpr uint32_t id_ph3 = idesc_i8(PH_N3, true, true);
             int stage = 0, gp = 0;
             uint32_t sph = 0;
-            for (Cursor cp = cursor_start(args); cp.valid; ++gp) {
+            for (Cursor cp = cursor_start(W); cp.valid; ++gp) {
                 const int ib = cp.local & 1;
                 if (!mbar_wait_helper(&full[stage], sph) ||
                     (cp.c == cp.c0 && !mbar_wait_helper(&a_full_ph[ib], (uint32_t)((cp.local >> 1) & 1))) ||
                     !mbar_wait_helper(p_empty, (uint32_t)((gp + 1) & 1))) {
-                    atomicOr(args.err, 2u);
+                    report(W, 2u);
                     break;
                 }
                 tc_fence_after();
@@ -506,11 +533,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     stage = 0;
                     sph ^= 1u;
                 }
-                cursor_next(args, cp);
+                cursor_next(W, cp);
             }
             // Every issued MMA completes before TMEM is released.
             tc_commit(&done[1]);
-            if (!mbar_wait(&done[1], 0)) atomicOr(args.err, 8u);
+            if (!mbar_wait(&done[1], 0)) report(W, 8u);
         }
         __syncwarp();
     } else if (warp == MMA_WARP) {
@@ -521,10 +548,10 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             constexpr uint32_t id_c1 = idesc_i8(N, true, true);  // signed low digit of M
             int stage = 0, gc = 0;
             uint32_t sph = 0;
-            for (Cursor cc = cursor_start(args); cc.valid; ++gc) {
+            for (Cursor cc = cursor_start(W); cc.valid; ++gc) {
                 if (!mbar_wait_helper(&full[stage], sph) || !mbar_wait_helper(a_full, (uint32_t)(gc & 1)) ||
                     (cc.c == cc.c0 && !mbar_wait_helper(d_empty, (uint32_t)(cc.local & 1)))) {
-                    atomicOr(args.err, 4u);
+                    report(W, 4u);
                     break;
                 }
                 tc_fence_after();
@@ -544,11 +571,11 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                     stage = 0;
                     sph ^= 1u;
                 }
-                cursor_next(args, cc);
+                cursor_next(W, cc);
             }
             // Every issued MMA completes before TMEM is released.
             tc_commit(&done[0]);
-            if (!mbar_wait(&done[0], 0)) atomicOr(args.err, 8u);
+            if (!mbar_wait(&done[0], 0)) report(W, 8u);
         }
         __syncwarp();
     } else {
@@ -575,7 +602,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             if (lane == 0) mbar_arrive(d_empty);
         }
         const uint32_t m8 = args.mul8, m16 = args.mul16, m24 = args.mul24, m25 = args.mul25;
-        const int n_items = args.tiles * args.slabs;
+        const int n_items = W.n_items;
         int g = 0, stage = 0, prev_stage = 0;
         uint32_t sph = 0, prev_sph = 0;
         // Phase classes w = 7..3 (columns (7 - w) * 32) of this warp's 8 spins,
@@ -597,17 +624,18 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             if (lane == 0) mbar_arrive(p_empty);
             return true;
         };
-        Cursor cu = cursor_start(args);
+        Cursor cu = cursor_start(W);
         if (cu.valid && !load_phase(0)) {
-            if (lane == 0) atomicOr(args.err, 16u);
+            if (lane == 0) report(W, 16u);
             dead = true;
         }
-        for (; cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(args, cu)) {
-            const uint32_t base = args.rows[2 * ((size_t)cu.tile * TM + row)];
-            const float tj = __uint_as_float(args.rows[2 * ((size_t)cu.tile * TM + row) + 1]);
+        for (; cu.valid && !dead; cu.i += gridDim.x, ++cu.local, cursor_item(W, cu)) {
+            const KernelJob &J = sjobs[cu.job];
+            const uint32_t base = J.rows[2 * ((size_t)cu.tile * TM + row)];
+            const float tj = __uint_as_float(J.rows[2 * ((size_t)cu.tile * TM + row) + 1]);
             for (int c = cu.c0; c < cu.c1; ++c, ++g) {
                 if (!wait_all(&full[stage], sph)) {
-                    if (lane == 0) atomicOr(args.err, 32u);
+                    if (lane == 0) report(W, 32u);
                     dead = true;
                     break;
                 }
@@ -683,7 +711,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 // MMAs, which read the buffer, are complete), then take the next
                 // chunk's phase classes.
                 if (g > 0 && !wait_all(&empty[prev_stage], prev_sph)) {
-                    if (lane == 0) atomicOr(args.err, 128u);
+                    if (lane == 0) report(W, 128u);
                     dead = true;
                     break;
                 }
@@ -701,7 +729,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
                 if (lane == 0) mbar_arrive(a_full);
                 const bool more = c + 1 < cu.c1 || cu.i + (int)gridDim.x < n_items;
                 if (more && !load_phase(g + 1)) {
-                    if (lane == 0) atomicOr(args.err, 16u);
+                    if (lane == 0) report(W, 16u);
                     dead = true;
                     break;
                 }
@@ -710,12 +738,12 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(KernelArgs
             // Item end: the coil classes of this warp's rows and columns into the
             // item's FP64 partial, then clear them for the next item.
             if (!wait_all(d_full, (uint32_t)(cu.local & 1))) {
-                if (lane == 0) atomicOr(args.err, 512u);
+                if (lane == 0) report(W, 512u);
                 dead = true;
                 break;
             }
             tc_fence_after();
-            double *dst = args.partial + (((size_t)cu.tile * args.slabs + cu.z) * TM + row) * (size_t)N + cq * NQ;
+            double *dst = J.partial + (((size_t)cu.tile * J.slabs + cu.z) * TM + row) * (size_t)N + cq * NQ;
             const uint32_t z[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
             for (int cb = 0; cb < NQ; cb += 4) {
@@ -1372,9 +1400,9 @@ cudaError_t split_prepare(SplitResident &r, int64_t ns, int32_t nc, const void *
     return cudaGetLastError();
 }
 
-// Shared memory: 1 KB alignment slack, two phase A tiles, NSTAGE stages, the barriers.
+// Shared memory: 1 KB alignment slack, two phase A tiles, NSTAGE stages, the barriers and the job table.
 constexpr size_t SMEM_LIMIT = 227 * 1024;
-constexpr size_t SMEM_FIXED = 1024 + 2 * PHASE_A_BYTES + 256;
+constexpr size_t SMEM_FIXED = 1024 + 2 * PHASE_A_BYTES + 256 + MAX_JOBS * sizeof(KernelJob);
 
 static size_t stage_bytes(int n_cols) { return (size_t)coil_b_bytes(n_cols) + PHASE_B_BYTES + PARAM_BYTES; }
 
@@ -1422,9 +1450,54 @@ static cudaError_t launch_precession(int n_cols, const KernelArgs &ka, unsigned 
     }
 }
 
-// One precession segment.
-static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi,
-                                 int64_t sample0, int64_t nsamples, cudaStream_t stream, std::string *err) {
+static int sm_count() {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return nsm;
+}
+
+cudaError_t split_launch(const SplitJobDesc *jobs, int n_jobs, cudaStream_t stream) {
+    if (n_jobs <= 0) return cudaSuccess;
+    if (n_jobs > MAX_JOBS) return cudaErrorInvalidValue;
+    const int n_mma = jobs[0].n_mma;
+    KernelArgs ka;
+    std::memset(&ka, 0, sizeof(ka));
+    int64_t items = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        const SplitJobDesc &d = jobs[j];
+        if (d.n_mma != n_mma) return cudaErrorInvalidValue;
+        KernelJob &k = ka.job[j];
+        k.phase_a = (const uint8_t *)d.phase_a;
+        k.phase_b = (const uint8_t *)d.phase_b;
+        k.coil_b = (const uint8_t *)d.coil_b;
+        k.params = (const uint8_t *)d.params;
+        k.rows = (const uint32_t *)d.rows;
+        k.partial = (double *)d.partial;
+        k.err = d.err;
+        k.n_chunks = d.n_chunks;
+        k.tiles = d.tiles;
+        k.slabs = d.slabs;
+        k.item0 = (int)items;
+        items += (int64_t)d.tiles * d.slabs;
+    }
+    if (items > INT32_MAX / 2) return cudaErrorInvalidValue;
+    if (items == 0) return cudaSuccess;
+    ka.n_jobs = n_jobs;
+    ka.n_items = (int)items;
+    ka.nstage = kernel_stages(n_mma);
+    ka.mul8 = 1u << 8;
+    ka.mul16 = 1u << 16;
+    ka.mul24 = 1u << 24;
+    ka.mul25 = 1u << 25;
+    const int64_t G = std::min<int64_t>(sm_count(), items);
+    return launch_precession(n_mma, ka, (unsigned)G, kernel_smem(n_mma), stream);
+}
+
+// Prologue of one precession segment: the prefix table, the spin parameters
+// and amplitude scale, the phase A tiles and the work-item split.
+cudaError_t split_segment_begin(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
+                                int64_t nsamples, cudaStream_t stream, std::string *err, SplitSegment *seg) {
     cudaError_t e;
     const int64_t nchunks = r.ns_pad / KC;
     const int64_t tiles = (nsamples + TM - 1) / TM;
@@ -1432,6 +1505,10 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
         *err = "internal: split segment without its ADC rank and column tables";
         return cudaSuccess;
     }
+    seg->nsamples = nsamples;
+    seg->tiles = tiles;
+    seg->nchunks = nchunks;
+    seg->slabs = 0;
     const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2);
     if ((e = grow(r.prefix, r.prefix_bytes, prefix_rows * PREFIX_STRIDE * sizeof(double))) != cudaSuccess) return e;
     if ((e = grow(r.params, r.params_bytes, (size_t)nchunks * PARAM_BYTES)) != cudaSuccess) return e;
@@ -1447,68 +1524,59 @@ static cudaError_t split_segment(SplitResident &r, const SplitRunArgs &a, int64_
                                                             (const unsigned long long *)r.amp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (a.launches) *a.launches += 3;
-    if (nsamples > 0) {
-        if ((e = grow(r.phase_a, r.phase_a_bytes, (size_t)tiles * PHASE_A_BYTES)) != cudaSuccess) return e;
-        if ((e = grow(r.rows, r.rows_bytes, (size_t)tiles * TM * 2 * sizeof(uint32_t))) != cudaSuccess) return e;
-        phase_a_kernel<<<grid_for(tiles * TM), 256, 0, stream>>>(
-            (const double *)r.prefix, nsamples, tiles * TM, (const unsigned long long *)r.term_max,
-            (unsigned int *)r.err, (uint8_t *)r.phase_a, (uint32_t *)r.rows);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (a.launches) *a.launches += 1;
-        int dev = 0, nsm = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-        const int slabs = choose_slabs(tiles, nchunks, nsm);
-        const int64_t n_items = tiles * slabs;
-        if (tiles > INT32_MAX / slabs || nchunks > INT32_MAX || slabs > nchunks) {
-            *err = "split mode: segment too large for one launch";
-            return cudaSuccess;
-        }
-        const int64_t G = std::min<int64_t>(nsm, n_items);
-        const size_t pbytes = sizeof(double) * (size_t)tiles * slabs * TM * r.n_mma;
-        if ((e = grow(r.partial, r.partial_bytes, pbytes)) != cudaSuccess) return e;
-        const size_t smem = kernel_smem(r.n_mma);
-        const int *cexp = reinterpret_cast<const int *>(reinterpret_cast<const unsigned long long *>(r.coil_exp) + r.nc);
-        KernelArgs ka;
-        ka.phase_a = (const uint8_t *)r.phase_a;
-        ka.phase_b = (const uint8_t *)r.phase_b;
-        ka.params = (const uint8_t *)r.params;
-        ka.rows = (const uint32_t *)r.rows;
-        ka.amp_max = (const unsigned long long *)r.amp;
-        ka.partial = (double *)r.partial;
-        ka.err = (unsigned int *)r.err;
-        ka.n_chunks = (int)nchunks;
-        ka.tiles = (int)tiles;
-        ka.slabs = slabs;
-        ka.nstage = kernel_stages(r.n_mma);
-        ka.mul8 = 1u << 8;
-        ka.mul16 = 1u << 16;
-        ka.mul24 = 1u << 24;
-        ka.mul25 = 1u << 25;
-        const unsigned ev_flags = a.capture ? cudaEventRecordExternal : cudaEventRecordDefault;
-        if (a.ev_start) cudaEventRecordWithFlags(a.ev_start, stream, ev_flags);
-        // One pass per group of GROUP_COILS coils.
-        for (int grp = 0; grp < r.ngroups; ++grp) {
-            const int coil0 = grp * GROUP_COILS;
-            const int ncg = std::min<int>(GROUP_COILS, r.nc - coil0);
-            ka.coil_b = (const uint8_t *)r.coil_b + (size_t)grp * nchunks * coil_b_bytes(r.n_mma);
-            e = launch_precession(r.n_mma, ka, (unsigned)G, smem, stream);
-            if (a.ev_stop && grp + 1 == r.ngroups) cudaEventRecordWithFlags(a.ev_stop, stream, ev_flags);
-            if (a.launches) *a.launches += 2;
-            if (e != cudaSuccess) return e;
-            const int fin_blocks = (int)std::min<int64_t>(tiles * (TM / 32), 148 * 8);
-            if (a.sizeof_T == 8)
-                split_finalize_kernel<double><<<fin_blocks, 256, 0, stream>>>(
-                    (const double *)r.partial, nsamples, ncg, r.n_mma, slabs,
-                    (const long long *)r.colsum + (size_t)grp * r.n_mma, cexp + coil0,
-                    (const unsigned long long *)r.amp, (cplx<double> *)a.sig + sample0 + (int64_t)coil0 * a.nadc,
-                    a.nadc);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        }
+    if (nsamples == 0) return cudaSuccess;
+    if ((e = grow(r.phase_a, r.phase_a_bytes, (size_t)tiles * PHASE_A_BYTES)) != cudaSuccess) return e;
+    if ((e = grow(r.rows, r.rows_bytes, (size_t)tiles * TM * 2 * sizeof(uint32_t))) != cudaSuccess) return e;
+    phase_a_kernel<<<grid_for(tiles * TM), 256, 0, stream>>>((const double *)r.prefix, nsamples, tiles * TM,
+                                                             (const unsigned long long *)r.term_max,
+                                                             (unsigned int *)r.err, (uint8_t *)r.phase_a,
+                                                             (uint32_t *)r.rows);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (a.launches) *a.launches += 1;
+    const int slabs = choose_slabs(tiles, nchunks, sm_count());
+    if (tiles > INT32_MAX / slabs || nchunks > INT32_MAX || slabs > nchunks) {
+        *err = "split mode: segment too large for one launch";
+        return cudaSuccess;
     }
+    seg->slabs = slabs;
+    const size_t pbytes = sizeof(double) * (size_t)tiles * slabs * TM * r.n_mma;
+    return grow(r.partial, r.partial_bytes, pbytes);
+}
+
+SplitJobDesc split_segment_job(const SplitResident &r, const SplitSegment &seg, int grp) {
+    SplitJobDesc d;
+    d.phase_a = r.phase_a;
+    d.phase_b = r.phase_b;
+    d.coil_b = (const uint8_t *)r.coil_b + (size_t)grp * seg.nchunks * coil_b_bytes(r.n_mma);
+    d.params = r.params;
+    d.rows = r.rows;
+    d.partial = r.partial;
+    d.err = (unsigned int *)r.err;
+    d.n_chunks = (int32_t)seg.nchunks;
+    d.tiles = (int32_t)seg.tiles;
+    d.slabs = seg.slabs;
+    d.n_mma = r.n_mma;
+    return d;
+}
+
+cudaError_t split_segment_finalize(SplitResident &r, const SplitRunArgs &a, const SplitSegment &seg, int grp,
+                                   int64_t sample0, cudaStream_t stream) {
+    const int coil0 = grp * GROUP_COILS;
+    const int ncg = std::min<int>(GROUP_COILS, r.nc - coil0);
+    const int *cexp = reinterpret_cast<const int *>(reinterpret_cast<const unsigned long long *>(r.coil_exp) + r.nc);
+    const int fin_blocks = (int)std::min<int64_t>(seg.tiles * (TM / 32), 148 * 8);
+    if (a.sizeof_T == 8)
+        split_finalize_kernel<double><<<fin_blocks, 256, 0, stream>>>(
+            (const double *)r.partial, seg.nsamples, ncg, r.n_mma, seg.slabs,
+            (const long long *)r.colsum + (size_t)grp * r.n_mma, cexp + coil0, (const unsigned long long *)r.amp,
+            (cplx<double> *)a.sig + sample0 + (int64_t)coil0 * a.nadc, a.nadc);
+    return cudaGetLastError();
+}
+
+cudaError_t split_segment_end(SplitResident &r, const SplitRunArgs &a, const SplitSegment &seg, cudaStream_t stream) {
     if (a.launches) *a.launches += 1;
     state_update_kernel<<<grid_for(r.ns), 256, 0, stream>>>(
-        (const double *)r.basis, (const double *)a.dw, (const double *)r.prefix + (size_t)nsamples * PREFIX_STRIDE,
+        (const double *)r.basis, (const double *)a.dw, (const double *)r.prefix + (size_t)seg.nsamples * PREFIX_STRIDE,
         (const double *)a.T1, (const double *)a.T2, (const double *)a.rho, r.ns, (cplx<double> *)a.xy,
         (double *)a.mz);
     return cudaGetLastError();
@@ -1559,9 +1627,26 @@ cudaError_t split_reset_error(SplitResident &r, cudaStream_t stream) {
     return cudaMemsetAsync(r.err, 0, sizeof(unsigned int), stream);
 }
 
+// One precession segment on its own: the prologue, per coil group one launch
+// and its finalize, the state update.
 cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
                               int64_t nsamples, cudaStream_t stream, std::string *err) {
-    return split_segment(r, a, n_lo, n_hi, sample0, nsamples, stream, err);
+    SplitSegment seg;
+    cudaError_t e = split_segment_begin(r, a, n_lo, n_hi, sample0, nsamples, stream, err, &seg);
+    if (e != cudaSuccess || !err->empty()) return e;
+    if (nsamples > 0) {
+        const unsigned ev_flags = a.capture ? cudaEventRecordExternal : cudaEventRecordDefault;
+        if (a.ev_start) cudaEventRecordWithFlags(a.ev_start, stream, ev_flags);
+        for (int grp = 0; grp < r.ngroups; ++grp) {
+            const SplitJobDesc d = split_segment_job(r, seg, grp);
+            e = split_launch(&d, 1, stream);
+            if (a.ev_stop && grp + 1 == r.ngroups) cudaEventRecordWithFlags(a.ev_stop, stream, ev_flags);
+            if (a.launches) *a.launches += 2;
+            if (e != cudaSuccess) return e;
+            if ((e = split_segment_finalize(r, a, seg, grp, sample0, stream)) != cudaSuccess) return e;
+        }
+    }
+    return split_segment_end(r, a, seg, stream);
 }
 
 cudaError_t split_check(SplitResident &r, cudaStream_t stream, std::string *err) {

@@ -114,6 +114,31 @@ void split_column_sources(uint32_t method, const void *const h[16], const void *
 cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
                               int64_t nsamples, cudaStream_t stream, std::string *err);
 
+// One precession segment in pieces, for runs that share launches: the
+// prologue (split_segment_begin), per coil group grp one job
+// (split_segment_job) run by split_launch (alone, or with other runs' jobs of
+// the same n_mma in one persistent launch) and its finalize, then the state
+// update (split_segment_end).  split_run_segment is exactly this sequence for
+// one run.
+struct SplitSegment {
+    int64_t nsamples = 0, tiles = 0, nchunks = 0;
+    int32_t slabs = 0;
+};
+struct SplitJobDesc {
+    const void *phase_a, *phase_b, *coil_b, *params, *rows;
+    void *partial;
+    unsigned int *err;
+    int32_t n_chunks, tiles, slabs, n_mma;
+};
+constexpr int SPLIT_MAX_JOBS = 32;  // jobs per launch
+cudaError_t split_segment_begin(SplitResident &r, const SplitRunArgs &a, int64_t n_lo, int64_t n_hi, int64_t sample0,
+                                int64_t nsamples, cudaStream_t stream, std::string *err, SplitSegment *seg);
+SplitJobDesc split_segment_job(const SplitResident &r, const SplitSegment &seg, int grp);
+cudaError_t split_launch(const SplitJobDesc *jobs, int n_jobs, cudaStream_t stream);
+cudaError_t split_segment_finalize(SplitResident &r, const SplitRunArgs &a, const SplitSegment &seg, int grp,
+                                   int64_t sample0, cudaStream_t stream);
+cudaError_t split_segment_end(SplitResident &r, const SplitRunArgs &a, const SplitSegment &seg, cudaStream_t stream);
+
 // Launch the bounded-wait self-test: a wait that nothing completes runs out
 // after `budget_cycles` and sets code 256 in *err (device word, cleared first).
 cudaError_t wait_selftest(unsigned int *err, long long budget_cycles, cudaStream_t stream);
