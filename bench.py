@@ -300,7 +300,7 @@ def config_legs(ctx):
     return out
 
 
-def serving_benchmark(n_pool=16, passes=10, load=0.9, slots=4, resident=False):
+def serving_benchmark(n_pool=16, passes=10, load=0.95, slots=4, resident=False, spin_sample_rate=None):
     """Serving stream of mixed simulations through homs.Server.
 
     Batch mode submits every request at once (the server's capacity);
@@ -309,12 +309,17 @@ def serving_benchmark(n_pool=16, passes=10, load=0.9, slots=4, resident=False):
     sustained throughput is total units over first submit to last finish.
     With ``resident`` every distinct phantom is put on the device once, before
     the timed streams (homs.ResidentPhantom), and requests carry only their
-    sequences; otherwise every request uploads its phantom."""
+    sequences; otherwise every request uploads its phantom.
+
+    ``spin_sample_rate`` (the headline kernel's spin*sample/s) gives the mix's
+    kernel bound: units count coils, so a mix of 1- to 32-coil requests
+    reaches at most that rate times its spin*sample-weighted coil count."""
     import homs
     from homs import workloads as W
     pool = W.serving_pool(n_pool)
     reqs = [pool[i % n_pool] for i in range(n_pool * passes)]
     units = float(sum(r.units for r in reqs))
+    spin_samples = float(sum(len(r.obj) * int(np.count_nonzero(np.asarray(r.seq.adc))) for r in reqs))
     residents = {}
     if resident:
         for r in pool:
@@ -357,12 +362,21 @@ def serving_benchmark(n_pool=16, passes=10, load=0.9, slots=4, resident=False):
     makespan = max(f for _, _, f in spans) - min(s for s, _, _ in spans)
     sustained = units / makespan
     batch = units / batch_s
+    bound = {}
+    if spin_sample_rate:
+        kb = spin_sample_rate * units / spin_samples
+        bound = {"mix_coils_per_spin_sample": units / spin_samples, "kernel_bound_units_per_s": kb,
+                 "batch_fraction_of_kernel_bound": batch / kb,
+                 "kernel_bound": "the headline split kernel's spin*sample rate x the mix's spin*sample-weighted "
+                                 "coil count"}
     return {"requests": len(reqs), "distinct": n_pool, "slots": slots, "load": load,
             "arrival_rate_per_s": rate, "batch_units_per_s": batch, "sustained_units_per_s": sustained,
+            **bound,
             "fraction_of_batch": sustained / batch, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
             "mix": "spins log-uniform 1e3-1e6, 2D/3D, ADC U[1k,20k] at 1-5 us, coils {1,8,16,32}, random masks, "
-                   "f32 or f64 arrays, all on the split kernel",
+                   "f32 or f64 arrays, all on the split kernel (the server's rounds: one persistent launch per "
+                   "output width over all requests' current segments)",
             "phantoms": "resident on the device (uploaded once, before the streams)" if resident else
                         "uploaded from pageable host memory by every request"}
 
@@ -770,9 +784,10 @@ def run_homs(args):
     if ws == 1 and not args.no_configs and args.config == CONFIG_INDEX and args.spin_stride == 1:
         out["configs"] = config_legs(ctx)
     if ws == 1 and not args.no_serve:
-        out["serving"] = serving_benchmark()
+        ss_rate = value / nc if args.mode == "split" and args.spin_stride == 1 else None
+        out["serving"] = serving_benchmark(spin_sample_rate=ss_rate)
         out["serving"]["plain_per_request_units_per_s"] = plain_per_request()
-        out["serving_resident"] = serving_benchmark(resident=True)
+        out["serving_resident"] = serving_benchmark(resident=True, spin_sample_rate=ss_rate)
     if ws == 1 and not args.no_refgpu and args.config == CONFIG_INDEX and args.spin_stride == 1:
         out["reference_gpu_equivalent"] = reference_gpu_leg(w, sig_dev, ms_max, units)
     if ws == 1 and not args.no_kspace:

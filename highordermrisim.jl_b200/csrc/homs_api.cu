@@ -1875,6 +1875,8 @@ homs_status server_run_after(ServerRun *run, cudaStream_t stream) {
     }
 }
 
+cudaStream_t server_run_stream(const ServerRun *run) { return run->ctx->stream; }
+
 void server_run_done(ServerRun *run, cudaStream_t stream) {
     DeviceGuard g(run->ctx->device);
     if (run->done && cudaEventRecord(run->done, stream) == cudaSuccess) run->done_recorded = true;

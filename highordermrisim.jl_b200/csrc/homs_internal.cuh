@@ -44,6 +44,7 @@ homs_status server_run_prepare(homs_context *ctx, const homs_phantom *phantom, c
 homs_status server_run_next(ServerRun *run, cudaStream_t stream, SplitJobDesc *job, bool *has_job);
 homs_status server_run_after(ServerRun *run, cudaStream_t stream);
 void server_run_done(ServerRun *run, cudaStream_t stream);
+cudaStream_t server_run_stream(const ServerRun *run);  // the run's context's stream
 homs_status server_run_finish(ServerRun *run, void *sig, homs_memory sig_memory, homs_state *state);
 void server_run_free(ServerRun *run);
 

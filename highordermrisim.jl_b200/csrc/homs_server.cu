@@ -181,18 +181,29 @@ struct homs_server {
         cudaSetDevice(device);
         cudaStream_t ds = nullptr;
         cudaStreamCreateWithFlags(&ds, cudaStreamNonBlocking);
+        // A run's own work (RF blocks, prologues, finalizes) goes on its
+        // context's stream, so that the runs' small kernels overlap; the
+        // round's fused launches go on `ds` after every run's prologue
+        // (pre events), and each run's finalize after them (fused event).
         // At most two rounds ahead of the device.
-        cudaEvent_t round_ev[2] = {nullptr, nullptr};
+        cudaEvent_t round_ev[2] = {nullptr, nullptr}, fused = nullptr;
         cudaEventCreateWithFlags(&round_ev[0], cudaEventDisableTiming);
         cudaEventCreateWithFlags(&round_ev[1], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&fused, cudaEventDisableTiming);
         std::vector<Active *> act;
+        std::map<Active *, cudaEvent_t> pre;
         int64_t k = 0;
         for (;;) {
             {
                 std::unique_lock<std::mutex> lk(mu);
                 cv_dispatch.wait(lk, [&] { return !pending.empty() || !act.empty() || stop_dispatch; });
                 if (act.empty() && pending.empty()) break;  // stopping
-                for (Active *a : pending) act.push_back(a);
+                for (Active *a : pending) {
+                    act.push_back(a);
+                    cudaEvent_t e = nullptr;
+                    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+                    pre[a] = e;
+                }
                 pending.clear();
             }
             cudaEventSynchronize(round_ev[k & 1]);
@@ -203,12 +214,15 @@ struct homs_server {
             for (Active *a : act) {
                 homs::SplitJobDesc d;
                 bool has = false;
-                const homs_status s = homs::server_run_next(a->run, ds, &d, &has);
+                cudaStream_t rs = homs::server_run_stream(a->run);
+                const homs_status s = homs::server_run_next(a->run, rs, &d, &has);
                 if (s != HOMS_OK) {
                     a->status = s;
                     fin.push_back(a);
                 } else if (has) {
                     jobs.emplace_back(a, d);
+                    cudaEventRecord(pre[a], rs);
+                    cudaStreamWaitEvent(ds, pre[a], 0);
                 } else {
                     fin.push_back(a);
                 }
@@ -225,12 +239,15 @@ struct homs_server {
                     for (size_t q = b; q < e; ++q) jobs[q].first->status = HOMS_ECUDA;
                 b = e;
             }
+            cudaEventRecord(fused, ds);
             for (auto &ja : jobs) {
                 Active *a = ja.first;
-                if (a->status == HOMS_OK) a->status = homs::server_run_after(a->run, ds);
+                cudaStream_t rs = homs::server_run_stream(a->run);
+                cudaStreamWaitEvent(rs, fused, 0);
+                if (a->status == HOMS_OK) a->status = homs::server_run_after(a->run, rs);
                 if (a->status != HOMS_OK) fin.push_back(a);
             }
-            for (Active *a : fin) homs::server_run_done(a->run, ds);
+            for (Active *a : fin) homs::server_run_done(a->run, homs::server_run_stream(a->run));
             cudaEventRecord(round_ev[k & 1], ds);
             ++k;
             if (!fin.empty()) {
@@ -238,6 +255,8 @@ struct homs_server {
                 for (Active *a : fin) {
                     a->finished = true;
                     act.erase(std::find(act.begin(), act.end(), a));
+                    cudaEventDestroy(pre[a]);
+                    pre.erase(a);
                 }
                 rounds = k;
                 cv_run.notify_all();
@@ -246,6 +265,7 @@ struct homs_server {
         cudaStreamSynchronize(ds);
         cudaEventDestroy(round_ev[0]);
         cudaEventDestroy(round_ev[1]);
+        cudaEventDestroy(fused);
         cudaStreamDestroy(ds);
     }
 };
