@@ -28,11 +28,11 @@
 //   u = sum_{w>=3} S_w 2^(8w-32) mod 2^32
 // is exact up to the rounding of B and K and that 12 * 2^-32 turn.
 //
-// Trigonometry.  u is reduced to the nearest quarter turn in integers
-// (|x| <= pi/4, which keeps the float scale of the angle from biasing the
-// phase at the wrap), then sin/cos.approx and a quadrant rotation; the decay
-// is ex2.approx of a small argument.  |M| <= 1 after a power-of-two scale per
-// segment.
+// Trigonometry.  u is reduced to the nearest half turn in integers
+// (|x| <= pi/2, which keeps the float scale of the angle from biasing the
+// phase at the wrap), then sin/cos.approx and a sign (cis(x + h pi) =
+// (-1)^h cis(x)); the decay is ex2.approx of a small argument.  |M| < 1 after
+// a power-of-two scale per segment.
 //
 // Coil contraction, exactly.  M becomes a 30-bit integer (|M| < 2^30), four
 // int8 digits: F = rint(M 2^22) gives three unsigned bytes (the top one offset
@@ -40,11 +40,12 @@
 // signed low byte; 30 bits keep spins of small amplitude (outside an excited
 // slice, for instance) precise against a signal that cancels, and a spin of
 // zero amplitude contributes exactly nothing.  The per-coil scaled
-// sensitivities become 22-bit integers, three balanced digits.  Eight int8
-// MMAs per 32-spin chunk accumulate the digit classes T5..T2 (weights
-// 2^40..2^16 of the 2^52 full scale; lower classes lie below 2^-28 of it) in
-// int32 TMEM for a whole work item, with no rounding at all; each item's
-// classes become one FP64 split-K partial.  The offset of the top digit is
+// sensitivities become integers of 23 bits (|c| <= 127 2^16), three balanced
+// digits.  Eight int8 MMAs per 32-spin chunk accumulate the digit classes
+// T5..T2 (weights 2^40..2^16 of the 2^53 full scale; lower classes lie below
+// 2^-29 of it) in int32 TMEM for a whole work item (at most 256 chunks:
+// |T| < 1.34e9 < 2^31), with no rounding at all; each item's classes become
+// one FP64 split-K partial.  The offset of the top digit is
 // removed once per output column in the finalize.
 //
 // Kernel organisation (one CTA per SM, persistent, slab-major work items of
@@ -329,7 +330,7 @@ struct KernelJob {
 struct KernelArgs {
     KernelJob job[MAX_JOBS];
     int n_jobs, n_items, nstage;
-    uint32_t mul8, mul16, mul24, mul25;  // 2^8, 2^16, 2^24, 2^25 (multipliers of mad_lo / mad_hi)
+    uint32_t mul8, mul16, mul24;  // 2^8, 2^16, 2^24 (multipliers of mad_lo / mad_hi)
 };
 
 // The launch's job table (in shared memory) and item count.
@@ -372,15 +373,15 @@ __device__ __forceinline__ void report(const Work &w, unsigned int code) {
     for (int j = 0; j < w.n_jobs; ++j) atomicOr(w.jobs[j].err, code);
 }
 
-constexpr float TWO_PI_2M25 = 1.8725351414619534e-07f;  // 2 pi / 2^25: one unit of the 23-bit quarter-turn angle
+constexpr float TWO_PI_2M24 = 3.7450702829239069e-07f;  // 2 pi / 2^24: one unit of the 23-bit half-turn angle
 constexpr float MAGIC_1P5_2P23 = 12582912.0f;           // 1.5 * 2^23
-// The angle is one FFMA, fb * TWO_PI_2M25 + ANGLE_OFFSET with fb = 2^23 + the
-// 23-bit remainder; ANGLE_OFFSET is -1.5 * 2^23 * TWO_PI_2M25 rounded to float,
-// so every angle carries the same offset angle_offset_error() (a few 1e-8
+// The angle is one FFMA, fb * TWO_PI_2M24 + ANGLE_OFFSET with fb = 2^23 + the
+// 23-bit remainder; ANGLE_OFFSET is -1.5 * 2^23 * TWO_PI_2M24 rounded to float,
+// so every angle carries the same offset angle_offset_error() (about 1e-7
 // rad), which the finalize removes exactly by a rotation of the signal.
-constexpr float ANGLE_OFFSET = -MAGIC_1P5_2P23 * TWO_PI_2M25;
+constexpr float ANGLE_OFFSET = -MAGIC_1P5_2P23 * TWO_PI_2M24;
 inline __host__ __device__ double angle_offset_error() {
-    return (double)ANGLE_OFFSET + (double)MAGIC_1P5_2P23 * (double)TWO_PI_2M25;
+    return (double)ANGLE_OFFSET + (double)MAGIC_1P5_2P23 * (double)TWO_PI_2M24;
 }
 // Low magnetisation digit: rint(r * 2^30 (1 - 2^-7)) for the rounding residual
 // |r| <= 2^-23 of the top three digits, so |digit| <= 127 without a clamp.
@@ -601,7 +602,7 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(const __gr
             __syncwarp();
             if (lane == 0) mbar_arrive(d_empty);
         }
-        const uint32_t m8 = args.mul8, m16 = args.mul16, m24 = args.mul24, m25 = args.mul25;
+        const uint32_t m8 = args.mul8, m16 = args.mul16, m24 = args.mul24;
         const int n_items = W.n_items;
         int g = 0, stage = 0, prev_stage = 0;
         uint32_t sph = 0, prev_sph = 0;
@@ -665,24 +666,21 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(const __gr
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         const int i = 2 * pp + h;
-                        // u = turn + 2^29 + 64: classes 7, 6, 5 shifted left by 24, 16, 8 bits,
+                        // u = turn + 2^30 + 128: classes 7, 6, 5 shifted left by 24, 16, 8 bits,
                         // class 4 as is, class 3 shifted right (arithmetic) by 8.
                         uint32_t u = base + th[i] + pc[3][i];
                         u = mad_lo(pc[2][i], m8, u);
                         u = mad_lo(pc[1][i], m16, u);
                         u = mad_lo(pc[0][i], m24, u);
                         u = mad_hi_s(pc[4][i], m24, u);
-                        // Quarter-turn reduction: quadrant u >> 30, remainder (u & (2^30 - 1)) - 2^29
-                        // to 23 bits (the +64 of u rounds it).
-                        const uint32_t fb = (mul_hi_u(u, m25) & 0x7FFFFFu) | 0x4B000000u;
-                        const float x = __fmaf_rn(__uint_as_float(fb), TWO_PI_2M25, ANGLE_OFFSET);
-                        const float sn = sin_approx(x), cs = cos_approx(x);
-                        const bool odd = (u & 0x40000000u) != 0u;
-                        const float re = odd ? sn : cs, im = odd ? cs : sn;
+                        // Half-turn reduction: half h = u >> 31 (the sign of M), remainder
+                        // (u & (2^31 - 1)) - 2^30 to 23 bits (the +128 of u rounds it).
+                        const uint32_t fb = (mul_hi_u(u, m24) & 0x7FFFFFu) | 0x4B000000u;
+                        const float x = __fmaf_rn(__uint_as_float(fb), TWO_PI_2M24, ANGLE_OFFSET);
+                        const float re = cos_approx(x), im = sin_approx(x);
                         const uint32_t ab =
                             __float_as_uint(ex2_approx(fmaf(tj, __uint_as_float(r2b[i]), __uint_as_float(l2b[i]))));
-                        const float are = __uint_as_float(ab ^ ((u + 0x40000000u) & 0x80000000u));
-                        const float aim = __uint_as_float(ab ^ (u & 0x80000000u));
+                        const float are = __uint_as_float(ab ^ (u & 0x80000000u)), aim = are;
                         // 3 + rint(M 2^22) 2^-22 (|M| < 1, so the sum stays in [2, 4) where the
                         // float grid is 2^-22): bits 0x40400000 + F for F = rint(M 2^22), bytes
                         // 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64.  The residual
@@ -831,9 +829,12 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
             const int c = q / FIN_ROWS, row = q % FIN_ROWS;
             const int64_t j = tile * TM + r0 + row;
             if (j < nsamples) {
-                const int e = coil_exp[c] + ea;
+                // undo 2^-e_A of M and coil_scale of the sensitivities (the 2^23 of
+                // the latter against the 2^-52 of the partials' units: one net 2^-1)
+                const int e = coil_exp[c] + ea - 1;
                 const double re = sacc[row * n_cols + c], im = sacc[row * n_cols + ncg + c];
-                sig[j + (int64_t)c * ldsig] = cplx<T>{T(ldexp(re * rc - im * rs, e)), T(ldexp(re * rs + im * rc, e))};
+                sig[j + (int64_t)c * ldsig] =
+                    cplx<T>{T(ldexp(re * rc - im * rs, e) * (128.0 / 127.0)), T(ldexp(re * rs + im * rc, e) * (128.0 / 127.0))};
             }
         }
         __syncthreads();
@@ -982,17 +983,22 @@ __global__ void coil_exp_kernel(const unsigned long long *mx, int32_t nc, int *c
         coil_exp[c] = pow2_ceil_exp(mx[c]);
 }
 
+// Scale of a coil's sensitivities: 2^(23 - e_coil) 127/128, so that the
+// integers stay within 127 2^16 and their top balanced digit within [-127,
+// 127] (2^-23 relative precision; undone exactly by the finalize's 128/127).
+__host__ __device__ inline double coil_scale(int e_coil) { return ldexp(127.0 / 128.0, 23 - e_coil); }
+
 // Sensitivity integer of output column n (coil group coil0, ncg coils) for
 // component comp of M (0: Re M, 1: Im M) of spin sp: Re S = sum Re M Re c -
 // Im M Im c (column n < ncg), Im S = sum Re M Im c + Im M Re c (column ncg + n),
-// each sensitivity scaled by 2^(22 - e_coil), so |value| <= 2^22.
+// each sensitivity times coil_scale.
 __device__ __forceinline__ long long coil_int(const cplx<double> *csm_rows, int64_t ns, int32_t nc, int coil0,
                                               int ncg, const int *coil_exp, int n, int comp, int64_t sp) {
     if (sp >= ns || n >= 2 * ncg) return 0;
     const int coil = coil0 + (n < ncg ? n : n - ncg);
     const cplx<double> cv = csm_rows[sp * nc + coil];
     const double v = n < ncg ? (comp == 0 ? cv.re : -cv.im) : (comp == 0 ? cv.im : cv.re);
-    return llrint(ldexp(v, 22 - coil_exp[coil]));
+    return llrint(v * coil_scale(coil_exp[coil]));
 }
 
 // Coil B operand per coil group and chunk: K-step ks (spins 16 ks .. +15,
@@ -1050,9 +1056,9 @@ __global__ void colsum_kernel(const cplx<double> *csm_rows, int64_t ns, int32_t 
         const int grp = coil / GROUP_COILS, c = coil - grp * GROUP_COILS;
         const int ncg = min(GROUP_COILS, nc - grp * GROUP_COILS);
         const cplx<double> cv = csm_rows[i];
-        const int e = 22 - coil_exp[coil];
+        const double sc = coil_scale(coil_exp[coil]);
         // the terms of coil_int: column c is Re c (Re M) + (-Im c) (Im M), column ncg + c is Im c + Re c
-        const long long re = llrint(ldexp(cv.re, e)), im = llrint(ldexp(cv.im, e)), mim = llrint(ldexp(-cv.im, e));
+        const long long re = llrint(cv.re * sc), im = llrint(cv.im * sc), mim = llrint(-cv.im * sc);
         atomicAdd(&csum[grp * n_cols + c], (unsigned long long)(re + mim));
         atomicAdd(&csum[grp * n_cols + ncg + c], (unsigned long long)(im + re));
     }
@@ -1195,7 +1201,7 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
 // sample j the integers K_k(j) = rint(kappa_k(j) bmax_k 2^26) of the 16 terms
 // as five balanced digits, placed as the A' tiles [a4|a3], [a2|a1], [a0|0]
 // (row j % 128 of tile j / 128), the base turn rint(frac(kappa_0) 2^32) +
-// 2^29 + 64 (quarter-turn offset and the rounding of the 23-bit angle) and
+// 2^30 + 128 (quarter-turn offset and the rounding of the 23-bit angle) and
 // the elapsed time.  Rows past nsamples are zero.  Sets error bit 64 when a
 // term's range bmax_k max|kappa_k| exceeds PHASE_RANGE_LIMIT turns.
 __global__ void phase_a_kernel(const double *prefix, int64_t nsamples, int64_t nrows,
@@ -1213,7 +1219,7 @@ __global__ void phase_a_kernel(const double *prefix, int64_t nsamples, int64_t n
         for (int d = 0; d < PHASE_DIGITS; ++d)
 #pragma unroll
             for (int w = 0; w < 4; ++w) dig[d][w] = 0u;
-        uint32_t base = 0x20000040u;
+        uint32_t base = 0x40000080u;
         float tj = 0.0f;
         if (j < nsamples) {
             const double *pr = prefix + (size_t)j * PREFIX_STRIDE;
@@ -1489,7 +1495,6 @@ cudaError_t split_launch(const SplitJobDesc *jobs, int n_jobs, cudaStream_t stre
     ka.mul8 = 1u << 8;
     ka.mul16 = 1u << 16;
     ka.mul24 = 1u << 24;
-    ka.mul25 = 1u << 25;
     const int64_t G = std::min<int64_t>(sm_count(), items);
     return launch_precession(n_mma, ka, (unsigned)G, kernel_smem(n_mma), stream);
 }
