@@ -20,8 +20,8 @@
 // When a request's last job is done its worker copies the results out.
 // Plain-mode requests run homs_simulate on their worker's context.  Either way
 // a request computes exactly what homs_simulate computes for it: each job's
-// work items, partial slots and finalize order are its own, so its result
-// does not depend on what runs beside it.
+// work items and integer accumulators are its own, and their sums are exact,
+// so its result does not depend on what runs beside it.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -78,11 +78,11 @@ size_t estimate_bytes(int64_t nspins, int32_t ncoils, homs_dtype dtype, const ho
     if (o.mode == HOMS_SPLIT) {
         if (!resident) b += ns * homs::split_bytes_per_spin(ncoils);  // basis, phase and coil digit operands
         b += ns * 12.0;                                               // per-segment spin parameters
-        // split-K partials: per segment (tiles x slabs) items of 128 x 64 FP64, slabs about 2 per 148 SMs
-        // and at least one per 256 chunks of spins; plus the phase prefix, phase A tiles and sample rows
+        // coil accumulators: per tile of 128 samples and slot of 2^18 chunks, 128 x 64 int64;
+        // plus the phase prefix, phase A tiles and sample rows
         const double nchunks = std::ceil(ns / 32.0), tiles = std::ceil((double)nadc / 128.0) + q.nblocks;
-        const double items = std::min(tiles * nchunks, std::max(148.0 * 8, 2.0 * tiles * std::ceil(nchunks / 256.0)));
-        b += items * 128 * 64 * 8 + (double)nadc * (192.0 + 96.0 + 8.0);
+        const double slots = std::ceil(nchunks / 262144.0);
+        b += tiles * slots * 128 * 64 * 8 + (double)nadc * (192.0 + 96.0 + 8.0);
     } else {
         const double grid = std::ceil(ns / 256.0);
         b += std::min(768.0 * (1 << 20), grid * nc * 2 * es * (double)nadc);  // split-K partials

@@ -44,9 +44,12 @@
 // digits.  Eight int8 MMAs per 32-spin chunk accumulate the digit classes
 // T5..T2 (weights 2^40..2^16 of the 2^53 full scale; lower classes lie below
 // 2^-29 of it) in int32 TMEM for a whole work item (at most 256 chunks:
-// |T| < 1.34e9 < 2^31), with no rounding at all; each item's classes become
-// one FP64 split-K partial.  The offset of the top digit is
-// removed once per output column in the finalize.
+// |T| < 1.34e9 < 2^31), with no rounding at all.  At the end of an item its
+// classes become one integer per output element, added (red.global.add.u64)
+// into the tile's int64 accumulator: the slabs' sums are exact, so their order
+// does not matter and a result is the same bit for bit on every run.  The
+// finalize removes the offset of the top digit from the integer, then rounds
+// once to FP64.
 //
 // Kernel organisation (one CTA per SM, persistent, slab-major work items of
 // (time tile of 128 samples) x (range of 32-spin chunks)):
@@ -54,7 +57,7 @@
 //               TMEM lane quarter) and spins 8(w/4) .. +7 of every chunk:
 //               reads the phase classes, forms the turn, M and its digits,
 //               writes the coil MMA's A operand to TMEM; drains the coil
-//               classes into the item's FP64 partial.
+//               classes into the tile's int64 accumulator.
 //   warp 16     coil MMA issuer: per chunk 8 coil MMAs (A in TMEM, B: the
 //               chunk's sensitivity digits); one commit releases both the
 //               shared-memory stage and the A buffer.
@@ -98,6 +101,14 @@ constexpr int THREADS = 608;
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int MAX_STAGE = 6;
 constexpr int MAX_ITEM_CHUNKS = 256;  // int32 coil classes stay below 2^31 over an item
+// A spin adds less than 2^39 to an accumulator element (units of 2^16: digit
+// values below 2^31 and 2^23, two products per output), so one int64 holds the
+// sum over 2^24 spins.  Items go to accumulator slot (first chunk >> 18): at
+// most 2^18 + MAX_ITEM_CHUNKS chunks, under 2^23 + 2^13 spins, per slot.
+constexpr int ACC_SLOT_LOG2 = 18;
+__host__ __device__ constexpr int acc_slots(int64_t n_chunks) {
+    return (int)((n_chunks + (1 << ACC_SLOT_LOG2) - 1) >> ACC_SLOT_LOG2);
+}
 constexpr long long WAIT_BUDGET = 4000000000LL;  // cycles (~2 s)
 constexpr double PHASE_RANGE_LIMIT = 4096.0;     // turns: bmax_k * max|kappa_k| per term and segment
 
@@ -313,8 +324,8 @@ __host__ __device__ constexpr uint32_t idesc_i8(int n, bool a_signed, bool b_sig
 // k % tiles, and the launch's items are the jobs' items one job after the
 // other.  CTA b takes items b, b + G, b + 2G, ...  The CTAs running at any
 // one time thus read the chunks of two or three consecutive slabs, which stay
-// in L2 for every tile that needs them.  Item (tile, z) owns partial slot z of
-// its job.
+// in L2 for every tile that needs them.  Item (tile, z) adds into its job's
+// accumulator of that tile (spin-range slot of its first chunk).
 constexpr int MAX_JOBS = SPLIT_MAX_JOBS;
 struct KernelJob {
     const uint8_t *phase_a;    // [tiles][PHASE_A_BYTES]
@@ -322,7 +333,7 @@ struct KernelJob {
     const uint8_t *coil_b;     // [nchunks][coil_b_bytes(N)] of this coil group
     const uint8_t *params;     // [nchunks][PARAM_BYTES]
     const uint32_t *rows;      // [tiles * TM][2]: base turn, elapsed time (float bits)
-    double *partial;           // [tiles][slabs][TM][N]
+    unsigned long long *acc;   // [tiles][acc_slots(n_chunks)][N][TM] int64, zero before the launch
     unsigned int *err;         // the job's device error word
     int n_chunks, tiles, slabs;
     int item0;                 // launch index of the job's first item
@@ -733,15 +744,17 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(const __gr
                 }
             }
             if (dead) break;
-            // Item end: the coil classes of this warp's rows and columns into the
-            // item's FP64 partial, then clear them for the next item.
+            // Item end: the coil classes of this warp's rows and columns, one
+            // integer per element, added into the tile's accumulator (the lanes'
+            // rows are consecutive there), then cleared for the next item.
             if (!wait_all(d_full, (uint32_t)(cu.local & 1))) {
                 if (lane == 0) report(W, 512u);
                 dead = true;
                 break;
             }
             tc_fence_after();
-            double *dst = J.partial + (((size_t)cu.tile * J.slabs + cu.z) * TM + row) * (size_t)N + cq * NQ;
+            unsigned long long *dst =
+                J.acc + (((size_t)cu.tile * acc_slots(J.n_chunks) + (cu.c0 >> ACC_SLOT_LOG2)) * N + cq * NQ) * TM + row;
             const uint32_t z[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
             for (int cb = 0; cb < NQ; cb += 4) {
@@ -752,16 +765,13 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(const __gr
                 tmem_ld_x4(col + (uint32_t)(2 * N), t3);
                 tmem_ld_x4(col + (uint32_t)(3 * N), t2);
                 tmem_wait_ld();
-                double v[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    // classes in units of 2^16 of the 2^52 full scale (|sum| < 2^55: exact in int64)
+                    // classes in units of 2^16 (|sum| < 2^55 over an item: exact in int64)
                     const long long s = ((long long)(int32_t)t5[e] << 24) + ((long long)(int32_t)t4[e] << 16) +
                                         ((long long)(int32_t)t3[e] << 8) + (long long)(int32_t)t2[e];
-                    v[e] = ldexp((double)s, -36);
+                    atomicAdd(dst + (size_t)(cb + e) * TM, (unsigned long long)s);
                 }
-                *reinterpret_cast<double2 *>(dst + cb) = make_double2(v[0], v[1]);
-                *reinterpret_cast<double2 *>(dst + cb + 2) = make_double2(v[2], v[3]);
 #pragma unroll
                 for (int t = 0; t < 4; ++t) tmem_st_x4(col + (uint32_t)(t * N), z);
             }
@@ -779,21 +789,23 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(const __gr
     }
 }
 
-// Sum the split-K partials of each (sample, column) in slab order (FP64),
-// remove the offset of the top magnetisation digit (64 * 2^24 times the
-// column's sensitivity integers, 2^-22 colsum after the 2^-52 scale), rotate
-// by -angle_offset_error() (the constant offset of the kernel's angles), undo
-// the power-of-two scaling of the operands and write complex samples: column
-// n < ncg is Re S(j, coil0 + n), ncg <= n < 2 ncg is Im.
+// Per (sample, column): the accumulator's integer less the offset of the top
+// magnetisation digit (64 * 2^24 times the column's sensitivity integers:
+// colsum * 2^14 in the accumulator's units of 2^16), exact in int64 for one
+// slot and rounded once to FP64 (several slots: each rounded, summed in slot
+// order); then the rotation by -angle_offset_error() (the constant offset of
+// the kernel's angles), the power-of-two scales of the operands undone, and
+// complex samples written: column n < ncg is Re S(j, coil0 + n), ncg <= n <
+// 2 ncg is Im.  The accumulator is left zero for the next launch.
 template <typename T>
-__global__ void __launch_bounds__(256) split_finalize_kernel(const double *partial, int64_t nsamples, int32_t ncg,
-                                                             int n_cols, int slabs, const long long *colsum,
+__global__ void __launch_bounds__(256) split_finalize_kernel(unsigned long long *acc, int64_t nsamples, int32_t ncg,
+                                                             int n_cols, int nacc, const long long *colsum,
                                                              const int *coil_exp,
                                                              const unsigned long long *amp_max, cplx<T> *sig,
                                                              int64_t ldsig) {
-    // A block sums FIN_ROWS rows x n_cols columns of one time tile over the
-    // slabs (each slab's rows are contiguous: coalesced reads), in slab order,
-    // then writes every coil's samples of those rows from shared memory.
+    // A block takes FIN_ROWS rows x n_cols columns of one time tile (the
+    // accumulator's rows are contiguous per column: coalesced), then writes
+    // every coil's samples of those rows from shared memory.
     constexpr int FIN_ROWS = 32, PER = FIN_ROWS * 64 / 256;
     __shared__ double sacc[FIN_ROWS * 64];
     const int ea = amp_exp(*amp_max);
@@ -805,23 +817,26 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
     for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
         const int64_t tile = u / (TM / FIN_ROWS);
         const int r0 = (int)(u % (TM / FIN_ROWS)) * FIN_ROWS;
-        double acc[PER];
-#pragma unroll
-        for (int k = 0; k < PER; ++k) acc[k] = 0.0;
-        for (int z = 0; z < slabs; ++z) {
-            const double *src = partial + (((size_t)tile * slabs + z) * TM + r0) * (size_t)n_cols;
-#pragma unroll
-            for (int k = 0; k < PER; ++k) {
-                const int e = threadIdx.x + k * 256;
-                if (e < elems) acc[k] += src[e];
-            }
-        }
 #pragma unroll
         for (int k = 0; k < PER; ++k) {
             const int e = threadIdx.x + k * 256;
             if (e < elems) {
-                const double cs = (double)colsum[e % n_cols];
-                sacc[e] = acc[k] - ldexp(cs, -22);
+                const int col = e / FIN_ROWS, row = e % FIN_ROWS;
+                unsigned long long *src = acc + ((size_t)tile * nacc * n_cols + col) * TM + r0 + row;
+                const long long off = colsum[col] * (1ll << 14);
+                double v;
+                if (nacc == 1) {
+                    v = (double)((long long)*src - off);
+                    *src = 0ull;
+                } else {
+                    v = -(double)off;
+                    for (int z = 0; z < nacc; ++z) {
+                        unsigned long long *p = src + (size_t)z * n_cols * TM;
+                        v += (double)(long long)*p;
+                        *p = 0ull;
+                    }
+                }
+                sacc[col * FIN_ROWS + row] = v;
             }
         }
         __syncthreads();
@@ -829,10 +844,10 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(const double *parti
             const int c = q / FIN_ROWS, row = q % FIN_ROWS;
             const int64_t j = tile * TM + r0 + row;
             if (j < nsamples) {
-                // undo 2^-e_A of M and coil_scale of the sensitivities (the 2^23 of
-                // the latter against the 2^-52 of the partials' units: one net 2^-1)
-                const int e = coil_exp[c] + ea - 1;
-                const double re = sacc[row * n_cols + c], im = sacc[row * n_cols + ncg + c];
+                // undo the scales: M's integers are M 2^(30 - e_A), the
+                // sensitivities' c 2^(23 - e_c) 127/128, the accumulator's unit 2^16
+                const int e = coil_exp[c] + ea - 37;
+                const double re = sacc[c * FIN_ROWS + row], im = sacc[(ncg + c) * FIN_ROWS + row];
                 sig[j + (int64_t)c * ldsig] =
                     cplx<T>{T(ldexp(re * rc - im * rs, e) * (128.0 / 127.0)), T(ldexp(re * rs + im * rc, e) * (128.0 / 127.0))};
             }
@@ -1317,7 +1332,7 @@ double split_bytes_per_spin(int32_t ncoils) {
 }
 
 SplitResident::~SplitResident() {
-    for (void *p : {params, prefix, phase_a, rows, partial, amp, err})
+    for (void *p : {params, prefix, phase_a, rows, accum, amp, err})
         if (p) cudaFree(p);
     if (!phantom_view)
         for (void *p : {basis, phase_b, coil_b, colsum, term_max, coil_exp})
@@ -1479,7 +1494,7 @@ cudaError_t split_launch(const SplitJobDesc *jobs, int n_jobs, cudaStream_t stre
         k.coil_b = (const uint8_t *)d.coil_b;
         k.params = (const uint8_t *)d.params;
         k.rows = (const uint32_t *)d.rows;
-        k.partial = (double *)d.partial;
+        k.acc = (unsigned long long *)d.accum;
         k.err = d.err;
         k.n_chunks = d.n_chunks;
         k.tiles = d.tiles;
@@ -1544,8 +1559,11 @@ cudaError_t split_segment_begin(SplitResident &r, const SplitRunArgs &a, int64_t
         return cudaSuccess;
     }
     seg->slabs = slabs;
-    const size_t pbytes = sizeof(double) * (size_t)tiles * slabs * TM * r.n_mma;
-    return grow(r.partial, r.partial_bytes, pbytes);
+    seg->nacc = acc_slots(nchunks);
+    // the coil accumulators start at zero (each group's finalize leaves them so)
+    const size_t abytes = sizeof(unsigned long long) * (size_t)tiles * seg->nacc * TM * r.n_mma;
+    if ((e = grow(r.accum, r.accum_bytes, abytes)) != cudaSuccess) return e;
+    return cudaMemsetAsync(r.accum, 0, abytes, stream);
 }
 
 SplitJobDesc split_segment_job(const SplitResident &r, const SplitSegment &seg, int grp) {
@@ -1555,7 +1573,7 @@ SplitJobDesc split_segment_job(const SplitResident &r, const SplitSegment &seg, 
     d.coil_b = (const uint8_t *)r.coil_b + (size_t)grp * seg.nchunks * coil_b_bytes(r.n_mma);
     d.params = r.params;
     d.rows = r.rows;
-    d.partial = r.partial;
+    d.accum = r.accum;
     d.err = (unsigned int *)r.err;
     d.n_chunks = (int32_t)seg.nchunks;
     d.tiles = (int32_t)seg.tiles;
@@ -1572,7 +1590,7 @@ cudaError_t split_segment_finalize(SplitResident &r, const SplitRunArgs &a, cons
     const int fin_blocks = (int)std::min<int64_t>(seg.tiles * (TM / 32), 148 * 8);
     if (a.sizeof_T == 8)
         split_finalize_kernel<double><<<fin_blocks, 256, 0, stream>>>(
-            (const double *)r.partial, seg.nsamples, ncg, r.n_mma, seg.slabs,
+            (unsigned long long *)r.accum, seg.nsamples, ncg, r.n_mma, seg.nacc,
             (const long long *)r.colsum + (size_t)grp * r.n_mma, cexp + coil0, (const unsigned long long *)r.amp,
             (cplx<double> *)a.sig + sample0 + (int64_t)coil0 * a.nadc, a.nadc);
     return cudaGetLastError();

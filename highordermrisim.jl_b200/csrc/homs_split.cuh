@@ -37,12 +37,12 @@ struct SplitResident {
     void *prefix = nullptr;   // FP64 trapezoid prefix table, [rows][24]
     void *phase_a = nullptr;  // per 128-sample tile: the phase MMAs' A operand
     void *rows = nullptr;     // per sample: base turn (h0 term + offsets), elapsed time
-    void *partial = nullptr;  // FP64 split-K partials, [tiles][slabs][128][N]
+    void *accum = nullptr;    // int64 coil accumulators, [tiles][slots][N][128], zero between launches
     void *amp = nullptr;      // bits of the largest |m0| of the segment (u64)
     void *err = nullptr;      // device error word
     size_t basis_bytes = 0, phase_b_bytes = 0, coil_b_bytes = 0, colsum_bytes = 0, term_max_bytes = 0,
            coil_exp_bytes = 0, params_bytes = 0, prefix_bytes = 0, phase_a_bytes = 0, rows_bytes = 0,
-           partial_bytes = 0;
+           accum_bytes = 0;
     int64_t ns = 0, ns_pad = 0;
     int32_t nc = 0, n_mma = 0, ngroups = 1;
     // The phantom operands belong to another SplitResident (a device-resident
@@ -56,7 +56,7 @@ struct SplitResident {
         return (phantom_view ? 0
                              : basis_bytes + phase_b_bytes + coil_b_bytes + colsum_bytes + term_max_bytes +
                                    coil_exp_bytes) +
-               params_bytes + prefix_bytes + phase_a_bytes + rows_bytes + partial_bytes;
+               params_bytes + prefix_bytes + phase_a_bytes + rows_bytes + accum_bytes;
     }
 };
 
@@ -122,11 +122,11 @@ cudaError_t split_run_segment(SplitResident &r, const SplitRunArgs &a, int64_t n
 // one run.
 struct SplitSegment {
     int64_t nsamples = 0, tiles = 0, nchunks = 0;
-    int32_t slabs = 0;
+    int32_t slabs = 0, nacc = 0;
 };
 struct SplitJobDesc {
     const void *phase_a, *phase_b, *coil_b, *params, *rows;
-    void *partial;
+    void *accum;
     unsigned int *err;
     int32_t n_chunks, tiles, slabs, n_mma;
 };
