@@ -142,6 +142,11 @@ struct homs_context {
     DevBuf selftest_err;  // error word of homs_selftest_wait_timeout
     cudaEvent_t kspace_ev[2] = {nullptr, nullptr};
     bool kspace_timed = false;
+    // Page-locked staging of pageable host inputs: two chunks and the events
+    // that mark the copies reading them (created on first use).
+    void *stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    int stage_next = 0;  // the chunk the next staged copy fills
     // Device workspace of homs_simulate, kept between calls (per dtype) so that
     // repeated simulations reuse their buffers instead of reallocating them.
     std::unique_ptr<struct ResidentBase> cache[2];
@@ -165,6 +170,54 @@ struct DeviceGuard {
     }
 };
 
+constexpr size_t STAGE_CHUNK = size_t(8) << 20;  // bytes per staging chunk
+constexpr size_t STAGE_MIN = size_t(1) << 20;    // smaller pageable copies go to the driver as they are
+
+bool stage_ready(homs_context *ctx) {
+    if (ctx->stage[1]) return true;
+    for (int b = 0; b < 2; ++b) {
+        if (!ctx->stage[b] && cudaHostAlloc(&ctx->stage[b], STAGE_CHUNK, cudaHostAllocDefault) != cudaSuccess) {
+            ctx->stage[b] = nullptr;
+            break;
+        }
+        if (!ctx->stage_ev[b] && cudaEventCreateWithFlags(&ctx->stage_ev[b], cudaEventDisableTiming) != cudaSuccess) {
+            ctx->stage_ev[b] = nullptr;
+            break;
+        }
+    }
+    cudaGetLastError();
+    return ctx->stage[0] && ctx->stage[1] && ctx->stage_ev[0] && ctx->stage_ev[1];
+}
+
+// Host -> device copy of `bytes` on the context's stream.  A page-locked
+// source (allocated or registered through CUDA) goes to the copy engine as it
+// is.  A pageable one is staged through the context's two page-locked
+// chunks: this thread copies chunk k into one while the copy engine reads
+// chunk k - 1 from the other, so contexts driven by different threads upload
+// side by side.  Returns once the source may be reused, as a copy from
+// pageable memory does.
+void h2d(homs_context *ctx, void *dst, const void *src, size_t bytes) {
+    if (bytes == 0) return;
+    cudaPointerAttributes at;
+    const bool locked = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (locked || bytes < STAGE_MIN || !stage_ready(ctx)) {
+        HOMS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        return;
+    }
+    const char *s = static_cast<const char *>(src);
+    char *d = static_cast<char *>(dst);
+    for (size_t off = 0; off < bytes; off += STAGE_CHUNK) {
+        const size_t n = std::min(STAGE_CHUNK, bytes - off);
+        const int b = ctx->stage_next;
+        ctx->stage_next ^= 1;
+        HOMS_CUDA(cudaEventSynchronize(ctx->stage_ev[b]));  // the copy that last read this chunk is done
+        std::memcpy(ctx->stage[b], s + off, n);
+        HOMS_CUDA(cudaMemcpyAsync(d + off, ctx->stage[b], n, cudaMemcpyHostToDevice, ctx->stream));
+        HOMS_CUDA(cudaEventRecord(ctx->stage_ev[b], ctx->stream));
+    }
+}
+
 // Copy `n` elements of dtype `src_dt` at `src` (host or device) into a device
 // buffer of type T.
 template <typename T>
@@ -174,8 +227,10 @@ void upload(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype src_dt, 
     HOMS_REQUIRE(src != nullptr, "a required input array is NULL");
     const bool same = (src_dt == HOMS_F64) == (sizeof(T) == 8);
     if (same) {
-        HOMS_CUDA(cudaMemcpyAsync(dst.p, src, sizeof(T) * (size_t)n,
-                                  mem == HOMS_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, ctx->stream));
+        if (mem == HOMS_HOST)
+            h2d(ctx, dst.p, src, sizeof(T) * (size_t)n);
+        else
+            HOMS_CUDA(cudaMemcpyAsync(dst.p, src, sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
         return;
     }
     if (mem == HOMS_HOST) {
@@ -184,7 +239,7 @@ void upload(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype src_dt, 
         // conversion, in stream order.
         const size_t raw = dsize(src_dt) * (size_t)n;
         HOMS_CUDA(ctx->scratch_conv.ensure(raw));
-        HOMS_CUDA(cudaMemcpyAsync(ctx->scratch_conv.p, src, raw, cudaMemcpyHostToDevice, ctx->stream));
+        h2d(ctx, ctx->scratch_conv.p, src, raw);
         src = ctx->scratch_conv.p;
     }
     if (src_dt == HOMS_F64)
@@ -206,7 +261,7 @@ void upload_csm_rows(homs_context *ctx, DevBuf &dst, const void *src, homs_dtype
         // Staged through the context's scratch buffer (kept between calls).
         const size_t bytes = 2 * dsize(src_dt) * (size_t)(ld * (nc - 1) + ns);
         HOMS_CUDA(ctx->scratch_csm.ensure(bytes));
-        HOMS_CUDA(cudaMemcpyAsync(ctx->scratch_csm.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        h2d(ctx, ctx->scratch_csm.p, src, bytes);
         dsrc = ctx->scratch_csm.p;
     }
     if (src_dt == HOMS_F64)
@@ -1087,6 +1142,12 @@ homs_status homs_context_destroy(homs_context *ctx) {
         ctx->build_work.release();
         ctx->build_out.release();
         ctx->selftest_err.release();
+        for (int b = 0; b < 2; ++b) {
+            if (ctx->stage[b]) cudaFreeHost(ctx->stage[b]);
+            if (ctx->stage_ev[b]) cudaEventDestroy(ctx->stage_ev[b]);
+            ctx->stage[b] = nullptr;
+            ctx->stage_ev[b] = nullptr;
+        }
         for (cudaEvent_t &e : ctx->kspace_ev)
             if (e) cudaEventDestroy(e);
         ctx->cache[0].reset();
