@@ -218,6 +218,44 @@ void h2d(homs_context *ctx, void *dst, const void *src, size_t bytes) {
     }
 }
 
+// Device -> host copy of `bytes` on the context's stream, the mirror of h2d: a
+// page-locked destination is written by the copy engine as it is (the call
+// returns at once); a pageable one receives the data through the two
+// page-locked chunks (the copy engine fills one while this thread copies the
+// other out) and holds it when the call returns.
+void d2h(homs_context *ctx, void *dst, const void *src, size_t bytes) {
+    if (bytes == 0) return;
+    cudaPointerAttributes at;
+    const bool locked = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (locked || bytes < STAGE_MIN || !stage_ready(ctx)) {
+        HOMS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        return;
+    }
+    const char *s = static_cast<const char *>(src);
+    char *d = static_cast<char *>(dst);
+    int prev = -1;
+    size_t prev_off = 0, prev_n = 0;
+    for (size_t off = 0; off < bytes; off += STAGE_CHUNK) {
+        const size_t n = std::min(STAGE_CHUNK, bytes - off);
+        const int b = ctx->stage_next;
+        ctx->stage_next ^= 1;
+        // The chunk's last reader was a transfer earlier on this stream, or this
+        // thread's copy-out two chunks back, which has returned.
+        HOMS_CUDA(cudaMemcpyAsync(ctx->stage[b], s + off, n, cudaMemcpyDeviceToHost, ctx->stream));
+        HOMS_CUDA(cudaEventRecord(ctx->stage_ev[b], ctx->stream));
+        if (prev >= 0) {
+            HOMS_CUDA(cudaEventSynchronize(ctx->stage_ev[prev]));
+            std::memcpy(d + prev_off, ctx->stage[prev], prev_n);
+        }
+        prev = b;
+        prev_off = off;
+        prev_n = n;
+    }
+    HOMS_CUDA(cudaEventSynchronize(ctx->stage_ev[prev]));
+    std::memcpy(d + prev_off, ctx->stage[prev], prev_n);
+}
+
 // Copy `n` elements of dtype `src_dt` at `src` (host or device) into a device
 // buffer of type T.
 template <typename T>
@@ -904,9 +942,11 @@ void run_resident(homs_context *ctx, Resident<T> &r, const homs_run_options *opt
 template <typename T>
 void download(homs_context *ctx, void *dst, homs_memory mem, const void *src, int64_t n, homs_dtype out_dt) {
     if (n == 0) return;
-    const cudaMemcpyKind kind = mem == HOMS_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
     if ((out_dt == HOMS_F64) == (sizeof(T) == 8)) {
-        HOMS_CUDA(cudaMemcpyAsync(dst, src, sizeof(T) * (size_t)n, kind, ctx->stream));
+        if (mem == HOMS_HOST)
+            d2h(ctx, dst, src, sizeof(T) * (size_t)n);
+        else
+            HOMS_CUDA(cudaMemcpyAsync(dst, src, sizeof(T) * (size_t)n, cudaMemcpyDeviceToDevice, ctx->stream));
         return;
     }
     HOMS_REQUIRE(sizeof(T) == 8 && out_dt == HOMS_F32, "internal: unsupported output conversion");
@@ -917,8 +957,7 @@ void download(homs_context *ctx, void *dst, homs_memory mem, const void *src, in
     }
     convert_kernel<float, double><<<grid_for(n), 256, 0, ctx->stream>>>(narrow, static_cast<const double *>(src), n);
     HOMS_CUDA(cudaGetLastError());
-    if (mem == HOMS_HOST)
-        HOMS_CUDA(cudaMemcpyAsync(dst, narrow, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (mem == HOMS_HOST) d2h(ctx, dst, narrow, sizeof(float) * (size_t)n);
 }
 
 // Signal and final state out, in the caller's dtype `out_dt`.
