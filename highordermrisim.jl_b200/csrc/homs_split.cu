@@ -1131,32 +1131,50 @@ __global__ void l2_shift_kernel(uint32_t *params, int64_t nchunks, const unsigne
     }
 }
 
-// Prefix table of one segment.  Blocks 0..16: column k, a deterministic
-// chunked scan of the trapezoid sums (f(n)+f(n+1)) dt(n), written at every
-// ADC node (row = sample index) and at the end node (row nsamples), plus the
-// column's largest |value| at row nsamples+1.  Block 17: elapsed time t
-// (entry PREFIX_T) and the constant columns 17 (= 1) and 18, 19 (= 0).
-__global__ void prefix_kernel(const double *dt, const double *const *src, const uint8_t *adc, const int32_t *rank,
-                              int64_t rank_base, int64_t n_lo, int64_t n_hi, int64_t nsamples, double gamma,
-                              double *prefix) {
-    __shared__ double part[256];
-    const int col = blockIdx.x;
-    const double *f = col < 17 ? src[col] : reinterpret_cast<const double *>(1);  // nullptr: zero; 1: constant one
-    const bool one = f == reinterpret_cast<const double *>(1);
-    const bool zero = f == nullptr;
-    const double scale = col < 16 ? -gamma * 0.5 : (col == 16 ? -0.5 : 0.5);
-    const int out_col = col < 17 ? col : PREFIX_T;
-    const int64_t nint = n_hi - n_lo;
-    const int64_t per = (nint + blockDim.x - 1) / blockDim.x;
-    const int64_t i0 = min(nint, per * threadIdx.x), i1 = min(nint, i0 + per);
-    double local = 0.0;
-    for (int64_t i = i0; i < i1; ++i) {
-        const int64_t n = n_lo + i;
-        const double term = zero ? 0.0 : (one ? 2.0 : (f[n] + f[n + 1])) * dt[n];
-        local += term;
-    }
+// Prefix table of one segment, over blocks (column, part): columns 0..16 are
+// kappa_k, the scaled running trapezoid sums (f(n)+f(n+1)) dt(n), written at
+// every ADC node (row = sample index) and at the end node (row nsamples), with
+// the column's largest |value| at row nsamples+1; column 17 is the elapsed
+// time t (entry PREFIX_T) and the constant columns 17 (= 1) and 18, 19 (= 0).
+// A column's intervals are cut into PREFIX_PARTS contiguous parts, and a
+// part into one contiguous run per thread.  Every sum is taken in a fixed
+// order (within a run, runs in thread order, parts in part order), so the
+// table does not depend on timing.  Two launches: the part totals
+// (prefix_part_kernel, into rows nsamples+2 ..), then the scan itself
+// (prefix_kernel), each part starting from the sum of the parts before it.
+constexpr int PREFIX_PARTS = 8;
+constexpr int PREFIX_COLS = 18;
+struct PrefixColumn {
+    const double *f;
+    bool one, zero;
+    double scale;
+    int out_col;
+};
+__device__ __forceinline__ PrefixColumn prefix_column(const double *const *src, int col, double gamma) {
+    PrefixColumn c;
+    c.f = col < 17 ? src[col] : reinterpret_cast<const double *>(1);  // nullptr: zero; 1: constant one
+    c.one = c.f == reinterpret_cast<const double *>(1);
+    c.zero = c.f == nullptr;
+    c.scale = col < 16 ? -gamma * 0.5 : (col == 16 ? -0.5 : 0.5);
+    c.out_col = col < 17 ? col : PREFIX_T;
+    return c;
+}
+__device__ __forceinline__ double prefix_term(const PrefixColumn &c, const double *dt, int64_t n) {
+    return c.zero ? 0.0 : (c.one ? 2.0 : (c.f[n] + c.f[n + 1])) * dt[n];
+}
+// This thread's run [i0, i1) of part `part` of nint intervals.
+__device__ __forceinline__ void prefix_run(int64_t nint, int part, int64_t &i0, int64_t &i1) {
+    const int64_t p0 = nint * part / PREFIX_PARTS, p1 = nint * (part + 1) / PREFIX_PARTS;
+    const int64_t per = (p1 - p0 + blockDim.x - 1) / blockDim.x;
+    i0 = min(p1, p0 + per * threadIdx.x);
+    i1 = min(p1, i0 + per);
+}
+// Sum of the runs' values in thread order (thread 0), and each run's exclusive
+// prefix in part[].
+__device__ double block_exclusive(double *part, double local) {
     part[threadIdx.x] = local;
     __syncthreads();
+    __shared__ double total;
     if (threadIdx.x == 0) {
         double run = 0.0;
         for (int i = 0; i < (int)blockDim.x; ++i) {
@@ -1164,18 +1182,51 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
             part[i] = run;
             run += v;
         }
+        total = run;
     }
     __syncthreads();
-    double cum = part[threadIdx.x];
+    return total;
+}
+
+__global__ void prefix_part_kernel(const double *dt, const double *const *src, int64_t n_lo, int64_t n_hi,
+                                   int64_t nsamples, double gamma, double *prefix) {
+    __shared__ double part[256];
+    const int col = blockIdx.x, pt = blockIdx.y;
+    const PrefixColumn c = prefix_column(src, col, gamma);
+    int64_t i0, i1;
+    prefix_run(n_hi - n_lo, pt, i0, i1);
+    double local = 0.0;
+    for (int64_t i = i0; i < i1; ++i) local += prefix_term(c, dt, n_lo + i);
+    const double total = block_exclusive(part, local);
+    if (threadIdx.x == 0) {
+        prefix[(size_t)(nsamples + 2 + pt) * PREFIX_STRIDE + col] = total;
+        if (pt == 0 && col < 17) prefix[(size_t)(nsamples + 1) * PREFIX_STRIDE + col] = 0.0;  // the maximum, below
+    }
+}
+
+__global__ void prefix_kernel(const double *dt, const double *const *src, const uint8_t *adc, const int32_t *rank,
+                              int64_t rank_base, int64_t n_lo, int64_t n_hi, int64_t nsamples, double gamma,
+                              double *prefix) {
+    __shared__ double part[256];
+    const int col = blockIdx.x, pt = blockIdx.y;
+    const PrefixColumn c = prefix_column(src, col, gamma);
+    const int64_t nint = n_hi - n_lo;
+    int64_t i0, i1;
+    prefix_run(nint, pt, i0, i1);
+    double carry = 0.0;
+    for (int q = 0; q < pt; ++q) carry += prefix[(size_t)(nsamples + 2 + q) * PREFIX_STRIDE + col];
+    double local = 0.0;
+    for (int64_t i = i0; i < i1; ++i) local += prefix_term(c, dt, n_lo + i);
+    block_exclusive(part, local);
+    double cum = carry + part[threadIdx.x];
     double peak = 0.0;
     for (int64_t i = i0; i < i1; ++i) {
         const int64_t n = n_lo + i;
-        const double term = zero ? 0.0 : (one ? 2.0 : (f[n] + f[n + 1])) * dt[n];
-        cum += term;
-        peak = fmax(peak, fabs(scale * cum));
+        cum += prefix_term(c, dt, n);
+        peak = fmax(peak, fabs(c.scale * cum));
         if (adc[n + 1]) {
             double *pr = prefix + (size_t)(rank[n + 1] - rank_base) * PREFIX_STRIDE;
-            pr[out_col] = scale * cum;
+            pr[c.out_col] = c.scale * cum;
             if (col == 17) {
                 pr[17] = 1.0;
                 pr[18] = 0.0;
@@ -1184,7 +1235,7 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
         }
         if (n + 1 == n_hi) {
             double *pr = prefix + (size_t)nsamples * PREFIX_STRIDE;
-            pr[out_col] = scale * cum;
+            pr[c.out_col] = c.scale * cum;
             if (col == 17) {
                 pr[17] = 1.0;
                 pr[18] = 0.0;
@@ -1192,23 +1243,26 @@ __global__ void prefix_kernel(const double *dt, const double *const *src, const 
             }
         }
     }
-    if (nint == 0 && threadIdx.x == 0) {
+    if (nint == 0 && pt == 0 && threadIdx.x == 0) {
         double *pr = prefix + (size_t)nsamples * PREFIX_STRIDE;
-        pr[out_col] = 0.0;
+        pr[c.out_col] = 0.0;
         if (col == 17) {
             pr[17] = 1.0;
             pr[18] = 0.0;
             pr[19] = 0.0;
         }
     }
-    // Largest |kappa| of the column (row nsamples+1) for the phase-range check.
+    // Largest |kappa| of the column (row nsamples+1) for the phase-range check:
+    // the block's maximum, then the parts' by an integer maximum of the bits
+    // (the values are non-negative, so their bits order as they do).
     __syncthreads();
     part[threadIdx.x] = peak;
     __syncthreads();
     if (threadIdx.x == 0 && col < 17) {
         double mx = 0.0;
         for (int i = 0; i < (int)blockDim.x; ++i) mx = fmax(mx, part[i]);
-        prefix[(size_t)(nsamples + 1) * PREFIX_STRIDE + col] = mx;
+        atomicMax(reinterpret_cast<unsigned long long *>(prefix + (size_t)(nsamples + 1) * PREFIX_STRIDE + col),
+                  (unsigned long long)__double_as_longlong(mx));
     }
 }
 
@@ -1529,13 +1583,16 @@ cudaError_t split_segment_begin(SplitResident &r, const SplitRunArgs &a, int64_t
     seg->tiles = tiles;
     seg->nchunks = nchunks;
     seg->slabs = 0;
-    const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2);
+    const size_t prefix_rows = (size_t)std::max<int64_t>(tiles * TM, nsamples + 2 + PREFIX_PARTS);
     if ((e = grow(r.prefix, r.prefix_bytes, prefix_rows * PREFIX_STRIDE * sizeof(double))) != cudaSuccess) return e;
     if ((e = grow(r.params, r.params_bytes, (size_t)nchunks * PARAM_BYTES)) != cudaSuccess) return e;
     // The segment's samples are the global ADC indices sample0 .. sample0 + nsamples - 1.
-    prefix_kernel<<<18, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(a.src_dev),
-                                          (const uint8_t *)a.adc, a.grank, sample0, n_lo, n_hi, nsamples, a.gamma,
-                                          (double *)r.prefix);
+    const dim3 pgrid(PREFIX_COLS, PREFIX_PARTS);
+    prefix_part_kernel<<<pgrid, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(a.src_dev),
+                                                  n_lo, n_hi, nsamples, a.gamma, (double *)r.prefix);
+    prefix_kernel<<<pgrid, 256, 0, stream>>>((const double *)a.dt, reinterpret_cast<const double *const *>(a.src_dev),
+                                             (const uint8_t *)a.adc, a.grank, sample0, n_lo, n_hi, nsamples, a.gamma,
+                                             (double *)r.prefix);
     if ((e = cudaMemsetAsync(r.amp, 0, sizeof(unsigned long long), stream)) != cudaSuccess) return e;
     spin_params_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>((const double *)a.T2, (const cplx<double> *)a.xy,
                                                                r.ns, nchunks, (unsigned long long *)r.amp,
@@ -1543,7 +1600,7 @@ cudaError_t split_segment_begin(SplitResident &r, const SplitRunArgs &a, int64_t
     l2_shift_kernel<<<grid_for(r.ns_pad), 256, 0, stream>>>((uint32_t *)r.params, nchunks,
                                                             (const unsigned long long *)r.amp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if (a.launches) *a.launches += 3;
+    if (a.launches) *a.launches += 4;
     if (nsamples == 0) return cudaSuccess;
     if ((e = grow(r.phase_a, r.phase_a_bytes, (size_t)tiles * PHASE_A_BYTES)) != cudaSuccess) return e;
     if ((e = grow(r.rows, r.rows_bytes, (size_t)tiles * TM * 2 * sizeof(uint32_t))) != cudaSuccess) return e;
