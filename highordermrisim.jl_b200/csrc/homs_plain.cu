@@ -193,6 +193,13 @@ __device__ void reduce_stage(const cplx<T> *X, cplx<T> *P, int na, const cplx<T>
     }
 }
 
+// Shared memory of a segment without ADC samples: the node cache alone (the
+// kernel stages no samples and no sensitivities then).
+template <typename T>
+size_t segment_smem_bytes_no_adc() {
+    return (sizeof(NodeCache<T>) + 127) & ~size_t(127);
+}
+
 template <typename T>
 size_t segment_smem_bytes(int32_t nc) {
     size_t bytes = sizeof(NodeCache<T>) + 2 * sizeof(cplx<T>) * PLAIN_STAGE * PLAIN_THREADS;
@@ -221,7 +228,10 @@ __global__ void __launch_bounds__(PLAIN_THREADS)
     const bool active = s < p.ns;
     const int nvalid = (int)imin64(PLAIN_THREADS, p.ns - spin0);
     const int32_t ncoil = p.nc;
-    const bool csm_in_smem = sizeof(cplx<T>) * (size_t)ncoil * PLAIN_THREADS <= 128 * 1024;
+    // A segment without ADC samples stages nothing (and is launched with the
+    // node cache alone).
+    const bool stage_adc = a.nsamples > 0;
+    const bool csm_in_smem = stage_adc && sizeof(cplx<T>) * (size_t)ncoil * PLAIN_THREADS <= 128 * 1024;
 
     // Stage this CTA's sensitivities (rows s, coil-fastest).
     const cplx<T> *csm_rows;
@@ -340,7 +350,7 @@ __global__ void __launch_bounds__(PLAIN_THREADS)
                     have = true;
                 }
             }
-            if (nc.adc[i + 1]) {
+            if (stage_adc && nc.adc[i + 1]) {
                 X[staged * PLAIN_THREADS + threadIdx.x] = active ? xs : cplx<T>{T(0), T(0)};
                 staged++;
                 if (staged == PLAIN_STAGE) {
@@ -498,7 +508,7 @@ __global__ void __launch_bounds__(CR_THREADS, CR_CTAS_PER_SM)
 template <typename T>
 cudaError_t launch_segment(bool rf, const PhantomDev<T> &p, const SeqDev<T> &q, StateDev<T> &st,
                            const SegmentArgs<T> &a, int grid, cudaStream_t stream) {
-    const size_t smem = segment_smem_bytes<T>(p.nc);
+    const size_t smem = a.nsamples > 0 ? segment_smem_bytes<T>(p.nc) : segment_smem_bytes_no_adc<T>();
     cudaError_t e;
     if (rf) {
         e = allow_max_dynamic_smem((const void *)segment_kernel<T, true>);
