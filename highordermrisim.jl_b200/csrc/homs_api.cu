@@ -1598,15 +1598,14 @@ BrainArgs brain_args(homs_context *ctx, const homs_brain_spec *spec) {
         const size_t cs = a.csm ? 2 * sizeof(double) * (size_t)nvox * (size_t)spec->ncoils : 0;
         HOMS_CUDA(ctx->build_in.ensure(lab + fm + cs));
         uint8_t *b = ctx->build_in.as<uint8_t>();
-        HOMS_CUDA(cudaMemcpyAsync(b, spec->labels, (size_t)nvox, cudaMemcpyHostToDevice, ctx->stream));
+        h2d(ctx, b, spec->labels, (size_t)nvox);
         a.labels = b;
         if (fm) {
-            HOMS_CUDA(cudaMemcpyAsync(b + lab, spec->fieldmap, sizeof(double) * (size_t)nvox, cudaMemcpyHostToDevice,
-                                      ctx->stream));
+            h2d(ctx, b + lab, spec->fieldmap, sizeof(double) * (size_t)nvox);
             a.fieldmap = reinterpret_cast<const double *>(b + lab);
         }
         if (cs) {
-            HOMS_CUDA(cudaMemcpyAsync(b + lab + fm, a.csm, cs, cudaMemcpyHostToDevice, ctx->stream));
+            h2d(ctx, b + lab + fm, a.csm, cs);
             a.csm = reinterpret_cast<const double *>(b + lab + fm);
         }
     }
@@ -1688,8 +1687,7 @@ homs_status homs_brain_phantom_fill(homs_context *ctx, const homs_brain_spec *sp
         if (out->memory == HOMS_HOST && n > 0)
             for (int k = 0; k < 9; ++k)
                 if (host[k])
-                    HOMS_CUDA(cudaMemcpyAsync(host[k], dev[k], sizeof(double) * len[k] * (size_t)n,
-                                              cudaMemcpyDeviceToHost, ctx->stream));
+                    d2h(ctx, host[k], dev[k], sizeof(double) * len[k] * (size_t)n);
         HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
         return HOMS_OK;
     } catch (const Failure &f) {
@@ -1715,7 +1713,7 @@ homs_status homs_csm_birdcage(homs_context *ctx, int64_t nx, int64_t ny, int32_t
             dst = ctx->build_out.as<double>();
         }
         HOMS_CUDA(birdcage(nx, ny, ncoils, relative_radius, dst, ctx->stream));
-        if (out_memory == HOMS_HOST) HOMS_CUDA(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        if (out_memory == HOMS_HOST) d2h(ctx, out, dst, bytes);
         HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
         return HOMS_OK;
     } catch (const Failure &f) {
@@ -1761,13 +1759,13 @@ homs_status homs_kspace(homs_context *ctx, const homs_sequence *seq, int32_t nrf
             const size_t col_bytes = (es * (size_t)nn + 255) & ~size_t(255);
             HOMS_CUDA(ctx->kspace_in.ensure(col_bytes * (NCOLS + 2)));
             uint8_t *base = ctx->kspace_in.as<uint8_t>();
-            HOMS_CUDA(cudaMemcpyAsync(base, seq->t, es * (size_t)nn, cudaMemcpyHostToDevice, ctx->stream));
-            HOMS_CUDA(cudaMemcpyAsync(base + col_bytes, seq->dt, es * (size_t)m, cudaMemcpyHostToDevice, ctx->stream));
+            h2d(ctx, base, seq->t, es * (size_t)nn);
+            h2d(ctx, base + col_bytes, seq->dt, es * (size_t)m);
             dev_t = base;
             dev_dt = base + col_bytes;
             for (int c = 0; c < NCOLS; ++c) {
                 uint8_t *dst = base + (size_t)(2 + c) * col_bytes;
-                HOMS_CUDA(cudaMemcpyAsync(dst, cols[c], es * (size_t)nn, cudaMemcpyHostToDevice, ctx->stream));
+                h2d(ctx, dst, cols[c], es * (size_t)nn);
                 cols[c] = dst;
             }
         }
@@ -1822,8 +1820,8 @@ homs_status homs_kspace(homs_context *ctx, const homs_sequence *seq, int32_t nrf
         HOMS_CUDA(kspace_launch(a, ctx->stream));
         HOMS_CUDA(cudaEventRecord(ctx->kspace_ev[1], ctx->stream));
         if (out_memory == HOMS_HOST) {
-            HOMS_CUDA(cudaMemcpyAsync(k, dk, k_bytes, cudaMemcpyDeviceToHost, ctx->stream));
-            if (nq > 0) HOMS_CUDA(cudaMemcpyAsync(k_q, dkq, kq_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+            d2h(ctx, k, dk, k_bytes);
+            if (nq > 0) d2h(ctx, k_q, dkq, kq_bytes);
         }
         HOMS_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->kspace_timed = true;
