@@ -162,7 +162,8 @@ def _finalize(params, sig, state_xy, state_z, parts, excitation, seqd, seconds, 
     if rt == "state":
         return Mag(state_xy, state_z)
     if comp is not None and sig.shape[0]:
-        sig = sig * comp.astype(sig.dtype)[:, None]
+        # in place: sig is always this module's own freshly filled array
+        np.multiply(sig, comp.astype(sig.dtype)[:, None], out=sig)
     if rt == "mat":
         return sig[:, :, None]
     counts = count_block_adc(seqd.adc, parts)
@@ -715,8 +716,9 @@ class Server:
             msg = self._lib.homs_server_error(self.handle, int(ticket))
             raise HomsError(status, (msg or b"").decode() or _lib.load().homs_status_string(status).decode())
         t0, t1, t2 = self.times(ticket)
-        return _finalize(req.params, np.asarray(req.sig), req.xy, req.z, req.parts, req.excitation, req.seqd, t2 - t1,
-                         req.comp)
+        # a copy when the phase compensation applies: result() may be asked again
+        sig = np.array(req.sig) if req.comp is not None else np.asarray(req.sig)
+        return _finalize(req.params, sig, req.xy, req.z, req.parts, req.excitation, req.seqd, t2 - t1, req.comp)
 
     def release(self, ticket: int) -> None:
         """Forget a finished request (its buffers are released)."""
