@@ -49,14 +49,18 @@ typedef enum homs_memory { HOMS_HOST = 0, HOMS_DEVICE = 1 } homs_memory;
 /* Arithmetic of a run.
  *   HOMS_PLAIN  -- the reference's per-spin sequential trapezoid and fused coil
  *                  sum in the phantom's dtype (CUDA cores only);
- *   HOMS_SPLIT  -- FP64 phase (prefix-integrated field table, FP64 tensor-core
- *                  phase tile, exact mod-2pi reduction), FP32 trigonometry and
- *                  decay, and the coil contraction on tcgen05 tensor cores with
- *                  FP16 hi/lo split operands and FP32 accumulation; RF blocks
- *                  in FP64.  Always computes in FP64: FP32 phantom and sequence
- *                  arrays are widened on upload and the signal and state are
- *                  returned in FP32 (signal NRMSE <= 1e-6 against an FP64
- *                  computation on the same FP32 inputs). */
+ *   HOMS_SPLIT  -- exact integer arithmetic on the tcgen05 tensor cores: the
+ *                  phase as a fixed-point turn fraction from int8 digit
+ *                  products of the prefix-integrated field table and the
+ *                  spins' basis values (the mod-2pi reduction is integer
+ *                  wraparound), FP32 trigonometry and decay, and the coil
+ *                  contraction as int8 digit products of 30-bit magnetisation
+ *                  and 23-bit sensitivity integers, summed exactly (int32 per
+ *                  work item, int64 across items); RF blocks and the state in
+ *                  FP64.  Results are the same bit for bit on every run.
+ *                  FP32 phantom and sequence arrays are widened on upload and
+ *                  the signal and state are returned in FP32 (signal NRMSE
+ *                  <= 1e-6 against an FP64 computation on the same inputs). */
 typedef enum homs_mode { HOMS_PLAIN = 0, HOMS_SPLIT = 1 } homs_mode;
 
 /* BlochHighOrder flags (src/simulation/BlochHighOrder.jl:21-43). */
