@@ -1,9 +1,9 @@
 """Size-independent properties at the full 3D 32-coil size (350,000 spins,
 4 x 9,500 ADC samples), where the CPU oracle is too slow to run.
 
-The split path scales the sensitivities per coil by exact powers of two
-before splitting them into FP16 hi/lo pairs, and every output column is its
-own dot product, so these hold bit for bit:
+The split path scales the sensitivities per coil by a power of two (times
+127/128) before rounding them to integers, and every output column is its
+own exact integer dot product, so these hold bit for bit:
   - S(2 csm) = 2 S(csm) and S(csm / 4) = S(csm) / 4;
   - permuting the coils permutes the signal's columns.
 Doubling rho doubles the signal to the split bound only: the decay exponent
