@@ -215,7 +215,7 @@ size_t segment_smem_bytes(int32_t nc) {
 // excitation (per-node hard-pulse spinor, :100-134; spinor of
 // kernels/HighOrderGPU.jl:181-192).
 template <typename T, bool RF>
-__global__ void __launch_bounds__(PLAIN_THREADS)
+__global__ void __launch_bounds__(PLAIN_THREADS, RF ? 3 : 1)
     segment_kernel(PhantomDev<T> p, SeqDev<T> q, StateDev<T> st, SegmentArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     NodeCache<T> &nc = *reinterpret_cast<NodeCache<T> *>(smem_raw);
