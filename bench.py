@@ -10,8 +10,11 @@ third-order field waveforms, mask 1111), synthetic and seed-generated.
 `value` is whole-job throughput with inputs resident on the device (a
 prepared plan, signal written to device memory); `e2e` is the same metric
 through the C ABI (homs_simulate) from pinned host buffers, with all
-host<->device copies inside the timed region.  With N > 1 every rank runs an
-independent replica (the engine does not shard spins across GPUs).
+host<->device copies inside the timed region; `e2e_pipelined` is the same
+again through the server (homs_server_submit, every step a request, two
+slots), where one request's copies run beside another's kernels.  With N > 1
+every rank runs an independent replica (the engine does not shard spins
+across GPUs).
 
 Further keys on one GPU: ``roofline`` (the algorithmic 8 flops per unit
 against dense bf16), ``pipes`` (what the split kernel issues: int8 tensor
@@ -656,7 +659,7 @@ def run_homs(args):
     plan.close()
 
     # End to end through the C ABI from pinned host memory.
-    e2e = None
+    e2e = e2e_pipelined = None
     if not args.no_e2e:
         keep = _lib._Keep()
         pin = lambda a: _pinned(torch, a)  # noqa: E731
@@ -709,6 +712,50 @@ def run_homs(args):
         e2e = {"value": e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "ms_per_step": e_max, "steps": n_e2e, "warmup": args.warmup,
                "timing": "host wall time of homs_simulate calls (pinned host buffers, copies inside)"}
+
+        # The same simulations through the server (homs_server_submit): all
+        # requests submitted at once to 2 slots, each with its own page-locked
+        # state and signal, so that one request's copies and operand builds run
+        # beside another's kernels.  Copies stay inside the timed region.
+        sopt = _lib.ServerOptions()
+        sopt.device = torch.cuda.current_device()
+        sopt.slots = 2
+        srv = ctypes.c_void_p()
+        _lib.check(lib.homs_server_create(ctypes.byref(sopt), ctypes.byref(srv)))
+        try:
+            def pipelined(n):
+                bufs = [(pin(np.zeros((nc, nadc), ct)), pin(np.zeros(len(obj), ct)),
+                         pin(np.asarray(obj.rho, rt).copy())) for _ in range(n)]
+                sts = [_lib.State(b[1].ctypes.data, b[2].ctypes.data, _lib.HOMS_HOST) for b in bufs]
+                barrier()
+                t0 = time.perf_counter()
+                tickets = []
+                for b, s in zip(bufs, sts):
+                    t = ctypes.c_int64()
+                    _lib.check(lib.homs_server_submit(srv, ctypes.byref(ph), ctypes.byref(sq), ctypes.byref(opts),
+                                                      ctypes.byref(s), b[0].ctypes.data, _lib.HOMS_HOST,
+                                                      ctypes.byref(t)))
+                    tickets.append(t.value)
+                for t in tickets:
+                    st_ = lib.homs_server_wait(srv, t, 600.0)
+                    if st_ != 0:
+                        raise RuntimeError((lib.homs_server_error(srv, t) or b"").decode())
+                dt_ = time.perf_counter() - t0
+                barrier()
+                for t in tickets:
+                    lib.homs_server_release(srv, t)
+                return dt_
+
+            pipelined(2)  # warm-up: both slots' workspaces grow
+            n_p = max(args.steps, 4)
+            p_ms = pipelined(n_p) * 1e3 / n_p
+            p_value, p_max = replica_throughput(p_ms, units, ws)
+            e2e_pipelined = {"value": p_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                             "d2h_bytes_per_step": int(d2h), "ms_per_step": p_max, "requests": n_p, "slots": 2,
+                             "timing": "host wall time from the first homs_server_submit to the last completion "
+                                       "(pinned host buffers, copies inside)"}
+        finally:
+            lib.homs_server_destroy(srv)
 
     if rank != 0:
         if ws > 1:
@@ -785,7 +832,7 @@ def run_homs(args):
                              (f", split operand {op_mb:.0f} MB)" if op_mb else ")")) if csm_mb > 126 else
                       f"inputs smaller than L2 (csm {csm_mb:.0f} MB)", "parallelism": f"replicas{ws}"},
            "roofline": roof, "pipes": pipes, "plain_f64": plain, "accuracy": accuracy, "cpu_baseline": base,
-           "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+           "e2e": e2e, "e2e_pipelined": e2e_pipelined, "gpu_launches": launches, "clocks": clk}
     if ws == 1 and not args.no_configs and args.config == CONFIG_INDEX and args.spin_stride == 1:
         out["configs"] = config_legs(ctx)
     if ws == 1 and not args.no_serve:
