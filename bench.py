@@ -59,7 +59,22 @@ FLOPS_PER_UNIT = 8.0  # one complex multiply-accumulate per spin*sample*coil
 I8_MACS_PER_SPIN_SAMPLE = (160 + 128 + 64 + 2 * (192 + 192 + 128 + 64)) * 32 / 32.0  # MACs per spin*sample
 SFU_OPS_PER_SPIN_SAMPLE = 3.0  # sin, cos, ex2 on the MUFU (XU) pipe
 SFU_PER_SM_CLK = 16.0  # MUFU results per SM and clock
+# FP32 FMA-pipe operations the magnetisation warps write per spin*sample: the angle (1 FFMA), the decay
+# argument (1), the top digits of Re/Im (2), their rounding residuals (2 FADD + 2 FFMA), the low digits (2).
+FP32_OPS_PER_SPIN_SAMPLE = 10.0
+FP32_PER_SM_CLK = 128.0  # FP32 lanes per SM and clock
+FP64_FMA_PER_SM_CLK = 64.0  # FP64 FMA per SM and clock (37 TFLOP/s at 1,965 MHz)
 N_SM = 148
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def _dist():
@@ -210,10 +225,13 @@ def cpu_baseline(seconds_target=20.0, threads=None, k=CONFIG_INDEX, stride=None)
         dt = time.perf_counter() - t0
         if fixed or dt >= seconds_target / 2 or stride == 1:
             break
-        stride = max(1, int(stride * dt / seconds_target))
+        # The oracle's cost per spin grows with the sample (cache), so a prediction from a small sample
+        # overshoots: aim at half the target and take at most 16x more spins per step.
+        stride = max(1, int(2.0 * stride * dt / seconds_target), stride // 16)
     from homs.model import count_block_adc
     nadc = sum(count_block_adc(w.seq.adc, w.parts))
-    return ({"value": _units(w) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+    return ({"value": _units(w) / dt, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": _cpu_model(),
+             "affinity_cpus": len(os.sched_getaffinity(0)),
              "sample": f"every {stride}th spin ({len(w.obj)} spins) x {nadc} samples x {w.obj.ncoils} coils, full "
                        f"sequence, {dt:.2f} s"}, stride, w, sig)
 
@@ -796,6 +814,10 @@ def run_homs(args):
                  "sfu_ops_per_spin_sample": SFU_OPS_PER_SPIN_SAMPLE, "sfu_peak_ops_per_s": sfu_peak,
                  "sfu_frac": SFU_OPS_PER_SPIN_SAMPLE * spin_samples / secs / sfu_peak,
                  "sfu_peak_source": f"{SFU_PER_SM_CLK:.0f} per SM and clock x {N_SM} SMs x {mhz:.0f} MHz (sampled)",
+                 "fp32_ops_per_spin_sample": FP32_OPS_PER_SPIN_SAMPLE,
+                 "fp32_frac": FP32_OPS_PER_SPIN_SAMPLE * spin_samples / secs / (FP32_PER_SM_CLK * N_SM * mhz * 1e6),
+                 "fp32_peak_source": f"{FP32_PER_SM_CLK:.0f} lanes per SM and clock x {N_SM} SMs x {mhz:.0f} MHz "
+                                     "(sampled); the ops are those the kernel's source writes",
                  "spin_samples_per_launch": spin_samples, "kernel_ms_per_launch": avg_launch_ms}
     base = accuracy = None
     if ws == 1 and not args.no_cpu_baseline:
@@ -805,7 +827,14 @@ def run_homs(args):
     plain = None
     if ws == 1 and args.mode == "split" and not args.no_plain:
         pl, sig_plain = time_plan(ctx, w, "plain", precision=args.precision, steps=3, warmup=1)
+        mhz = clk.get("sm_mhz") or 1965.0
+        fp64_peak = 2.0 * FP64_FMA_PER_SM_CLK * N_SM * mhz * 1e6
         plain = dict(pl, split_over_plain_f64=value / pl["units_per_s"],
+                     coil_fp64_flops_per_s=FLOPS_PER_UNIT * pl["units_per_s"],
+                     coil_fp64_frac=FLOPS_PER_UNIT * pl["units_per_s"] / fp64_peak,
+                     fp64_peak_source=f"{FP64_FMA_PER_SM_CLK:.0f} FMA per SM and clock x {N_SM} SMs x {mhz:.0f} MHz "
+                                      "(sampled; FP64 is not among the measured peaks); counts only the coil "
+                                      "contraction's 8 flops per unit, not the field, phase and sincos/exp",
                      note="the plain kernel (the reference's per-spin sequential trapezoid, FP64) on the same "
                           "workload, device-timed plan runs")
         d = float(torch.linalg.vector_norm(sig_plain).item())
