@@ -671,46 +671,60 @@ __global__ void __launch_bounds__(THREADS, 1) split_precession_kernel(const __gr
                     sph ^= 1u;
                 }
                 uint32_t wd[4][4];  // digit planes d1, d2, d3 (+64), d0 of spins (2p, 2p+1)
+                // In stages over the warp's 8 spins (8 independent operations per step
+                // for the schedulers to interleave).
+                // u = turn + 2^30 + 128: classes 7, 6, 5 shifted left by 24, 16, 8 bits,
+                // class 4 as is, class 3 shifted right (arithmetic) by 8.
+                uint32_t u[8];
+                float x[8], e[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    uint32_t v = base + th[i] + pc[3][i];
+                    v = mad_lo(pc[2][i], m8, v);
+                    v = mad_lo(pc[1][i], m16, v);
+                    v = mad_lo(pc[0][i], m24, v);
+                    u[i] = mad_hi_s(pc[4][i], m24, v);
+                }
+                // Half-turn reduction: half h = u >> 31 (the sign of M), remainder
+                // (u & (2^31 - 1)) - 2^30 to 23 bits (the +128 of u rounds it); the decay
+                // argument t r2 + (log2|m0| - eA).
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const uint32_t fb = (mul_hi_u(u[i], m24) & 0x7FFFFFu) | 0x4B000000u;
+                    x[i] = __fmaf_rn(__uint_as_float(fb), TWO_PI_2M24, ANGLE_OFFSET);
+                    e[i] = fmaf(tj, __uint_as_float(r2b[i]), __uint_as_float(l2b[i]));
+                }
+                float re[8], im[8], a[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    re[i] = cos_approx(x[i]);
+                    im[i] = sin_approx(x[i]);
+                    a[i] = __uint_as_float(__float_as_uint(ex2_approx(e[i])) ^ (u[i] & 0x80000000u));
+                }
+                // 3 + rint(M 2^22) 2^-22 (|M| < 1, so the sum stays in [2, 4) where the
+                // float grid is 2^-22): bits 0x40400000 + F for F = rint(M 2^22), bytes
+                // 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64.  The residual
+                // M - F 2^-22 (|.| <= 2^-23, exact before its one rounding) gives the
+                // signed low digit, byte 0 of MAGIC + rint(residual LOW_DIGIT_SCALE).
+                // A spin of zero amplitude gives zero digits (no offset but the top one's).
+                uint32_t vre[8], vim[8], lre[8], lim[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float hre = __fmaf_rn(a[i], re[i], 3.0f);
+                    const float him = __fmaf_rn(a[i], im[i], 3.0f);
+                    vre[i] = __float_as_uint(hre);
+                    vim[i] = __float_as_uint(him);
+                    const float rre = __fmaf_rn(a[i], re[i], __fsub_rn(3.0f, hre));
+                    const float rim = __fmaf_rn(a[i], im[i], __fsub_rn(3.0f, him));
+                    lre[i] = __float_as_uint(__fmaf_rn(rre, LOW_DIGIT_SCALE, MAGIC_1P5_2P23));
+                    lim[i] = __float_as_uint(__fmaf_rn(rim, LOW_DIGIT_SCALE, MAGIC_1P5_2P23));
+                }
+                // K order of a word: (re, im) of spin 2pp, then of spin 2pp+1.
 #pragma unroll
                 for (int pp = 0; pp < 4; ++pp) {
-                    uint32_t vre[2], vim[2], lre[2], lim[2];
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int i = 2 * pp + h;
-                        // u = turn + 2^30 + 128: classes 7, 6, 5 shifted left by 24, 16, 8 bits,
-                        // class 4 as is, class 3 shifted right (arithmetic) by 8.
-                        uint32_t u = base + th[i] + pc[3][i];
-                        u = mad_lo(pc[2][i], m8, u);
-                        u = mad_lo(pc[1][i], m16, u);
-                        u = mad_lo(pc[0][i], m24, u);
-                        u = mad_hi_s(pc[4][i], m24, u);
-                        // Half-turn reduction: half h = u >> 31 (the sign of M), remainder
-                        // (u & (2^31 - 1)) - 2^30 to 23 bits (the +128 of u rounds it).
-                        const uint32_t fb = (mul_hi_u(u, m24) & 0x7FFFFFu) | 0x4B000000u;
-                        const float x = __fmaf_rn(__uint_as_float(fb), TWO_PI_2M24, ANGLE_OFFSET);
-                        const float re = cos_approx(x), im = sin_approx(x);
-                        const uint32_t ab =
-                            __float_as_uint(ex2_approx(fmaf(tj, __uint_as_float(r2b[i]), __uint_as_float(l2b[i]))));
-                        const float are = __uint_as_float(ab ^ (u & 0x80000000u)), aim = are;
-                        // 3 + rint(M 2^22) 2^-22 (|M| < 1, so the sum stays in [2, 4) where the
-                        // float grid is 2^-22): bits 0x40400000 + F for F = rint(M 2^22), bytes
-                        // 0, 1 the digits d1, d2 and byte 2 the top digit d3 + 64.  The residual
-                        // M - F 2^-22 (|.| <= 2^-23, exact before its one rounding) gives the
-                        // signed low digit, byte 0 of MAGIC + rint(residual LOW_DIGIT_SCALE).
-                        // A spin of zero amplitude gives zero digits (no offset but the top one's).
-                        const float hre = __fmaf_rn(are, re, 3.0f);
-                        const float him = __fmaf_rn(aim, im, 3.0f);
-                        vre[h] = __float_as_uint(hre);
-                        vim[h] = __float_as_uint(him);
-                        const float rre = __fmaf_rn(are, re, __fsub_rn(3.0f, hre));
-                        const float rim = __fmaf_rn(aim, im, __fsub_rn(3.0f, him));
-                        lre[h] = __float_as_uint(__fmaf_rn(rre, LOW_DIGIT_SCALE, MAGIC_1P5_2P23));
-                        lim[h] = __float_as_uint(__fmaf_rn(rim, LOW_DIGIT_SCALE, MAGIC_1P5_2P23));
-                    }
-                    // K order of a word: (re, im) of spin 2pp, then of spin 2pp+1.
-                    const uint32_t p0 = prmt(vre[0], vim[0], 0x5140u), p1 = prmt(vre[1], vim[1], 0x5140u);
-                    const uint32_t q0 = prmt(vre[0], vim[0], 0x6262u), q1 = prmt(vre[1], vim[1], 0x6262u);
-                    const uint32_t r0 = prmt(lre[0], lim[0], 0x5140u), r1 = prmt(lre[1], lim[1], 0x5140u);
+                    const uint32_t p0 = prmt(vre[2 * pp], vim[2 * pp], 0x5140u), p1 = prmt(vre[2 * pp + 1], vim[2 * pp + 1], 0x5140u);
+                    const uint32_t q0 = prmt(vre[2 * pp], vim[2 * pp], 0x6262u), q1 = prmt(vre[2 * pp + 1], vim[2 * pp + 1], 0x6262u);
+                    const uint32_t r0 = prmt(lre[2 * pp], lim[2 * pp], 0x5140u), r1 = prmt(lre[2 * pp + 1], lim[2 * pp + 1], 0x5140u);
                     wd[0][pp] = prmt(p0, p1, 0x5410u);
                     wd[1][pp] = prmt(p0, p1, 0x7632u);
                     wd[2][pp] = prmt(q0, q1, 0x5410u);
