@@ -213,9 +213,12 @@ size_t segment_smem_bytes(int32_t nc) {
 // CTA-uniform.  RF=false: free precession (per-spin sequential trapezoid in
 // the CPU order, BlochHighOrderSimulatitonMethod.jl:76-92).  RF=true:
 // excitation (per-node hard-pulse spinor, :100-134; spinor of
-// kernels/HighOrderGPU.jl:181-192).
+// kernels/HighOrderGPU.jl:181-192).  The excitation variant asks for three
+// CTAs per SM (80 registers: its launches without ADC samples use the node
+// cache alone); the precession variant leaves the count to the compiler
+// (0: none asked), which keeps it at 64 (FP32) and 128 (FP64) registers.
 template <typename T, bool RF>
-__global__ void __launch_bounds__(PLAIN_THREADS, RF ? 3 : 1)
+__global__ void __launch_bounds__(PLAIN_THREADS, RF ? 3 : 0)
     segment_kernel(PhantomDev<T> p, SeqDev<T> q, StateDev<T> st, SegmentArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     NodeCache<T> &nc = *reinterpret_cast<NodeCache<T> *>(smem_raw);
