@@ -35,7 +35,7 @@ typedef enum homs_status {
     HOMS_OK = 0,
     HOMS_EINVAL = 1,       /* invalid argument (the reference's ArgumentError/DimensionMismatch) */
     HOMS_ENOMEM = 2,       /* device or host allocation failed, or admission refused */
-    HOMS_EUNSUPPORTED = 3, /* valid request this build cannot serve (e.g. no sm_100 device) */
+    HOMS_EUNSUPPORTED = 3, /* valid request this library cannot serve (e.g. no sm_100 device) */
     HOMS_ETIMEDOUT = 4,    /* a bounded device-side wait gave up; the context stays usable */
     HOMS_ECUDA = 5,        /* CUDA runtime error */
     HOMS_ECLOSED = 6,      /* object already closed */
