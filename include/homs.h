@@ -133,11 +133,11 @@ const char *homs_status_string(homs_status status);
 /* Bind a context to `device` and the caller's CUDA stream (cudaStream_t, NULL
  * for the per-thread default created by the library).  The reference binds work
  * to the current CUDA.jl device and stream (src/simulation/Simulate.jl:153-157).
- * HOST inputs of 1 MiB or more in pageable memory are staged through two
- * page-locked 8 MiB chunks that the context allocates on first use (the host
- * copy of one chunk overlaps the transfer of the other); page-locked inputs
- * are transferred as they are.  A call returns once its host inputs may be
- * reused either way. */
+ * HOST inputs and outputs of 1 MiB or more in pageable memory are staged
+ * through two page-locked 8 MiB chunks that the context allocates on first use
+ * (the host copy of one chunk overlaps the transfer of the other); page-locked
+ * arrays are transferred as they are.  Either way a call returns once its host
+ * inputs may be reused and its host outputs hold the results. */
 homs_status homs_context_create(int device, void *stream, homs_context **out);
 homs_status homs_context_destroy(homs_context *ctx);
 const char *homs_last_error(const homs_context *ctx);
