@@ -321,7 +321,7 @@ def config_legs(ctx):
     return out
 
 
-def serving_benchmark(n_pool=16, passes=10, load=0.95, slots=4, resident=False, spin_sample_rate=None):
+def serving_benchmark(n_pool=16, passes=20, load=0.95, slots=4, resident=False, spin_sample_rate=None):
     """Serving stream of mixed simulations through homs.Server.
 
     Batch mode submits every request at once (the server's capacity);
