@@ -212,4 +212,140 @@ function timing(plan::HomsPlan)
     return t[]
 end
 
+# A phantom kept on the device for many simulations (its arrays and, in split
+# mode, its digit operands built once).
+mutable struct HomsResident
+    handle::Ptr{Cvoid}
+    ctx::Ptr{Cvoid}
+end
+
+function resident(ph::HomsPhantom, mode::Cint)
+    ctx = context()
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    homs_check(ccall((:homs_resident_create, libhoms), Cint,
+                     (Ptr{Cvoid}, Ref{HomsPhantom}, Cint, Ref{Ptr{Cvoid}}), ctx, ph, mode, h), ctx)
+    res = HomsResident(h[], ctx)
+    finalizer(r -> r.handle == C_NULL || ccall((:homs_resident_destroy, libhoms), Cint, (Ptr{Cvoid},), r.handle),
+              res)
+    return res
+end
+
+function simulate_resident!(res::HomsResident, sq::HomsSequence, opts::HomsRunOptions, state::HomsState, sig;
+                            memory::Cint=HOMS_DEVICE)
+    homs_check(ccall((:homs_simulate_resident, libhoms), Cint,
+                     (Ptr{Cvoid}, Ptr{Cvoid}, Ref{HomsSequence}, Ref{HomsRunOptions}, Ref{HomsState}, Ptr{Cvoid},
+                      Cint), res.ctx, res.handle, sq, opts, state, devptr(sig), memory), res.ctx)
+    return sig
+end
+
+# The serving loop: simulations queued from any task, run by `slots` workers
+# (split-mode requests share one persistent kernel launch per round).  The
+# arrays behind a request must stay alive until its ticket has finished.
+mutable struct HomsServer
+    handle::Ptr{Cvoid}
+end
+
+function server(; device::Integer=CUDA.deviceid(CUDA.device()), slots::Integer=4, max_device_bytes::Integer=0)
+    opts = HomsServerOptions(Cint(device), Int32(slots), Int64(max_device_bytes), ntuple(_ -> Int32(0), 4))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    homs_check(ccall((:homs_server_create, libhoms), Cint, (Ref{HomsServerOptions}, Ref{Ptr{Cvoid}}), opts, h),
+               C_NULL)
+    srv = HomsServer(h[])
+    finalizer(s -> s.handle == C_NULL || ccall((:homs_server_destroy, libhoms), Cint, (Ptr{Cvoid},), s.handle), srv)
+    return srv
+end
+
+function server_check(srv::HomsServer, st::Integer, ticket::Int64)
+    st == HOMS_OK && return nothing
+    msg = unsafe_string(ccall((:homs_server_error, libhoms), Cstring, (Ptr{Cvoid}, Int64), srv.handle, ticket))
+    st == HOMS_EINVAL ? throw(ArgumentError(msg)) : error("libhoms: " * msg)
+end
+
+function submit!(srv::HomsServer, ph::HomsPhantom, sq::HomsSequence, opts::HomsRunOptions, state::HomsState,
+                 sig::Ptr{Cvoid}, memory::Cint)
+    t = Ref{Int64}(0)
+    homs_check(ccall((:homs_server_submit, libhoms), Cint,
+                     (Ptr{Cvoid}, Ref{HomsPhantom}, Ref{HomsSequence}, Ref{HomsRunOptions}, Ref{HomsState},
+                      Ptr{Cvoid}, Cint, Ref{Int64}), srv.handle, ph, sq, opts, state, sig, memory, t), C_NULL)
+    return t[]
+end
+
+function submit!(srv::HomsServer, res::HomsResident, sq::HomsSequence, opts::HomsRunOptions, state::HomsState,
+                 sig::Ptr{Cvoid}, memory::Cint)
+    t = Ref{Int64}(0)
+    homs_check(ccall((:homs_server_submit_resident, libhoms), Cint,
+                     (Ptr{Cvoid}, Ptr{Cvoid}, Ref{HomsSequence}, Ref{HomsRunOptions}, Ref{HomsState}, Ptr{Cvoid},
+                      Cint, Ref{Int64}), srv.handle, res.handle, sq, opts, state, sig, memory, t), C_NULL)
+    return t[]
+end
+
+finished(srv::HomsServer, ticket::Int64) =
+    ccall((:homs_server_poll, libhoms), Cint, (Ptr{Cvoid}, Int64), srv.handle, ticket) != HOMS_EBUSY
+
+function wait!(srv::HomsServer, ticket::Int64; timeout::Real=600.0)
+    st = ccall((:homs_server_wait, libhoms), Cint, (Ptr{Cvoid}, Int64, Cdouble), srv.handle, ticket, timeout)
+    server_check(srv, st, ticket)
+end
+
+function times(srv::HomsServer, ticket::Int64)
+    t = Ref{HomsRequestTimes}()
+    server_check(srv, ccall((:homs_server_times, libhoms), Cint, (Ptr{Cvoid}, Int64, Ref{HomsRequestTimes}),
+                            srv.handle, ticket, t), ticket)
+    return t[]
+end
+
+function estimate(srv::HomsServer, ticket::Int64)
+    b = Ref{Int64}(0)
+    server_check(srv, ccall((:homs_server_estimate, libhoms), Cint, (Ptr{Cvoid}, Int64, Ref{Int64}),
+                            srv.handle, ticket, b), ticket)
+    return b[]
+end
+
+release!(srv::HomsServer, ticket::Int64) =
+    ccall((:homs_server_release, libhoms), Cint, (Ptr{Cvoid}, Int64), srv.handle, ticket)
+
+# get_kspace (src/datatypes/HO_Sequence.jl:236-287) on the device: k at every
+# interval (nnodes - 1 x 19, column-major: gx, gy, gz, h0..h15) and at the
+# query times (nq x 19).  rf_start / rf_sign are the RF breaks and their part
+# signs, as KomaMRIBase's get_RF_types gives them.
+function kspace!(sq::HomsSequence, rf_start::Vector{Int64}, rf_sign::Vector{Int8}, q_times, k, k_q;
+                 memory::Cint=HOMS_DEVICE)
+    ctx = context()
+    GC.@preserve rf_start rf_sign q_times k k_q begin
+        homs_check(ccall((:homs_kspace, libhoms), Cint,
+                         (Ptr{Cvoid}, Ref{HomsSequence}, Int32, Ptr{Int64}, Ptr{Int8}, Int64, Ptr{Cvoid}, Ptr{Cvoid},
+                          Ptr{Cvoid}, Cint),
+                         ctx, sq, Int32(length(rf_start)), pointer(rf_start), pointer(rf_sign), Int64(length(q_times)),
+                         devptr(q_times), devptr(k), devptr(k_q), memory), ctx)
+    end
+    return k, k_q
+end
+
+# hophantom_brain's spin arrays from a class volume (src/phantom/hophantom_brain.jl:2-58):
+# the count first, then the arrays into the caller's buffers.
+function brain_phantom_count(spec::HomsBrainSpec)
+    ctx = context()
+    n = Ref{Int64}(0)
+    homs_check(ccall((:homs_brain_phantom_count, libhoms), Cint, (Ptr{Cvoid}, Ref{HomsBrainSpec}, Ref{Int64}),
+                     ctx, spec, n), ctx)
+    return n[]
+end
+
+function brain_phantom_fill!(spec::HomsBrainSpec, out::HomsBrainOut)
+    ctx = context()
+    homs_check(ccall((:homs_brain_phantom_fill, libhoms), Cint, (Ptr{Cvoid}, Ref{HomsBrainSpec}, Ref{HomsBrainOut}),
+                     ctx, spec, out), ctx)
+    return out
+end
+
+# csm_Birdcage (src/phantom/csm/Birdcage.jl:21-42): nx x ny x ncoils complex.
+function csm_birdcage!(out, nx::Integer, ny::Integer, ncoils::Integer, relative_radius::Real;
+                       memory::Cint=HOMS_DEVICE)
+    ctx = context()
+    homs_check(ccall((:homs_csm_birdcage, libhoms), Cint,
+                     (Ptr{Cvoid}, Int64, Int64, Int32, Cdouble, Ptr{Cvoid}, Cint),
+                     ctx, Int64(nx), Int64(ny), Int32(ncoils), Float64(relative_radius), devptr(out), memory), ctx)
+    return out
+end
+
 end  # module Homs

@@ -109,3 +109,67 @@ def test_a_changed_field_is_caught():
     fields, total = julia_structs()["homs_run_options"]
     assert fields[0] == ("method", 0, 4) and total == 32
     assert _jl_type("UInt64")[0] != fields[0][2]
+
+
+def _c_kind(decl):
+    """Kind of a C parameter or return type: ptr, i64, i32, u32, f64."""
+    d = decl.replace("const", " ").strip()
+    if "*" in d:
+        return "ptr"
+    t = d.split()[0]
+    return {"int64_t": "i64", "size_t": "i64", "int32_t": "i32", "int": "i32", "uint32_t": "u32", "double": "f64",
+            "homs_status": "i32", "homs_mode": "i32", "homs_memory": "i32", "homs_dtype": "i32"}[t]
+
+
+def _jl_kind(t):
+    t = t.strip()
+    if t.startswith(("Ptr{", "Ref{")) or t == "Cstring":
+        return "ptr"
+    return {"Int64": "i64", "Int32": "i32", "Cint": "i32", "UInt32": "u32", "Cdouble": "f64", "Float64": "f64"}[t]
+
+
+def header_functions():
+    """{name: (return kind, [parameter kinds])} of the header's prototypes."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"^([\w ]+?\**)\s*\**\s*(homs_\w+)\(([^;]*?)\);", text, re.M | re.S):
+        ret = m.group(1) + ("*" if "*" in text[m.start():m.start(2)] else "")
+        params = [p.strip() for p in m.group(3).split(",") if p.strip() and p.strip() != "void"]
+        kinds = []
+        for p in params:
+            star = "*" in p
+            typ = p.rsplit(None, 1)[0] if not star else p
+            kinds.append(_c_kind(typ if not star else "x *"))
+        out[m.group(2)] = (_c_kind(ret), kinds)
+    return out
+
+
+def shim_calls():
+    """[(name, return kind, [argument kinds])] of every ccall into libhoms in the shim."""
+    text = open(SHIM).read()
+    out = []
+    for m in re.finditer(r"ccall\(\(:(homs_\w+), libhoms\),\s*(\w+),\s*\(([^()]*)\)", text, re.S):
+        args = [a for a in (x.strip() for x in m.group(3).split(",")) if a]
+        out.append((m.group(1), _jl_kind(m.group(2)), [_jl_kind(a) for a in args]))
+    return out
+
+
+def test_shim_calls_match_the_header():
+    # Every ccall of the shim names a function of include/homs.h, with as many
+    # arguments as the prototype and of the same kinds (pointer, 64- or 32-bit
+    # integer, double), and the same kind of return value.
+    hdr = header_functions()
+    calls = shim_calls()
+    assert len(calls) >= 20
+    for name, ret, args in calls:
+        assert name in hdr, f"{name} is not declared in include/homs.h"
+        c_ret, c_args = hdr[name]
+        assert ret == c_ret, (name, ret, c_ret)
+        assert args == c_args, (name, args, c_args)
+    # and the shim covers the whole-simulation, plan, resident, server, export and builder entry points
+    covered = {n for n, _, _ in calls}
+    for need in ("homs_simulate", "homs_plan_create", "homs_plan_run", "homs_resident_create",
+                 "homs_simulate_resident", "homs_server_create", "homs_server_submit", "homs_server_submit_resident",
+                 "homs_server_wait", "homs_server_release", "homs_kspace", "homs_brain_phantom_fill",
+                 "homs_csm_birdcage"):
+        assert need in covered, need
