@@ -189,6 +189,16 @@ bool stage_ready(homs_context *ctx) {
     return ctx->stage[0] && ctx->stage[1] && ctx->stage_ev[0] && ctx->stage_ev[1];
 }
 
+// Ordinary pageable host memory: the only kind the staging below copies with
+// the CPU.  Page-locked, managed and device memory (the last one a caller
+// error under HOMS_HOST) go to cudaMemcpyAsync as they are.
+bool pageable(const void *p) {
+    cudaPointerAttributes at;
+    const bool ok = cudaPointerGetAttributes(&at, p) == cudaSuccess;
+    cudaGetLastError();
+    return ok && at.type == cudaMemoryTypeUnregistered;
+}
+
 // Host -> device copy of `bytes` on the context's stream.  A page-locked
 // source (allocated or registered through CUDA) goes to the copy engine as it
 // is.  A pageable one is staged through the context's two page-locked
@@ -198,10 +208,7 @@ bool stage_ready(homs_context *ctx) {
 // pageable memory does.
 void h2d(homs_context *ctx, void *dst, const void *src, size_t bytes) {
     if (bytes == 0) return;
-    cudaPointerAttributes at;
-    const bool locked = cudaPointerGetAttributes(&at, src) == cudaSuccess && at.type == cudaMemoryTypeHost;
-    cudaGetLastError();
-    if (locked || bytes < STAGE_MIN || !stage_ready(ctx)) {
+    if (!pageable(src) || bytes < STAGE_MIN || !stage_ready(ctx)) {
         HOMS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
         return;
     }
@@ -225,10 +232,7 @@ void h2d(homs_context *ctx, void *dst, const void *src, size_t bytes) {
 // other out) and holds it when the call returns.
 void d2h(homs_context *ctx, void *dst, const void *src, size_t bytes) {
     if (bytes == 0) return;
-    cudaPointerAttributes at;
-    const bool locked = cudaPointerGetAttributes(&at, dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
-    cudaGetLastError();
-    if (locked || bytes < STAGE_MIN || !stage_ready(ctx)) {
+    if (!pageable(dst) || bytes < STAGE_MIN || !stage_ready(ctx)) {
         HOMS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
         return;
     }
