@@ -837,13 +837,15 @@ __global__ void __launch_bounds__(256) split_finalize_kernel(unsigned long long 
             if (e < elems) {
                 const int col = e / FIN_ROWS, row = e % FIN_ROWS;
                 unsigned long long *src = acc + ((size_t)tile * nacc * n_cols + col) * TM + r0 + row;
-                const long long off = colsum[col] * (1ll << 14);
                 double v;
                 if (nacc == 1) {
-                    v = (double)((long long)*src - off);
+                    // at most 2^23 + 2^13 spins: |colsum| < 2^46, the offset and the
+                    // difference fit in int64
+                    v = (double)((long long)*src - colsum[col] * (1ll << 14));
                     *src = 0ull;
                 } else {
-                    v = -(double)off;
+                    // more spins: the offset in FP64 (colsum 2^14 can leave int64)
+                    v = -ldexp((double)colsum[col], 14);
                     for (int z = 0; z < nacc; ++z) {
                         unsigned long long *p = src + (size_t)z * n_cols * TM;
                         v += (double)(long long)*p;
